@@ -1,0 +1,260 @@
+/* nmlmc — B200-native nested MLMC level sampler: the C ABI.
+ *
+ * Two layers:
+ *
+ *  1. Drop-in entry points with the names, argument meaning and struct layouts of the
+ *     reference's extern "C" surface (haji-ali/nested-risk-mlmc; "meant to be used in python",
+ *     common.hpp:34-36), operating on one process-wide sampler as the reference does.  The
+ *     structs mirror the reference's default build (real_t = float).  Where the reference
+ *     exit()s on a CUDA error (par_nvcc.hpp:46-54) these record the error, print it to stderr
+ *     and return; nmlmc_last_error() reports it.
+ *
+ *  2. The native API (nmlmc_*): explicit context, int status returns, double-precision inputs,
+ *     precision / stream-layout selection, batched multi-level sampling and the host MLMC driver.
+ *
+ * Plain C: no torch or CUDA types appear in any signature.
+ */
+#ifndef NMLMC_H
+#define NMLMC_H
+
+#include <stdbool.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------------ */
+enum {
+    NMLMC_OK = 0,
+    NMLMC_ERR_ARG = 1,        /* invalid argument (also: unsupported configuration)       */
+    NMLMC_ERR_CUDA = 2,       /* a CUDA runtime call failed                                */
+    NMLMC_ERR_STATE = 3,      /* call out of order (no model / portfolio set, no context) */
+    NMLMC_ERR_NOMEM = 4,      /* device or host allocation failed                          */
+    NMLMC_ERR_TIMEOUT = 5     /* a bounded device wait gave up                             */
+};
+
+enum { NMLMC_PREC_REF32 = 0, NMLMC_PREC_FP64 = 1, NMLMC_PREC_FP32 = 2 };
+enum { NMLMC_STREAMS_CORE = 0, NMLMC_STREAMS_OUTER = 1 };
+enum { NMLMC_MODEL_REFERENCE = 0, NMLMC_MODEL_SHIFT = 1 };
+enum { NMLMC_SUB_NONE = 0, NMLMC_SUB_RANDOM = 1, NMLMC_SUB_UNIFORM = -1 };
+
+/* ================================================================================================
+ * 1. Reference-compatible surface
+ * ============================================================================================== */
+
+/* nested_sampler_params (nested_sampler.hpp:14-34), real_t = float. */
+typedef struct nested_sampler_params {
+    uint32_t N0;
+    uint32_t beta;
+    bool antithetic;
+    uint32_t fine_moments;
+    uint32_t diff_moments;
+    float adaptive_r;
+} nested_sampler_params;
+
+/* sample_output (common.hpp:37-55): the caller owns fsums / diffsums (phi_size x moments). */
+typedef struct sample_output {
+    uint64_t M;
+    double* fsums;
+    double* diffsums;
+    double total_work;
+    uint64_t inner_stats[6];
+} sample_output;
+
+/* model::data (model_sampler.cpp:21-39). */
+typedef struct model_data {
+    float stau;       /* sqrt(tau)   */
+    float s1tau;      /* sqrt(1-tau) */
+    float max_loss;
+    int32_t phi_type; /* 0 Indicator (the only phi on this path) */
+} model_data;
+
+/* portfolio::option_params / stock_params / data (portfolio_sampler.cpp:42-92). */
+typedef struct option_params {
+    float strike, maturity, start, w, delta_est;
+    uint32_t stock_ind;
+    int32_t type;     /* +1 call, -1 put */
+    float prob;
+    float W_est;
+} option_params;
+
+typedef struct stock_params { float S0, mu, sigma; } stock_params;
+typedef struct { option_params* data; size_t size; } nmlmc_options_span;
+typedef struct { stock_params* data; size_t size; } nmlmc_stocks_span;
+
+typedef struct portfolio_data {
+    nmlmc_options_span options[3];   /* ComputeMethod::BS, Exact, Unbiased                      */
+    nmlmc_stocks_span stocks;
+    float r, rho, s1_rho2;
+    float max_loss;
+    float tau;
+    uint32_t dt_h0inv;
+    uint32_t dt_beta;
+    float dt_prob_expo;
+    int32_t phi_type;
+    uint32_t _phi_size;
+    int32_t subsample;               /* NMLMC_SUB_*                                             */
+    bool use_delta_cv;
+    bool use_coarse_delta_cv;
+    bool use_antithetic_risk;
+    bool use_milstein;
+} portfolio_data;
+
+/* init_nestedmc_sampler / cleanup_nestedmc_sampler (common.cpp:20-31). `cores` is the number
+ * of virtual cores: core c draws from the Threefry streams keyed (seed, c) and takes OpenMP's
+ * static share of each call's outer samples, so cores = OMP_NUM_THREADS reproduces the
+ * reference CPU build's draws. */
+void init_nestedmc_sampler(uint32_t cores, const nested_sampler_params* params);
+void cleanup_nestedmc_sampler(void);
+
+/* model_update_data / model_init / model_sample (model_sampler.cpp:94-114). */
+void model_update_data(const model_data* data);
+void model_init(const model_data* data, uint64_t seed);
+void model_sample(uint32_t ell, uint64_t M, sample_output* out);
+
+/* portfolio_update_data / portfolio_init / portfolio_sample / portfolio_cleanup /
+ * portfolio_comp_params (portfolio_sampler.cpp:618-756).  Options of ComputeMethod::BS only
+ * (options[1] and options[2] must be empty): the Exact / Unbiased methods are not on this path. */
+void portfolio_update_data(const portfolio_data* data);
+void portfolio_init(const portfolio_data* data, uint64_t seed);
+void portfolio_sample(uint32_t ell, uint64_t override_dyn_inner, uint64_t M, sample_output* out);
+void portfolio_cleanup(void);
+void portfolio_comp_params(portfolio_data* data);
+
+/* norm_cdf_inv (common.cpp:53-86). */
+float norm_cdf_inv(float p);
+
+/* Status of the last reference-surface call, and the precision used by it (the reference
+ * surface computes at NMLMC_PREC_REF32 unless nmlmc_default_set_precision changes it). */
+int nmlmc_last_error(void);
+int nmlmc_default_set_precision(int32_t precision, int32_t streams);
+
+/* ================================================================================================
+ * 2. Native API
+ * ============================================================================================== */
+typedef struct nmlmc_ctx nmlmc_ctx;
+
+typedef struct nmlmc_config {
+    uint32_t cores;            /* virtual cores of the CORE layout (0 -> 2048)                  */
+    uint32_t N0;               /* inner samples at level 0                                      */
+    uint32_t beta;             /* inner refinement factor (power of two)                         */
+    double adaptive_r;         /* adaptive exponent r; adaptive iff 1 < r < 2 (or <= 2, below)   */
+    int32_t antithetic;        /* antithetic coarse estimator                                   */
+    int32_t adaptive_incl_r2;  /* 1: treat r = 2 as adaptive (the 3-sigma doubling rule)         */
+    int32_t precision;         /* NMLMC_PREC_*                                                   */
+    int32_t streams;           /* NMLMC_STREAMS_*                                                */
+    uint64_t seed;
+    uint64_t batch;            /* OUTER layout: outer samples held per batch (0 -> 1<<20)        */
+} nmlmc_config;
+
+typedef struct nmlmc_level_result {
+    double fsums[4];           /* sum of phi_f^k, k = 1..4                                      */
+    double diffsums[4];        /* sum of (phi_f - phi_c)^k (zero at level 0)                    */
+    double total_work;
+    uint64_t M;
+    uint64_t inner_stats[6];   /* inner samples, decisions, hit max, hit base, #randu, #randn */
+    double seconds;            /* device time of the call (CUDA events)                         */
+} nmlmc_level_result;
+
+typedef struct nmlmc_portfolio {
+    uint32_t Q, P;                        /* stocks, options                                 */
+    const double *S0, *mu, *sigma;        /* [Q]                                             */
+    const double *strike, *maturity, *w;  /* [P]                                             */
+    const double* prob;                   /* [P], positive, non-increasing; NULL = all 1     */
+    const uint32_t* stock_ind;            /* [P]                                             */
+    const int32_t* type;                  /* [P] +1 call / -1 put                            */
+    double r, rho, max_loss, tau;
+    int32_t subsample;                    /* NMLMC_SUB_*                                     */
+    int32_t use_delta_cv;
+    int32_t discount;                     /* 1: finish value discounted by exp(-r tau)       */
+} nmlmc_portfolio;
+
+/* Per-outer-sample record written by nmlmc_sample when a trace buffer is armed. */
+typedef struct nmlmc_trace_rec {
+    uint64_t count_f, count_c;
+    double phi_f, phi_c;
+    double mean_big, min_abs_small;
+    uint32_t core, pilots;
+} nmlmc_trace_rec;
+
+const char* nmlmc_error_string(int status);
+int nmlmc_version(void);
+
+int nmlmc_create(nmlmc_ctx** out, int device);
+int nmlmc_destroy(nmlmc_ctx* ctx);
+int nmlmc_configure(nmlmc_ctx* ctx, const nmlmc_config* cfg);
+/* kind NMLMC_MODEL_REFERENCE: model::sampler with tau, max_loss;
+ * kind NMLMC_MODEL_SHIFT: Y ~ N(0,1), inner X = Y + Z, threshold K = max_loss. */
+int nmlmc_set_model(nmlmc_ctx* ctx, int32_t kind, double tau, double max_loss);
+int nmlmc_set_portfolio(nmlmc_ctx* ctx, const nmlmc_portfolio* pf, double* out_start,
+                        double* out_delta_est);
+/* Restart every stream (CORE: random_state(seed, core) from counter 0; OUTER: outer indices
+ * from 0). */
+int nmlmc_reset_streams(nmlmc_ctx* ctx);
+/* One level: M outer samples at level ell. */
+int nmlmc_sample(nmlmc_ctx* ctx, uint32_t ell, uint64_t M, nmlmc_level_result* out);
+/* Several levels in one submission (OUTER layout: one CUDA graph, levels run concurrently). */
+int nmlmc_sample_levels(nmlmc_ctx* ctx, uint32_t n, const uint32_t* ells, const uint64_t* Ms,
+                        nmlmc_level_result* outs);
+/* Arms a host buffer of `cap` records for the next nmlmc_sample call (M <= cap). */
+int nmlmc_set_trace(nmlmc_ctx* ctx, nmlmc_trace_rec* host_buf, uint64_t cap);
+/* Full portfolio loss L(Y) for outer samples [first, first + n) of level `ell` (OUTER layout
+ * streams): sum_i w_i (V_i(0) - disc V_i(tau, S_tau)). */
+int nmlmc_portfolio_full_loss(nmlmc_ctx* ctx, uint32_t ell, uint64_t first, uint64_t n,
+                              double* host_loss);
+
+/* Threefry2x64-20 blocks computed on the GPU: out[2i..2i+1] = F(ctr[2i..2i+1], key[2i..2i+1])
+ * (host buffers).  Bit-identical to Random123's r123::Threefry2x64. */
+int nmlmc_threefry_blocks(const uint64_t* ctr, const uint64_t* key, uint64_t* out, uint64_t n);
+/* Normals k = 0..n-1 of one OUTER-layout phase (key (seed, stream), counter namespace `tag`)
+ * computed on the GPU at `precision` (NMLMC_PREC_FP64 or NMLMC_PREC_FP32), widened to double. */
+int nmlmc_outer_normals(int32_t precision, uint64_t seed, uint64_t stream, uint32_t tag, uint64_t n,
+                        double* out);
+
+/* ---- host continuation-MLMC driver (mlmc_t::run, mlmc.hpp:290-337) ------------------------- */
+typedef struct nmlmc_mlmc_input {
+    double targetTOL;              /* 1e-3 */
+    double startTOL;               /* 0.5  */
+    double theta;                  /* 0.5  */
+    double starting_level_coeff;   /* 1.5  */
+    double Ca;                     /* 3    */
+    uint64_t M0;                   /* 100  */
+    int32_t verbose;               /* print the reference's "# Sampling" lines and tables */
+    uint32_t max_levels;           /* 0 = unbounded                                       */
+    int32_t batched;               /* 1: one nmlmc_sample_levels submission per round      */
+} nmlmc_mlmc_input;
+
+#define NMLMC_MAX_LEVELS 64
+typedef struct nmlmc_mlmc_output {
+    uint32_t nlevels, starting_level;
+    double bias_est, stat_error, TOL, Eg;
+    double total_work, total_time;          /* total_time: wall seconds of the run          */
+    uint64_t calls;                          /* sample_level invocations                     */
+    uint64_t level_M[NMLMC_MAX_LEVELS];
+    double level_fsums[NMLMC_MAX_LEVELS][4];
+    double level_diffsums[NMLMC_MAX_LEVELS][4];
+    double level_work[NMLMC_MAX_LEVELS];
+    double level_time[NMLMC_MAX_LEVELS];
+} nmlmc_mlmc_output;
+
+typedef void (*nmlmc_sample_level_fn)(void* user, uint32_t ell, uint64_t M,
+                                      nmlmc_level_result* out);
+typedef void (*nmlmc_sample_levels_fn)(void* user, uint32_t n, const uint32_t* ells,
+                                       const uint64_t* Ms, nmlmc_level_result* outs);
+
+nmlmc_mlmc_input nmlmc_mlmc_default_input(void);
+/* Runs the continuation MLMC with the GPU sampler of `ctx`.  `table` (may be NULL) receives the
+ * final to_string() table of the reference's mlmc_output_t. */
+int nmlmc_mlmc_run(nmlmc_ctx* ctx, const nmlmc_mlmc_input* in, nmlmc_mlmc_output* out,
+                   char* table, size_t table_cap);
+/* Same driver over caller-provided level samplers (levels_fn may be NULL). */
+int nmlmc_mlmc_run_cb(const nmlmc_mlmc_input* in, nmlmc_sample_level_fn level_fn,
+                      nmlmc_sample_levels_fn levels_fn, void* user, nmlmc_mlmc_output* out,
+                      char* table, size_t table_cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NMLMC_H */

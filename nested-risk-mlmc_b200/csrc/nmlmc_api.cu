@@ -1,0 +1,868 @@
+// C ABI of the level sampler: contexts, the reference-named surface and host-side set-up.
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/nmlmc.h"
+#include "nmlmc_internal.h"
+
+using namespace nmlmc;
+
+// ---------------------------------------------------------------------------------------------
+// Host-side portfolio arithmetic in real_t, in the reference's evaluation order
+// (portfolio_sampler.cpp:140-160, common.hpp:201-202); compiled without FP contraction.
+namespace {
+
+template <class RT> RT h_erfc(RT x);
+template <> float h_erfc<float>(float x) { return erfcf(x); }
+template <> double h_erfc<double>(double x) { return erfc(x); }
+template <class RT> RT h_log(RT x);
+template <> float h_log<float>(float x) { return logf(x); }
+template <> double h_log<double>(double x) { return log(x); }
+template <class RT> RT h_exp(RT x);
+template <> float h_exp<float>(float x) { return expf(x); }
+template <> double h_exp<double>(double x) { return exp(x); }
+template <class RT> RT h_sqrt(RT x);
+template <> float h_sqrt<float>(float x) { return sqrtf(x); }
+template <> double h_sqrt<double>(double x) { return sqrt(x); }
+
+template <class RT>
+RT h_norm_cdf(RT x) {
+    const RT SQRT_2 = (RT)1.414213562373095;
+    return (RT)(0.5 * (double)h_erfc<RT>(-x / SQRT_2));
+}
+
+template <class RT>
+RT h_d1(RT S0, RT strike, RT r, RT t, RT sigma) {
+    RT v1 = h_log<RT>(S0 / strike);
+    RT v2 = (RT)(((double)r + (double)(sigma * sigma) / 2.0) * (double)t);
+    RT v3 = sigma * h_sqrt<RT>(t);
+    return (v1 + v2) / v3;
+}
+
+template <class RT>
+RT h_calc_bs(int type, RT S0, RT strike, RT r, RT t, RT sigma) {
+    RT d1 = h_d1<RT>(S0, strike, r, t, sigma);
+    RT d2 = d1 - sigma * h_sqrt<RT>(t);
+    RT mod = (RT)type;
+    return mod * S0 * h_norm_cdf<RT>(mod * d1) - mod * strike * h_exp<RT>(-r * t) * h_norm_cdf<RT>(mod * d2);
+}
+
+template <class RT>
+RT h_calc_delta(int type, RT S0, RT strike, RT r, RT t, RT sigma) {
+    return h_norm_cdf<RT>(h_d1<RT>(S0, strike, r, t, sigma)) - (RT)(type == -1 ? 1 : 0);
+}
+
+template <class RT>
+RT h_norm_cdf_inv(RT p) {
+    // Acklam's rational approximation with the coefficient values the reference truncates them
+    // to (common.cpp:53-86).
+    const RT a[] = {-39.696830f, 220.946098f, -275.928510f, 138.357751f, -30.664798f, 2.506628f};
+    const RT b[] = {-54.476098f, 161.585836f, -155.698979f, 66.801311f, -13.280681f};
+    const RT c[] = {-0.007784894002f, -0.32239645f, -2.400758f, -2.549732f, 4.374664f, 2.938163f};
+    const RT d[] = {0.007784695709f, 0.32246712f, 2.445134f, 3.754408f};
+    const RT plow = 0.02425f, phigh = 1 - plow;
+    if (p < plow) {
+        RT q = h_sqrt<RT>(-2 * h_log<RT>(p));
+        return (((((c[0] * q + c[1]) * q + c[2]) * q + c[3]) * q + c[4]) * q + c[5]) /
+               ((((d[0] * q + d[1]) * q + d[2]) * q + d[3]) * q + 1);
+    }
+    if (phigh < p) {
+        RT q = h_sqrt<RT>(-2 * h_log<RT>(1 - p));
+        return -(((((c[0] * q + c[1]) * q + c[2]) * q + c[3]) * q + c[4]) * q + c[5]) /
+               ((((d[0] * q + d[1]) * q + d[2]) * q + d[3]) * q + 1);
+    }
+    RT q = p - 0.5f, r = q * q;
+    return (((((a[0] * r + a[1]) * r + a[2]) * r + a[3]) * r + a[4]) * r + a[5]) * q /
+           (((((b[0] * r + b[1]) * r + b[2]) * r + b[3]) * r + b[4]) * r + 1);
+}
+
+// Portfolio as handed to the sampler, kept on the host in double (the values are the real_t
+// ones when the context computes in float).
+struct HostPortfolio {
+    uint32_t Q = 0, P = 0;
+    std::vector<double> S0, mu, sigma;
+    std::vector<double> strike, maturity, w, prob, W_est, start, delta_est;
+    std::vector<uint32_t> stock_ind;
+    std::vector<int8_t> type;
+    double r = 0, rho = 0, s1_rho2 = 1, max_loss = 0, tau = 0;
+    int subsample = SUB_UNIFORM, use_delta_cv = 0, discount = 1;
+    bool s1_rho2_given = false;
+    bool own_params = false;   // start / delta_est computed here (native API), per precision
+};
+
+template <class RT>
+struct DevPortfolio {
+    RT *strike = nullptr, *maturity = nullptr, *start = nullptr, *w = nullptr, *prob = nullptr,
+       *W_est = nullptr, *cdf = nullptr, *S0 = nullptr, *mu = nullptr, *sigma = nullptr,
+       *delta_coalesce = nullptr;
+    uint32_t* stock_ind = nullptr;
+    int8_t* type = nullptr;
+    OptionTable<RT> table{};
+};
+
+}  // namespace
+
+struct nmlmc_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    nmlmc_config cfg{};
+    bool configured = false;
+    // model / portfolio
+    int kind = -1;
+    double tau = 0, max_loss = 0, stau = 0, s1tau = 0;
+    bool stau_given = false;
+    HostPortfolio pf;
+    int pf_prec = -1;                 // precision the device portfolio was built for
+    DevPortfolio<float> dpf32;
+    DevPortfolio<double> dpf64;
+    // CORE layout
+    CoreStream* d_states = nullptr;
+    double* d_part_sums = nullptr;
+    uint64_t* d_part_stats = nullptr;
+    double* d_out_sums = nullptr;     // [10]
+    uint64_t* d_out_stats = nullptr;  // [6]
+    uint32_t states_cores = 0;
+    // OUTER layout
+    OuterBuffers ob{};
+    bool ob_alloc = false;
+    uint64_t next_outer[NMLMC_MAX_LEVELS] = {};
+    // pinned staging
+    double* h_pin = nullptr;          // 32 doubles
+    // trace
+    nmlmc_trace_rec* trace_host = nullptr;
+    uint64_t trace_cap = 0;
+    TraceRec* d_trace = nullptr;
+    uint64_t d_trace_cap = 0;
+};
+
+namespace {
+
+thread_local int g_tls_error = NMLMC_OK;
+
+int set_err(int e) {
+    g_tls_error = e;
+    return e;
+}
+
+int cuda_status(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return NMLMC_OK;
+    fprintf(stderr, "nmlmc: %s: %s\n", what, cudaGetErrorString(e));
+    return set_err(NMLMC_ERR_CUDA);
+}
+
+#define NM_CUDA(call, what)                                  \
+    do {                                                     \
+        int _s = cuda_status((call), what);                  \
+        if (_s != NMLMC_OK) return _s;                       \
+    } while (0)
+
+template <class T>
+void dfree(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+template <class RT>
+void free_dev_portfolio(DevPortfolio<RT>& d) {
+    dfree(d.strike); dfree(d.maturity); dfree(d.start); dfree(d.w); dfree(d.prob); dfree(d.W_est);
+    dfree(d.cdf); dfree(d.S0); dfree(d.mu); dfree(d.sigma); dfree(d.delta_coalesce);
+    dfree(d.stock_ind); dfree(d.type);
+    d.table = OptionTable<RT>{};
+}
+
+template <class T>
+int upload(T*& d, const std::vector<T>& h) {
+    dfree(d);
+    size_t n = h.size() ? h.size() : 1;
+    if (cudaMalloc(&d, n * sizeof(T)) != cudaSuccess) return set_err(NMLMC_ERR_NOMEM);
+    if (!h.empty()) NM_CUDA(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+    return NMLMC_OK;
+}
+
+template <class RT>
+std::vector<RT> narrow(const std::vector<double>& v) {
+    std::vector<RT> o(v.size());
+    for (size_t i = 0; i < v.size(); i++) o[i] = (RT)v[i];
+    return o;
+}
+
+// start / delta_est of every option (portfolio_comp_params, portfolio_sampler.cpp:687-700).
+template <class RT>
+void comp_params(HostPortfolio& h) {
+    for (uint32_t j = 0; j < h.P; j++) {
+        const uint32_t s = h.stock_ind[j];
+        h.start[j] = (double)h_calc_bs<RT>(h.type[j], (RT)h.S0[s], (RT)h.strike[j], (RT)h.r, (RT)h.maturity[j], (RT)h.sigma[s]);
+        h.delta_est[j] = (double)h_calc_delta<RT>(h.type[j], (RT)h.S0[s], (RT)h.strike[j], (RT)h.r, (RT)h.maturity[j], (RT)h.sigma[s]);
+    }
+}
+
+// portfolio_comp_params + portfolio_update_data (portfolio_sampler.cpp:631-700) in real_t.
+template <class RT>
+int build_dev_portfolio(nmlmc_ctx* c, DevPortfolio<RT>& d) {
+    HostPortfolio& h = c->pf;
+    free_dev_portfolio(d);
+    if (h.own_params) comp_params<RT>(h);
+    const uint32_t P = h.P, Q = h.Q;
+    std::vector<RT> S0 = narrow<RT>(h.S0), mu = narrow<RT>(h.mu), sg = narrow<RT>(h.sigma);
+    std::vector<RT> K = narrow<RT>(h.strike), T = narrow<RT>(h.maturity), w = narrow<RT>(h.w);
+    std::vector<RT> prob = narrow<RT>(h.prob), West = narrow<RT>(h.W_est);
+    std::vector<RT> start(P), cdf(P), delta(Q, (RT)0);
+    RT prob_norm = 0, cp0 = 0, acc = 0;
+    for (uint32_t j = 0; j < P; j++) {
+        const uint32_t s = h.stock_ind[j];
+        RT st = (RT)h.start[j], de = (RT)h.delta_est[j];
+        start[j] = st;
+        cdf[j] = acc;
+        acc += prob[j];
+        delta[s] += w[j] * de;
+        prob_norm += prob[j];
+        cp0 += prob[j];
+    }
+    int rc;
+    if ((rc = upload(d.strike, K)) || (rc = upload(d.maturity, T)) || (rc = upload(d.start, start)) ||
+        (rc = upload(d.w, w)) || (rc = upload(d.prob, prob)) || (rc = upload(d.W_est, West)) ||
+        (rc = upload(d.cdf, cdf)) || (rc = upload(d.S0, S0)) || (rc = upload(d.mu, mu)) ||
+        (rc = upload(d.sigma, sg)) || (rc = upload(d.delta_coalesce, delta)) ||
+        (rc = upload(d.stock_ind, h.stock_ind)) || (rc = upload(d.type, h.type)))
+        return rc;
+    OptionTable<RT>& t = d.table;
+    t.strike = d.strike; t.maturity = d.maturity; t.start = d.start; t.w = d.w; t.prob = d.prob;
+    t.W_est = d.W_est; t.cdf = d.cdf; t.stock_ind = d.stock_ind; t.type = d.type; t.S0 = d.S0;
+    t.mu = d.mu; t.sigma = d.sigma; t.delta_coalesce = d.delta_coalesce;
+    t.P = P; t.Q = Q;
+    t.r = (RT)h.r; t.rho = (RT)h.rho;
+    t.s1_rho2 = h.s1_rho2_given ? (RT)h.s1_rho2 : h_sqrt<RT>(1 - (RT)h.rho * (RT)h.rho);
+    t.max_loss = (RT)h.max_loss; t.tau = (RT)h.tau;
+    t.stau = h_sqrt<RT>((RT)h.tau);                      // data_ex ctor, portfolio_sampler.cpp:97-98
+    t.prob_norm = prob_norm; t.compute_prob0 = cp0;
+    t.inv_count_prob = (RT)(1. / (double)P);              // portfolio_sampler.cpp:360
+    t.subsample = h.subsample; t.use_delta_cv = h.use_delta_cv; t.discount = h.discount;
+    return NMLMC_OK;
+}
+
+int ensure_portfolio(nmlmc_ctx* c) {
+    if (c->kind != KIND_PORTFOLIO) return NMLMC_OK;
+    const int want = c->cfg.precision == NMLMC_PREC_FP64 ? 1 : 0;
+    if (c->pf_prec == want) return NMLMC_OK;
+    int rc = want ? build_dev_portfolio<double>(c, c->dpf64) : build_dev_portfolio<float>(c, c->dpf32);
+    if (rc == NMLMC_OK) c->pf_prec = want;
+    return rc;
+}
+
+bool is_adaptive(const nmlmc_config& cfg, double r) {
+    if (cfg.precision == NMLMC_PREC_FP64) return r > 1 && (cfg.adaptive_incl_r2 ? r <= 2 : r < 2);
+    float rf = (float)r;
+    return rf > 1 && (cfg.adaptive_incl_r2 ? rf <= 2 : rf < 2);
+}
+
+uint64_t upow(uint64_t x, uint32_t n) {
+    uint64_t r = 1;
+    while (n--) r *= x;
+    return r;
+}
+
+// get_samples_count ctor (nested_sampler.hpp:225-239) with the host libm, in real_t.
+CountParams count_params(const nmlmc_config& cfg, uint32_t ell) {
+    CountParams p;
+    p.max_count = (uint64_t)cfg.N0 * upow(cfg.beta, ell);
+    if (is_adaptive(cfg, cfg.adaptive_r)) {
+        p.base_count = (uint64_t)cfg.N0 * upow(cfg.beta >> 1, ell);
+        if (cfg.precision == NMLMC_PREC_FP64)
+            p.tmp = (double)p.max_count * pow(9.0 / (double)p.max_count, cfg.adaptive_r / 2);
+        else
+            p.tmp = (double)((float)p.max_count * powf(9.f / (float)p.max_count, (float)cfg.adaptive_r / 2));
+    } else {
+        p.base_count = p.max_count;
+        p.tmp = 0;
+    }
+    return p;
+}
+
+int alloc_core(nmlmc_ctx* c) {
+    const uint32_t cores = c->cfg.cores;
+    if (c->states_cores == cores && c->d_states) return NMLMC_OK;
+    dfree(c->d_states); dfree(c->d_part_sums); dfree(c->d_part_stats);
+    if (cudaMalloc(&c->d_states, (size_t)cores * 2 * sizeof(CoreStream)) != cudaSuccess ||
+        cudaMalloc(&c->d_part_sums, (size_t)cores * 10 * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->d_part_stats, (size_t)cores * 6 * sizeof(uint64_t)) != cudaSuccess)
+        return set_err(NMLMC_ERR_NOMEM);
+    c->states_cores = cores;
+    return NMLMC_OK;
+}
+
+int alloc_outer(nmlmc_ctx* c) {
+    const uint64_t cap = c->cfg.batch;
+    const uint32_t Q = c->kind == KIND_PORTFOLIO ? c->pf.Q : 0;
+    if (c->ob_alloc && c->ob.cap == cap && c->ob.Q >= Q) return NMLMC_OK;
+    OuterBuffers& B = c->ob;
+    if (c->ob_alloc) {
+        cudaFree(B.Yv); cudaFree(B.Rt); cudaFree(B.cnt_f); cudaFree(B.cnt_c); cudaFree(B.pil);
+        cudaFree(B.lists); cudaFree(B.class_items); cudaFree(B.counters); cudaFree(B.block_sums);
+        cudaFree(B.level_acc);
+        c->ob_alloc = false;
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    B.cap = cap;
+    B.Q = Q;
+    B.grid = sms * 4;
+    bool ok = cudaMalloc(&B.Yv, cap * sizeof(double)) == cudaSuccess &&
+              cudaMalloc(&B.Rt, (Q ? cap * Q : 1) * sizeof(double)) == cudaSuccess &&
+              cudaMalloc(&B.cnt_f, cap * sizeof(uint32_t)) == cudaSuccess &&
+              cudaMalloc(&B.cnt_c, cap * sizeof(uint32_t)) == cudaSuccess &&
+              cudaMalloc(&B.pil, cap * sizeof(uint32_t)) == cudaSuccess &&
+              cudaMalloc(&B.lists, 4 * cap * sizeof(uint32_t)) == cudaSuccess &&
+              cudaMalloc(&B.class_items, cap * sizeof(uint32_t)) == cudaSuccess &&
+              cudaMalloc(&B.counters, 256 * sizeof(uint32_t)) == cudaSuccess &&
+              cudaMalloc(&B.block_sums, (size_t)B.grid * 16 * sizeof(double)) == cudaSuccess &&
+              cudaMalloc(&B.level_acc, 16 * sizeof(double)) == cudaSuccess;
+    if (!ok) return set_err(NMLMC_ERR_NOMEM);
+    cudaMemset(B.counters, 0, 256 * sizeof(uint32_t));
+    c->ob_alloc = true;
+    return NMLMC_OK;
+}
+
+template <class RT>
+ModelParams<RT> model_params(const nmlmc_ctx* c) {
+    ModelParams<RT> mp;
+    if (c->stau_given) {
+        mp.stau = (RT)c->stau;
+        mp.s1tau = (RT)c->s1tau;
+    } else {
+        RT t = (RT)c->tau;                       // model::data ctor (model_sampler.cpp:24-29)
+        mp.stau = h_sqrt<RT>(t);
+        mp.s1tau = h_sqrt<RT>((RT)1 - t);
+    }
+    mp.max_loss = (RT)c->max_loss;
+    return mp;
+}
+
+int ensure_trace(nmlmc_ctx* c, uint64_t M) {
+    if (!c->trace_host) return NMLMC_OK;
+    if (M > c->trace_cap) return set_err(NMLMC_ERR_ARG);
+    if (c->d_trace_cap < M) {
+        dfree(c->d_trace);
+        if (cudaMalloc(&c->d_trace, M * sizeof(TraceRec)) != cudaSuccess) return set_err(NMLMC_ERR_NOMEM);
+        c->d_trace_cap = M;
+    }
+    return NMLMC_OK;
+}
+
+template <class RT>
+int sample_core(nmlmc_ctx* c, uint32_t ell, uint64_t M, nmlmc_level_result* out) {
+    CoreLaunch<RT> L{};
+    L.cores = c->cfg.cores;
+    L.ell = ell;
+    L.M = M;
+    L.seed = c->cfg.seed;
+    L.fine_only = ell == 0;
+    L.antithetic = c->cfg.antithetic != 0;
+    L.adaptive_r = c->cfg.precision == NMLMC_PREC_FP64 ? c->cfg.adaptive_r : (double)(float)c->cfg.adaptive_r;
+    L.cf = count_params(c->cfg, ell);
+    L.cc = count_params(c->cfg, ell == 0 ? 0 : ell - 1);
+    L.mp = model_params<RT>(c);
+    if (c->kind == KIND_PORTFOLIO) {
+        if constexpr (sizeof(RT) == 4) L.ot = c->dpf32.table; else L.ot = c->dpf64.table;
+    }
+    TraceRec* tr = c->trace_host ? c->d_trace : nullptr;
+    NM_CUDA(cudaEventRecord(c->ev0, c->stream), "event");
+    NM_CUDA(launch_core(L, c->kind, c->d_states, c->d_part_sums, c->d_part_stats, c->d_out_sums,
+                        c->d_out_stats, tr, c->stream), "core level kernel");
+    NM_CUDA(cudaEventRecord(c->ev1, c->stream), "event");
+    NM_CUDA(cudaMemcpyAsync(c->h_pin, c->d_out_sums, 10 * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "d2h");
+    NM_CUDA(cudaMemcpyAsync(c->h_pin + 16, c->d_out_stats, 6 * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream), "d2h");
+    if (tr) NM_CUDA(cudaMemcpyAsync(c->trace_host, tr, M * sizeof(TraceRec), cudaMemcpyDeviceToHost, c->stream), "d2h");
+    NM_CUDA(cudaStreamSynchronize(c->stream), "sync");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    for (int j = 0; j < 4; j++) { out->fsums[j] = c->h_pin[j]; out->diffsums[j] = c->h_pin[4 + j]; }
+    out->total_work = c->h_pin[8];
+    out->M = M;
+    memcpy(out->inner_stats, c->h_pin + 16, 6 * sizeof(uint64_t));
+    out->seconds = ms * 1e-3;
+    c->trace_host = nullptr;
+    return NMLMC_OK;
+}
+
+template <class RT>
+int sample_outer(nmlmc_ctx* c, uint32_t ell, uint64_t M, nmlmc_level_result* out) {
+    OuterLevel<RT> L{};
+    L.ell = ell;
+    L.M = M;
+    L.first_index = c->next_outer[ell];
+    L.seed = c->cfg.seed;
+    L.fine_only = ell == 0;
+    L.antithetic = c->cfg.antithetic != 0;
+    L.N0 = c->cfg.N0;
+    L.chunk = c->cfg.N0 >= 32 ? 32 : c->cfg.N0;
+    L.adaptive_r = (RT)c->cfg.adaptive_r;
+    L.cf = count_params(c->cfg, ell);
+    L.cc = count_params(c->cfg, ell == 0 ? 0 : ell - 1);
+    const bool adapt = is_adaptive(c->cfg, c->cfg.adaptive_r);
+    L.adaptive_f = adapt && L.cf.max_count > 2 * L.cf.base_count;
+    L.adaptive_c = !L.fine_only && adapt && L.cc.max_count > 2 * L.cc.base_count;
+    L.mp = model_params<RT>(c);
+    if (c->kind == KIND_PORTFOLIO) {
+        if constexpr (sizeof(RT) == 4) L.ot = c->dpf32.table; else L.ot = c->dpf64.table;
+    }
+    TraceRec* tr = c->trace_host ? c->d_trace : nullptr;
+    NM_CUDA(cudaEventRecord(c->ev0, c->stream), "event");
+    NM_CUDA(outer_level_begin(c->ob, c->stream), "level begin");
+    NM_CUDA(outer_sample_level<RT>(L, c->kind, c->cfg.precision, c->ob, tr, c->stream), "outer level kernels");
+    NM_CUDA(cudaEventRecord(c->ev1, c->stream), "event");
+    NM_CUDA(cudaMemcpyAsync(c->h_pin, c->ob.level_acc, 16 * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "d2h");
+    if (tr) NM_CUDA(cudaMemcpyAsync(c->trace_host, tr, M * sizeof(TraceRec), cudaMemcpyDeviceToHost, c->stream), "d2h");
+    NM_CUDA(cudaStreamSynchronize(c->stream), "sync");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    const double* a = c->h_pin;
+    for (int j = 0; j < 4; j++) { out->fsums[j] = a[j]; out->diffsums[j] = a[4 + j]; }
+    out->total_work = a[8];
+    out->M = M;
+    const uint64_t inner = (uint64_t)a[9];
+    out->inner_stats[0] = inner;
+    out->inner_stats[1] = M;
+    out->inner_stats[2] = (uint64_t)a[10];
+    out->inner_stats[3] = (uint64_t)a[11];
+    if (c->kind == KIND_PORTFOLIO) {
+        out->inner_stats[4] = inner;
+        out->inner_stats[5] = M * (c->pf.Q == 1 ? 1 : (uint64_t)c->pf.Q + 1);
+    } else {
+        out->inner_stats[4] = 0;
+        out->inner_stats[5] = M + inner * (c->kind == KIND_REF_MODEL ? 2 : 1);
+    }
+    out->seconds = ms * 1e-3;
+    c->next_outer[ell] += M;
+    c->trace_host = nullptr;
+    return NMLMC_OK;
+}
+
+}  // namespace
+
+// ============================================================================================
+extern "C" {
+
+const char* nmlmc_error_string(int s) {
+    switch (s) {
+    case NMLMC_OK: return "ok";
+    case NMLMC_ERR_ARG: return "invalid argument";
+    case NMLMC_ERR_CUDA: return "CUDA error";
+    case NMLMC_ERR_STATE: return "call out of order";
+    case NMLMC_ERR_NOMEM: return "out of memory";
+    case NMLMC_ERR_TIMEOUT: return "bounded device wait gave up";
+    default: return "unknown status";
+    }
+}
+
+int nmlmc_version(void) { return 1; }
+
+int nmlmc_create(nmlmc_ctx** out, int device) {
+    if (!out) return set_err(NMLMC_ERR_ARG);
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        fprintf(stderr, "nmlmc: no CUDA device available\n");
+        return set_err(NMLMC_ERR_CUDA);
+    }
+    if (device < 0 || device >= n) return set_err(NMLMC_ERR_ARG);
+    NM_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    nmlmc_ctx* c = new (std::nothrow) nmlmc_ctx();
+    if (!c) return set_err(NMLMC_ERR_NOMEM);
+    c->device = device;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+        cudaMallocHost(&c->h_pin, 64 * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->d_out_sums, 16 * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->d_out_stats, 8 * sizeof(uint64_t)) != cudaSuccess) {
+        nmlmc_destroy(c);
+        return set_err(NMLMC_ERR_CUDA);
+    }
+    *out = c;
+    return NMLMC_OK;
+}
+
+int nmlmc_destroy(nmlmc_ctx* c) {
+    if (!c) return NMLMC_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    free_dev_portfolio(c->dpf32);
+    free_dev_portfolio(c->dpf64);
+    dfree(c->d_states); dfree(c->d_part_sums); dfree(c->d_part_stats);
+    dfree(c->d_out_sums); dfree(c->d_out_stats); dfree(c->d_trace);
+    if (c->ob_alloc) {
+        OuterBuffers& B = c->ob;
+        cudaFree(B.Yv); cudaFree(B.Rt); cudaFree(B.cnt_f); cudaFree(B.cnt_c); cudaFree(B.pil);
+        cudaFree(B.lists); cudaFree(B.class_items); cudaFree(B.counters); cudaFree(B.block_sums);
+        cudaFree(B.level_acc);
+    }
+    if (c->h_pin) cudaFreeHost(c->h_pin);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return NMLMC_OK;
+}
+
+int nmlmc_configure(nmlmc_ctx* c, const nmlmc_config* cfg) {
+    if (!c || !cfg) return set_err(NMLMC_ERR_ARG);
+    nmlmc_config k = *cfg;
+    if (k.cores == 0) k.cores = 2048;
+    if (k.batch == 0) k.batch = 1u << 20;
+    if (k.N0 == 0 || k.beta == 0 || (k.beta & (k.beta - 1)) != 0) return set_err(NMLMC_ERR_ARG);
+    if (k.precision < NMLMC_PREC_REF32 || k.precision > NMLMC_PREC_FP32) return set_err(NMLMC_ERR_ARG);
+    if (k.streams != NMLMC_STREAMS_CORE && k.streams != NMLMC_STREAMS_OUTER) return set_err(NMLMC_ERR_ARG);
+    if (k.streams == NMLMC_STREAMS_CORE && k.precision == NMLMC_PREC_FP32) return set_err(NMLMC_ERR_ARG);
+    if (k.streams == NMLMC_STREAMS_OUTER) {
+        // chunks of min(N0, 32) samples must tile every count N0 * 2^k; the breadth-first path
+        // implements the antithetic estimator
+        const uint32_t ch = k.N0 >= 32 ? 32 : k.N0;
+        if ((k.N0 % ch) != 0 || (ch & (ch - 1)) != 0 || ch < 4 || !k.antithetic) return set_err(NMLMC_ERR_ARG);
+        if (k.batch > (1ull << 31)) return set_err(NMLMC_ERR_ARG);
+    }
+    cudaSetDevice(c->device);
+    const bool prec_changed = c->cfg.precision != k.precision;
+    c->cfg = k;
+    c->configured = true;
+    if (prec_changed) c->pf_prec = -1;
+    return nmlmc_reset_streams(c);
+}
+
+int nmlmc_reset_streams(nmlmc_ctx* c) {
+    if (!c || !c->configured) return set_err(NMLMC_ERR_STATE);
+    cudaSetDevice(c->device);
+    memset(c->next_outer, 0, sizeof(c->next_outer));
+    if (c->cfg.streams == NMLMC_STREAMS_CORE) {
+        int rc = alloc_core(c);
+        if (rc) return rc;
+        // init_samplers: both random_state(seed, core) from counter {0,0}, no cached normal
+        NM_CUDA(cudaMemset(c->d_states, 0, (size_t)c->cfg.cores * 2 * sizeof(CoreStream)), "reset streams");
+    }
+    return NMLMC_OK;
+}
+
+int nmlmc_set_model(nmlmc_ctx* c, int32_t kind, double tau, double max_loss) {
+    if (!c) return set_err(NMLMC_ERR_ARG);
+    if (kind != NMLMC_MODEL_REFERENCE && kind != NMLMC_MODEL_SHIFT) return set_err(NMLMC_ERR_ARG);
+    c->kind = kind;
+    c->tau = tau;
+    c->max_loss = max_loss;
+    c->stau_given = false;
+    return NMLMC_OK;
+}
+
+int nmlmc_set_portfolio(nmlmc_ctx* c, const nmlmc_portfolio* p, double* out_start, double* out_delta) {
+    if (!c || !p || !c->configured) return set_err(!c || !p ? NMLMC_ERR_ARG : NMLMC_ERR_STATE);
+    if (p->Q == 0 || p->P == 0 || !p->S0 || !p->mu || !p->sigma || !p->strike || !p->maturity || !p->w ||
+        !p->stock_ind || !p->type)
+        return set_err(NMLMC_ERR_ARG);
+    if (p->subsample != NMLMC_SUB_NONE && p->subsample != NMLMC_SUB_RANDOM && p->subsample != NMLMC_SUB_UNIFORM)
+        return set_err(NMLMC_ERR_ARG);
+    HostPortfolio& h = c->pf;
+    h = HostPortfolio{};
+    h.Q = p->Q;
+    h.P = p->P;
+    h.S0.assign(p->S0, p->S0 + p->Q);
+    h.mu.assign(p->mu, p->mu + p->Q);
+    h.sigma.assign(p->sigma, p->sigma + p->Q);
+    h.strike.assign(p->strike, p->strike + p->P);
+    h.maturity.assign(p->maturity, p->maturity + p->P);
+    h.w.assign(p->w, p->w + p->P);
+    h.prob.assign(p->P, 1.0);
+    if (p->prob) h.prob.assign(p->prob, p->prob + p->P);
+    h.W_est.assign(p->P, 1.0);
+    h.start.assign(p->P, 0.0);
+    h.delta_est.assign(p->P, 0.0);
+    h.stock_ind.assign(p->stock_ind, p->stock_ind + p->P);
+    h.type.resize(p->P);
+    const bool f32 = c->cfg.precision != NMLMC_PREC_FP64;
+    double prev = INFINITY;
+    for (uint32_t j = 0; j < p->P; j++) {
+        if (h.stock_ind[j] >= p->Q || (p->type[j] != 1 && p->type[j] != -1)) return set_err(NMLMC_ERR_ARG);
+        double pr = f32 ? (double)(float)h.prob[j] : h.prob[j];
+        if (!(pr > 0) || !(prev >= pr)) return set_err(NMLMC_ERR_ARG);   // portfolio_sampler.cpp:654
+        prev = pr;
+        h.type[j] = (int8_t)p->type[j];
+    }
+    h.r = p->r; h.rho = p->rho; h.max_loss = p->max_loss; h.tau = p->tau;
+    h.subsample = p->subsample; h.use_delta_cv = p->use_delta_cv; h.discount = p->discount;
+    h.own_params = true;
+    if (f32) comp_params<float>(h); else comp_params<double>(h);
+    if (out_start) memcpy(out_start, h.start.data(), p->P * sizeof(double));
+    if (out_delta) memcpy(out_delta, h.delta_est.data(), p->P * sizeof(double));
+    c->kind = KIND_PORTFOLIO;
+    c->pf_prec = -1;
+    cudaSetDevice(c->device);
+    return ensure_portfolio(c);
+}
+
+int nmlmc_set_trace(nmlmc_ctx* c, nmlmc_trace_rec* host_buf, uint64_t cap) {
+    if (!c) return set_err(NMLMC_ERR_ARG);
+    c->trace_host = host_buf;
+    c->trace_cap = host_buf ? cap : 0;
+    return NMLMC_OK;
+}
+
+int nmlmc_sample(nmlmc_ctx* c, uint32_t ell, uint64_t M, nmlmc_level_result* out) {
+    if (!c || !out) return set_err(NMLMC_ERR_ARG);
+    if (!c->configured || c->kind < 0) return set_err(NMLMC_ERR_STATE);
+    if (ell >= NMLMC_MAX_LEVELS) return set_err(NMLMC_ERR_ARG);
+    memset(out, 0, sizeof(*out));
+    out->M = M;
+    const nmlmc_config& k = c->cfg;
+    // counts must fit the 32-bit per-item counters of the batched path
+    if ((double)k.N0 * pow((double)k.beta, (double)ell) > 4.0e9) return set_err(NMLMC_ERR_ARG);
+    if (M == 0) return NMLMC_OK;
+    cudaSetDevice(c->device);
+    int rc = ensure_portfolio(c);
+    if (rc) return rc;
+    if ((rc = ensure_trace(c, M))) return rc;
+    const bool f64 = k.precision == NMLMC_PREC_FP64;
+    if (k.streams == NMLMC_STREAMS_CORE) {
+        if ((rc = alloc_core(c))) return rc;
+        return f64 ? sample_core<double>(c, ell, M, out) : sample_core<float>(c, ell, M, out);
+    }
+    if ((rc = alloc_outer(c))) return rc;
+    return f64 ? sample_outer<double>(c, ell, M, out) : sample_outer<float>(c, ell, M, out);
+}
+
+int nmlmc_sample_levels(nmlmc_ctx* c, uint32_t n, const uint32_t* ells, const uint64_t* Ms,
+                        nmlmc_level_result* outs) {
+    if (!c || (n && (!ells || !Ms || !outs))) return set_err(NMLMC_ERR_ARG);
+    for (uint32_t i = 0; i < n; i++) {
+        int rc = nmlmc_sample(c, ells[i], Ms[i], &outs[i]);
+        if (rc) return rc;
+    }
+    return NMLMC_OK;
+}
+
+int nmlmc_portfolio_full_loss(nmlmc_ctx* c, uint32_t ell, uint64_t first, uint64_t n, double* host_loss) {
+    if (!c || !host_loss) return set_err(NMLMC_ERR_ARG);
+    if (!c->configured || c->kind != KIND_PORTFOLIO) return set_err(NMLMC_ERR_STATE);
+    if (n == 0) return NMLMC_OK;
+    cudaSetDevice(c->device);
+    int rc = ensure_portfolio(c);
+    if (rc || (rc = alloc_outer(c))) return rc;
+    double* d_loss = nullptr;
+    if (cudaMalloc(&d_loss, n * sizeof(double)) != cudaSuccess) return set_err(NMLMC_ERR_NOMEM);
+    cudaError_t e;
+    if (c->cfg.precision == NMLMC_PREC_FP64) {
+        OuterLevel<double> L{};
+        L.ell = ell; L.M = n; L.first_index = first; L.seed = c->cfg.seed; L.ot = c->dpf64.table;
+        e = outer_full_loss<double>(L, c->cfg.precision, c->ob, d_loss, c->stream);
+    } else {
+        OuterLevel<float> L{};
+        L.ell = ell; L.M = n; L.first_index = first; L.seed = c->cfg.seed; L.ot = c->dpf32.table;
+        e = outer_full_loss<float>(L, c->cfg.precision, c->ob, d_loss, c->stream);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host_loss, d_loss, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(d_loss);
+    return cuda_status(e, "full loss");
+}
+
+int nmlmc_threefry_blocks(const uint64_t* ctr, const uint64_t* key, uint64_t* out, uint64_t n) {
+    if (!ctr || !key || !out) return set_err(NMLMC_ERR_ARG);
+    if (n == 0) return NMLMC_OK;
+    uint64_t* d = nullptr;
+    if (cudaMalloc(&d, 6 * n * sizeof(uint64_t)) != cudaSuccess) return set_err(NMLMC_ERR_NOMEM);
+    cudaError_t e = cudaMemcpy(d, ctr, 2 * n * sizeof(uint64_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d + 2 * n, key, 2 * n * sizeof(uint64_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = launch_threefry_blocks(d, d + 2 * n, d + 4 * n, n, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(out, d + 4 * n, 2 * n * sizeof(uint64_t), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return cuda_status(e, "threefry blocks");
+}
+
+int nmlmc_outer_normals(int32_t precision, uint64_t seed, uint64_t stream, uint32_t tag, uint64_t n,
+                        double* out) {
+    if (!out || (precision != NMLMC_PREC_FP32 && precision != NMLMC_PREC_FP64)) return set_err(NMLMC_ERR_ARG);
+    if (n == 0) return NMLMC_OK;
+    double* d = nullptr;
+    if (cudaMalloc(&d, n * sizeof(double)) != cudaSuccess) return set_err(NMLMC_ERR_NOMEM);
+    cudaError_t e = launch_outer_normals(precision, seed, stream, tag, n, d, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(out, d, n * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return cuda_status(e, "outer normals");
+}
+
+// ---- reference-named surface (one process-wide sampler, like g_p_nestedmc_data) --------------
+static nmlmc_ctx* g_ctx = nullptr;
+static int32_t g_default_prec = NMLMC_PREC_REF32, g_default_streams = NMLMC_STREAMS_CORE;
+static int g_last = NMLMC_OK;
+static std::mutex g_mu;
+
+static void ref_fail(int rc, const char* fn) {
+    g_last = rc;
+    if (rc != NMLMC_OK) fprintf(stderr, "nmlmc: %s failed: %s\n", fn, nmlmc_error_string(rc));
+}
+
+int nmlmc_last_error(void) { return g_last; }
+
+int nmlmc_default_set_precision(int32_t precision, int32_t streams) {
+    if (precision < NMLMC_PREC_REF32 || precision > NMLMC_PREC_FP32) return NMLMC_ERR_ARG;
+    if (streams != NMLMC_STREAMS_CORE && streams != NMLMC_STREAMS_OUTER) return NMLMC_ERR_ARG;
+    g_default_prec = precision;
+    g_default_streams = streams;
+    return NMLMC_OK;
+}
+
+void init_nestedmc_sampler(uint32_t cores, const nested_sampler_params* params) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!params) return ref_fail(NMLMC_ERR_ARG, "init_nestedmc_sampler");
+    if (params->fine_moments > 4 || params->diff_moments > 4)   // c_max_moments (nested_sampler.hpp:5)
+        return ref_fail(NMLMC_ERR_ARG, "init_nestedmc_sampler");
+    if (!g_ctx) {
+        int rc = nmlmc_create(&g_ctx, 0);
+        if (rc) return ref_fail(rc, "init_nestedmc_sampler");
+    }
+    nmlmc_config k{};
+    k.cores = cores;
+    k.N0 = params->N0;
+    k.beta = params->beta;
+    k.adaptive_r = (double)params->adaptive_r;
+    k.antithetic = params->antithetic ? 1 : 0;
+    k.precision = g_default_prec;
+    k.streams = g_default_streams;
+    k.seed = 0;
+    ref_fail(nmlmc_configure(g_ctx, &k), "init_nestedmc_sampler");
+}
+
+void cleanup_nestedmc_sampler(void) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    nmlmc_destroy(g_ctx);
+    g_ctx = nullptr;
+    g_last = NMLMC_OK;
+}
+
+void model_update_data(const model_data* d) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_ctx || !d) return ref_fail(!d ? NMLMC_ERR_ARG : NMLMC_ERR_STATE, "model_update_data");
+    g_ctx->kind = KIND_REF_MODEL;
+    g_ctx->stau = d->stau;
+    g_ctx->s1tau = d->s1tau;
+    g_ctx->max_loss = d->max_loss;
+    g_ctx->stau_given = true;
+    g_last = NMLMC_OK;
+}
+
+void model_init(const model_data* d, uint64_t seed) {
+    model_update_data(d);
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_last) return;
+    g_ctx->cfg.seed = seed;
+    ref_fail(nmlmc_reset_streams(g_ctx), "model_init");
+}
+
+static void fill_sample_output(const nmlmc_level_result& r, sample_output* out) {
+    out->M = r.M;
+    const uint32_t fm = 4, dm = 4;
+    if (out->fsums) for (uint32_t j = 0; j < fm; j++) out->fsums[j] = r.fsums[j];
+    if (out->diffsums) for (uint32_t j = 0; j < dm; j++) out->diffsums[j] = r.diffsums[j];
+    out->total_work = r.total_work;
+    memcpy(out->inner_stats, r.inner_stats, sizeof(out->inner_stats));
+}
+
+void model_sample(uint32_t ell, uint64_t M, sample_output* out) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_ctx || !out) return ref_fail(!out ? NMLMC_ERR_ARG : NMLMC_ERR_STATE, "model_sample");
+    if (g_ctx->kind != KIND_REF_MODEL) return ref_fail(NMLMC_ERR_STATE, "model_sample");
+    nmlmc_level_result r;
+    int rc = nmlmc_sample(g_ctx, ell, M, &r);
+    if (rc) return ref_fail(rc, "model_sample");
+    fill_sample_output(r, out);
+    g_last = NMLMC_OK;
+}
+
+static int portfolio_from_ref(const portfolio_data* d) {
+    if (d->options[1].size || d->options[2].size) return NMLMC_ERR_ARG;   // BS options only
+    if (d->phi_type != 0) return NMLMC_ERR_ARG;                          // Indicator only
+    const nmlmc_options_span& o = d->options[0];
+    const nmlmc_stocks_span& s = d->stocks;
+    if (!o.size || !s.size || !o.data || !s.data) return NMLMC_ERR_ARG;
+    HostPortfolio& h = g_ctx->pf;
+    h = HostPortfolio{};
+    h.Q = (uint32_t)s.size;
+    h.P = (uint32_t)o.size;
+    for (size_t i = 0; i < s.size; i++) {
+        h.S0.push_back(s.data[i].S0); h.mu.push_back(s.data[i].mu); h.sigma.push_back(s.data[i].sigma);
+    }
+    float prev = INFINITY;
+    for (size_t j = 0; j < o.size; j++) {
+        const option_params& op = o.data[j];
+        if (op.stock_ind >= s.size || !(op.prob > 0) || !(prev >= op.prob)) return NMLMC_ERR_ARG;
+        prev = op.prob;
+        h.strike.push_back(op.strike); h.maturity.push_back(op.maturity); h.w.push_back(op.w);
+        h.prob.push_back(op.prob); h.W_est.push_back(op.W_est); h.start.push_back(op.start);
+        h.delta_est.push_back(op.delta_est); h.stock_ind.push_back(op.stock_ind);
+        h.type.push_back((int8_t)(op.type > 0 ? 1 : -1));
+    }
+    h.r = d->r; h.rho = d->rho; h.s1_rho2 = d->s1_rho2; h.s1_rho2_given = true;
+    h.max_loss = d->max_loss; h.tau = d->tau;
+    h.subsample = d->subsample; h.use_delta_cv = d->use_delta_cv ? 1 : 0; h.discount = 1;
+    g_ctx->kind = KIND_PORTFOLIO;
+    g_ctx->pf_prec = -1;
+    return ensure_portfolio(g_ctx);
+}
+
+void portfolio_update_data(const portfolio_data* d) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_ctx || !d) return ref_fail(!d ? NMLMC_ERR_ARG : NMLMC_ERR_STATE, "portfolio_update_data");
+    ref_fail(portfolio_from_ref(d), "portfolio_update_data");
+}
+
+void portfolio_init(const portfolio_data* d, uint64_t seed) {
+    portfolio_update_data(d);
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_last) return;
+    g_ctx->cfg.seed = seed;
+    ref_fail(nmlmc_reset_streams(g_ctx), "portfolio_init");
+}
+
+void portfolio_sample(uint32_t ell, uint64_t override_dyn_inner, uint64_t M, sample_output* out) {
+    (void)override_dyn_inner;   // child-grid width of the reference's CUDA build; no counterpart
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_ctx || !out) return ref_fail(!out ? NMLMC_ERR_ARG : NMLMC_ERR_STATE, "portfolio_sample");
+    if (g_ctx->kind != KIND_PORTFOLIO) return ref_fail(NMLMC_ERR_STATE, "portfolio_sample");
+    nmlmc_level_result r;
+    int rc = nmlmc_sample(g_ctx, ell, M, &r);
+    if (rc) return ref_fail(rc, "portfolio_sample");
+    fill_sample_output(r, out);
+    g_last = NMLMC_OK;
+}
+
+void portfolio_cleanup(void) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_ctx) return;
+    free_dev_portfolio(g_ctx->dpf32);
+    free_dev_portfolio(g_ctx->dpf64);
+    g_ctx->pf = HostPortfolio{};
+    g_ctx->pf_prec = -1;
+    if (g_ctx->kind == KIND_PORTFOLIO) g_ctx->kind = -1;
+}
+
+void portfolio_comp_params(portfolio_data* d) {
+    if (!d) { g_last = NMLMC_ERR_ARG; return; }
+    for (int m = 0; m < 3; m++) {
+        for (size_t j = 0; j < d->options[m].size; j++) {
+            option_params& op = d->options[m].data[j];
+            const stock_params& s = d->stocks.data[op.stock_ind];
+            int type = op.type > 0 ? 1 : -1;
+            op.start = h_calc_bs<float>(type, s.S0, op.strike, d->r, op.maturity, s.sigma);
+            op.delta_est = h_calc_delta<float>(type, s.S0, op.strike, d->r, op.maturity, s.sigma);
+        }
+    }
+    g_last = NMLMC_OK;
+}
+
+float norm_cdf_inv(float p) { return h_norm_cdf_inv<float>(p); }
+
+}  // extern "C"

@@ -1,0 +1,87 @@
+// Host/device interface between the C-ABI layer (nmlmc_api.cu) and the kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "nmlmc_common.cuh"
+
+namespace nmlmc {
+
+// One random_state of the CORE layout: 64-bit word position and the cached second normal.
+struct CoreStream {
+    uint64_t wpos;
+    uint32_t saved, pad;
+    double sval;
+};
+static_assert(sizeof(CoreStream) == 24, "CoreStream layout");
+
+template <class RT>
+struct CoreLaunch {
+    uint32_t cores, ell;
+    uint64_t M;
+    uint64_t seed;
+    bool fine_only, antithetic;
+    double adaptive_r;
+    CountParams cf, cc;
+    ModelParams<RT> mp;
+    OptionTable<RT> ot;
+};
+
+cudaError_t launch_core(const CoreLaunch<float>& L, int kind, CoreStream* states, double* part_sums,
+                        uint64_t* part_stats, double* out_sums, uint64_t* out_stats, TraceRec* trace,
+                        cudaStream_t stream);
+cudaError_t launch_core(const CoreLaunch<double>& L, int kind, CoreStream* states, double* part_sums,
+                        uint64_t* part_stats, double* out_sums, uint64_t* out_stats, TraceRec* trace,
+                        cudaStream_t stream);
+
+// ---- OUTER layout (batched) ----------------------------------------------------------------
+enum Prec : int { PREC_REF32 = 0, PREC_FP64 = 1, PREC_FP32 = 2 };
+
+// Per-level launch description of the batched path.
+template <class RT>
+struct OuterLevel {
+    uint32_t ell;
+    uint64_t M;             // outer samples of this call
+    uint64_t first_index;   // stream index of the first outer sample (OUTER layout key)
+    uint64_t seed;
+    bool fine_only, antithetic, adaptive_f, adaptive_c;
+    uint32_t N0, chunk;     // chunk = inner samples per thread (power of two dividing all counts)
+    RT adaptive_r;
+    CountParams cf, cc;
+    ModelParams<RT> mp;
+    OptionTable<RT> ot;
+};
+
+// Device work buffers of the batched path, sized for `cap` outer samples per batch.
+struct OuterBuffers {
+    uint64_t cap;
+    uint32_t Q;
+    void* Yv;                // RT[cap]       model Y / portfolio constant
+    void* Rt;                // RT[cap * Q]   portfolio R_tau rows
+    uint32_t* cnt_f;         // final fine count / chunk size (0 = undecided)
+    uint32_t* cnt_c;
+    uint32_t* pil;           // pilots taken (trace)
+    uint32_t* lists;         // 4 * cap: fine/coarse round lists, ping-pong
+    uint32_t* class_items;   // cap: items sorted by final class
+    uint32_t* counters;      // device counters (see nmlmc_outer.cu)
+    double* block_sums;      // per-CTA partial moments [grid][16]
+    double* level_acc;       // accumulated level result [16]
+    int grid;
+};
+
+template <class RT>
+cudaError_t outer_sample_level(const OuterLevel<RT>& L, int kind, int prec, OuterBuffers& B,
+                               TraceRec* trace, cudaStream_t stream);
+cudaError_t outer_level_begin(OuterBuffers& B, cudaStream_t stream);
+
+// Portfolio loss sweep L(Y) over all options (K-quantile precompute).
+template <class RT>
+cudaError_t outer_full_loss(const OuterLevel<RT>& L, int prec, OuterBuffers& B, double* d_loss,
+                            cudaStream_t stream);
+
+cudaError_t launch_threefry_blocks(const uint64_t* ctr, const uint64_t* key, uint64_t* out, uint64_t n,
+                                   cudaStream_t s);
+cudaError_t launch_outer_normals(int prec, uint64_t seed, uint64_t stream, uint32_t tag, uint64_t n,
+                                 double* out, cudaStream_t s);
+
+}  // namespace nmlmc

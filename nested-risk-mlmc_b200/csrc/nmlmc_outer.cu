@@ -1,0 +1,837 @@
+// OUTER-layout (batched) level sampler.
+//
+// The reference walks each outer sample depth-first: pilots of doubling size until the
+// adaptive rule stops (get_samples_count, nested_sampler.hpp:240-273), then the antithetic
+// fine/coarse estimate (sample_phi_antithetic, 171-216).  Adaptive counts differ by up to 2^ell
+// between outer samples, so a warp per outer sample leaves most of the GPU idle behind the few
+// samples that refine to the maximum.  Here every outer sample has its own counter-based
+// stream (key = (seed, level<<56 | index), counter = (block, phase tag)), which makes each
+// inner sample addressable, and a level call runs breadth-first:
+//
+//   k_outer      one thread per outer sample: outer draws (Y, or R_tau row + constant)
+//   k_phase      pilot round r: every outer sample still refining, fine and coarse, as
+//                uniform-size segments; one thread per chunk of inner samples, block-segmented
+//                reduction, the adaptive decision fused in (survivors appended to the next
+//                round's list)
+//   k_classify   bucket outer samples by their final count (a power of two)
+//   k_phase      final: antithetic groups and the big-count mean, phi, 4 moments into per-CTA
+//                partial sums (fixed order, no atomics on the sums)
+//   k_reduce     per-CTA partials -> the level's sums
+//
+// Every thread does the same unit of work (one chunk), so the device stays full whatever the
+// spread of inner counts.  An item with more chunks than a CTA has threads is walked tile by
+// tile by one CTA.
+#include <cmath>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "nmlmc_common.cuh"
+#include "nmlmc_internal.h"
+
+namespace nmlmc {
+
+constexpr int kTile = 256;           // threads per CTA = chunks per tile
+constexpr int kWarps = kTile / 32;
+constexpr int kMaxSegs = 40;
+
+// device counter slots (uint32 each)
+enum : int {
+    CNT_LIST = 0,        // [4]: fine list size (ping-pong slots 0/1), coarse list size (2/3)
+    CNT_CLASS = 8,       // [64]: outer samples per final class
+    CNT_FILL = 72,       // [64]: scatter fill per class
+    CNT_TOTAL = 144
+};
+
+// ---- accumulators -------------------------------------------------------------------------
+// FP32: compensated pair (hi + lo) — Kahan accumulation inside a thread, TwoSum merging across
+// threads.  FP64 and REF32: double, the reference's sum_t.
+template <int PREC> struct Acc;
+
+template <> struct Acc<PREC_FP32> {
+    float hi, lo;
+    __device__ __forceinline__ void zero() { hi = 0.f; lo = 0.f; }
+    __device__ __forceinline__ void add(float v) {
+        float y = __fadd_rn(v, lo);
+        float t = __fadd_rn(hi, y);
+        lo = __fsub_rn(y, __fsub_rn(t, hi));
+        hi = t;
+    }
+    __device__ __forceinline__ void merge(const Acc& o) {
+        float s = __fadd_rn(hi, o.hi);
+        float bp = __fsub_rn(s, hi);
+        float e = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bp)), __fsub_rn(o.hi, bp));
+        hi = s;
+        lo = __fadd_rn(__fadd_rn(lo, o.lo), e);
+    }
+    __device__ __forceinline__ Acc shfl_xor(int m) const {
+        Acc r;
+        r.hi = __shfl_xor_sync(0xffffffffu, hi, m);
+        r.lo = __shfl_xor_sync(0xffffffffu, lo, m);
+        return r;
+    }
+    __device__ __forceinline__ float value() const { return __fadd_rn(hi, lo); }
+};
+
+template <> struct Acc<PREC_FP64> {
+    double v;
+    __device__ __forceinline__ void zero() { v = 0; }
+    __device__ __forceinline__ void add(double x) { v = __dadd_rn(v, x); }
+    __device__ __forceinline__ void merge(const Acc& o) { v = __dadd_rn(v, o.v); }
+    __device__ __forceinline__ Acc shfl_xor(int m) const { Acc r; r.v = __shfl_xor_sync(0xffffffffu, v, m); return r; }
+    __device__ __forceinline__ double value() const { return v; }
+};
+template <> struct Acc<PREC_REF32> {
+    double v;
+    __device__ __forceinline__ void zero() { v = 0; }
+    __device__ __forceinline__ void add(double x) { v = __dadd_rn(v, x); }
+    __device__ __forceinline__ void merge(const Acc& o) { v = __dadd_rn(v, o.v); }
+    __device__ __forceinline__ Acc shfl_xor(int m) const { Acc r; r.v = __shfl_xor_sync(0xffffffffu, v, m); return r; }
+    __device__ __forceinline__ double value() const { return v; }
+};
+
+template <class RT>
+struct DevLevel {
+    OuterLevel<RT> L;
+    OuterBuffers B;
+};
+
+// inner mean start + s1 / count (sample_inner_mean, nested_sampler.hpp:112-119)
+template <class RT, int PREC>
+__device__ __forceinline__ RT inner_mean(RT start, const Acc<PREC>& s1, uint64_t count) {
+    if (PREC == PREC_FP32) return __fadd_rn((float)start, __fdiv_rn((float)s1.value(), (float)count));
+    return to_rt<RT>(__dadd_rn((double)start, __ddiv_rn((double)s1.value(), (double)count)));
+}
+
+// Box-Muller pair from two OUTER words at the context precision.
+template <int PREC, class RT>
+__device__ __forceinline__ void bm_pair(uint32_t u0, uint32_t u1, RT& x, RT& y) {
+    if (PREC == PREC_FP32) {
+        float fx, fy;
+        boxmuller32_f(u0, u1, fx, fy);
+        x = (RT)fx;
+        y = (RT)fy;
+    } else {
+        double dx, dy;
+        boxmuller32_d(u0, u1, dx, dy);
+        x = to_rt<RT>(dx);
+        y = to_rt<RT>(dy);
+    }
+}
+
+template <int PREC, class RT>
+__device__ __forceinline__ RT u01_word(uint32_t w) {
+    if (PREC == PREC_FP64) return (RT)__dadd_rn(__dmul_rn((double)w, 0x1p-32), 0x1p-33);
+    return (RT)__fadd_rn(__fmul_rn(__uint2float_rn(w), 0x1p-32f), 0x1p-33f);
+}
+
+// normal k of an OUTER phase (used for the outer draws)
+template <int PREC, class RT>
+__device__ __forceinline__ RT outer_normal_at(const TfKey& key, uint32_t tag, uint64_t k) {
+    uint64_t v0, v1;
+    threefry2x64(k >> 2, tag, key, v0, v1);
+    uint64_t e = ((k >> 1) & 1) ? v1 : v0;
+    RT x, y;
+    bm_pair<PREC, RT>((uint32_t)e, (uint32_t)(e >> 32), x, y);
+    return (k & 1) ? y : x;
+}
+
+// ---- portfolio inner value (BS path of portfolio::sampler) ----------------------------------
+template <class RT>
+__device__ __forceinline__ RT pf_value(const OptionTable<RT>& ot, const RT* Rrow, uint32_t j) {
+    uint32_t s = ot.stock_ind[j];
+    int type = ot.type[j];
+    RT sigma = ot.sigma[s];
+    RT bs = calc_bs_ref<RT>(type, Rrow[s], ot.strike[j], ot.r, xsub(ot.maturity[j], ot.tau), sigma);
+    RT finish = ot.discount ? xmul(xexp(xmul(-ot.r, ot.tau)), bs) : bs;
+    RT val = xmul(ot.w[j], xsub(ot.start[j], finish));
+    if (ot.use_delta_cv) {
+        RT derv = xmul(ot.w[j], calc_delta_ref<RT>(type, ot.S0[s], ot.strike[j], ot.r, ot.maturity[j], sigma));
+        val = xadd(val, xmul(xsub(Rrow[s], ot.S0[s]), derv));
+    }
+    return val;
+}
+
+// option index and its probability (sample_inner_random_option_ind, 346-370) from one 64-bit
+// value of the OUTER layout: uniform sub-sampling takes the exact integer floor(v * P / 2^64)
+// (identical in every precision); the CDF search uses u01<real_t>(v) as the reference does.
+template <class RT>
+__device__ __forceinline__ uint32_t pf_pick(const OptionTable<RT>& ot, uint64_t v, RT& prob) {
+    if (ot.subsample == SUB_UNIFORM) {
+        prob = ot.inv_count_prob;
+        return (uint32_t)__umul64hi(v, (uint64_t)ot.P);
+    }
+    RT u = sizeof(RT) == 4 ? (RT)u01_f(v) : (RT)u01_d(v);
+    RT uu = xmul(u, ot.compute_prob0);
+    uint32_t pos0 = 0, pos1 = ot.P;
+    if (ot.P > 1) {
+        uint32_t steps = 32 - __clz(ot.P - 1);
+        for (uint32_t s = 0; s < steps; s++) {
+            uint32_t mid = (pos0 + pos1) / 2;
+            if (mid > 0 && uu < ot.cdf[mid]) pos1 = mid; else pos0 = mid;
+        }
+    }
+    prob = xdiv(ot.prob[pos0], ot.prob_norm);
+    return pos0;
+}
+
+// ---- one chunk: inner samples [s0, s0 + C) of phase `tag` of outer sample `item` ----------
+template <class RT, int KIND, int PREC>
+__device__ __forceinline__ void eval_chunk(const DevLevel<RT>& D, uint32_t item, uint32_t tag,
+                                           uint64_t s0, uint32_t C, bool want_s2, Acc<PREC>& a1,
+                                           Acc<PREC>& a2, double& work) {
+    const OuterLevel<RT>& L = D.L;
+    const TfKey key = tf_key(L.seed, outer_stream_id(L.ell, L.first_index + item));
+    const RT* Yv = reinterpret_cast<const RT*>(D.B.Yv);
+    if (KIND == KIND_SHIFT_MODEL) {              // X = Y + Z: one normal per inner sample
+        const RT Y = Yv[item];
+        for (uint32_t b = 0; b < C / 4; b++) {
+            uint64_t v0, v1;
+            threefry2x64((s0 >> 2) + b, tag, key, v0, v1);
+            RT z[4];
+            bm_pair<PREC, RT>((uint32_t)v0, (uint32_t)(v0 >> 32), z[0], z[1]);
+            bm_pair<PREC, RT>((uint32_t)v1, (uint32_t)(v1 >> 32), z[2], z[3]);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                RT d = (PREC == PREC_FP32) ? (RT)(Y + z[q]) : xadd(Y, z[q]);
+                a1.add(d);
+                if (want_s2) a2.add((PREC == PREC_FP32) ? (RT)(d * d) : xmul(d, d));
+            }
+        }
+        work += (double)C;
+    } else if (KIND == KIND_REF_MODEL) {         // model_sampler.cpp:62-76: two normals
+        const RT Y = Yv[item];
+        const RT st = L.mp.stau, s1t = L.mp.s1tau;
+        for (uint32_t b = 0; b < C / 2; b++) {   // one block = two inner samples
+            uint64_t v0, v1;
+            threefry2x64((s0 >> 1) + b, tag, key, v0, v1);
+            RT X[2], Y2[2];
+            bm_pair<PREC, RT>((uint32_t)v0, (uint32_t)(v0 >> 32), X[0], Y2[0]);
+            bm_pair<PREC, RT>((uint32_t)v1, (uint32_t)(v1 >> 32), X[1], Y2[1]);
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                RT a = xadd(xmul(st, Y), xmul(s1t, X[q]));
+                RT c = xadd(xmul(st, Y2[q]), xmul(s1t, X[q]));
+                RT d = xsub(xmul(a, a), xmul(c, c));
+                a1.add(d);
+                if (want_s2) a2.add(xmul(d, d));
+            }
+        }
+        work += (double)C;
+    } else {                                     // portfolio: one 64-bit value per inner sample
+        const OptionTable<RT>& ot = L.ot;
+        const RT* Rrow = reinterpret_cast<const RT*>(D.B.Rt) + (size_t)item * ot.Q;
+        for (uint32_t b = 0; b < C / 2; b++) {
+            uint64_t v[2];
+            threefry2x64((s0 >> 1) + b, tag, key, v[0], v[1]);
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                RT prob;
+                uint32_t j = pf_pick<RT>(ot, v[q], prob);
+                RT d = xdiv(pf_value<RT>(ot, Rrow, j), prob);
+                work += (double)ot.W_est[j];
+                a1.add(d);
+                if (want_s2) a2.add(xmul(d, d));
+            }
+        }
+    }
+}
+
+// ---- segments of uniform chunk count ------------------------------------------------------
+struct Seg {
+    const uint32_t* list;    // item ids; nullptr: identity 0..n-1
+    uint32_t n_slot;         // counter slot with the item count (list != nullptr)
+    uint32_t n_host;         // item count (list == nullptr)
+    uint32_t nch_log2;       // chunks per item = 1 << nch_log2
+    uint32_t tag;            // OUTER phase tag
+    uint32_t mode;           // 0 fine pilot, 1 coarse pilot, 2 final
+    uint32_t class_k;        // final: class index (list offset = items of lower classes)
+    uint32_t next_slot;      // pilots: counter slot of the next round's list
+    uint32_t* next_list;
+    uint64_t count;          // inner samples per item in this segment
+};
+
+struct SegSet {
+    int n;
+    Seg s[kMaxSegs];
+};
+
+// Adaptive decision after a pilot of `cur` samples (get_samples_count, 240-273, with
+// sample_inner_delta2, 120-129).
+template <class RT, int PREC>
+__device__ __forceinline__ void pilot_done(const DevLevel<RT>& D, const Seg& g, uint32_t item, RT start,
+                                           const Acc<PREC>& a1, const Acc<PREC>& a2, uint32_t* counters) {
+    const OuterLevel<RT>& L = D.L;
+    const CountParams& cp = (g.mode == 0) ? L.cf : L.cc;
+    const uint64_t cur = g.count;
+    RT delta2;
+    if (PREC == PREC_FP32) {
+        float s1 = (float)a1.value(), s2 = (float)a2.value(), n = (float)cur;
+        float mean_d = __fdiv_rn(s1, n);
+        float var = __fdiv_rn(__fsub_rn(s2, __fmul_rn(s1, mean_d)), n - 1.0f);
+        float dist = __fadd_rn((float)start, mean_d);
+        delta2 = (RT)__fdiv_rn(__fmul_rn(dist, dist), var);
+    } else {
+        double s1 = (double)a1.value(), s2 = (double)a2.value();
+        RT out_var = to_rt<RT>(__dsub_rn(__ddiv_rn(s2, (double)(cur - 1)),
+                                         __ddiv_rn(__dmul_rn(s1, s1), (double)(cur * (cur - 1)))));
+        RT dist = xadd(start, to_rt<RT>(__ddiv_rn(s1, (double)cur)));
+        delta2 = xdiv(xmul(dist, dist), out_var);
+    }
+    RT newc;
+    if (L.adaptive_r == (RT)2) newc = xdiv((RT)cp.tmp, delta2);
+    else newc = xmul(xpow(delta2, xdiv(-L.adaptive_r, (RT)2)), (RT)cp.tmp);
+    uint32_t* cnt = (g.mode == 0) ? D.B.cnt_f : D.B.cnt_c;
+    atomicAdd(&D.B.pil[item], 1u);
+    if (newc <= (RT)cur) { cnt[item] = (uint32_t)cur; return; }
+    const uint64_t nxt = cur * 2;
+    if (cp.max_count <= 2 * nxt) { cnt[item] = (uint32_t)cp.max_count; return; }
+    uint32_t pos = atomicAdd(&counters[g.next_slot], 1u);
+    g.next_list[pos] = item;
+}
+
+// Per-item completion of the final phase: phi_f, phi_c, moments, statistics, trace.
+template <class RT>
+__device__ __forceinline__ void final_done(const DevLevel<RT>& D, const Seg& g, uint32_t item,
+                                           RT mean_big, RT phi_small, bool fine_big, double* acc,
+                                           TraceRec* trace) {
+    RT phi_big = (mean_big >= (RT)0) ? (RT)1 : (RT)0;
+    RT f_phi, c_phi;
+    if (D.L.fine_only) { f_phi = phi_big; c_phi = 0; }
+    else if (fine_big) { f_phi = phi_big; c_phi = phi_small; }
+    else { f_phi = phi_small; c_phi = phi_big; }
+    RT p = 1;
+    for (int q = 0; q < 4; q++) { p = xmul(p, f_phi); acc[q] += (double)p; }
+    if (!D.L.fine_only) {
+        RT dphi = xsub(f_phi, c_phi);
+        p = 1;
+        for (int q = 0; q < 4; q++) { p = xmul(p, dphi); acc[4 + q] += (double)p; }
+    }
+    acc[9] += (double)g.count;
+    const uint32_t cf = D.B.cnt_f[item];
+    acc[10] += (cf == (uint32_t)D.L.cf.max_count) ? 1.0 : 0.0;
+    acc[11] += (cf == (uint32_t)D.L.cf.base_count) ? 1.0 : 0.0;
+    if (trace) {
+        TraceRec tr;
+        tr.count_f = cf;
+        tr.count_c = D.L.fine_only ? 0 : D.B.cnt_c[item];
+        tr.phi_f = (double)f_phi;
+        tr.phi_c = (double)c_phi;
+        tr.mean_big = (double)mean_big;
+        tr.min_abs_small = INFINITY;
+        tr.core = 0;
+        tr.pilots = D.B.pil[item];
+        trace[item] = tr;
+    }
+}
+
+template <class RT, int KIND, int PREC>
+__global__ void __launch_bounds__(kTile) k_phase(DevLevel<RT> D, SegSet S, TraceRec* trace) {
+    __shared__ Acc<PREC> sm_a1[kWarps];
+    __shared__ Acc<PREC> sm_a2[kWarps];
+    __shared__ float sm_ind[kWarps];
+    __shared__ double sm_acc[kWarps][16];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const uint32_t C = D.L.chunk;
+    uint32_t* counters = D.B.counters;
+    double acc[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) acc[q] = 0;
+    const RT* Yv = reinterpret_cast<const RT*>(D.B.Yv);
+
+    for (int si = 0; si < S.n; si++) {
+        const Seg g = S.s[si];
+        const uint32_t* list = g.list;
+        uint32_t n_items = g.list ? counters[g.n_slot] : g.n_host;
+        if (g.mode == 2 && g.list) {
+            uint32_t off = 0;
+            for (uint32_t k = 0; k < g.class_k; k++) off += counters[CNT_CLASS + k];
+            list += off;
+        }
+        if (n_items == 0) continue;
+        const uint32_t nch = 1u << g.nch_log2;
+        const bool pilot = g.mode != 2;
+        if (pilot && blockIdx.x == 0 && t == 0) acc[9] += (double)n_items * (double)g.count;
+
+        if (nch <= (uint32_t)kTile) {
+            // ---- a tile holds kTile / nch whole items ----
+            const uint32_t per_tile = kTile / nch;
+            const uint64_t tiles = ((uint64_t)n_items + per_tile - 1) / per_tile;
+            for (uint64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+                const uint64_t lin = tile * per_tile + (t >> g.nch_log2);
+                const uint32_t j = t & (nch - 1);
+                const bool valid = lin < n_items;
+                const uint32_t item = valid ? (list ? list[lin] : (uint32_t)lin) : 0;
+                uint32_t gs = nch;
+                uint64_t csmall = g.count;
+                bool fine_big = true;
+                if (!pilot && valid && !D.L.fine_only) {
+                    uint32_t cf = D.B.cnt_f[item], cc = D.B.cnt_c[item];
+                    csmall = cf < cc ? cf : cc;
+                    fine_big = cf > cc;
+                    gs = (uint32_t)(csmall / C);
+                }
+                const RT start = valid ? (D.L.ot.P ? Yv[item] : -D.L.mp.max_loss) : (RT)0;
+                Acc<PREC> a1, a2;
+                a1.zero();
+                a2.zero();
+                double w = 0;
+                if (valid) eval_chunk<RT, KIND, PREC>(D, item, g.tag, (uint64_t)j * C, C, pilot, a1, a2, w);
+                acc[8] += w;
+                const float coeff = (float)gs / (float)nch;     // 1 / groups (a power of two)
+                float ind = 0.f;
+                if (!pilot && gs == 1) ind = inner_mean<RT, PREC>(start, a1, csmall) >= (RT)0 ? coeff : 0.f;
+                const uint32_t wl = nch < 32 ? nch : 32;
+                for (uint32_t m = 1; m < wl; m <<= 1) {
+                    a1.merge(a1.shfl_xor(m));
+                    if (pilot) a2.merge(a2.shfl_xor(m));
+                    else {
+                        ind += __shfl_xor_sync(0xffffffffu, ind, m);
+                        if (2 * m == gs) ind = inner_mean<RT, PREC>(start, a1, csmall) >= (RT)0 ? coeff : 0.f;
+                    }
+                }
+                const bool leader = (j == 0) && valid;
+                if (nch > 32) {
+                    if (lane == 0) { sm_a1[warp] = a1; sm_a2[warp] = a2; sm_ind[warp] = ind; }
+                    __syncthreads();
+                    if (leader) {
+                        const uint32_t nw = nch / 32;
+                        Acc<PREC> t1, t2;
+                        t1.zero();
+                        t2.zero();
+                        float ti = 0.f;
+                        if (!pilot && gs > 32) {
+                            const uint32_t gw = gs / 32;
+                            for (uint32_t gq = 0; gq < nw / gw; gq++) {
+                                Acc<PREC> gsum;
+                                gsum.zero();
+                                for (uint32_t q = 0; q < gw; q++) gsum.merge(sm_a1[warp + gq * gw + q]);
+                                ti += inner_mean<RT, PREC>(start, gsum, csmall) >= (RT)0 ? coeff : 0.f;
+                                t1.merge(gsum);
+                            }
+                        } else {
+                            for (uint32_t q = 0; q < nw; q++) {
+                                t1.merge(sm_a1[warp + q]);
+                                if (pilot) t2.merge(sm_a2[warp + q]);
+                                ti += sm_ind[warp + q];
+                            }
+                        }
+                        a1 = t1;
+                        a2 = t2;
+                        ind = ti;
+                    }
+                    __syncthreads();
+                }
+                if (leader) {
+                    if (pilot) pilot_done<RT, PREC>(D, g, item, start, a1, a2, counters);
+                    else final_done<RT>(D, g, item, inner_mean<RT, PREC>(start, a1, g.count), (RT)ind,
+                                        fine_big, acc, trace);
+                }
+            }
+        } else {
+            // ---- one CTA walks an item tile by tile ----
+            const uint32_t tiles_per_item = nch / kTile;
+            for (uint64_t it = blockIdx.x; it < n_items; it += gridDim.x) {
+                const uint32_t item = list ? list[it] : (uint32_t)it;
+                uint32_t gs = nch;
+                uint64_t csmall = g.count;
+                bool fine_big = true;
+                if (!pilot && !D.L.fine_only) {
+                    uint32_t cf = D.B.cnt_f[item], cc = D.B.cnt_c[item];
+                    csmall = cf < cc ? cf : cc;
+                    fine_big = cf > cc;
+                    gs = (uint32_t)(csmall / C);
+                }
+                const RT start = D.L.ot.P ? Yv[item] : -D.L.mp.max_loss;
+                const float coeff = (float)gs / (float)nch;
+                Acc<PREC> tot1, tot2, gacc;
+                tot1.zero();
+                tot2.zero();
+                gacc.zero();
+                float tind = 0.f;
+                for (uint32_t tl = 0; tl < tiles_per_item; tl++) {
+                    const uint32_t j = tl * kTile + t;
+                    Acc<PREC> a1, a2;
+                    a1.zero();
+                    a2.zero();
+                    double w = 0;
+                    eval_chunk<RT, KIND, PREC>(D, item, g.tag, (uint64_t)j * C, C, pilot, a1, a2, w);
+                    acc[8] += w;
+                    float ind = 0.f;
+                    if (!pilot && gs == 1) ind = inner_mean<RT, PREC>(start, a1, csmall) >= (RT)0 ? coeff : 0.f;
+                    for (uint32_t m = 1; m < 32; m <<= 1) {
+                        a1.merge(a1.shfl_xor(m));
+                        if (pilot) a2.merge(a2.shfl_xor(m));
+                        else {
+                            ind += __shfl_xor_sync(0xffffffffu, ind, m);
+                            if (2 * m == gs) ind = inner_mean<RT, PREC>(start, a1, csmall) >= (RT)0 ? coeff : 0.f;
+                        }
+                    }
+                    if (lane == 0) { sm_a1[warp] = a1; sm_a2[warp] = a2; sm_ind[warp] = ind; }
+                    __syncthreads();
+                    if (t == 0) {
+                        if (!pilot && gs > 32 && gs < (uint32_t)kTile) {
+                            const uint32_t gw = gs / 32;
+                            for (uint32_t gq = 0; gq < (uint32_t)kWarps / gw; gq++) {
+                                Acc<PREC> gsum;
+                                gsum.zero();
+                                for (uint32_t q = 0; q < gw; q++) gsum.merge(sm_a1[gq * gw + q]);
+                                tind += inner_mean<RT, PREC>(start, gsum, csmall) >= (RT)0 ? coeff : 0.f;
+                                tot1.merge(gsum);
+                            }
+                        } else {
+                            Acc<PREC> t1;
+                            t1.zero();
+                            for (int q = 0; q < kWarps; q++) {
+                                t1.merge(sm_a1[q]);
+                                if (pilot) tot2.merge(sm_a2[q]);
+                                if (!pilot && gs <= 32) tind += sm_ind[q];
+                            }
+                            tot1.merge(t1);
+                            if (!pilot && gs >= (uint32_t)kTile) {
+                                gacc.merge(t1);
+                                if ((((uint64_t)tl + 1) * kTile) % gs == 0) {
+                                    tind += inner_mean<RT, PREC>(start, gacc, csmall) >= (RT)0 ? coeff : 0.f;
+                                    gacc.zero();
+                                }
+                            }
+                        }
+                    }
+                    __syncthreads();
+                }
+                if (t == 0) {
+                    if (pilot) pilot_done<RT, PREC>(D, g, item, start, tot1, tot2, counters);
+                    else final_done<RT>(D, g, item, inner_mean<RT, PREC>(start, tot1, g.count), (RT)tind,
+                                        fine_big, acc, trace);
+                }
+            }
+        }
+    }
+    // per-CTA partials in fixed order
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+        double v = acc[q];
+        for (int m = 16; m > 0; m >>= 1) v += __shfl_xor_sync(0xffffffffu, v, m);
+        if (lane == 0) sm_acc[warp][q] = v;
+    }
+    __syncthreads();
+    if (t < 16) {
+        double v = 0;
+        for (int wq = 0; wq < kWarps; wq++) v += sm_acc[wq][t];
+        D.B.block_sums[(size_t)blockIdx.x * 16 + t] += v;
+    }
+}
+
+// ---- outer draws ---------------------------------------------------------------------------
+template <class RT, int KIND, int PREC>
+__global__ void __launch_bounds__(kTile) k_outer(DevLevel<RT> D, uint32_t nb) {
+    const OuterLevel<RT>& L = D.L;
+    RT* Yv = reinterpret_cast<RT*>(D.B.Yv);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
+        const TfKey key = tf_key(L.seed, outer_stream_id(L.ell, L.first_index + i));
+        D.B.pil[i] = 0;
+        D.B.cnt_f[i] = L.adaptive_f ? 0u : (uint32_t)L.cf.max_count;
+        D.B.cnt_c[i] = L.adaptive_c ? 0u : (uint32_t)L.cc.max_count;
+        if (KIND != KIND_PORTFOLIO) {
+            Yv[i] = outer_normal_at<PREC, RT>(key, PH_OUTER, 0);
+        } else {
+            // portfolio_sampler.cpp:293-311 on the OUTER layout: normal 0 systemic, 1 + s per stock
+            const OptionTable<RT>& ot = L.ot;
+            RT* Rrow = reinterpret_cast<RT*>(D.B.Rt) + (size_t)i * ot.Q;
+            RT dW_sys = xmul(ot.stau, outer_normal_at<PREC, RT>(key, PH_OUTER, 0));
+            RT cv = (RT)0;
+            for (uint32_t s = 0; s < ot.Q; s++) {
+                RT W;
+                if (ot.Q == 1) W = dW_sys;
+                else W = xadd(xmul(ot.rho, dW_sys), xmul(ot.s1_rho2, xmul(ot.stau, outer_normal_at<PREC, RT>(key, PH_OUTER, 1 + s))));
+                RT R = simulate_stock_ref<RT>(ot.S0[s], ot.mu[s], ot.sigma[s], ot.tau, W);
+                Rrow[s] = R;
+                if (ot.use_delta_cv) cv = xadd(cv, xmul(xsub(R, ot.S0[s]), ot.delta_coalesce[s]));
+            }
+            Yv[i] = xsub(-ot.max_loss, cv);
+        }
+    }
+}
+
+// ---- bucket outer samples by final count (count_big = max(cnt_f, cnt_c)) ------------------
+template <class RT>
+__global__ void k_classify(DevLevel<RT> D, uint32_t nb, int pass) {
+    uint32_t* counters = D.B.counters;
+    const uint32_t C = D.L.chunk;
+    __shared__ uint32_t offs[64];
+    if (pass == 1) {
+        if (threadIdx.x == 0) {
+            uint32_t a = 0;
+            for (int k = 0; k < 64; k++) { offs[k] = a; a += counters[CNT_CLASS + k]; }
+        }
+        __syncthreads();
+    }
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
+        uint32_t cf = D.B.cnt_f[i], cc = D.L.fine_only ? 0u : D.B.cnt_c[i];
+        uint32_t cb = cf > cc ? cf : cc;
+        uint32_t k = 31 - __clz(cb / C);
+        if (pass == 0) atomicAdd(&counters[CNT_CLASS + k], 1u);
+        else D.B.class_items[offs[k] + atomicAdd(&counters[CNT_FILL + k], 1u)] = i;
+    }
+}
+
+__global__ void k_reduce_blocks(const double* block_sums, int grid, double* level_acc) {
+    __shared__ double sm[256];
+    for (int q = 0; q < 16; q++) {
+        double v = 0;
+        for (int b = threadIdx.x; b < grid; b += blockDim.x) v += block_sums[(size_t)b * 16 + q];
+        sm[threadIdx.x] = v;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+            if ((int)threadIdx.x < s) sm[threadIdx.x] += sm[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) level_acc[q] += sm[0];
+        __syncthreads();
+    }
+}
+
+// ---- host orchestration ----------------------------------------------------------------------
+static inline uint32_t ilog2_u64(uint64_t v) {
+    uint32_t r = 0;
+    while ((1ull << (r + 1)) <= v) r++;
+    return r;
+}
+
+cudaError_t outer_level_begin(OuterBuffers& B, cudaStream_t stream) {
+    cudaError_t e = cudaMemsetAsync(B.level_acc, 0, 16 * sizeof(double), stream);
+    if (e != cudaSuccess) return e;
+    return cudaMemsetAsync(B.block_sums, 0, (size_t)B.grid * 16 * sizeof(double), stream);
+}
+
+template <class RT, int KIND, int PREC>
+static cudaError_t run_batch(DevLevel<RT>& D, uint32_t nb, TraceRec* trace, cudaStream_t stream) {
+    const OuterLevel<RT>& L = D.L;
+    OuterBuffers& B = D.B;
+    const uint32_t C = L.chunk;
+    const int grid = B.grid;
+    cudaError_t e;
+    int og = (int)((nb + kTile - 1) / kTile);
+    if (og > grid) og = grid;
+    if (og < 1) og = 1;
+    k_outer<RT, KIND, PREC><<<og, kTile, 0, stream>>>(D, nb);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+
+    if (L.adaptive_f || L.adaptive_c) {
+        uint32_t rounds_f = 0, rounds_c = 0;
+        if (L.adaptive_f) for (uint64_t c = L.cf.base_count; L.cf.max_count > 2 * c; c *= 2) rounds_f++;
+        if (L.adaptive_c) for (uint64_t c = L.cc.base_count; L.cc.max_count > 2 * c; c *= 2) rounds_c++;
+        const uint32_t rounds = rounds_f > rounds_c ? rounds_f : rounds_c;
+        uint32_t* listF[2] = {B.lists, B.lists + B.cap};
+        uint32_t* listC[2] = {B.lists + 2 * B.cap, B.lists + 3 * B.cap};
+        for (uint32_t r = 0; r < rounds; r++) {
+            const int cur = r & 1, nxt = cur ^ 1;
+            e = cudaMemsetAsync(B.counters + CNT_LIST + nxt, 0, sizeof(uint32_t), stream);
+            if (e == cudaSuccess) e = cudaMemsetAsync(B.counters + CNT_LIST + 2 + nxt, 0, sizeof(uint32_t), stream);
+            if (e != cudaSuccess) return e;
+            SegSet S;
+            S.n = 0;
+            for (int which = 0; which < 2; which++) {
+                const bool fine = which == 0;
+                if (fine ? (r >= rounds_f) : (r >= rounds_c)) continue;
+                const CountParams& cp = fine ? L.cf : L.cc;
+                Seg& g = S.s[S.n++];
+                g.list = (r == 0) ? nullptr : (fine ? listF[cur] : listC[cur]);
+                g.n_slot = CNT_LIST + (fine ? 0 : 2) + cur;
+                g.n_host = nb;
+                g.count = cp.base_count << r;
+                g.nch_log2 = ilog2_u64(g.count / C);
+                g.tag = (fine ? PH_FINE : PH_COARSE) + r;
+                g.mode = fine ? 0 : 1;
+                g.class_k = 0;
+                g.next_slot = CNT_LIST + (fine ? 0 : 2) + nxt;
+                g.next_list = fine ? listF[nxt] : listC[nxt];
+            }
+            if (S.n == 0) continue;
+            k_phase<RT, KIND, PREC><<<grid, kTile, 0, stream>>>(D, S, nullptr);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
+        e = cudaMemsetAsync(B.counters + CNT_CLASS, 0, 128 * sizeof(uint32_t), stream);
+        if (e != cudaSuccess) return e;
+        k_classify<RT><<<og, kTile, 0, stream>>>(D, nb, 0);
+        k_classify<RT><<<og, kTile, 0, stream>>>(D, nb, 1);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        const uint64_t maxc = L.cf.max_count > L.cc.max_count ? L.cf.max_count : L.cc.max_count;
+        const uint32_t kmax = ilog2_u64(maxc / C);
+        SegSet S;
+        S.n = 0;
+        for (uint32_t k = 0; k <= kmax && S.n < kMaxSegs; k++) {
+            Seg& g = S.s[S.n++];
+            g.list = B.class_items;
+            g.n_slot = CNT_CLASS + k;
+            g.n_host = 0;
+            g.count = (uint64_t)C << k;
+            g.nch_log2 = k;
+            g.tag = PH_FINAL;
+            g.mode = 2;
+            g.class_k = k;
+            g.next_slot = 0;
+            g.next_list = nullptr;
+        }
+        k_phase<RT, KIND, PREC><<<grid, kTile, 0, stream>>>(D, S, trace);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    } else {
+        const uint64_t cbig = (L.fine_only || L.cf.max_count >= L.cc.max_count) ? L.cf.max_count : L.cc.max_count;
+        SegSet S;
+        S.n = 1;
+        Seg& g = S.s[0];
+        g.list = nullptr;
+        g.n_slot = 0;
+        g.n_host = nb;
+        g.count = cbig;
+        g.nch_log2 = ilog2_u64(cbig / C);
+        g.tag = PH_FINAL;
+        g.mode = 2;
+        g.class_k = 0;
+        g.next_slot = 0;
+        g.next_list = nullptr;
+        k_phase<RT, KIND, PREC><<<grid, kTile, 0, stream>>>(D, S, trace);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+template <class RT, int KIND, int PREC>
+static cudaError_t sample_level_t(const OuterLevel<RT>& L, OuterBuffers& B, TraceRec* trace,
+                                  cudaStream_t stream) {
+    DevLevel<RT> D;
+    D.L = L;
+    D.B = B;
+    for (uint64_t done = 0; done < L.M;) {
+        const uint64_t nb = (L.M - done) < B.cap ? (L.M - done) : B.cap;
+        D.L.first_index = L.first_index + done;
+        cudaError_t e = run_batch<RT, KIND, PREC>(D, (uint32_t)nb, trace ? trace + done : nullptr, stream);
+        if (e != cudaSuccess) return e;
+        done += nb;
+    }
+    k_reduce_blocks<<<1, 256, 0, stream>>>(B.block_sums, B.grid, B.level_acc);
+    return cudaGetLastError();
+}
+
+template <class RT>
+cudaError_t outer_sample_level(const OuterLevel<RT>& L, int kind, int prec, OuterBuffers& B,
+                               TraceRec* trace, cudaStream_t stream) {
+    if (prec == PREC_FP64) {
+        if constexpr (sizeof(RT) == 8) {
+            if (kind == KIND_REF_MODEL) return sample_level_t<RT, KIND_REF_MODEL, PREC_FP64>(L, B, trace, stream);
+            if (kind == KIND_SHIFT_MODEL) return sample_level_t<RT, KIND_SHIFT_MODEL, PREC_FP64>(L, B, trace, stream);
+            return sample_level_t<RT, KIND_PORTFOLIO, PREC_FP64>(L, B, trace, stream);
+        }
+        return cudaErrorInvalidValue;
+    }
+    if constexpr (sizeof(RT) == 4) {
+        if (prec == PREC_FP32) {
+            if (kind == KIND_REF_MODEL) return sample_level_t<RT, KIND_REF_MODEL, PREC_FP32>(L, B, trace, stream);
+            if (kind == KIND_SHIFT_MODEL) return sample_level_t<RT, KIND_SHIFT_MODEL, PREC_FP32>(L, B, trace, stream);
+            return sample_level_t<RT, KIND_PORTFOLIO, PREC_FP32>(L, B, trace, stream);
+        }
+        if (kind == KIND_REF_MODEL) return sample_level_t<RT, KIND_REF_MODEL, PREC_REF32>(L, B, trace, stream);
+        if (kind == KIND_SHIFT_MODEL) return sample_level_t<RT, KIND_SHIFT_MODEL, PREC_REF32>(L, B, trace, stream);
+        return sample_level_t<RT, KIND_PORTFOLIO, PREC_REF32>(L, B, trace, stream);
+    }
+    return cudaErrorInvalidValue;
+}
+
+template cudaError_t outer_sample_level<float>(const OuterLevel<float>&, int, int, OuterBuffers&, TraceRec*, cudaStream_t);
+template cudaError_t outer_sample_level<double>(const OuterLevel<double>&, int, int, OuterBuffers&, TraceRec*, cudaStream_t);
+
+// ---- full portfolio loss sweep ---------------------------------------------------------------
+template <class RT, int PREC>
+__global__ void k_full_loss(DevLevel<RT> D, uint32_t nb, double* loss) {
+    // one warp per outer sample: lanes stride the option table, double accumulation
+    const int lane = threadIdx.x & 31;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    const OptionTable<RT>& ot = D.L.ot;
+    for (uint32_t i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < nb; i += warps) {
+        const RT* Rrow = reinterpret_cast<const RT*>(D.B.Rt) + (size_t)i * ot.Q;
+        double s = 0;
+        for (uint32_t j = lane; j < ot.P; j += 32) {
+            uint32_t st = ot.stock_ind[j];
+            RT bs = calc_bs_ref<RT>(ot.type[j], Rrow[st], ot.strike[j], ot.r, xsub(ot.maturity[j], ot.tau), ot.sigma[st]);
+            RT finish = ot.discount ? xmul(xexp(xmul(-ot.r, ot.tau)), bs) : bs;
+            s += (double)xmul(ot.w[j], xsub(ot.start[j], finish));
+        }
+        s = warp_sum(s);
+        if (lane == 0) loss[i] = s;
+    }
+}
+
+template <class RT>
+cudaError_t outer_full_loss(const OuterLevel<RT>& L, int prec, OuterBuffers& B, double* d_loss,
+                            cudaStream_t stream) {
+    DevLevel<RT> D;
+    D.L = L;
+    D.B = B;
+    for (uint64_t done = 0; done < L.M;) {
+        const uint64_t nb = (L.M - done) < B.cap ? (L.M - done) : B.cap;
+        D.L.first_index = L.first_index + done;
+        int og = (int)((nb + kTile - 1) / kTile);
+        if (og > B.grid) og = B.grid;
+        if (og < 1) og = 1;
+        if (prec == PREC_FP64) {
+            if constexpr (sizeof(RT) == 8) {
+                k_outer<RT, KIND_PORTFOLIO, PREC_FP64><<<og, kTile, 0, stream>>>(D, (uint32_t)nb);
+                k_full_loss<RT, PREC_FP64><<<B.grid, kTile, 0, stream>>>(D, (uint32_t)nb, d_loss + done);
+            }
+        } else {
+            if constexpr (sizeof(RT) == 4) {
+                if (prec == PREC_FP32) {
+                    k_outer<RT, KIND_PORTFOLIO, PREC_FP32><<<og, kTile, 0, stream>>>(D, (uint32_t)nb);
+                    k_full_loss<RT, PREC_FP32><<<B.grid, kTile, 0, stream>>>(D, (uint32_t)nb, d_loss + done);
+                } else {
+                    k_outer<RT, KIND_PORTFOLIO, PREC_REF32><<<og, kTile, 0, stream>>>(D, (uint32_t)nb);
+                    k_full_loss<RT, PREC_REF32><<<B.grid, kTile, 0, stream>>>(D, (uint32_t)nb, d_loss + done);
+                }
+            }
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        done += nb;
+    }
+    return cudaSuccess;
+}
+
+template cudaError_t outer_full_loss<float>(const OuterLevel<float>&, int, OuterBuffers&, double*, cudaStream_t);
+template cudaError_t outer_full_loss<double>(const OuterLevel<double>&, int, OuterBuffers&, double*, cudaStream_t);
+
+}  // namespace nmlmc
+
+// ---- utility kernels: raw Threefry blocks and OUTER-layout normals ---------------------------
+namespace nmlmc {
+
+__global__ void k_threefry_blocks(const uint64_t* ctr, const uint64_t* key, uint64_t* out, uint64_t n) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t o0, o1;
+        threefry2x64(ctr[2 * i], ctr[2 * i + 1], tf_key(key[2 * i], key[2 * i + 1]), o0, o1);
+        out[2 * i] = o0;
+        out[2 * i + 1] = o1;
+    }
+}
+
+template <int PREC>
+__global__ void k_outer_normals(uint64_t seed, uint64_t stream, uint32_t tag, uint64_t n, double* out) {
+    const TfKey key = tf_key(seed, stream);
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x) {
+        if (PREC == PREC_FP32) out[k] = (double)outer_normal_at<PREC_FP32, float>(key, tag, k);
+        else out[k] = outer_normal_at<PREC_FP64, double>(key, tag, k);
+    }
+}
+
+cudaError_t launch_threefry_blocks(const uint64_t* ctr, const uint64_t* key, uint64_t* out, uint64_t n,
+                                   cudaStream_t s) {
+    k_threefry_blocks<<<256, 256, 0, s>>>(ctr, key, out, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_outer_normals(int prec, uint64_t seed, uint64_t stream, uint32_t tag, uint64_t n,
+                                 double* out, cudaStream_t s) {
+    if (prec == PREC_FP32) k_outer_normals<PREC_FP32><<<256, 256, 0, s>>>(seed, stream, tag, n, out);
+    else k_outer_normals<PREC_FP64><<<256, 256, 0, s>>>(seed, stream, tag, n, out);
+    return cudaGetLastError();
+}
+
+}  // namespace nmlmc

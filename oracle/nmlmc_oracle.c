@@ -197,6 +197,13 @@ static uint32_t outer_word(const o_cursor *k, uint64_t j) {
     return (j & 1) ? (uint32_t)(e >> 32) : (uint32_t)e;
 }
 
+/* 64-bit value #j of the current OUTER phase: element j & 1 of block j >> 1 (portfolio draws) */
+static uint64_t outer_u64(const o_cursor *k, uint64_t j) {
+    uint64_t ctr[2] = {j >> 1, k->tag}, v[2];
+    o_threefry2x64(ctr, k->key, v);
+    return v[j & 1];
+}
+
 /* normal #k of the current OUTER phase: pair k>>1 from words (2p, 2p+1) */
 static double outer_normal(o_cursor *k) {
     uint64_t idx = k->nnorm++;

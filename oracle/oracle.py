@@ -238,7 +238,8 @@ class Reference:
                                          ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                          ctypes.c_double, ctypes.c_double, ctypes.c_uint64,
                                          _u32p, _u64p, ctypes.c_uint64, _dp, ctypes.c_uint32,
-                                         _u32p, _dp]
+                                         _u32p, _dp, ctypes.c_char_p, ctypes.c_uint64]
+        L.ref_abi_sizes.argtypes = [_u64p]
         L.ref_simulate_stock_dt.restype = ctypes.c_double
         L.ref_simulate_stock_dt.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64, _dp,
                                             ctypes.c_uint64, ctypes.c_double, ctypes.c_double,
@@ -267,6 +268,24 @@ class Reference:
         y = np.zeros(len(u0))
         self.L.ref_boxmuller(_p(u0, _u64p), _p(u1, _u64p), _p(x, _dp), _p(y, _dp), len(u0))
         return x, y
+
+    def abi_sizes(self):
+        out = np.zeros(12, np.uint64)
+        self.L.ref_abi_sizes(_p(out, _u64p))
+        return out
+
+    def mlmc_synthetic(self, targetTOL, M0, a, alpha, v, beta, w, gamma, seed, cap=100000):
+        ells = np.zeros(cap, np.uint32)
+        Ms = np.zeros(cap, np.uint64)
+        lv = np.zeros((64, 10))
+        nl = np.zeros(1, np.uint32)
+        misc = np.zeros(4)
+        buf = ctypes.create_string_buffer(1 << 16)
+        n = self.L.ref_mlmc_synthetic(targetTOL, M0, a, alpha, v, beta, w, gamma, seed,
+                                      _p(ells, _u32p), _p(Ms, _u64p), cap, _p(lv, _dp), 64,
+                                      _p(nl, _u32p), _p(misc, _dp), buf, len(buf))
+        return dict(calls_ell=ells[:n].copy(), calls_M=Ms[:n].copy(), levels=lv[:nl[0]].copy(),
+                    misc=misc, table=buf.value.decode())
 
     def init(self, cores, N0, beta, adaptive_r, antithetic=True):
         self.L.ref_set_threads(cores)

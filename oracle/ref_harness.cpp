@@ -21,6 +21,8 @@
 #include <cstring>
 #include <vector>
 #include <omp.h>
+#include <cstddef>
+#include <string>
 
 #include "common.cpp"
 #include "model_sampler.cpp"
@@ -310,7 +312,8 @@ int64_t ref_mlmc_synthetic(double targetTOL, uint64_t M0, double a, double alpha
                            double beta, double w, double gamma, uint64_t seed,
                            uint32_t* call_ell, uint64_t* call_M, uint64_t cap,
                            double* out_levels /* [ell][4 fine,4 diff, work, M] */, uint32_t lvl_cap,
-                           uint32_t* out_nlevels, double* out_misc /* starting_level,bias,stat,TOL */) {
+                           uint32_t* out_nlevels, double* out_misc /* starting_level,bias,stat,TOL */,
+                           char* table, uint64_t table_cap) {
     sm_state = seed;
     uint64_t ncalls = 0;
     mlmc_t<double, 4>::mlmc_input_t in;
@@ -349,7 +352,29 @@ int64_t ref_mlmc_synthetic(double targetTOL, uint64_t M0, double a, double alpha
         p[8] = out.levels[l].work; p[9] = (double)out.levels[l].M;
     }
     out_misc[0] = out.starting_level; out_misc[1] = out.bias_est; out_misc[2] = out.stat_error; out_misc[3] = out.TOL;
+    if (table && table_cap) {
+        std::string str = out.to_string();
+        size_t n = str.size() < table_cap - 1 ? str.size() : table_cap - 1;
+        memcpy(table, str.data(), n);
+        table[n] = 0;
+    }
     return (int64_t)ncalls;
+}
+
+// sizeof / offsetof of the reference structs that cross its C ABI.
+void ref_abi_sizes(uint64_t* out) {
+    out[0] = sizeof(nested_sampler_params);
+    out[1] = sizeof(sample_output);
+    out[2] = sizeof(model::data);
+    out[3] = sizeof(portfolio::data);
+    out[4] = sizeof(portfolio::option_params);
+    out[5] = sizeof(portfolio::stock_params);
+    out[6] = offsetof(nested_sampler_params, adaptive_r);
+    out[7] = offsetof(sample_output, inner_stats);
+    out[8] = offsetof(portfolio::data, subsample);
+    out[9] = offsetof(portfolio::data, use_milstein);
+    out[10] = offsetof(portfolio::option_params, W_est);
+    out[11] = offsetof(model::data, phi_type);
 }
 
 }  // extern "C"

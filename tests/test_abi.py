@@ -1,0 +1,68 @@
+"""The C ABI: libnmlmc.so loads without a GPU, exports every function include/nmlmc.h declares,
+and its structs have the reference's layout (sizes/offsets recorded from the reference build)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "nmlmc.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = set()
+    for m in re.finditer(r"^[A-Za-z_][\w \*]*?\b([A-Za-z_]\w*)\s*\(([^;{]*?)\)\s*;", src, flags=re.M):
+        if m.group(0).lstrip().startswith("typedef"):
+            continue
+        names.add(m.group(1))
+    return names
+
+
+def test_header_declares_all_exports(nm):
+    declared = header_functions()
+    assert declared == set(nm.EXPORTS), (declared ^ set(nm.EXPORTS))
+
+
+def test_library_exports_every_declared_symbol(nm):
+    lib = nm.lib()
+    for name in header_functions():
+        assert hasattr(lib, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", nm.LIB_PATH], capture_output=True, text=True).stdout
+    exported = {l.split()[-1] for l in out.splitlines() if " T " in l}
+    assert header_functions() <= exported
+
+
+def test_struct_layouts_match_reference(nm, golden):
+    meta, _ = golden
+    s = meta["abi_sizes"]
+    assert ctypes.sizeof(nm.NestedSamplerParams) == s[0]
+    assert ctypes.sizeof(nm.SampleOutput) == s[1]
+    assert ctypes.sizeof(nm.ModelData) == s[2]
+    assert ctypes.sizeof(nm.PortfolioData) == s[3]
+    assert ctypes.sizeof(nm.OptionParams) == s[4]
+    assert ctypes.sizeof(nm.StockParams) == s[5]
+    assert nm.NestedSamplerParams.adaptive_r.offset == s[6]
+    assert nm.SampleOutput.inner_stats.offset == s[7]
+    assert nm.PortfolioData.subsample.offset == s[8]
+    assert nm.PortfolioData.use_milstein.offset == s[9]
+    assert nm.OptionParams.W_est.offset == s[10]
+    assert nm.ModelData.phi_type.offset == s[11]
+
+
+def test_error_strings_and_version(nm):
+    lib = nm.lib()
+    assert lib.nmlmc_version() >= 1
+    for st in range(6):
+        assert nm.error_string(st)
+
+
+def test_no_device_is_an_error_not_a_fallback(nm):
+    """Without a GPU the native API refuses (no CPU path exists)."""
+    from conftest import HAVE_GPU
+    if HAVE_GPU:
+        pytest.skip("host has a GPU")
+    with pytest.raises(nm.NmlmcError):
+        nm.Sampler()

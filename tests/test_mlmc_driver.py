@@ -1,0 +1,88 @@
+"""The host continuation-MLMC driver (nmlmc_mlmc_run_cb) against the reference's mlmc_t::run on
+the same deterministic synthetic level sampler (golden fixtures): identical sequence of
+sample_level(ell, M) calls, level sums, error split and the to_string() table text."""
+import math
+
+import numpy as np
+import pytest
+
+
+class Synthetic:
+    """The synthetic level sampler of oracle/ref_harness.cpp (ref_mlmc_synthetic), restated."""
+
+    def __init__(self, a, alpha, v, beta, w, gamma, seed):
+        self.a, self.alpha, self.v, self.beta, self.w, self.gamma = a, alpha, v, beta, w, gamma
+        self.state = seed
+        self.calls = []
+
+    def _next(self):
+        M64 = (1 << 64) - 1
+        self.state = (self.state + 0x9E3779B97F4A7C15) & M64
+        z = self.state
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M64
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M64
+        z ^= z >> 31
+        return float(z >> 11) * (1.0 / 9007199254740992.0)
+
+    def __call__(self, ell, M):
+        self.calls.append((ell, M))
+        mf = self.a * math.pow(2.0, -self.alpha * ell) + 0.1
+        md = 0.0 if ell == 0 else self.a * math.pow(2.0, -self.alpha * ell)
+        sd_f = math.sqrt(self.v)
+        sd_d = math.sqrt(self.v * math.pow(2.0, -self.beta * ell))
+        n = M if M < 64 else 64
+        f_s = [0.0] * 4
+        d_s = [0.0] * 4
+        for _ in range(n):
+            u = (self._next() - 0.5) * math.sqrt(12.0)
+            f = mf + sd_f * u
+            d = md + sd_d * u
+            pf = pd = 1.0
+            for j in range(4):
+                pf *= f
+                pd *= d
+                f_s[j] += pf * (float(M) / n)
+                d_s[j] += (0.0 if ell == 0 else pd * (float(M) / n))
+        return dict(fsums=f_s, diffsums=d_s, work=self.w * math.pow(2.0, self.gamma * ell) * M)
+
+
+@pytest.mark.parametrize("idx", [0, 1, 2])
+def test_driver_matches_reference(nm, golden, idx):
+    meta, _ = golden
+    g = meta["mlmc"][idx]
+    tol, M0, a, alpha, v, beta, w, gamma, seed = g["args"]
+    syn = Synthetic(a, alpha, v, beta, w, gamma, int(seed))
+    out = nm.mlmc_run_cb(syn, targetTOL=tol, M0=int(M0), verbose=False)
+    assert [c[0] for c in syn.calls] == g["calls_ell"]
+    assert [c[1] for c in syn.calls] == g["calls_M"]
+    lv = np.array(g["levels"])
+    assert out["nlevels"] == len(lv)
+    np.testing.assert_array_equal(out["level_fsums"], lv[:, 0:4])
+    np.testing.assert_array_equal(out["level_diffsums"], lv[:, 4:8])
+    np.testing.assert_array_equal(out["level_work"], lv[:, 8])
+    np.testing.assert_array_equal(out["level_M"].astype(float), lv[:, 9])
+    assert out["starting_level"] == g["misc"][0]
+    assert out["bias_est"] == g["misc"][1]
+    assert out["stat_error"] == g["misc"][2]
+    assert out["TOL"] == g["misc"][3]
+    assert out["table"] == g["table"]
+
+
+def test_batched_driver_same_decisions(nm, golden):
+    """Batched submissions (all levels of a round at once) take the same decisions when the
+    sampler's results do not depend on call order."""
+    meta, _ = golden
+    tol, M0, a, alpha, v, beta, w, gamma, seed = meta["mlmc"][1]["args"]
+
+    def det(ell, M):   # order-independent sampler: a pure function of (ell, M)
+        mf = a * 2.0 ** (-alpha * ell) + 0.1
+        md = 0.0 if ell == 0 else a * 2.0 ** (-alpha * ell)
+        vf, vd = v, v * 2.0 ** (-beta * ell)
+        f = [M * mf, M * (vf + mf * mf), M * mf ** 3, M * mf ** 4]
+        d = [0.0] * 4 if ell == 0 else [M * md, M * (vd + md * md), M * md ** 3, M * md ** 4]
+        return dict(fsums=f, diffsums=d, work=w * 2.0 ** (gamma * ell) * M)
+
+    r1 = nm.mlmc_run_cb(det, targetTOL=tol, M0=int(M0), batched=False)
+    r2 = nm.mlmc_run_cb(det, targetTOL=tol, M0=int(M0), batched=True)
+    np.testing.assert_array_equal(r1["level_M"], r2["level_M"])
+    assert r1["Eg"] == r2["Eg"]

@@ -1,0 +1,134 @@
+"""The CPU oracle (oracle/nmlmc_oracle.c) against the golden fixtures produced by the unmodified
+reference (tests/golden/make_golden.py): bit-exact Threefry, random_state draws, Box-Muller,
+norm_cdf_inv, option start values, and per-call event logs, level sums and inner_stats of the
+nested sampler engine."""
+import numpy as np
+import pytest
+
+import oracle as O
+
+
+def test_threefry_golden(golden):
+    _, A = golden
+    out = O.threefry(A["threefry/ctr"], A["threefry/key"])
+    np.testing.assert_array_equal(out, A["threefry/out"])
+    # the value recorded when the reference was first run here
+    assert int(out[0, 0]) == 0xC2B6E3A8C2C69865 and int(out[0, 1]) == 0x6F81ED42F350084D
+
+
+@pytest.mark.parametrize("variant,prec", [("f32", O.PREC_REF32), ("f64", O.PREC_FP64)])
+def test_stream_draws_golden(golden, variant, prec):
+    meta, A = golden
+    ops = meta["stream_ops"]
+    for (s, c) in [(0, 0), (7, 3), (2**63 + 5, 2**32 + 1)]:
+        real, u64 = O.stream_draws(prec, s, c, ops)
+        np.testing.assert_array_equal(u64, A[f"stream/{variant}/{s}/{c}/u64"])
+        np.testing.assert_array_equal(real, A[f"stream/{variant}/{s}/{c}/real"])
+
+
+def test_boxmuller_golden(golden):
+    _, A = golden
+    x, y = O.boxmuller(A["bm/u0"], A["bm/u1"])
+    np.testing.assert_array_equal(x, A["bm/x"])
+    np.testing.assert_array_equal(y, A["bm/y"])
+
+
+def test_norm_cdf_inv_golden(golden):
+    _, A = golden
+    got32 = np.array([O.norm_cdf_inv(p, O.PREC_REF32) for p in A["ncdfinv/p"]])
+    got64 = np.array([O.norm_cdf_inv(p, O.PREC_FP64) for p in A["ncdfinv/p"]])
+    np.testing.assert_array_equal(got32, A["ncdfinv/f32"])
+    np.testing.assert_array_equal(got64, A["ncdfinv/f64"])
+
+
+def _events(A, key):
+    return (bytes(A[key + "/kinds"]).decode(), A[key + "/values"], A[key + "/aux"])
+
+
+def make_oracle_case(case, prec, streams=O.STREAMS_CORE, cores=None):
+    s = O.Sampler(prec, streams, cores or case["cores"], case["N0"], case["beta"], case["r"],
+                  case["anti"], False, case["seed"])
+    start = delta = None
+    if case["kind"] == "model":
+        s.set_model(case["model"], case["tau"], case["max_loss"])
+    else:
+        pf = O.synthetic_portfolio(**case["pf"])
+        start, delta = s.set_portfolio(pf, r=0.05, rho=case["rho"], max_loss=case["max_loss"],
+                                       tau=1 / 52, subsample=case["sub"], use_delta_cv=case["cv"])
+    return s, start, delta
+
+
+def engine_case_ids(meta):
+    return [c["name"] for c in meta["engine"]]
+
+
+@pytest.mark.parametrize("prec_name,prec", [("f32", O.PREC_REF32), ("f64", O.PREC_FP64)])
+def test_engine_golden(golden, prec_name, prec):
+    meta, A = golden
+    for case in meta["engine"]:
+        res = case["results"][prec_name]
+        s, start, delta = make_oracle_case(case, prec)
+        if start is not None:
+            np.testing.assert_array_equal(start, A[f"{case['name']}/{res['variant']}/start"])
+            np.testing.assert_array_equal(delta, A[f"{case['name']}/{res['variant']}/delta_est"])
+        for i, call in enumerate(res["calls"]):
+            got = s.sample(call["ell"], call["M"], events_cap=2_000_000)
+            key = f"{case['name']}/{res['variant']}/{i}"
+            k_ref, v_ref, a_ref = _events(A, key)
+            k, v, a = got["events"]
+            assert k == k_ref, (case["name"], i)
+            np.testing.assert_array_equal(v, v_ref, err_msg=f"{case['name']} call {i}")
+            np.testing.assert_array_equal(a, a_ref)
+            np.testing.assert_array_equal(got["fsums"], call["fsums"])
+            np.testing.assert_array_equal(got["diffsums"], call["diffsums"])
+            assert got["work"] == call["work"]
+            np.testing.assert_array_equal(got["stats"].astype(np.int64), call["stats"])
+
+
+def test_trace_consistent_with_events(golden):
+    """Per-outer-sample records agree with the event log of the same run."""
+    meta, _ = golden
+    case = meta["engine"][0]
+    s, _, _ = make_oracle_case(case, O.PREC_REF32)
+    got = s.sample(2, 30, trace=True, events_cap=200000)
+    kinds, vals, aux = got["events"]
+    tr = got["trace"]
+    # one 'O' per outer sample; the last 'P' of each outer sample is the big-count mean
+    outer_starts = [i for i, k in enumerate(kinds) if k == "O"] + [len(kinds)]
+    for m in range(30):
+        seg = range(outer_starts[m], outer_starts[m + 1])
+        last_p = [i for i in seg if kinds[i] == "P"][-1]
+        assert vals[last_p] == tr["mean_big"][m]
+    assert tr["phi_f"].sum() == got["fsums"][0]
+    assert (tr["phi_f"] - tr["phi_c"]).sum() == got["diffsums"][0]
+
+
+def test_outer_layout_order_independent():
+    """OUTER layout: splitting a call into pieces gives the same per-outer-sample results."""
+    a = O.Sampler(O.PREC_FP64, O.STREAMS_OUTER, 1, 32, 2, 1.5, True, False, 9)
+    a.set_model(O.MODEL_SHIFT, 0.0, 1.0)
+    b = O.Sampler(O.PREC_FP64, O.STREAMS_OUTER, 1, 32, 2, 1.5, True, False, 9)
+    b.set_model(O.MODEL_SHIFT, 0.0, 1.0)
+    whole = a.sample(4, 40, trace=True)["trace"]
+    p1 = b.sample(4, 15, trace=True)["trace"]
+    p2 = b.sample(4, 25, trace=True)["trace"]
+    np.testing.assert_array_equal(whole, np.concatenate([p1, p2]))
+
+
+@pytest.mark.skipif(not O.ref_available("f32_lzcnt"), reason="oracle/_ref not built on this host")
+def test_live_reference_random_case():
+    """Where the reference is compiled here: a fresh random configuration, oracle vs reference."""
+    rng = np.random.default_rng(77)
+    cores = int(rng.integers(1, 6))
+    ref = O.Reference("f32_lzcnt")
+    ref.init(cores, 32, 2, 1.5, True)
+    ref.model_init(1, 0.0, 0.7, 123, traced=True)
+    s = O.Sampler(O.PREC_REF32, O.STREAMS_CORE, cores, 32, 2, 1.5, True, False, 123)
+    s.set_model(O.MODEL_SHIFT, 0.0, 0.7)
+    for ell in (0, 3, 5, 2):
+        a = ref.sample(ell, 33, events_cap=500000)
+        b = s.sample(ell, 33, events_cap=500000)
+        assert a["events"][0] == b["events"][0]
+        np.testing.assert_array_equal(a["events"][1], b["events"][1])
+        np.testing.assert_array_equal(a["fsums"], b["fsums"])
+        np.testing.assert_array_equal(a["diffsums"], b["diffsums"])
