@@ -1,0 +1,370 @@
+"""Benchmark: time-to-eps of the nested-MLMC estimate of P(E[X|Y] > K) on B200.
+
+Workload (the adaptive model-problem configuration): Y ~ N(0,1), inner X = Y + Z, K = 1 (exact
+1 - Phi(1)); N0 = 32 inner samples at level 0, beta = 2, adaptive inner sampling with the r = 2
+rule (double while |mean - K| < 3 sigma / sqrt(N)), antithetic coarse estimator, 4 moments,
+continuation MLMC to RMSE eps = 1e-4.  A step is one complete MLMC run (host driver + level
+sampler) to eps; synthetic inputs (the model problem has no data).
+
+Our arm: the batched FP32 sampler (OUTER streams, Kahan FP32 inner sums, FP64 moments), all levels
+of an MLMC round in one submission.  Reported next to it, on the same GPU and seed:
+  * the all-FP64 run of the same sampler on the same streams (accuracy and speed),
+  * the plain FP64 drop-in: the reference's stream semantics (a warp per virtual core, 2048
+    cores like the reference's CUDA main), one synchronous launch per sample_level call.
+
+`value` is the device time of the run's kernels (CUDA events around every level call); `e2e` is
+the wall time of the whole run through the C ABI (host driver decisions, launches, the
+device->host copy of every level result).  Multi-GPU (torchrun): every rank samples its share of
+each level call and the level results are all-reduced (16 doubles), so the estimate equals the
+single-GPU one and total work is fixed (strong scaling).
+
+--impl reference times the reference's own CPU implementation (oracle/_ref: the reference
+sources compiled here, OpenMP on all host threads; the C restatement if absent) on bounded
+per-level samples and multiplies its per-outer-sample cost by the level sample counts the
+MLMC run needs at eps (bench_schedule.json).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "nested-risk-mlmc_b200")
+SCHEDULE = os.path.join(ROOT, "bench_schedule.json")
+
+EPS = 1e-4
+METRIC = "time-to-ε (s) for MLMC P(loss>K) at ε=1e-4, batched FP32 vs plain FP64, 1 B200"
+WORKLOAD = dict(workload="model problem X=Y+Z, K=1, adaptive r=2 (3-sigma doubling), levels to eps",
+                N0=32, beta=2, adaptive_r=2.0, antithetic=True, moments=4, eps=EPS, M0=1024,
+                l2_flush="not needed: no input data; every inner draw is computed from a counter")
+# Algorithmic lane operations per inner sample of the X = Y + Z model on the FP32 path:
+#   Threefry2x64-20 block = 140 INT32 ops (20 rounds x (64-bit add 2 + rotate 2 + xor 2) less
+#   two 32-bit rotations, 6 key injections x 4) shared by 4 normals -> 35;
+#   Box-Muller pair ~ 22 FP32/ALU + 4 SFU ops shared by 2 normals -> 13;
+#   X = Y + Z (1) and a Kahan update of the inner sum (4) -> 5.
+OPS_PER_INNER = 35 + 13 + 5
+
+
+def exact_p():
+    return 0.5 * math.erfc(1 / math.sqrt(2))
+
+
+# ---------------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms in the background."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=["nvidia-smi unavailable"])
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return dict(sm_mhz=statistics.median(sm) if sm else None, sm_max_mhz=smax,
+                    reasons=sorted(reasons), samples=len(sm))
+
+
+# ---------------------------------------------------------------------------------------------
+def ddp_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def make_sampler(nm, device, precision, streams, seed, cores=2048):
+    s = nm.Sampler(device, cores=cores, N0=32, beta=2, adaptive_r=2.0, adaptive_incl_r2=True,
+                   precision=precision, streams=streams, seed=seed)
+    s.set_model(nm.MODEL_SHIFT, 0.0, 1.0)
+    return s
+
+
+def run_once(nm, s, batched, dist=None):
+    """One MLMC run to EPS. Returns (result dict, wall seconds)."""
+    if dist is None:
+        t0 = time.perf_counter()
+        out = s.mlmc_run(targetTOL=EPS, M0=WORKLOAD["M0"], batched=batched)
+        return out, time.perf_counter() - t0
+    import torch
+    torch_dist, dev = dist
+
+    def reduce(results):
+        t = torch.tensor([[*r["fsums"], *r["diffsums"], r["work"]] for r in results],
+                         dtype=torch.float64, device=dev)
+        torch_dist.all_reduce(t)
+        t = t.cpu().numpy()
+        out = []
+        for row, r in zip(t, results):   # sums over ranks; device time stays this rank's
+            out.append(dict(fsums=row[0:4], diffsums=row[4:8], work=row[8], seconds=r["seconds"]))
+        return out
+
+    def one(ell, M):
+        return reduce([s.sample(ell, M)])[0]
+
+    t0 = time.perf_counter()
+    out = nm.mlmc_run_cb(one, targetTOL=EPS, M0=WORKLOAD["M0"], batched=False)
+    return out, time.perf_counter() - t0
+
+
+# ---------------------------------------------------------------------------------------------
+def cpu_reference_time(schedule: dict, budget_s: float = 20.0, threads: int | None = None):
+    """The reference's CPU level sampler on bounded per-level samples; returns the time-to-eps
+    it implies for `schedule` (outer samples per level at eps) and a description."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle as O
+    threads = threads or os.cpu_count() or 1
+    r2minus = float(np.nextafter(np.float32(2), np.float32(0)))
+    levels = [int(l) for l in schedule["levels"]]
+    Ms = [int(m) for m in schedule["M"]]
+    per_level = budget_s / max(1, len(levels))
+    if O.ref_available("f32_lzcnt"):
+        kind = "reference"
+        ref = O.Reference("f32_lzcnt")
+        ref.init(threads, 32, 2, r2minus, True)
+        ref.model_init(1, 0.0, 1.0, 0, traced=False)
+        sample = ref.sample
+        cores = threads
+    else:
+        kind = "port"
+        s = O.Sampler(O.PREC_REF32, O.STREAMS_CORE, 1, 32, 2, 2.0, True, True, 0)
+        s.set_model(O.MODEL_SHIFT, 0.0, 1.0)
+        sample = s.sample
+        cores = 1
+    total = 0.0
+    details = []
+    for ell, M in zip(levels, Ms):
+        m = 64 * cores
+        while True:
+            t0 = time.perf_counter()
+            sample(ell, m)
+            dt = time.perf_counter() - t0
+            if dt >= per_level / 4 or m >= M:
+                break
+            m = min(M, m * max(2, int(per_level / 4 / max(dt, 1e-4))))
+        per_outer = dt / m
+        total += per_outer * M
+        details.append(f"l{ell}:{m}")
+    desc = (f"reference level sampler ({'oracle/_ref, real_t=float, r=2-ulp' if kind == 'reference' else 'C port'}"
+            f", {cores} threads) timed on bounded samples per level [{', '.join(details)} outer samples], "
+            f"cost per outer sample x the level counts of the eps={EPS:g} run; extrapolated")
+    return total, kind, cores, desc
+
+
+def reference_arm(args):
+    world, rank, _ = ddp_env()
+    if rank != 0:
+        return
+    if not os.path.exists(SCHEDULE):
+        print(json.dumps({"impl": "reference", "unavailable": "bench_schedule.json missing"}))
+        return
+    with open(SCHEDULE) as f:
+        schedule = json.load(f)
+    times = []
+    kind = cores = desc = None
+    t_all0 = time.perf_counter()
+    per_step = max(5.0, args.ref_budget * 3 / max(1, args.steps))
+    for _ in range(args.steps):
+        v, kind, cores, desc = cpu_reference_time(schedule, budget_s=per_step)
+        times.append(v)
+    value = statistics.median(times)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3,
+            "higher_is_better": False, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": WORKLOAD,
+            "cpu_baseline": {"value": value, "unit": "s", "cores": cores, "kind": kind, "sample": desc},
+            "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "measure_wall_s": time.perf_counter() - t_all0}
+    print(json.dumps(line))
+
+
+def small_case():
+    """Fixed level calls of the FP32 sampler (the profiling case): level 0 with 2^24 outer samples
+    (fine only, 32 inner samples each) and level 8 with 2^16 (adaptive pilots and the antithetic
+    final phase).  Device memory: the 2^20-sample batch buffers (~40 MB)."""
+    sys.path.insert(0, PKG)
+    import nmlmc as nm
+    s = make_sampler(nm, 0, nm.PREC_FP32, nm.STREAMS_OUTER, seed=0)
+    for ell, M in ((0, 1 << 24), (8, 1 << 16), (0, 1 << 24), (8, 1 << 16)):
+        r = s.sample(ell, M)
+        print(f"level {ell} M {M}: {r['seconds'] * 1e3:.3f} ms, {r['stats'][0] / r['seconds']:.3e} inner/s")
+
+
+# ---------------------------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ref-budget", type=float, default=20.0, help="CPU seconds of reference sampling")
+    ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison runs")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--case", default=None, choices=["small"],
+                    help="small: a few fixed level calls of the FP32 sampler (profiling case)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+    if args.case == "small":
+        return small_case()
+
+    sys.path.insert(0, PKG)
+    import nmlmc as nm
+    world, rank, local = ddp_env()
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as td
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        td.init_process_group("nccl", timeout=timedelta(seconds=120))
+        dist = (td, torch.device("cuda", local))
+
+    s = make_sampler(nm, local, nm.PREC_FP32, nm.STREAMS_OUTER, seed=0)
+    if world > 1:
+        s.set_shard(rank, world)
+
+    def barrier():
+        if dist:
+            dist[0].barrier()
+
+    for w in range(args.warmup):
+        s.configure(seed=1000 + w)
+        run_once(nm, s, batched=True, dist=dist)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    s.set_profiling(True)
+    launches0 = nm.kernel_launches()
+    barrier()
+    dev_times, walls, outs = [], [], []
+    t_region = time.perf_counter()
+    for k in range(args.steps):
+        s.configure(seed=k)
+        out, wall = run_once(nm, s, batched=True, dist=dist)
+        outs.append(out)
+        walls.append(wall)
+        dev_times.append(float(out["level_time"].sum()))
+    barrier()
+    region = time.perf_counter() - t_region
+    launches = nm.kernel_launches() - launches0
+    n_phase, t_phase = s.phase_kernel_time()
+    s.set_profiling(False)
+    clk = clocks.stop()
+
+    dev_t = sum(dev_times) / len(dev_times)
+    wall_t = sum(walls) / len(walls)
+    if dist:
+        import torch
+        t = torch.tensor([dev_t, wall_t], dtype=torch.float64, device=dist[1])
+        dist[0].all_reduce(t, op=dist[0].ReduceOp.MAX)
+        dev_t, wall_t = float(t[0]), float(t[1])
+
+    inner = sum(float(o["total_work"]) for o in outs)  # work = inner samples for this model
+    calls = sum(int(o["calls"]) for o in outs)
+    if rank != 0:
+        if dist:
+            dist[0].destroy_process_group()
+        return
+
+    ref = outs[0]
+    schedule = dict(eps=EPS, levels=list(range(int(ref["nlevels"]))),
+                    M=[int(x) for x in ref["level_M"]],
+                    note="outer samples per level of the eps run (seed 0) of the batched sampler")
+    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
+    with open(os.path.join(ROOT, "gpurun_out", "bench_schedule.json"), "w") as f:
+        json.dump(schedule, f)
+
+    # roofline of the phase kernel (the dominant kernel): lane-ops per inner sample x inner
+    # samples / its CUDA-event time; peak = issue slots at the sampled SM clock
+    sm_mhz = clk.get("sm_mhz") or 1965.0
+    achieved = inner * OPS_PER_INNER / t_phase / 1e9 if t_phase > 0 else None
+    peak = 148 * 128 * sm_mhz * 1e6 / 1e9
+    roof = {"bound": "alu", "achieved": achieved, "peak": peak, "unit": "Gop/s",
+            "frac": (achieved / peak) if achieved else None, "traffic": None,
+            "kernel": "k_phase (FP32, X=Y+Z)", "launches": n_phase,
+            "kernel_seconds": t_phase, "ops_per_inner_sample": OPS_PER_INNER,
+            "peak_source": "issue-slot peak 148 SM x 4 SMSP x 32 lanes x sampled SM clock "
+                           "(not in the measured-peaks file, which holds HBM and bf16 GEMM)"}
+
+    line = {"metric": METRIC, "value": dev_t, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_t * 1e3, "higher_is_better": False,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(WORKLOAD, parallelism=f"outer-sample shards x{world}"),
+            "e2e": {"value": wall_t, "unit": "s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": int(calls / len(outs) * 16 * 8)},
+            "roofline": roof, "clocks": clk, "gpu_launches": int(launches),
+            "inner_samples_per_step": inner / len(outs),
+            "inner_samples_per_s": inner / sum(dev_times),
+            "Eg": float(ref["Eg"]), "abs_err_vs_exact": abs(float(ref["Eg"]) - exact_p()),
+            "timed_region_s": region}
+
+    if world == 1 and not args.no_compare:
+        s64 = make_sampler(nm, local, nm.PREC_FP64, nm.STREAMS_OUTER, seed=0)
+        run_once(nm, s64, batched=True)
+        s64.configure(seed=0)
+        o64, w64 = run_once(nm, s64, batched=True)
+        line["fp64_same_streams"] = {
+            "value": float(o64["level_time"].sum()), "e2e": w64, "Eg": float(o64["Eg"]),
+            "Eg_diff_vs_fp32": float(o64["Eg"]) - float(ref["Eg"]),
+            "level_M_equal": bool((o64["level_M"] == ref["level_M"]).all()) if len(o64["level_M"]) == len(ref["level_M"]) else False}
+        sdrop = make_sampler(nm, local, nm.PREC_FP64, nm.STREAMS_CORE, seed=0, cores=2048)
+        od, wd = run_once(nm, sdrop, batched=False)
+        line["fp64_dropin"] = {"value": float(od["level_time"].sum()), "e2e": wd, "Eg": float(od["Eg"]),
+                               "streams": "reference (CORE) layout, 2048 virtual cores, per-call launches"}
+        line["speedup_vs_fp64_dropin"] = {"value": line["fp64_dropin"]["value"] / dev_t,
+                                          "e2e": wd / wall_t}
+        line["speedup_vs_fp64_same_streams"] = {"value": line["fp64_same_streams"]["value"] / dev_t,
+                                                "e2e": w64 / wall_t}
+    if world == 1 and not args.no_cpu:
+        v, kind, cores, desc = cpu_reference_time(schedule, budget_s=args.ref_budget)
+        line["cpu_baseline"] = {"value": v, "unit": "s", "cores": cores, "kind": kind, "sample": desc}
+    print(json.dumps(line))
+    if dist:
+        dist[0].destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

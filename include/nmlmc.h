@@ -205,6 +205,18 @@ int nmlmc_set_trace(nmlmc_ctx* ctx, nmlmc_trace_rec* host_buf, uint64_t cap);
 int nmlmc_portfolio_full_loss(nmlmc_ctx* ctx, uint32_t ell, uint64_t first, uint64_t n,
                               double* host_loss);
 
+/* Sharding over ranks (OUTER layout): each nmlmc_sample(ell, M) call then evaluates only this
+ * rank's static share [rank*M/world ...] of the call's M outer samples, with the stream indices
+ * a single device would give them; the caller sums the ranks' level results (an all-reduce of
+ * 16 doubles) and gets the single-device result.  world = 1 restores the default. */
+int nmlmc_set_shard(nmlmc_ctx* ctx, uint32_t rank, uint32_t world);
+/* CUDA-event timing of the phase kernel (the dominant kernel): 1 enables; the totals since
+ * enabling are read with nmlmc_phase_kernel_time. */
+int nmlmc_set_profiling(nmlmc_ctx* ctx, int32_t on);
+int nmlmc_phase_kernel_time(nmlmc_ctx* ctx, uint64_t* launches, double* seconds);
+/* Number of kernels this library has launched since it was loaded. */
+uint64_t nmlmc_kernel_launches(void);
+
 /* Threefry2x64-20 blocks computed on the GPU: out[2i..2i+1] = F(ctr[2i..2i+1], key[2i..2i+1])
  * (host buffers).  Bit-identical to Random123's r123::Threefry2x64. */
 int nmlmc_threefry_blocks(const uint64_t* ctr, const uint64_t* key, uint64_t* out, uint64_t n);

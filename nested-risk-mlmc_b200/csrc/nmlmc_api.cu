@@ -142,6 +142,14 @@ struct nmlmc_ctx {
     uint64_t trace_cap = 0;
     TraceRec* d_trace = nullptr;
     uint64_t d_trace_cap = 0;
+    // sharding over ranks (OUTER layout)
+    uint32_t shard_rank = 0, shard_world = 1;
+    // phase-kernel timing
+    bool prof = false;
+    std::vector<cudaEvent_t> pev;
+    size_t pn = 0;
+    uint64_t prof_launches = 0;
+    double prof_seconds = 0;
 };
 
 namespace {
@@ -393,12 +401,37 @@ int sample_core(nmlmc_ctx* c, uint32_t ell, uint64_t M, nmlmc_level_result* out)
     return NMLMC_OK;
 }
 
+void prof_mark(void* user, int end, cudaStream_t stream) {
+    nmlmc_ctx* c = static_cast<nmlmc_ctx*>(user);
+    const size_t idx = 2 * c->pn + (end ? 1 : 0);
+    while (c->pev.size() <= idx) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return;
+        c->pev.push_back(e);
+    }
+    cudaEventRecord(c->pev[idx], stream);
+    if (end) c->pn++;
+}
+
+void prof_collect(nmlmc_ctx* c) {
+    for (size_t i = 0; i < c->pn; i++) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, c->pev[2 * i], c->pev[2 * i + 1]) == cudaSuccess) c->prof_seconds += ms * 1e-3;
+    }
+    c->prof_launches += c->pn;
+    c->pn = 0;
+}
+
 template <class RT>
-int sample_outer(nmlmc_ctx* c, uint32_t ell, uint64_t M, nmlmc_level_result* out) {
+int sample_outer(nmlmc_ctx* c, uint32_t ell, uint64_t Mtotal, nmlmc_level_result* out) {
+    // this rank's static share of the call's outer samples (all of them when world = 1)
+    const uint64_t q = Mtotal / c->shard_world, rem = Mtotal % c->shard_world;
+    const uint64_t lo = q * c->shard_rank + (c->shard_rank < rem ? c->shard_rank : rem);
+    const uint64_t M = q + (c->shard_rank < rem ? 1 : 0);
     OuterLevel<RT> L{};
     L.ell = ell;
     L.M = M;
-    L.first_index = c->next_outer[ell];
+    L.first_index = c->next_outer[ell] + lo;
     L.seed = c->cfg.seed;
     L.fine_only = ell == 0;
     L.antithetic = c->cfg.antithetic != 0;
@@ -415,13 +448,16 @@ int sample_outer(nmlmc_ctx* c, uint32_t ell, uint64_t M, nmlmc_level_result* out
         if constexpr (sizeof(RT) == 4) L.ot = c->dpf32.table; else L.ot = c->dpf64.table;
     }
     TraceRec* tr = c->trace_host ? c->d_trace : nullptr;
+    c->ob.prof_mark = c->prof ? prof_mark : nullptr;
+    c->ob.prof_user = c;
     NM_CUDA(cudaEventRecord(c->ev0, c->stream), "event");
     NM_CUDA(outer_level_begin(c->ob, c->stream), "level begin");
-    NM_CUDA(outer_sample_level<RT>(L, c->kind, c->cfg.precision, c->ob, tr, c->stream), "outer level kernels");
+    if (M) NM_CUDA(outer_sample_level<RT>(L, c->kind, c->cfg.precision, c->ob, tr, c->stream), "outer level kernels");
     NM_CUDA(cudaEventRecord(c->ev1, c->stream), "event");
     NM_CUDA(cudaMemcpyAsync(c->h_pin, c->ob.level_acc, 16 * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "d2h");
-    if (tr) NM_CUDA(cudaMemcpyAsync(c->trace_host, tr, M * sizeof(TraceRec), cudaMemcpyDeviceToHost, c->stream), "d2h");
+    if (tr && M) NM_CUDA(cudaMemcpyAsync(c->trace_host, tr, M * sizeof(TraceRec), cudaMemcpyDeviceToHost, c->stream), "d2h");
     NM_CUDA(cudaStreamSynchronize(c->stream), "sync");
+    if (c->prof) prof_collect(c);
     float ms = 0;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
     const double* a = c->h_pin;
@@ -441,7 +477,7 @@ int sample_outer(nmlmc_ctx* c, uint32_t ell, uint64_t M, nmlmc_level_result* out
         out->inner_stats[5] = M + inner * (c->kind == KIND_REF_MODEL ? 2 : 1);
     }
     out->seconds = ms * 1e-3;
-    c->next_outer[ell] += M;
+    c->next_outer[ell] += Mtotal;
     c->trace_host = nullptr;
     return NMLMC_OK;
 }
@@ -504,6 +540,7 @@ int nmlmc_destroy(nmlmc_ctx* c) {
         cudaFree(B.lists); cudaFree(B.class_items); cudaFree(B.counters); cudaFree(B.block_sums);
         cudaFree(B.level_acc);
     }
+    for (cudaEvent_t e : c->pev) cudaEventDestroy(e);
     if (c->h_pin) cudaFreeHost(c->h_pin);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -643,6 +680,32 @@ int nmlmc_sample_levels(nmlmc_ctx* c, uint32_t n, const uint32_t* ells, const ui
     }
     return NMLMC_OK;
 }
+
+int nmlmc_set_shard(nmlmc_ctx* c, uint32_t rank, uint32_t world) {
+    if (!c || world == 0 || rank >= world) return set_err(NMLMC_ERR_ARG);
+    if (world > 1 && c->cfg.streams != NMLMC_STREAMS_OUTER) return set_err(NMLMC_ERR_ARG);
+    c->shard_rank = rank;
+    c->shard_world = world;
+    return NMLMC_OK;
+}
+
+int nmlmc_set_profiling(nmlmc_ctx* c, int32_t on) {
+    if (!c) return set_err(NMLMC_ERR_ARG);
+    c->prof = on != 0;
+    c->prof_launches = 0;
+    c->prof_seconds = 0;
+    c->pn = 0;
+    return NMLMC_OK;
+}
+
+int nmlmc_phase_kernel_time(nmlmc_ctx* c, uint64_t* launches, double* seconds) {
+    if (!c || !launches || !seconds) return set_err(NMLMC_ERR_ARG);
+    *launches = c->prof_launches;
+    *seconds = c->prof_seconds;
+    return NMLMC_OK;
+}
+
+uint64_t nmlmc_kernel_launches(void) { return launches_total(); }
 
 int nmlmc_portfolio_full_loss(nmlmc_ctx* c, uint32_t ell, uint64_t first, uint64_t n, double* host_loss) {
     if (!c || !host_loss) return set_err(NMLMC_ERR_ARG);

@@ -463,6 +463,7 @@ static cudaError_t launch_core_t(const CoreLaunch<RT>& L, int kind, CoreStream* 
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     core_reduce_kernel<<<1, 256, 0, stream>>>(L.cores, part_sums, part_stats, out_sums, out_stats);
+    count_launch(2);
     return cudaGetLastError();
 }
 

@@ -67,7 +67,14 @@ struct OuterBuffers {
     double* block_sums;      // per-CTA partial moments [grid][16]
     double* level_acc;       // accumulated level result [16]
     int grid;
+    // optional CUDA-event timing of the phase kernel: called around each k_phase launch
+    void (*prof_mark)(void* user, int end, cudaStream_t stream);
+    void* prof_user;
 };
+
+// Kernel launches issued by the library (incremented at every launch site).
+void count_launch(uint64_t n = 1);
+uint64_t launches_total();
 
 template <class RT>
 cudaError_t outer_sample_level(const OuterLevel<RT>& L, int kind, int prec, OuterBuffers& B,

@@ -21,6 +21,7 @@
 // Every thread does the same unit of work (one chunk), so the device stays full whatever the
 // spread of inner counts.  An item with more chunks than a CTA has threads is walked tile by
 // tile by one CTA.
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -591,6 +592,18 @@ __global__ void k_reduce_blocks(const double* block_sums, int grid, double* leve
 }
 
 // ---- host orchestration ----------------------------------------------------------------------
+static std::atomic<uint64_t> g_launches{0};
+void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+uint64_t launches_total() { return g_launches.load(std::memory_order_relaxed); }
+
+template <class RT, int KIND, int PREC>
+static void launch_phase(const DevLevel<RT>& D, const SegSet& S, TraceRec* trace, cudaStream_t stream) {
+    if (D.B.prof_mark) D.B.prof_mark(D.B.prof_user, 0, stream);
+    k_phase<RT, KIND, PREC><<<D.B.grid, kTile, 0, stream>>>(D, S, trace);
+    if (D.B.prof_mark) D.B.prof_mark(D.B.prof_user, 1, stream);
+    count_launch();
+}
+
 static inline uint32_t ilog2_u64(uint64_t v) {
     uint32_t r = 0;
     while ((1ull << (r + 1)) <= v) r++;
@@ -614,6 +627,7 @@ static cudaError_t run_batch(DevLevel<RT>& D, uint32_t nb, TraceRec* trace, cuda
     if (og > grid) og = grid;
     if (og < 1) og = 1;
     k_outer<RT, KIND, PREC><<<og, kTile, 0, stream>>>(D, nb);
+    count_launch();
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
 
     if (L.adaptive_f || L.adaptive_c) {
@@ -647,13 +661,14 @@ static cudaError_t run_batch(DevLevel<RT>& D, uint32_t nb, TraceRec* trace, cuda
                 g.next_list = fine ? listF[nxt] : listC[nxt];
             }
             if (S.n == 0) continue;
-            k_phase<RT, KIND, PREC><<<grid, kTile, 0, stream>>>(D, S, nullptr);
+            launch_phase<RT, KIND, PREC>(D, S, nullptr, stream);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         e = cudaMemsetAsync(B.counters + CNT_CLASS, 0, 128 * sizeof(uint32_t), stream);
         if (e != cudaSuccess) return e;
         k_classify<RT><<<og, kTile, 0, stream>>>(D, nb, 0);
         k_classify<RT><<<og, kTile, 0, stream>>>(D, nb, 1);
+        count_launch(2);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         const uint64_t maxc = L.cf.max_count > L.cc.max_count ? L.cf.max_count : L.cc.max_count;
         const uint32_t kmax = ilog2_u64(maxc / C);
@@ -672,7 +687,7 @@ static cudaError_t run_batch(DevLevel<RT>& D, uint32_t nb, TraceRec* trace, cuda
             g.next_slot = 0;
             g.next_list = nullptr;
         }
-        k_phase<RT, KIND, PREC><<<grid, kTile, 0, stream>>>(D, S, trace);
+        launch_phase<RT, KIND, PREC>(D, S, trace, stream);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     } else {
         const uint64_t cbig = (L.fine_only || L.cf.max_count >= L.cc.max_count) ? L.cf.max_count : L.cc.max_count;
@@ -689,7 +704,7 @@ static cudaError_t run_batch(DevLevel<RT>& D, uint32_t nb, TraceRec* trace, cuda
         g.class_k = 0;
         g.next_slot = 0;
         g.next_list = nullptr;
-        k_phase<RT, KIND, PREC><<<grid, kTile, 0, stream>>>(D, S, trace);
+        launch_phase<RT, KIND, PREC>(D, S, trace, stream);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -709,6 +724,7 @@ static cudaError_t sample_level_t(const OuterLevel<RT>& L, OuterBuffers& B, Trac
         done += nb;
     }
     k_reduce_blocks<<<1, 256, 0, stream>>>(B.block_sums, B.grid, B.level_acc);
+    count_launch();
     return cudaGetLastError();
 }
 

@@ -105,15 +105,25 @@ __device__ __forceinline__ void boxmuller32_d(uint32_t u0, uint32_t u1, double& 
 }
 
 // FP32 fast Box-Muller on the SFU: MUFU sin/cos of pi*a (absolute error <= 2^-21.4 on
-// [-pi, pi]), MUFU lg2 for the log and MUFU rsqrt for the root.  |z - z_double| <= 2e-6 for
-// |z| < 6.8 (checked against boxmuller32_d in the tests).
+// [-pi, pi]), MUFU lg2 for the log and MUFU rsqrt for the root.  Near u = 1 the MUFU log's
+// absolute error (2^-22) would dominate the small radius, so there t = -2 ln(1 - q) is summed
+// from its series in the exact complement q = 1 - u = (~u1 + 1/2) 2^-32 (five terms; truncation
+// below 5e-12 relative for q < 1/64).  |z - z_double| <= 4e-6 over the whole range (checked
+// against boxmuller32_d in the tests).
 __device__ __forceinline__ void boxmuller32_f(uint32_t u0, uint32_t u1, float& x, float& y) {
     const float PI = 3.14159265358979f;
     float a = fmaf((float)(int32_t)u0, 0x1p-31f, 0x1p-32f);
     float u = fmaf((float)u1, 0x1p-32f, 0x1p-33f);
+    float q = fmaf((float)(~u1), 0x1p-32f, 0x1p-33f);
     float s, c;
     __sincosf(PI * a, &s, &c);
-    float t = -2.0f * 0.69314718055994531f * __log2f(u);   // -2 ln u  (>= 0)
+    float t_log = -2.0f * 0.69314718055994531f * __log2f(u);
+    float p = fmaf(q, 0.2f, 0.25f);
+    p = fmaf(q, p, 0.33333333f);
+    p = fmaf(q, p, 0.5f);
+    p = fmaf(q, p, 1.0f);
+    float t_ser = 2.0f * q * p;
+    float t = (q < 0.015625f) ? t_ser : t_log;   // -2 ln u  (>= 0)
     float r = t * rsqrtf(fmaxf(t, 1e-30f));
     x = s * r;
     y = c * r;

@@ -159,7 +159,8 @@ EXPORTS = [
     "nmlmc_destroy", "nmlmc_configure", "nmlmc_set_model", "nmlmc_set_portfolio",
     "nmlmc_reset_streams", "nmlmc_sample", "nmlmc_sample_levels", "nmlmc_set_trace",
     "nmlmc_portfolio_full_loss", "nmlmc_mlmc_default_input", "nmlmc_mlmc_run",
-    "nmlmc_mlmc_run_cb", "nmlmc_threefry_blocks", "nmlmc_outer_normals",
+    "nmlmc_mlmc_run_cb", "nmlmc_threefry_blocks", "nmlmc_outer_normals", "nmlmc_set_shard",
+    "nmlmc_set_profiling", "nmlmc_phase_kernel_time", "nmlmc_kernel_launches",
 ]
 
 
@@ -190,6 +191,10 @@ def lib() -> ctypes.CDLL:
     L.nmlmc_mlmc_run_cb.argtypes = [ctypes.POINTER(MlmcInput), SAMPLE_LEVEL_FN, SAMPLE_LEVELS_FN,
                                     ctypes.c_void_p, ctypes.POINTER(MlmcOutput), ctypes.c_char_p,
                                     ctypes.c_size_t]
+    L.nmlmc_set_shard.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32]
+    L.nmlmc_set_profiling.argtypes = [ctypes.c_void_p, ctypes.c_int32]
+    L.nmlmc_phase_kernel_time.argtypes = [ctypes.c_void_p, _u64p, _dp]
+    L.nmlmc_kernel_launches.restype = ctypes.c_uint64
     L.nmlmc_threefry_blocks.argtypes = [_u64p, _u64p, _u64p, ctypes.c_uint64]
     L.nmlmc_outer_normals.argtypes = [ctypes.c_int32, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32,
                                       ctypes.c_uint64, _dp]
@@ -297,6 +302,18 @@ class Sampler:
                "nmlmc_sample_levels")
         return [r.as_dict() for r in res]
 
+    def set_shard(self, rank: int, world: int):
+        _check(self.L.nmlmc_set_shard(self.h, rank, world), "nmlmc_set_shard")
+
+    def set_profiling(self, on: bool):
+        _check(self.L.nmlmc_set_profiling(self.h, int(on)), "nmlmc_set_profiling")
+
+    def phase_kernel_time(self):
+        n = ctypes.c_uint64(0)
+        s = ctypes.c_double(0)
+        _check(self.L.nmlmc_phase_kernel_time(self.h, ctypes.byref(n), ctypes.byref(s)), "phase_kernel_time")
+        return int(n.value), float(s.value)
+
     def full_loss(self, ell: int, first: int, n: int) -> np.ndarray:
         out = np.zeros(n)
         _check(self.L.nmlmc_portfolio_full_loss(self.h, ell, first, n, _p(out, _dp)), "full_loss")
@@ -363,6 +380,11 @@ def mlmc_run_cb(sample_level, sample_levels=None, *, targetTOL=1e-3, M0=100, ver
     _check(L.nmlmc_mlmc_run_cb(ctypes.byref(inp), f1, f2, None, ctypes.byref(out), buf, len(buf)),
            "nmlmc_mlmc_run_cb")
     return mlmc_output_dict(out, buf.value.decode())
+
+
+def kernel_launches() -> int:
+    """Kernels launched by libnmlmc.so since it was loaded."""
+    return int(lib().nmlmc_kernel_launches())
 
 
 def threefry_blocks(ctr, key) -> np.ndarray:
