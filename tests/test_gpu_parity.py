@@ -72,8 +72,9 @@ def make_pair(case, o_prec, streams_o, streams_n, cores=None, seed=None):
                   subsample=case["sub"], use_delta_cv=case["cv"])
         st_o, de_o = s_o.set_portfolio(pf, **kw)
         st_g, de_g = s_g.set_portfolio(pf, **kw)
-        np.testing.assert_array_equal(st_g, st_o)      # host set-up: same libm as the reference
-        np.testing.assert_array_equal(de_g, de_o)
+        if case.get("gpu_prec", nm_prec(o_prec)) == nm_prec(o_prec):
+            np.testing.assert_array_equal(st_g, st_o)  # host set-up: same libm as the reference
+            np.testing.assert_array_equal(de_g, de_o)
     return s_o, s_g
 
 
