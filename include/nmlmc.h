@@ -225,6 +225,30 @@ int nmlmc_threefry_blocks(const uint64_t* ctr, const uint64_t* key, uint64_t* ou
 int nmlmc_outer_normals(int32_t precision, uint64_t seed, uint64_t stream, uint32_t tag, uint64_t n,
                         double* out);
 
+/* ---- allocation-free level call ------------------------------------------------------------
+ * No counterpart in the reference.  For callers that may not allocate device memory: code that
+ * runs while a framework owns the device memory pool, code replayed inside a captured CUDA
+ * graph, hosts that reserve all device memory up front.  One level call of the model problem
+ * (kind NMLMC_MODEL_REFERENCE or NMLMC_MODEL_SHIFT; the OUTER stream layout, precision
+ * NMLMC_PREC_FP32 or NMLMC_PREC_FP64, antithetic) over outer samples [first_index,
+ * first_index + M) of level `ell`, on `stream` (a cudaStream_t; NULL = the default stream) of the
+ * current device.  It allocates nothing: all scratch lives in one file-scope device array of
+ * NMLMC_NOALLOC_SCRATCH_BYTES that every process loading this library reserves on each GPU it
+ * uses until exit, which limits a call to M <= NMLMC_NOALLOC_MAX_OUTER (larger M is rejected
+ * with NMLMC_ERR_ARG).  The first call on a device looks the array's device address up
+ * (cudaGetSymbolAddress), so make that first call before any stream capture.  Calls share the
+ * array — each clears what it accumulates into, but calls that overlap on the GPU race.
+ * d_out (device memory, 16 doubles) receives: sums of phi_f^k (k = 1..4), sums of
+ * (phi_f - phi_c)^k, work, inner samples, outer samples that hit the maximum count, outer
+ * samples that stayed at the base count, and 4 zeros.  The copy into d_out is ordered on
+ * `stream`; synchronize the stream before reading it. */
+#define NMLMC_NOALLOC_MAX_OUTER 65536u
+#define NMLMC_NOALLOC_SCRATCH_BYTES (3u << 20)
+int nmlmc_sample_level_noalloc(int32_t kind, double tau, double max_loss, uint32_t N0,
+                               uint32_t beta, double adaptive_r, int32_t adaptive_incl_r2,
+                               int32_t precision, uint64_t seed, uint32_t ell,
+                               uint64_t first_index, uint64_t M, double* d_out, void* stream);
+
 /* ---- host continuation-MLMC driver (mlmc_t::run, mlmc.hpp:290-337) ------------------------- */
 typedef struct nmlmc_mlmc_input {
     double targetTOL;              /* 1e-3 */

@@ -161,6 +161,7 @@ EXPORTS = [
     "nmlmc_portfolio_full_loss", "nmlmc_mlmc_default_input", "nmlmc_mlmc_run",
     "nmlmc_mlmc_run_cb", "nmlmc_threefry_blocks", "nmlmc_outer_normals", "nmlmc_set_shard",
     "nmlmc_set_profiling", "nmlmc_phase_kernel_time", "nmlmc_kernel_launches",
+    "nmlmc_sample_level_noalloc",
 ]
 
 
@@ -195,6 +196,11 @@ def lib() -> ctypes.CDLL:
     L.nmlmc_set_profiling.argtypes = [ctypes.c_void_p, ctypes.c_int32]
     L.nmlmc_phase_kernel_time.argtypes = [ctypes.c_void_p, _u64p, _dp]
     L.nmlmc_kernel_launches.restype = ctypes.c_uint64
+    L.nmlmc_sample_level_noalloc.argtypes = [ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double,
+                                             ctypes.c_int32, ctypes.c_int32, ctypes.c_uint64,
+                                             ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64,
+                                             ctypes.c_void_p, ctypes.c_void_p]
     L.nmlmc_threefry_blocks.argtypes = [_u64p, _u64p, _u64p, ctypes.c_uint64]
     L.nmlmc_outer_normals.argtypes = [ctypes.c_int32, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32,
                                       ctypes.c_uint64, _dp]
