@@ -554,7 +554,8 @@ int nmlmc_configure(nmlmc_ctx* c, const nmlmc_config* cfg) {
     nmlmc_config k = *cfg;
     if (k.cores == 0) k.cores = 2048;
     if (k.batch == 0) k.batch = 1u << 20;
-    if (k.N0 == 0 || k.beta == 0 || (k.beta & (k.beta - 1)) != 0) return set_err(NMLMC_ERR_ARG);
+    // beta: a power of two >= 2 (the adaptive base count N0 * (beta/2)^ell is 0 for beta = 1)
+    if (k.N0 == 0 || k.beta < 2 || (k.beta & (k.beta - 1)) != 0) return set_err(NMLMC_ERR_ARG);
     if (k.precision < NMLMC_PREC_REF32 || k.precision > NMLMC_PREC_FP32) return set_err(NMLMC_ERR_ARG);
     if (k.streams != NMLMC_STREAMS_CORE && k.streams != NMLMC_STREAMS_OUTER) return set_err(NMLMC_ERR_ARG);
     if (k.streams == NMLMC_STREAMS_CORE && k.precision == NMLMC_PREC_FP32) return set_err(NMLMC_ERR_ARG);

@@ -176,15 +176,18 @@ __device__ __forceinline__ uint32_t pf_pick(const OptionTable<RT>& ot, uint64_t 
 }
 
 // ---- one chunk: inner samples [s0, s0 + C) of phase `tag` of outer sample `item` ----------
-template <class RT, int KIND, int PREC>
-__device__ __forceinline__ void eval_chunk(const DevLevel<RT>& D, uint32_t item, uint32_t tag,
-                                           uint64_t s0, uint32_t C, bool want_s2, Acc<PREC>& a1,
-                                           Acc<PREC>& a2, double& work) {
+// C (inner samples per chunk) is a compile-time constant so the independent Threefry blocks of a
+// chunk can be interleaved (two at a time) for instruction-level parallelism.
+template <class RT, int KIND, int PREC, uint32_t C>
+__device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t item, uint32_t tag,
+                                             uint64_t s0, bool want_s2, Acc<PREC>& a1,
+                                             Acc<PREC>& a2, double& work) {
     const OuterLevel<RT>& L = D.L;
     const TfKey key = tf_key(L.seed, outer_stream_id(L.ell, L.first_index + item));
     const RT* Yv = reinterpret_cast<const RT*>(D.B.Yv);
     if (KIND == KIND_SHIFT_MODEL) {              // X = Y + Z: one normal per inner sample
         const RT Y = Yv[item];
+#pragma unroll 2
         for (uint32_t b = 0; b < C / 4; b++) {
             uint64_t v0, v1;
             threefry2x64((s0 >> 2) + b, tag, key, v0, v1);
@@ -202,6 +205,7 @@ __device__ __forceinline__ void eval_chunk(const DevLevel<RT>& D, uint32_t item,
     } else if (KIND == KIND_REF_MODEL) {         // model_sampler.cpp:62-76: two normals
         const RT Y = Yv[item];
         const RT st = L.mp.stau, s1t = L.mp.s1tau;
+#pragma unroll 2
         for (uint32_t b = 0; b < C / 2; b++) {   // one block = two inner samples
             uint64_t v0, v1;
             threefry2x64((s0 >> 1) + b, tag, key, v0, v1);
@@ -221,6 +225,7 @@ __device__ __forceinline__ void eval_chunk(const DevLevel<RT>& D, uint32_t item,
     } else {                                     // portfolio: one 64-bit value per inner sample
         const OptionTable<RT>& ot = L.ot;
         const RT* Rrow = reinterpret_cast<const RT*>(D.B.Rt) + (size_t)item * ot.Q;
+#pragma unroll 2
         for (uint32_t b = 0; b < C / 2; b++) {
             uint64_t v[2];
             threefry2x64((s0 >> 1) + b, tag, key, v[0], v[1]);
@@ -234,6 +239,18 @@ __device__ __forceinline__ void eval_chunk(const DevLevel<RT>& D, uint32_t item,
                 if (want_s2) a2.add(xmul(d, d));
             }
         }
+    }
+}
+
+template <class RT, int KIND, int PREC>
+__device__ __forceinline__ void eval_chunk(const DevLevel<RT>& D, uint32_t item, uint32_t tag,
+                                           uint64_t s0, uint32_t C, bool want_s2, Acc<PREC>& a1,
+                                           Acc<PREC>& a2, double& work) {
+    switch (C) {
+    case 32: eval_chunk_c<RT, KIND, PREC, 32>(D, item, tag, s0, want_s2, a1, a2, work); break;
+    case 16: eval_chunk_c<RT, KIND, PREC, 16>(D, item, tag, s0, want_s2, a1, a2, work); break;
+    case 8: eval_chunk_c<RT, KIND, PREC, 8>(D, item, tag, s0, want_s2, a1, a2, work); break;
+    default: eval_chunk_c<RT, KIND, PREC, 4>(D, item, tag, s0, want_s2, a1, a2, work); break;
     }
 }
 
@@ -290,27 +307,29 @@ __device__ __forceinline__ void pilot_done(const DevLevel<RT>& D, const Seg& g, 
     g.next_list[pos] = item;
 }
 
-// Per-item completion of the final phase: phi_f, phi_c, moments, statistics, trace.
+// Per-item completion of the final phase: phi_f, phi_c, the 4 + 4 moments, statistics and the
+// trace record.  c[0..3] += phi_f^k, c[4..7] += (phi_f - phi_c)^k, c[8] inner samples,
+// c[9] hit the maximum count, c[10] stayed at the base count.
 template <class RT>
-__device__ __forceinline__ void final_done(const DevLevel<RT>& D, const Seg& g, uint32_t item,
-                                           RT mean_big, RT phi_small, bool fine_big, double* acc,
-                                           TraceRec* trace) {
+__device__ __forceinline__ void final_contrib(const DevLevel<RT>& D, const Seg& g, uint32_t item,
+                                              RT mean_big, RT phi_small, bool fine_big, double* c,
+                                              TraceRec* trace) {
     RT phi_big = (mean_big >= (RT)0) ? (RT)1 : (RT)0;
     RT f_phi, c_phi;
     if (D.L.fine_only) { f_phi = phi_big; c_phi = 0; }
     else if (fine_big) { f_phi = phi_big; c_phi = phi_small; }
     else { f_phi = phi_small; c_phi = phi_big; }
     RT p = 1;
-    for (int q = 0; q < 4; q++) { p = xmul(p, f_phi); acc[q] += (double)p; }
+    for (int q = 0; q < 4; q++) { p = xmul(p, f_phi); c[q] = (double)p; }
     if (!D.L.fine_only) {
         RT dphi = xsub(f_phi, c_phi);
         p = 1;
-        for (int q = 0; q < 4; q++) { p = xmul(p, dphi); acc[4 + q] += (double)p; }
+        for (int q = 0; q < 4; q++) { p = xmul(p, dphi); c[4 + q] = (double)p; }
     }
-    acc[9] += (double)g.count;
+    c[8] = (double)g.count;
     const uint32_t cf = D.B.cnt_f[item];
-    acc[10] += (cf == (uint32_t)D.L.cf.max_count) ? 1.0 : 0.0;
-    acc[11] += (cf == (uint32_t)D.L.cf.base_count) ? 1.0 : 0.0;
+    c[9] = (cf == (uint32_t)D.L.cf.max_count) ? 1.0 : 0.0;
+    c[10] = (cf == (uint32_t)D.L.cf.base_count) ? 1.0 : 0.0;
     if (trace) {
         TraceRec tr;
         tr.count_f = cf;
@@ -325,6 +344,17 @@ __device__ __forceinline__ void final_done(const DevLevel<RT>& D, const Seg& g, 
     }
 }
 
+// Per-warp accumulators, written only by lane 0 of the warp (no atomics): [0..3] phi_f
+// moments, [4..7] difference moments, [8] work, [9] inner samples, [10] hit max, [11] stayed at
+// base (the layout of OuterBuffers::block_sums).
+__device__ __forceinline__ void add_contrib(double* slot, const double* c) {
+#pragma unroll
+    for (int q = 0; q < 8; q++) slot[q] += c[q];
+    slot[9] += c[8];
+    slot[10] += c[9];
+    slot[11] += c[10];
+}
+
 template <class RT, int KIND, int PREC>
 __global__ void __launch_bounds__(kTile) k_phase(DevLevel<RT> D, SegSet S, TraceRec* trace) {
     __shared__ Acc<PREC> sm_a1[kWarps];
@@ -334,9 +364,9 @@ __global__ void __launch_bounds__(kTile) k_phase(DevLevel<RT> D, SegSet S, Trace
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const uint32_t C = D.L.chunk;
     uint32_t* counters = D.B.counters;
-    double acc[16];
-#pragma unroll
-    for (int q = 0; q < 16; q++) acc[q] = 0;
+    double wsum = 0;                                     // work of this thread's chunks
+    if (lane < 16) sm_acc[warp][lane] = 0;
+    __syncthreads();
     const RT* Yv = reinterpret_cast<const RT*>(D.B.Yv);
 
     for (int si = 0; si < S.n; si++) {
@@ -351,7 +381,7 @@ __global__ void __launch_bounds__(kTile) k_phase(DevLevel<RT> D, SegSet S, Trace
         if (n_items == 0) continue;
         const uint32_t nch = 1u << g.nch_log2;
         const bool pilot = g.mode != 2;
-        if (pilot && blockIdx.x == 0 && t == 0) acc[9] += (double)n_items * (double)g.count;
+        if (pilot && blockIdx.x == 0 && t == 0) sm_acc[0][9] += (double)n_items * (double)g.count;
 
         if (nch <= (uint32_t)kTile) {
             // ---- a tile holds kTile / nch whole items ----
@@ -375,9 +405,7 @@ __global__ void __launch_bounds__(kTile) k_phase(DevLevel<RT> D, SegSet S, Trace
                 Acc<PREC> a1, a2;
                 a1.zero();
                 a2.zero();
-                double w = 0;
-                if (valid) eval_chunk<RT, KIND, PREC>(D, item, g.tag, (uint64_t)j * C, C, pilot, a1, a2, w);
-                acc[8] += w;
+                if (valid) eval_chunk<RT, KIND, PREC>(D, item, g.tag, (uint64_t)j * C, C, pilot, a1, a2, wsum);
                 const float coeff = (float)gs / (float)nch;     // 1 / groups (a power of two)
                 float ind = 0.f;
                 if (!pilot && gs == 1) ind = inner_mean<RT, PREC>(start, a1, csmall) >= (RT)0 ? coeff : 0.f;
@@ -422,10 +450,23 @@ __global__ void __launch_bounds__(kTile) k_phase(DevLevel<RT> D, SegSet S, Trace
                     }
                     __syncthreads();
                 }
-                if (leader) {
-                    if (pilot) pilot_done<RT, PREC>(D, g, item, start, a1, a2, counters);
-                    else final_done<RT>(D, g, item, inner_mean<RT, PREC>(start, a1, g.count), (RT)ind,
-                                        fine_big, acc, trace);
+                if (pilot) {
+                    if (leader) pilot_done<RT, PREC>(D, g, item, start, a1, a2, counters);
+                } else {
+                    double c[11];
+#pragma unroll
+                    for (int q = 0; q < 11; q++) c[q] = 0;
+                    if (leader) final_contrib<RT>(D, g, item, inner_mean<RT, PREC>(start, a1, g.count), (RT)ind,
+                                                  fine_big, c, trace);
+                    if (nch < 32) {
+                        // several items per warp: reduce the warp's contributions first
+#pragma unroll
+                        for (int q = 0; q < 11; q++)
+                            for (int m = 16; m > 0; m >>= 1) c[q] += __shfl_down_sync(0xffffffffu, c[q], m);
+                        if (lane == 0) add_contrib(sm_acc[warp], c);
+                    } else if (leader) {
+                        add_contrib(sm_acc[warp], c);   // the leader is lane 0 of its warp
+                    }
                 }
             }
         } else {
@@ -454,9 +495,7 @@ __global__ void __launch_bounds__(kTile) k_phase(DevLevel<RT> D, SegSet S, Trace
                     Acc<PREC> a1, a2;
                     a1.zero();
                     a2.zero();
-                    double w = 0;
-                    eval_chunk<RT, KIND, PREC>(D, item, g.tag, (uint64_t)j * C, C, pilot, a1, a2, w);
-                    acc[8] += w;
+                    eval_chunk<RT, KIND, PREC>(D, item, g.tag, (uint64_t)j * C, C, pilot, a1, a2, wsum);
                     float ind = 0.f;
                     if (!pilot && gs == 1) ind = inner_mean<RT, PREC>(start, a1, csmall) >= (RT)0 ? coeff : 0.f;
                     for (uint32_t m = 1; m < 32; m <<= 1) {
@@ -500,24 +539,26 @@ __global__ void __launch_bounds__(kTile) k_phase(DevLevel<RT> D, SegSet S, Trace
                     __syncthreads();
                 }
                 if (t == 0) {
-                    if (pilot) pilot_done<RT, PREC>(D, g, item, start, tot1, tot2, counters);
-                    else final_done<RT>(D, g, item, inner_mean<RT, PREC>(start, tot1, g.count), (RT)tind,
-                                        fine_big, acc, trace);
+                    if (pilot) {
+                        pilot_done<RT, PREC>(D, g, item, start, tot1, tot2, counters);
+                    } else {
+                        double c[11];
+                        for (int q = 0; q < 11; q++) c[q] = 0;
+                        final_contrib<RT>(D, g, item, inner_mean<RT, PREC>(start, tot1, g.count), (RT)tind,
+                                          fine_big, c, trace);
+                        add_contrib(sm_acc[0], c);
+                    }
                 }
             }
         }
     }
-    // per-CTA partials in fixed order
-#pragma unroll
-    for (int q = 0; q < 16; q++) {
-        double v = acc[q];
-        for (int m = 16; m > 0; m >>= 1) v += __shfl_xor_sync(0xffffffffu, v, m);
-        if (lane == 0) sm_acc[warp][q] = v;
-    }
+    // work of the block's chunks, then the block totals into this CTA's partial-sum slot
+    for (int m = 16; m > 0; m >>= 1) wsum += __shfl_down_sync(0xffffffffu, wsum, m);
+    if (lane == 0) sm_acc[warp][8] += wsum;
     __syncthreads();
     if (t < 16) {
         double v = 0;
-        for (int wq = 0; wq < kWarps; wq++) v += sm_acc[wq][t];
+        for (int w = 0; w < kWarps; w++) v += sm_acc[w][t];
         D.B.block_sums[(size_t)blockIdx.x * 16 + t] += v;
     }
 }
@@ -554,24 +595,38 @@ __global__ void __launch_bounds__(kTile) k_outer(DevLevel<RT> D, uint32_t nb) {
 }
 
 // ---- bucket outer samples by final count (count_big = max(cnt_f, cnt_c)) ------------------
+// Pass 0 counts the outer samples of each class, pass 1 scatters their indices into class order.
+// Each CTA histograms a tile in shared memory first, so the global counters see one atomic per
+// class per tile instead of one per outer sample.
 template <class RT>
 __global__ void k_classify(DevLevel<RT> D, uint32_t nb, int pass) {
     uint32_t* counters = D.B.counters;
     const uint32_t C = D.L.chunk;
-    __shared__ uint32_t offs[64];
-    if (pass == 1) {
-        if (threadIdx.x == 0) {
-            uint32_t a = 0;
-            for (int k = 0; k < 64; k++) { offs[k] = a; a += counters[CNT_CLASS + k]; }
+    __shared__ uint32_t offs[64], hist[64], base[64];
+    if (pass == 1 && threadIdx.x == 0) {
+        uint32_t a = 0;
+        for (int k = 0; k < 64; k++) { offs[k] = a; a += counters[CNT_CLASS + k]; }
+    }
+    for (uint32_t t0 = blockIdx.x * blockDim.x; t0 < nb; t0 += gridDim.x * blockDim.x) {
+        if (threadIdx.x < 64) hist[threadIdx.x] = 0;
+        __syncthreads();
+        const uint32_t i = t0 + threadIdx.x;
+        const bool valid = i < nb;
+        uint32_t k = 0, rank = 0;
+        if (valid) {
+            uint32_t cf = D.B.cnt_f[i], cc = D.L.fine_only ? 0u : D.B.cnt_c[i];
+            uint32_t q = (cf > cc ? cf : cc) / C;
+            k = q ? 31 - __clz(q) : 0;
+            rank = atomicAdd(&hist[k], 1u);
         }
         __syncthreads();
-    }
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
-        uint32_t cf = D.B.cnt_f[i], cc = D.L.fine_only ? 0u : D.B.cnt_c[i];
-        uint32_t cb = cf > cc ? cf : cc;
-        uint32_t k = 31 - __clz(cb / C);
-        if (pass == 0) atomicAdd(&counters[CNT_CLASS + k], 1u);
-        else D.B.class_items[offs[k] + atomicAdd(&counters[CNT_FILL + k], 1u)] = i;
+        if (threadIdx.x < 64 && hist[threadIdx.x]) {
+            if (pass == 0) atomicAdd(&counters[CNT_CLASS + threadIdx.x], hist[threadIdx.x]);
+            else base[threadIdx.x] = atomicAdd(&counters[CNT_FILL + threadIdx.x], hist[threadIdx.x]);
+        }
+        __syncthreads();
+        if (pass == 1 && valid) D.B.class_items[offs[k] + base[k] + rank] = i;
+        __syncthreads();
     }
 }
 
