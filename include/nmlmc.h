@@ -171,6 +171,24 @@ typedef struct nmlmc_portfolio {
     int32_t discount;                     /* 1: finish value discounted by exp(-r tau)       */
 } nmlmc_portfolio;
 
+/* Seeded synthetic portfolio: Q stocks with spot S0, drift mu and sigma ~ U[sigma_lo, sigma_hi];
+ * P options, each on a uniformly chosen stock, a call with probability call_fraction, strike ~
+ * U[strike_lo, strike_hi] * S0, maturity ~ U[maturity_lo, maturity_hi], position ~ N(0, 1).
+ * Every field comes from a counter-based Threefry2x64-20 stream keyed by the seed, so the
+ * portfolio depends only on (spec, seed).  No counterpart in the reference (whose demo generator,
+ * portfolio_gen_data, builds a different portfolio).  Arrays are caller-owned ([Q] and [P]). */
+typedef struct nmlmc_portfolio_spec {
+    uint32_t Q, P;
+    double S0, r, mu;
+    double sigma_lo, sigma_hi;
+    double strike_lo, strike_hi;
+    double maturity_lo, maturity_hi;
+    double call_fraction;
+} nmlmc_portfolio_spec;
+int nmlmc_portfolio_generate(const nmlmc_portfolio_spec* spec, uint64_t seed, double* S0,
+                             double* mu, double* sigma, double* strike, double* maturity,
+                             double* w, uint32_t* stock_ind, int32_t* type);
+
 /* Per-outer-sample record written by nmlmc_sample when a trace buffer is armed. */
 typedef struct nmlmc_trace_rec {
     uint64_t count_f, count_c;

@@ -105,6 +105,7 @@ struct DevPortfolio {
        *delta_coalesce = nullptr;
     uint32_t* stock_ind = nullptr;
     int8_t* type = nullptr;
+    FastOption* fast = nullptr;       // packed records of the FP32 path
     OptionTable<RT> table{};
 };
 
@@ -183,7 +184,7 @@ template <class RT>
 void free_dev_portfolio(DevPortfolio<RT>& d) {
     dfree(d.strike); dfree(d.maturity); dfree(d.start); dfree(d.w); dfree(d.prob); dfree(d.W_est);
     dfree(d.cdf); dfree(d.S0); dfree(d.mu); dfree(d.sigma); dfree(d.delta_coalesce);
-    dfree(d.stock_ind); dfree(d.type);
+    dfree(d.stock_ind); dfree(d.type); dfree(d.fast);
     d.table = OptionTable<RT>{};
 }
 
@@ -254,6 +255,35 @@ int build_dev_portfolio(nmlmc_ctx* c, DevPortfolio<RT>& d) {
     t.prob_norm = prob_norm; t.compute_prob0 = cp0;
     t.inv_count_prob = (RT)(1. / (double)P);              // portfolio_sampler.cpp:360
     t.subsample = h.subsample; t.use_delta_cv = h.use_delta_cv; t.discount = h.discount;
+    t.fast = nullptr;
+    if constexpr (sizeof(RT) == 4) {
+        // packed FP32 records (nmlmc_bs.cuh): per-option constants folded in double, rounded once;
+        // only for unit work estimates (every option of the BS method costs one evaluation)
+        bool unit = true;
+        for (uint32_t j = 0; j < P; j++) unit = unit && h.W_est[j] == 1.0;
+        if (unit) {
+            std::vector<FastOption> fo(P);
+            const double disc = h.discount ? exp(-h.r * h.tau) : 1.0;
+            for (uint32_t j = 0; j < P; j++) {
+                const uint32_t s = h.stock_ind[j];
+                const double sg = h.sigma[s], K = h.strike[j], T = h.maturity[j], Tr = T - h.tau;
+                const double m = h.type[j] > 0 ? 1.0 : -1.0;
+                const double sd = sg * sqrt(Tr);
+                const double V0 = h_calc_bs<double>(h.type[j], h.S0[s], K, h.r, T, sg);
+                FastOption& o = fo[j];
+                o.c1 = (float)(-log(K) + (h.r + 0.5 * sg * sg) * Tr);
+                o.inv_s = (float)(1.0 / sd);
+                o.s = (float)sd;
+                o.wR = (float)(-h.w[j] * disc * m);
+                o.wK = (float)(h.w[j] * disc * m * K * exp(-h.r * Tr));
+                o.wV0 = (float)(h.w[j] * V0);
+                o.cv = h.use_delta_cv ? (float)(h.w[j] * h_calc_delta<double>(h.type[j], h.S0[s], K, h.r, T, sg)) : 0.f;
+                o.asset_type = s | (h.type[j] > 0 ? 0u : 0x80000000u);
+            }
+            if ((rc = upload(d.fast, fo))) return rc;
+            t.fast = d.fast;
+        }
+    }
     return NMLMC_OK;
 }
 

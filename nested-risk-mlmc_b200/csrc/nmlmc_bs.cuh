@@ -1,0 +1,67 @@
+// FP32 Black-Scholes on the SFU for the batched portfolio path.
+//
+// The loss of option i at the outer sample Y (option_diff_from_blackscholes and the delta control
+// variate of sample_inner_bs, portfolio_sampler.cpp:186-210, 453-468) is regrouped so that all
+// per-option constants are folded on the host (in double, then rounded once):
+//
+//   d1 = (ln R + c1) * inv_s,   d2 = d1 - s,   m = +1 call / -1 put
+//   V  = m (R Phi(m d1) - K e^{-r(T-tau)} Phi(m d2))          (BS at tau, remaining time T - tau)
+//   loss_i = w V0 - w e^{-r tau} V  +  cv (R - S0)            (cv = w Delta_BS(S0, T) when the
+//                                                             delta control variate is on)
+// with c1 = -ln K + (r + sigma^2/2)(T - tau), s = sigma sqrt(T - tau), inv_s = 1/s.  The record
+// stores wR = -w e^{-r tau} m, wK = w e^{-r tau} m K e^{-r(T - tau)}, wV0 = w V0 and cv.
+//
+// Phi(x) = erfc(-x/sqrt 2) / 2 with the rational-Chebyshev erfc of Numerical Recipes in C
+// (2nd ed., §6.2, "erfcc": fractional error below 1.2e-7 for all arguments), its exponential and
+// reciprocal on MUFU (__expf, __frcp_rn).  Measured against double erfc over |x| <= 10 the
+// composite Phi has relative error <= 4e-7 (tests/test_gpu_portfolio.py); the loss of one option
+// is then within 1e-6 * (|wV0| + |wR R| + |wK|) of the double-precision value.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace nmlmc {
+
+// Packed option record of the FP32 path: 32 bytes, two 16-byte loads.
+struct __align__(16) FastOption {
+    float c1, inv_s, s, wR;
+    float wK, wV0, cv;
+    uint32_t asset_type;    // stock index in bits 0..30, bit 31 set for a put
+};
+static_assert(sizeof(FastOption) == 32, "FastOption layout");
+
+#ifdef __CUDACC__
+// erfc(z) for z >= 0 on the SFU (Numerical Recipes "erfcc" coefficients).
+__device__ __forceinline__ float erfc_pos_fast(float z) {
+    float t = __frcp_rn(fmaf(0.5f, z, 1.0f));
+    float p = fmaf(t, 0.17087277f, -0.82215223f);
+    p = fmaf(t, p, 1.48851587f);
+    p = fmaf(t, p, -1.13520398f);
+    p = fmaf(t, p, 0.27886807f);
+    p = fmaf(t, p, -0.18628806f);
+    p = fmaf(t, p, 0.09678418f);
+    p = fmaf(t, p, 0.37409196f);
+    p = fmaf(t, p, 1.00002368f);
+    p = fmaf(t, p, -1.26551223f);
+    return t * __expf(fmaf(-z, z, p));
+}
+
+// Phi(x) = erfc(-x / sqrt 2) / 2 for any x.
+__device__ __forceinline__ float norm_cdf_fast(float x) {
+    const float z = fabsf(x) * 0.70710678118654752f;
+    const float h = 0.5f * erfc_pos_fast(z);          // Phi(-|x|)
+    return x >= 0.f ? 1.0f - h : h;
+}
+
+// loss_i(R) of one option (see the header comment); lnR = ln R of its stock at this outer sample.
+__device__ __forceinline__ float option_loss_fast(const FastOption& o, float R, float lnR, float S0) {
+    const float m = (o.asset_type & 0x80000000u) ? -1.0f : 1.0f;
+    const float d1 = (lnR + o.c1) * o.inv_s;
+    const float d2 = d1 - o.s;
+    const float n1 = norm_cdf_fast(m * d1), n2 = norm_cdf_fast(m * d2);
+    float v = fmaf(o.wR * R, n1, fmaf(o.wK, n2, o.wV0));
+    return fmaf(o.cv, R - S0, v);
+}
+#endif
+
+}  // namespace nmlmc

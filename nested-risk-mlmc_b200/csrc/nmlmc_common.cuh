@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "nmlmc_bs.cuh"
 #include "nmlmc_rng.cuh"
 
 namespace nmlmc {
@@ -46,6 +47,7 @@ struct OptionTable {
     const RT* mu;
     const RT* sigma;
     const RT* delta_coalesce;
+    const struct FastOption* fast;   // FP32 path: packed records (nmlmc_bs.cuh), else nullptr
     uint32_t P, Q;
     RT r, rho, s1_rho2, max_loss, tau, stau, prob_norm, compute_prob0, inv_count_prob;
     int subsample, use_delta_cv, discount;

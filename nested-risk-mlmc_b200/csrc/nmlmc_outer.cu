@@ -222,6 +222,28 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
             }
         }
         work += (double)C;
+    } else if (PREC == PREC_FP32 && L.ot.fast && L.ot.subsample == SUB_UNIFORM) {
+        // portfolio, FP32: packed records and the SFU Black-Scholes (nmlmc_bs.cuh); X = P * loss_i
+        const OptionTable<RT>& ot = L.ot;
+        const float* Rrow = reinterpret_cast<const float*>(D.B.Rt) + (size_t)item * ot.Q;
+        const float Pf = (float)ot.P;
+#pragma unroll 2
+        for (uint32_t b = 0; b < C / 2; b++) {
+            uint64_t v[2];
+            threefry2x64((s0 >> 1) + b, tag, key, v[0], v[1]);
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const uint32_t j = (uint32_t)__umul64hi(v[q], (uint64_t)ot.P);
+                const FastOption o = ot.fast[j];
+                const uint32_t st = o.asset_type & 0x7fffffffu;
+                const float R = Rrow[st];
+                const float S0 = o.cv != 0.f ? (float)ot.S0[st] : 0.f;
+                const float d = Pf * option_loss_fast(o, R, __logf(R), S0);
+                a1.add((RT)d);
+                if (want_s2) a2.add((RT)(d * d));
+            }
+        }
+        work += (double)C;
     } else {                                     // portfolio: one 64-bit value per inner sample
         const OptionTable<RT>& ot = L.ot;
         const RT* Rrow = reinterpret_cast<const RT*>(D.B.Rt) + (size_t)item * ot.Q;
@@ -579,15 +601,30 @@ __global__ void __launch_bounds__(kTile) k_outer(DevLevel<RT> D, uint32_t nb) {
             // portfolio_sampler.cpp:293-311 on the OUTER layout: normal 0 systemic, 1 + s per stock
             const OptionTable<RT>& ot = L.ot;
             RT* Rrow = reinterpret_cast<RT*>(D.B.Rt) + (size_t)i * ot.Q;
-            RT dW_sys = xmul(ot.stau, outer_normal_at<PREC, RT>(key, PH_OUTER, 0));
-            RT cv = (RT)0;
-            for (uint32_t s = 0; s < ot.Q; s++) {
-                RT W;
-                if (ot.Q == 1) W = dW_sys;
-                else W = xadd(xmul(ot.rho, dW_sys), xmul(ot.s1_rho2, xmul(ot.stau, outer_normal_at<PREC, RT>(key, PH_OUTER, 1 + s))));
-                RT R = simulate_stock_ref<RT>(ot.S0[s], ot.mu[s], ot.sigma[s], ot.tau, W);
-                Rrow[s] = R;
-                if (ot.use_delta_cv) cv = xadd(cv, xmul(xsub(R, ot.S0[s]), ot.delta_coalesce[s]));
+            RT dW_sys = 0, cv = (RT)0;
+            const uint32_t nnorm = ot.Q == 1 ? 1 : ot.Q + 1;
+            for (uint32_t b = 0; 4 * b < nnorm; b++) {          // four normals per block
+                uint64_t v0, v1;
+                threefry2x64(b, PH_OUTER, key, v0, v1);
+                RT z[4];
+                bm_pair<PREC, RT>((uint32_t)v0, (uint32_t)(v0 >> 32), z[0], z[1]);
+                bm_pair<PREC, RT>((uint32_t)v1, (uint32_t)(v1 >> 32), z[2], z[3]);
+                for (uint32_t q = 0; q < 4; q++) {
+                    const uint32_t k = 4 * b + q;
+                    if (k >= nnorm) break;
+                    if (k == 0) { dW_sys = xmul(ot.stau, z[0]); if (ot.Q > 1) continue; }
+                    const uint32_t s = ot.Q == 1 ? 0 : k - 1;
+                    RT W = ot.Q == 1 ? dW_sys : xadd(xmul(ot.rho, dW_sys), xmul(ot.s1_rho2, xmul(ot.stau, z[q])));
+                    RT R;
+                    if (PREC == PREC_FP32) {     // GBM at tau in float (expf), the fast path's R
+                        const float sg = (float)ot.sigma[s];
+                        R = (RT)((float)ot.S0[s] * expf(sg * (float)W + ((float)ot.mu[s] - 0.5f * sg * sg) * (float)ot.tau));
+                    } else {
+                        R = simulate_stock_ref<RT>(ot.S0[s], ot.mu[s], ot.sigma[s], ot.tau, W);
+                    }
+                    Rrow[s] = R;
+                    if (ot.use_delta_cv) cv = xadd(cv, xmul(xsub(R, ot.S0[s]), ot.delta_coalesce[s]));
+                }
             }
             Yv[i] = xsub(-ot.max_loss, cv);
         }
@@ -831,6 +868,60 @@ __global__ void k_full_loss(DevLevel<RT> D, uint32_t nb, double* loss) {
     }
 }
 
+// FP32 sweep of the packed option table: a CTA takes a tile of kLossTile outer samples (their
+// R and ln R rows in shared memory) and streams the table once per tile, so every 32-byte
+// record fetched from L2/HBM feeds kLossTile Black-Scholes evaluations.  Per-thread partial sums
+// are float (each thread adds P/256 options), combined in double across the CTA.
+constexpr int kLossTile = 32;
+
+__global__ void __launch_bounds__(kTile) k_full_loss_fast(DevLevel<float> D, uint32_t nb, double* loss) {
+    extern __shared__ float sm_rows[];   // R[kLossTile][Q], lnR[kLossTile][Q]
+    __shared__ double red[kWarps][kLossTile];
+    const OptionTable<float>& ot = D.L.ot;
+    const uint32_t Q = ot.Q, P = ot.P;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    float* sR = sm_rows;
+    float* slnR = sm_rows + (size_t)kLossTile * Q;
+    const float* Rt = reinterpret_cast<const float*>(D.B.Rt);
+    const uint32_t ntiles = (nb + kLossTile - 1) / kLossTile;
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint32_t o0 = tile * kLossTile;
+        const uint32_t n_here = (nb - o0) < (uint32_t)kLossTile ? (nb - o0) : (uint32_t)kLossTile;
+        for (uint32_t k = t; k < (uint32_t)kLossTile * Q; k += blockDim.x) {
+            const uint32_t o = k / Q;
+            const float R = o < n_here ? Rt[(size_t)(o0 + o) * Q + (k - o * Q)] : 1.0f;
+            sR[k] = R;
+            slnR[k] = __logf(R);
+        }
+        __syncthreads();
+        float acc[kLossTile];
+#pragma unroll
+        for (int o = 0; o < kLossTile; o++) acc[o] = 0.f;
+        for (uint32_t j = t; j < P; j += blockDim.x) {
+            const FastOption op = ot.fast[j];
+            const uint32_t st = op.asset_type & 0x7fffffffu;
+#pragma unroll
+            for (int o = 0; o < kLossTile; o++) {
+                const float R = sR[o * Q + st];
+                acc[o] += option_loss_fast(op, R, slnR[o * Q + st], R);   // no control variate
+            }
+        }
+#pragma unroll
+        for (int o = 0; o < kLossTile; o++) {
+            double v = (double)acc[o];
+            for (int m = 16; m > 0; m >>= 1) v += __shfl_xor_sync(0xffffffffu, v, m);
+            if (lane == 0) red[warp][o] = v;
+        }
+        __syncthreads();
+        if (t < (int)n_here) {
+            double s = 0;
+            for (int w = 0; w < kWarps; w++) s += red[w][t];
+            loss[o0 + t] = s;
+        }
+        __syncthreads();
+    }
+}
+
 template <class RT>
 cudaError_t outer_full_loss(const OuterLevel<RT>& L, int prec, OuterBuffers& B, double* d_loss,
                             cudaStream_t stream) {
@@ -850,7 +941,18 @@ cudaError_t outer_full_loss(const OuterLevel<RT>& L, int prec, OuterBuffers& B, 
             }
         } else {
             if constexpr (sizeof(RT) == 4) {
-                if (prec == PREC_FP32) {
+                if (prec == PREC_FP32 && L.ot.fast) {
+                    k_outer<RT, KIND_PORTFOLIO, PREC_FP32><<<og, kTile, 0, stream>>>(D, (uint32_t)nb);
+                    const size_t smem = (size_t)2 * kLossTile * L.ot.Q * sizeof(float);
+                    if (smem > 200 * 1024) return cudaErrorInvalidValue;   // Q above 800 stocks
+                    if (smem > 48 * 1024) {
+                        cudaError_t ea = cudaFuncSetAttribute(k_full_loss_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                        if (ea != cudaSuccess) return ea;
+                    }
+                    const int lg = (int)((nb + kLossTile - 1) / kLossTile) < B.grid ? (int)((nb + kLossTile - 1) / kLossTile) : B.grid;
+                    k_full_loss_fast<<<lg, kTile, smem, stream>>>(D, (uint32_t)nb, d_loss + done);
+                    count_launch(2);
+                } else if (prec == PREC_FP32) {
                     k_outer<RT, KIND_PORTFOLIO, PREC_FP32><<<og, kTile, 0, stream>>>(D, (uint32_t)nb);
                     k_full_loss<RT, PREC_FP32><<<B.grid, kTile, 0, stream>>>(D, (uint32_t)nb, d_loss + done);
                 } else {

@@ -142,6 +142,22 @@ class MlmcOutput(ctypes.Structure):
                 ("level_time", ctypes.c_double * MAX_LEVELS)]
 
 
+class PortfolioSpec(ctypes.Structure):
+    _fields_ = [("Q", ctypes.c_uint32), ("P", ctypes.c_uint32), ("S0", ctypes.c_double),
+                ("r", ctypes.c_double), ("mu", ctypes.c_double), ("sigma_lo", ctypes.c_double),
+                ("sigma_hi", ctypes.c_double), ("strike_lo", ctypes.c_double),
+                ("strike_hi", ctypes.c_double), ("maturity_lo", ctypes.c_double),
+                ("maturity_hi", ctypes.c_double), ("call_fraction", ctypes.c_double)]
+
+
+# The benchmark portfolio configurations: d GBM stocks (S0 = 100, r = mu = 0.05,
+# sigma ~ U[0.1, 0.4], horizon tau = 1/52), P European options on uniformly chosen stocks,
+# 50/50 call/put, strike ~ U[0.8, 1.2] S0, maturity ~ U[0.25, 2], position ~ N(0, 1).
+PORTFOLIO_C2 = dict(Q=20, P=10_000, S0=100.0, r=0.05, mu=0.05, sigma_lo=0.1, sigma_hi=0.4,
+                    strike_lo=0.8, strike_hi=1.2, maturity_lo=0.25, maturity_hi=2.0, call_fraction=0.5)
+PORTFOLIO_C3 = dict(PORTFOLIO_C2, Q=200, P=1_000_000)
+TAU_WEEK = 1 / 52
+
 SAMPLE_LEVEL_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64,
                                    ctypes.POINTER(LevelResult))
 SAMPLE_LEVELS_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint32, _u32p, _u64p,
@@ -161,7 +177,7 @@ EXPORTS = [
     "nmlmc_portfolio_full_loss", "nmlmc_mlmc_default_input", "nmlmc_mlmc_run",
     "nmlmc_mlmc_run_cb", "nmlmc_threefry_blocks", "nmlmc_outer_normals", "nmlmc_set_shard",
     "nmlmc_set_profiling", "nmlmc_phase_kernel_time", "nmlmc_kernel_launches",
-    "nmlmc_sample_level_noalloc",
+    "nmlmc_sample_level_noalloc", "nmlmc_portfolio_generate",
 ]
 
 
@@ -192,6 +208,8 @@ def lib() -> ctypes.CDLL:
     L.nmlmc_mlmc_run_cb.argtypes = [ctypes.POINTER(MlmcInput), SAMPLE_LEVEL_FN, SAMPLE_LEVELS_FN,
                                     ctypes.c_void_p, ctypes.POINTER(MlmcOutput), ctypes.c_char_p,
                                     ctypes.c_size_t]
+    L.nmlmc_portfolio_generate.argtypes = [ctypes.POINTER(PortfolioSpec), ctypes.c_uint64, _dp, _dp, _dp,
+                                           _dp, _dp, _dp, _u32p, _i32p]
     L.nmlmc_set_shard.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32]
     L.nmlmc_set_profiling.argtypes = [ctypes.c_void_p, ctypes.c_int32]
     L.nmlmc_phase_kernel_time.argtypes = [ctypes.c_void_p, _u64p, _dp]
@@ -386,6 +404,29 @@ def mlmc_run_cb(sample_level, sample_levels=None, *, targetTOL=1e-3, M0=100, ver
     _check(L.nmlmc_mlmc_run_cb(ctypes.byref(inp), f1, f2, None, ctypes.byref(out), buf, len(buf)),
            "nmlmc_mlmc_run_cb")
     return mlmc_output_dict(out, buf.value.decode())
+
+
+def generate_portfolio(spec: dict, seed: int) -> dict:
+    """Seeded synthetic portfolio (nmlmc_portfolio_generate): arrays for Sampler.set_portfolio."""
+    sp = PortfolioSpec(**{k: spec[k] for k, _ in PortfolioSpec._fields_})
+    Q, P = sp.Q, sp.P
+    out = dict(S0=np.zeros(Q), mu=np.zeros(Q), sigma=np.zeros(Q), strike=np.zeros(P),
+               maturity=np.zeros(P), w=np.zeros(P), stock_ind=np.zeros(P, np.uint32),
+               type=np.zeros(P, np.int32))
+    _check(lib().nmlmc_portfolio_generate(ctypes.byref(sp), seed, _p(out["S0"], _dp), _p(out["mu"], _dp),
+                                          _p(out["sigma"], _dp), _p(out["strike"], _dp),
+                                          _p(out["maturity"], _dp), _p(out["w"], _dp),
+                                          _p(out["stock_ind"], _u32p), _p(out["type"], _i32p)),
+           "nmlmc_portfolio_generate")
+    out["prob"] = np.ones(P)
+    return out
+
+
+def loss_quantile(sampler: "Sampler", q: float, n: int, level: int = 63) -> float:
+    """q-quantile of the full portfolio loss L(Y) over n outer samples of the sampler's seed
+    (stream level `level`, kept apart from the MLMC levels)."""
+    L = sampler.full_loss(level, 0, n)
+    return float(np.quantile(L, q, method="inverted_cdf"))
 
 
 def kernel_launches() -> int:
