@@ -131,24 +131,10 @@ def run_once(nm, s, batched, dist=None):
         t0 = time.perf_counter()
         out = s.mlmc_run(targetTOL=EPS, M0=WORKLOAD["M0"], batched=batched)
         return out, time.perf_counter() - t0
-    import torch
-    torch_dist, dev = dist
-
-    def reduce(results):
-        t = torch.tensor([[*r["fsums"], *r["diffsums"], r["work"]] for r in results],
-                         dtype=torch.float64, device=dev)
-        torch_dist.all_reduce(t)
-        t = t.cpu().numpy()
-        out = []
-        for row, r in zip(t, results):   # sums over ranks; device time stays this rank's
-            out.append(dict(fsums=row[0:4], diffsums=row[4:8], work=row[8], seconds=r["seconds"]))
-        return out
-
-    def one(ell, M):
-        return reduce([s.sample(ell, M)])[0]
-
+    from nmlmc.distributed import sharded_mlmc_run
+    _, dev = dist
     t0 = time.perf_counter()
-    out = nm.mlmc_run_cb(one, targetTOL=EPS, M0=WORKLOAD["M0"], batched=False)
+    out = sharded_mlmc_run(s, device=dev, targetTOL=EPS, M0=WORKLOAD["M0"])
     return out, time.perf_counter() - t0
 
 

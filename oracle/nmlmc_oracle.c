@@ -130,9 +130,15 @@ struct o_ctx {
     int subsample, use_delta_cv, discount;
     /* CORE layout: persistent per-core streams */
     o_rs *rs_sync, *rs_inner;
-    /* OUTER layout: next outer index per level */
+    /* OUTER layout: next outer index per level, shard */
     uint64_t next_outer[64];
+    uint32_t shard_rank, shard_world;
 };
+
+void o_set_shard(o_ctx *c, uint32_t rank, uint32_t world) {
+    c->shard_rank = rank;
+    c->shard_world = world ? world : 1;
+}
 
 o_ctx *o_create(int prec, int streams, uint32_t cores, uint32_t N0, uint32_t beta,
                 double adaptive_r, int antithetic, int adaptive_incl_r2, uint64_t seed) {

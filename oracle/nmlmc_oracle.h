@@ -56,6 +56,9 @@ typedef struct o_ctx o_ctx;
 o_ctx *o_create(int prec, int streams, uint32_t cores, uint32_t N0, uint32_t beta,
                 double adaptive_r, int antithetic, int adaptive_incl_r2, uint64_t seed);
 void o_destroy(o_ctx *);
+/* OUTER layout sharding: each o_sample(ell, M) evaluates the rank's static share of the M outer
+ * samples with their single-device stream indices (the semantics of nmlmc_set_shard). */
+void o_set_shard(o_ctx *, uint32_t rank, uint32_t world);
 void o_set_model(o_ctx *, int kind, double tau, double max_loss);
 /* Portfolio of BS options (ComputeMethod::BS only).  start/delta_est are computed as
  * portfolio_comp_params does (portfolio_sampler.cpp:687-700) and returned. */

@@ -354,3 +354,18 @@ def synthetic_portfolio(Q: int, P: int, seed: int, prob: str = "uniform", S0=100
             pf[k] = pf[k][order]
         pf["prob"] = np.abs(pf["w"])
     return pf
+
+
+def _shard_bind():
+    L = lib()
+    if not getattr(L, "_shard_bound", False):
+        L.o_set_shard.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32]
+        L._shard_bound = True
+    return L
+
+
+def sampler_set_shard(s: "Sampler", rank: int, world: int):
+    _shard_bind().o_set_shard(s.h, rank, world)
+
+
+Sampler.set_shard = sampler_set_shard

@@ -1,0 +1,76 @@
+"""Multi-rank MLMC on CPU: two gloo ranks, each sampling its shard of every level call with the
+CPU oracle as the local sampler (the GPU sampler has the same set_shard / sample interface), the
+level results all-reduced (nmlmc.distributed.sharded_mlmc_run).  Both ranks must take exactly the
+decisions of a single-process run and end with the same estimate and level sums."""
+import os
+import socket
+import sys
+from datetime import timedelta
+
+import numpy as np
+
+from conftest import PKG, ROOT
+
+CFG = dict(N0=32, beta=2, r=1.5, seed=3, tol=4e-3, M0=256)
+
+
+class OracleShardSampler:
+    """CPU oracle on the OUTER layout, behind the nmlmc.Sampler interface used by the driver."""
+
+    def __init__(self):
+        import oracle as O
+        self.s = O.Sampler(O.PREC_FP64, O.STREAMS_OUTER, 1, CFG["N0"], CFG["beta"], CFG["r"],
+                           True, False, CFG["seed"])
+        self.s.set_model(O.MODEL_SHIFT, 0.0, 1.0)
+
+    def set_shard(self, rank, world):
+        self.s.set_shard(rank, world)
+
+    def sample(self, ell, M):
+        r = self.s.sample(ell, M)
+        return dict(fsums=r["fsums"], diffsums=r["diffsums"], work=r["work"], seconds=0.0)
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, q):
+    for p in (ROOT, PKG, os.path.join(ROOT, "oracle")):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import torch.distributed as dist
+    from nmlmc.distributed import sharded_mlmc_run
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    try:
+        out = sharded_mlmc_run(OracleShardSampler(), targetTOL=CFG["tol"], M0=CFG["M0"])
+        q.put((rank, [int(x) for x in out["level_M"]], out["Eg"], out["level_fsums"].tolist(),
+               out["level_diffsums"].tolist(), out["calls"]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_reproduce_single_process(nm):
+    import multiprocessing as mp
+    single = nm.mlmc_run_cb(OracleShardSampler().sample, targetTOL=CFG["tol"], M0=CFG["M0"])
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=300) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    res.sort()
+    for rank, level_M, Eg, fs, ds, calls in res:
+        assert level_M == [int(x) for x in single["level_M"]]
+        assert Eg == single["Eg"]
+        np.testing.assert_array_equal(np.array(fs), single["level_fsums"])
+        np.testing.assert_array_equal(np.array(ds), single["level_diffsums"])
+        assert calls == single["calls"]
