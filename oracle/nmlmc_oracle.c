@@ -128,6 +128,14 @@ struct o_ctx {
     o_opt *opt;
     double r, rho, s1_rho2, tau, prob_norm, compute_prob0;
     int subsample, use_delta_cv, discount;
+    /* compute methods (ComputeMethod BS / Exact / Unbiased): options are grouped by method,
+     * method m occupying [m_off[m], m_off[m] + m_n[m]); compute_prob[m] = sum of its probs */
+    uint32_t m_off[3], m_n[3];
+    double compute_prob[3];
+    int mixed;                  /* more than the BS method present */
+    int use_coarse_delta_cv, use_antithetic_risk, use_milstein;
+    uint32_t dt_h0inv, dt_beta;
+    double dt_prob_expo;
     /* CORE layout: persistent per-core streams */
     o_rs *rs_sync, *rs_inner;
     /* OUTER layout: next outer index per level, shard */
@@ -273,4 +281,23 @@ void o_portfolio_full_loss(o_ctx *c, uint32_t ell, uint64_t first, uint64_t n, d
 
 double o_norm_cdf_inv(double p, int prec) {
     return prec == O_PREC_REF32 ? (double)norm_cdf_inv_f32((float)p) : norm_cdf_inv_f64(p);
+}
+
+int o_set_portfolio_methods(o_ctx *c, uint32_t Q, const double *S0, const double *mu,
+                            const double *sigma, uint32_t P, const double *strike,
+                            const double *maturity, const double *w, const uint32_t *stock_ind,
+                            const int32_t *type, const double *prob, const int32_t *method,
+                            double r, double rho, double max_loss, double tau, int subsample,
+                            int use_delta_cv, int use_coarse_delta_cv, int use_antithetic_risk,
+                            int use_milstein, uint32_t dt_h0inv, uint32_t dt_beta,
+                            double dt_prob_expo) {
+    if (c->prec == O_PREC_REF32)
+        return set_portfolio_m_f32(c, Q, S0, mu, sigma, P, strike, maturity, w, stock_ind, type, prob,
+                                   method, r, rho, max_loss, tau, subsample, use_delta_cv, 1,
+                                   use_coarse_delta_cv, use_antithetic_risk, use_milstein, dt_h0inv,
+                                   dt_beta, dt_prob_expo, NULL, NULL);
+    return set_portfolio_m_f64(c, Q, S0, mu, sigma, P, strike, maturity, w, stock_ind, type, prob,
+                               method, r, rho, max_loss, tau, subsample, use_delta_cv, 1,
+                               use_coarse_delta_cv, use_antithetic_risk, use_milstein, dt_h0inv,
+                               dt_beta, dt_prob_expo, NULL, NULL);
 }

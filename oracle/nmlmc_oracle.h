@@ -67,6 +67,17 @@ int o_set_portfolio(o_ctx *, uint32_t Q, const double *S0, const double *mu, con
                     const uint32_t *stock_ind, const int32_t *type, const double *prob,
                     double r, double rho, double max_loss, double tau, int subsample,
                     int use_delta_cv, int discount, double *out_start, double *out_delta_est);
+/* Mixed compute methods (portfolio_sampler.cpp:17-22): method[j] = 0 BS, 1 Exact, 2 Unbiased.
+ * Options are grouped by method in the order given (prob non-increasing within a method), as
+ * portfolio::data.options[3] holds them.  CORE layout only. */
+int o_set_portfolio_methods(o_ctx *, uint32_t Q, const double *S0, const double *mu,
+                            const double *sigma, uint32_t P, const double *strike,
+                            const double *maturity, const double *w, const uint32_t *stock_ind,
+                            const int32_t *type, const double *prob, const int32_t *method,
+                            double r, double rho, double max_loss, double tau, int subsample,
+                            int use_delta_cv, int use_coarse_delta_cv, int use_antithetic_risk,
+                            int use_milstein, uint32_t dt_h0inv, uint32_t dt_beta,
+                            double dt_prob_expo);
 /* One sample(ell, M) call (nested_sampler.hpp:646-694).  trace (M records) and events may be
  * NULL.  Returns 0, or -1 if the events buffer is too small. */
 int o_sample(o_ctx *, uint32_t ell, uint64_t M, double fsums[4], double diffsums[4],

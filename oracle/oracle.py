@@ -165,6 +165,31 @@ class Sampler:
             raise ValueError("invalid portfolio (stock index, or prob not positive/non-increasing)")
         return start, delta
 
+    def set_portfolio_methods(self, pf: dict, method, r=0.05, rho=0.0, max_loss=0.0, tau=1 / 52,
+                              subsample=SUB_RANDOM, use_delta_cv=False, use_coarse_delta_cv=False,
+                              use_antithetic_risk=True, use_milstein=True, dt_h0inv=8, dt_beta=4,
+                              dt_prob_expo=-1.5):
+        """Mixed compute methods (0 BS, 1 Exact, 2 Unbiased); CORE layout only."""
+        L = _methods_bind()
+        Q = len(pf["S0"])
+        P = len(pf["strike"])
+        d = {k: np.ascontiguousarray(pf[k], np.float64) for k in
+             ("S0", "mu", "sigma", "strike", "maturity", "w", "prob")}
+        si = np.ascontiguousarray(pf["stock_ind"], np.uint32)
+        ty = np.ascontiguousarray(pf["type"], np.int32)
+        me = np.ascontiguousarray(method, np.int32)
+        rc = L.o_set_portfolio_methods(self.h, Q, _p(d["S0"], _dp), _p(d["mu"], _dp),
+                                       _p(d["sigma"], _dp), P, _p(d["strike"], _dp),
+                                       _p(d["maturity"], _dp), _p(d["w"], _dp), _p(si, _u32p),
+                                       _p(ty, _i32p), _p(d["prob"], _dp), _p(me, _i32p), r, rho,
+                                       max_loss, tau, subsample, int(use_delta_cv),
+                                       int(use_coarse_delta_cv), int(use_antithetic_risk),
+                                       int(use_milstein), dt_h0inv, dt_beta, dt_prob_expo)
+        if rc == -2:
+            raise ValueError("path-simulated compute methods need the CORE stream layout")
+        if rc != 0:
+            raise ValueError("invalid portfolio (stock index, or prob not positive/non-increasing)")
+
     def sample(self, ell: int, M: int, trace: bool = False, events_cap: int = 0):
         f = np.zeros(4)
         dd = np.zeros(4)
@@ -315,6 +340,34 @@ class Reference:
                                   _p(start, _dp), _p(delta, _dp))
         return start, delta
 
+    def portfolio_init_methods(self, pf, method, r=0.05, rho=0.0, max_loss=0.0, tau=1 / 52,
+                               subsample=SUB_RANDOM, use_delta_cv=False, use_coarse_delta_cv=False,
+                               use_antithetic_risk=True, use_milstein=True, dt_h0inv=8, dt_beta=4,
+                               dt_prob_expo=-1.5, seed=0, traced=True):
+        self.kind = "portfolio"
+        L = self.L
+        L.ref_portfolio_init_methods.argtypes = [
+            ctypes.c_uint32, _dp, _dp, _dp, ctypes.c_uint32, _dp, _dp, _dp, _u32p, _i32p, _dp,
+            _i32p, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+            ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint32,
+            ctypes.c_uint32, ctypes.c_double, ctypes.c_uint64, ctypes.c_int]
+        Q = len(pf["S0"])
+        P = len(pf["strike"])
+        self._pf = {k: np.ascontiguousarray(pf[k], np.float64) for k in
+                    ("S0", "mu", "sigma", "strike", "maturity", "w", "prob")}
+        d = self._pf
+        si = np.ascontiguousarray(pf["stock_ind"], np.uint32)
+        ty = np.ascontiguousarray(pf["type"], np.int32)
+        me = np.ascontiguousarray(method, np.int32)
+        self._keep = (si, ty, me)
+        L.ref_portfolio_init_methods(Q, _p(d["S0"], _dp), _p(d["mu"], _dp), _p(d["sigma"], _dp), P,
+                                     _p(d["strike"], _dp), _p(d["maturity"], _dp), _p(d["w"], _dp),
+                                     _p(si, _u32p), _p(ty, _i32p), _p(d["prob"], _dp),
+                                     _p(me, _i32p), r, rho, max_loss, tau, subsample,
+                                     int(use_delta_cv), int(use_coarse_delta_cv),
+                                     int(use_antithetic_risk), int(use_milstein), dt_h0inv,
+                                     dt_beta, dt_prob_expo, seed, int(traced))
+
     def sample(self, ell, M, events_cap=0):
         f = np.zeros(4)
         dd = np.zeros(4)
@@ -369,3 +422,16 @@ def sampler_set_shard(s: "Sampler", rank: int, world: int):
 
 
 Sampler.set_shard = sampler_set_shard
+
+
+def _methods_bind():
+    L = lib()
+    if not getattr(L, "_methods_bound", False):
+        L.o_set_portfolio_methods.restype = ctypes.c_int
+        L.o_set_portfolio_methods.argtypes = [
+            ctypes.c_void_p, ctypes.c_uint32, _dp, _dp, _dp, ctypes.c_uint32, _dp, _dp, _dp, _u32p,
+            _i32p, _dp, _i32p, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+            ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint32,
+            ctypes.c_uint32, ctypes.c_double]
+        L._methods_bound = True
+    return L

@@ -210,6 +210,53 @@ static std::vector<portfolio::option_params> g_opts;
 static std::vector<portfolio::stock_params> g_stocks;
 static bool g_port_traced = false;
 
+static std::vector<portfolio::option_params> g_opts_m[3];
+
+// Mixed compute methods: method[j] in {0 BS, 1 Exact, 2 Unbiased}; options keep their order
+// within a method (prob must be non-increasing within each method).  dt_* and the flags are the
+// portfolio::data fields of the path-simulated methods (portfolio_sampler.cpp:74-87).
+void ref_portfolio_init_methods(uint32_t Q, const double* S0, const double* mu, const double* sigma,
+                                uint32_t P, const double* strike, const double* maturity,
+                                const double* w, const uint32_t* stock_ind, const int32_t* type,
+                                const double* prob, const int32_t* method, double r, double rho,
+                                double max_loss, double tau, int subsample, int use_delta_cv,
+                                int use_coarse_delta_cv, int use_antithetic_risk, int use_milstein,
+                                uint32_t dt_h0inv, uint32_t dt_beta, double dt_prob_expo,
+                                uint64_t seed, int traced_run) {
+    g_stocks.resize(Q);
+    for (uint32_t i = 0; i < Q; i++) {
+        g_stocks[i].S0 = (real_t)S0[i]; g_stocks[i].mu = (real_t)mu[i]; g_stocks[i].sigma = (real_t)sigma[i];
+    }
+    for (int m = 0; m < 3; m++) g_opts_m[m].clear();
+    for (uint32_t j = 0; j < P; j++) {
+        portfolio::option_params o;
+        o.strike = (real_t)strike[j]; o.maturity = (real_t)maturity[j]; o.w = (real_t)w[j];
+        o.stock_ind = stock_ind[j];
+        o.type = type[j] > 0 ? portfolio::OptionType::Call : portfolio::OptionType::Put;
+        o.prob = (prob_t)prob[j]; o.W_est = 1; o.start = 0; o.delta_est = 0;
+        g_opts_m[method[j]].push_back(o);
+    }
+    portfolio::data& d = g_pdata;
+    for (int m = 0; m < 3; m++)
+        d.options[m] = portfolio::options_array::create(g_opts_m[m].empty() ? nullptr : g_opts_m[m].data(),
+                                                        g_opts_m[m].size());
+    d.stocks = portfolio::stocks_array::create(g_stocks.data(), Q);
+    d.r = (real_t)r; d.rho = (real_t)rho; d.s1_rho2 = std::sqrt(1 - POW2(d.rho));
+    d.max_loss = (real_t)max_loss; d.tau = (real_t)tau;
+    d.dt_h0inv = dt_h0inv; d.dt_beta = dt_beta; d.dt_prob_expo = (real_t)dt_prob_expo;
+    d.phi_type = portfolio::PhiType::Indicator; d._phi_size = 1;
+    d.subsample = (portfolio::Subsampling)subsample;
+    d.use_delta_cv = use_delta_cv != 0; d.use_coarse_delta_cv = use_coarse_delta_cv != 0;
+    d.use_antithetic_risk = use_antithetic_risk != 0; d.use_milstein = use_milstein != 0;
+    portfolio::portfolio_comp_params(&d);
+    portfolio::portfolio_update_data(&d);
+    g_port_traced = traced_run != 0;
+    if (g_port_traced)
+        init_samplers<traced<portfolio::sampler>>(seed, portfolio::sampler::GetWorkspaceSize(d));
+    else
+        init_samplers<portfolio::sampler>(seed, portfolio::sampler::GetWorkspaceSize(d));
+}
+
 void ref_portfolio_init(uint32_t Q, const double* S0, const double* mu, const double* sigma,
                         uint32_t P, const double* strike, const double* maturity, const double* w,
                         const uint32_t* stock_ind, const int32_t* type, const double* prob,

@@ -40,6 +40,13 @@ def engine_cases():
     pf_w = dict(Q=3, P=50, seed=5, prob="w")
     pf_1 = dict(Q=1, P=20, seed=7, prob="uniform")
     pf_n = dict(Q=5, P=40, seed=9, prob="w")
+    pf_m = dict(Q=3, P=24, seed=21, prob="w")
+    pf_m2 = dict(Q=2, P=12, seed=22, prob="uniform")
+    pf_m3 = dict(Q=2, P=6, seed=23, prob="w")
+    g = np.random.default_rng(2024)
+    methods_m = [int(x) for x in g.integers(0, 3, 24)]
+    methods_m2 = [int(x) for x in g.integers(0, 3, 12)]
+    methods_m3 = [0, 1, 2, 1, 2, 0]
     return [
         dict(name="A_refmodel_b4_r15", kind="model", model=0, tau=TAU, max_loss=ml, cores=3, N0=32,
              beta=4, r=1.5, anti=True, seed=0, calls=[(0, 40), (1, 40), (2, 30), (3, 20), (1, 17)]),
@@ -64,6 +71,19 @@ def engine_cases():
         dict(name="I_pf_none", kind="portfolio", pf=pf_n, sub=O.SUB_NONE, cv=False, rho=0.3,
              max_loss=0.4, cores=3, N0=32, beta=4, r=1.5, anti=True, seed=5,
              calls=[(0, 10), (1, 10), (2, 10)]),
+        # mixed compute methods (0 BS, 1 Exact, 2 Unbiased): path-simulated inner samples
+        dict(name="J_pf_methods_cdf_cv", kind="portfolio", pf=pf_m, methods=methods_m,
+             sub=O.SUB_RANDOM, cv=True, rho=0.2, max_loss=0.3, cores=3, N0=32, beta=4, r=1.5,
+             anti=True, seed=6, anti_risk=True, milstein=True, coarse_cv=False,
+             calls=[(0, 16), (1, 16), (2, 12)]),
+        dict(name="K_pf_methods_euler", kind="portfolio", pf=pf_m2, methods=methods_m2,
+             sub=O.SUB_UNIFORM, cv=True, rho=0.0, max_loss=0.2, cores=2, N0=32, beta=2, r=1.5,
+             anti=True, seed=8, anti_risk=False, milstein=False, coarse_cv=True, lzcnt=True,
+             calls=[(0, 12), (2, 12), (3, 8)]),
+        dict(name="L_pf_methods_none", kind="portfolio", pf=pf_m3, methods=methods_m3,
+             sub=O.SUB_NONE, cv=True, rho=0.3, max_loss=0.4, cores=3, N0=32, beta=4, r=1.5,
+             anti=True, seed=9, anti_risk=True, milstein=True, coarse_cv=True,
+             calls=[(0, 6), (1, 6)]),
     ]
 
 
@@ -75,12 +95,24 @@ def run_engine_case(case: dict, variant: str, arrays: dict) -> dict:
         ref.model_init(case["model"], case["tau"], case["max_loss"], case["seed"], traced=True)
     else:
         pf = O.synthetic_portfolio(**case["pf"])
+        if "methods" in case:
+            ref.portfolio_init_methods(pf, case["methods"], r=0.05, rho=case["rho"],
+                                       max_loss=case["max_loss"], tau=1 / 52,
+                                       subsample=case["sub"], use_delta_cv=case["cv"],
+                                       use_coarse_delta_cv=case["coarse_cv"],
+                                       use_antithetic_risk=case["anti_risk"],
+                                       use_milstein=case["milstein"], seed=case["seed"], traced=True)
+            return _record_calls(case, variant, ref, arrays, out)
         start, delta = ref.portfolio_init(pf, r=0.05, rho=case["rho"], max_loss=case["max_loss"],
                                           tau=1 / 52, subsample=case["sub"], use_delta_cv=case["cv"],
                                           seed=case["seed"], traced=True)
         key = f"{case['name']}/{variant}"
         arrays[key + "/start"] = start
         arrays[key + "/delta_est"] = delta
+    return _record_calls(case, variant, ref, arrays, out)
+
+
+def _record_calls(case: dict, variant: str, ref, arrays: dict, out: dict) -> dict:
     for i, (ell, M) in enumerate(case["calls"]):
         r = ref.sample(ell, M, events_cap=2_000_000)
         key = f"{case['name']}/{variant}/{i}"

@@ -53,6 +53,13 @@ def make_oracle_case(case, prec, streams=O.STREAMS_CORE, cores=None):
         s.set_model(case["model"], case["tau"], case["max_loss"])
     else:
         pf = O.synthetic_portfolio(**case["pf"])
+        if "methods" in case:
+            s.set_portfolio_methods(pf, case["methods"], r=0.05, rho=case["rho"],
+                                    max_loss=case["max_loss"], tau=1 / 52, subsample=case["sub"],
+                                    use_delta_cv=case["cv"], use_coarse_delta_cv=case["coarse_cv"],
+                                    use_antithetic_risk=case["anti_risk"],
+                                    use_milstein=case["milstein"])
+            return s, None, None
         start, delta = s.set_portfolio(pf, r=0.05, rho=case["rho"], max_loss=case["max_loss"],
                                        tau=1 / 52, subsample=case["sub"], use_delta_cv=case["cv"])
     return s, start, delta
@@ -132,3 +139,33 @@ def test_live_reference_random_case():
         np.testing.assert_array_equal(a["events"][1], b["events"][1])
         np.testing.assert_array_equal(a["fsums"], b["fsums"])
         np.testing.assert_array_equal(a["diffsums"], b["diffsums"])
+
+
+def test_methods_need_core_layout():
+    """Path-simulated compute methods are defined on the reference's CORE streams only."""
+    s = O.Sampler(O.PREC_FP64, O.STREAMS_OUTER, 1, 32, 4, 1.5, True, False, 1)
+    pf = O.synthetic_portfolio(2, 4, 1)
+    with pytest.raises(ValueError):
+        s.set_portfolio_methods(pf, [0, 1, 2, 0])
+    s2 = O.Sampler(O.PREC_FP64, O.STREAMS_OUTER, 1, 32, 4, 1.5, True, False, 1)
+    s2.set_portfolio_methods(pf, [0, 0, 0, 0])      # all BS: the OUTER layout applies
+
+
+@pytest.mark.skipif(not O.ref_available("f64_lzcnt"), reason="oracle/_ref not built on this host")
+def test_live_reference_methods_case():
+    """Where the reference is compiled here: a random mixed-method portfolio, oracle vs reference."""
+    rng = np.random.default_rng(78)
+    pf = O.synthetic_portfolio(3, 15, 31, prob="w")
+    meth = rng.integers(0, 3, 15).astype(np.int32)
+    ref = O.Reference("f64_lzcnt")
+    ref.init(2, 32, 2, 1.5, True)
+    ref.portfolio_init_methods(pf, meth, rho=0.1, max_loss=0.2, use_delta_cv=True, seed=44)
+    s = O.Sampler(O.PREC_FP64, O.STREAMS_CORE, 2, 32, 2, 1.5, True, False, 44)
+    s.set_portfolio_methods(pf, meth, rho=0.1, max_loss=0.2, use_delta_cv=True)
+    for ell in (0, 2, 1):
+        a = ref.sample(ell, 10, events_cap=500000)
+        b = s.sample(ell, 10, events_cap=500000)
+        assert a["events"][0] == b["events"][0]
+        np.testing.assert_array_equal(a["events"][1], b["events"][1])
+        np.testing.assert_array_equal(a["fsums"], b["fsums"])
+        assert a["work"] == b["work"]
