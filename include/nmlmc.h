@@ -32,8 +32,14 @@ enum {
     NMLMC_ERR_CUDA = 2,       /* a CUDA runtime call failed                                */
     NMLMC_ERR_STATE = 3,      /* call out of order (no model / portfolio set, no context) */
     NMLMC_ERR_NOMEM = 4,      /* device or host allocation failed                          */
-    NMLMC_ERR_TIMEOUT = 5     /* a bounded device wait gave up                             */
+    NMLMC_ERR_TIMEOUT = 5,    /* a bounded device wait gave up                             */
+    NMLMC_ERR_LIMIT = 6       /* a path-simulated inner sample drew a level whose step count
+                                 h0 beta^L exceeds NMLMC_MAX_PATH_STEPS (the call stops)   */
 };
+
+/* Time steps one Unbiased-method inner sample may take (P(L) ~ beta^(e L): at h0 = 8,
+ * beta = 4, e = -1.5 a draw above the limit has probability about 1e-10). */
+#define NMLMC_MAX_PATH_STEPS (1ull << 24)
 
 enum { NMLMC_PREC_REF32 = 0, NMLMC_PREC_FP64 = 1, NMLMC_PREC_FP32 = 2 };
 enum { NMLMC_STREAMS_CORE = 0, NMLMC_STREAMS_OUTER = 1 };
@@ -115,8 +121,9 @@ void model_init(const model_data* data, uint64_t seed);
 void model_sample(uint32_t ell, uint64_t M, sample_output* out);
 
 /* portfolio_update_data / portfolio_init / portfolio_sample / portfolio_cleanup /
- * portfolio_comp_params (portfolio_sampler.cpp:618-756).  Options of ComputeMethod::BS only
- * (options[1] and options[2] must be empty): the Exact / Unbiased methods are not on this path. */
+ * portfolio_comp_params (portfolio_sampler.cpp:618-756).  options[0..2] hold the BS, Exact and
+ * Unbiased options (portfolio_sampler.cpp:17-22); Exact / Unbiased options are sampled on the
+ * CORE streams (the reference-surface default). */
 void portfolio_update_data(const portfolio_data* data);
 void portfolio_init(const portfolio_data* data, uint64_t seed);
 void portfolio_sample(uint32_t ell, uint64_t override_dyn_inner, uint64_t M, sample_output* out);
@@ -208,6 +215,19 @@ int nmlmc_configure(nmlmc_ctx* ctx, const nmlmc_config* cfg);
 int nmlmc_set_model(nmlmc_ctx* ctx, int32_t kind, double tau, double max_loss);
 int nmlmc_set_portfolio(nmlmc_ctx* ctx, const nmlmc_portfolio* pf, double* out_start,
                         double* out_delta_est);
+/* Path-simulated inner values (portfolio_sampler.cpp:74-87, 470-604; gbm_approx.hpp:18-57):
+ * method[j] = 0 BS, 1 Exact (exact GBM from tau to maturity), 2 Unbiased (randomised
+ * Milstein / Euler level L, P(L) proportional to dt_beta^(dt_prob_expo L), h0 dt_beta^L steps).
+ * Options are grouped by method in the caller's order; prob must be non-increasing within each
+ * method.  Sampling with Exact / Unbiased options needs the CORE stream layout. */
+typedef struct nmlmc_path_methods {
+    const int32_t* method;                /* [P]                                             */
+    uint32_t dt_h0inv, dt_beta;           /* h0 = 1 / dt_h0inv steps at L = 0; beta >= 2     */
+    double dt_prob_expo;                  /* < 0                                             */
+    int32_t use_coarse_delta_cv, use_antithetic_risk, use_milstein;
+} nmlmc_path_methods;
+int nmlmc_set_portfolio_methods(nmlmc_ctx* ctx, const nmlmc_portfolio* pf, const nmlmc_path_methods* pm,
+                                double* out_start, double* out_delta_est);
 /* Restart every stream (CORE: random_state(seed, core) from counter 0; OUTER: outer indices
  * from 0). */
 int nmlmc_reset_streams(nmlmc_ctx* ctx);

@@ -96,6 +96,14 @@ struct HostPortfolio {
     int subsample = SUB_UNIFORM, use_delta_cv = 0, discount = 1;
     bool s1_rho2_given = false;
     bool own_params = false;   // start / delta_est computed here (native API), per precision
+    // compute methods: options are stored grouped by method (BS, Exact, Unbiased) in the order
+    // given; m_n counts them, order[k] is the caller's index of stored option k
+    uint32_t m_n[3] = {0, 0, 0};
+    std::vector<uint32_t> order;
+    uint32_t dt_h0inv = 8, dt_beta = 4;
+    double dt_prob_expo = -1.5;
+    int use_coarse_delta_cv = 0, use_antithetic_risk = 1, use_milstein = 1;
+    bool mixed() const { return m_n[1] + m_n[2] > 0; }
 };
 
 template <class RT>
@@ -225,16 +233,19 @@ int build_dev_portfolio(nmlmc_ctx* c, DevPortfolio<RT>& d) {
     std::vector<RT> K = narrow<RT>(h.strike), T = narrow<RT>(h.maturity), w = narrow<RT>(h.w);
     std::vector<RT> prob = narrow<RT>(h.prob), West = narrow<RT>(h.W_est);
     std::vector<RT> start(P), cdf(P), delta(Q, (RT)0);
-    RT prob_norm = 0, cp0 = 0, acc = 0;
+    RT prob_norm = 0, acc = 0, cprob[3] = {0, 0, 0};
+    uint32_t m_off[3] = {0, h.m_n[0], h.m_n[0] + h.m_n[1]};
     for (uint32_t j = 0; j < P; j++) {
         const uint32_t s = h.stock_ind[j];
+        const uint32_t m = j < m_off[1] ? 0 : (j < m_off[2] ? 1 : 2);
+        if (j == m_off[m]) acc = 0;                      // the CDF restarts for every method
         RT st = (RT)h.start[j], de = (RT)h.delta_est[j];
         start[j] = st;
         cdf[j] = acc;
         acc += prob[j];
         delta[s] += w[j] * de;
         prob_norm += prob[j];
-        cp0 += prob[j];
+        cprob[m] += prob[j];
     }
     int rc;
     if ((rc = upload(d.strike, K)) || (rc = upload(d.maturity, T)) || (rc = upload(d.start, start)) ||
@@ -252,16 +263,21 @@ int build_dev_portfolio(nmlmc_ctx* c, DevPortfolio<RT>& d) {
     t.s1_rho2 = h.s1_rho2_given ? (RT)h.s1_rho2 : h_sqrt<RT>(1 - (RT)h.rho * (RT)h.rho);
     t.max_loss = (RT)h.max_loss; t.tau = (RT)h.tau;
     t.stau = h_sqrt<RT>((RT)h.tau);                      // data_ex ctor, portfolio_sampler.cpp:97-98
-    t.prob_norm = prob_norm; t.compute_prob0 = cp0;
+    t.prob_norm = prob_norm; t.compute_prob0 = cprob[0];
     t.inv_count_prob = (RT)(1. / (double)P);              // portfolio_sampler.cpp:360
     t.subsample = h.subsample; t.use_delta_cv = h.use_delta_cv; t.discount = h.discount;
+    for (int m = 0; m < 3; m++) { t.m_off[m] = m_off[m]; t.m_n[m] = h.m_n[m]; t.compute_prob[m] = cprob[m]; }
+    t.mixed = h.mixed() ? 1 : 0;
+    t.dt_h0inv = h.dt_h0inv; t.dt_beta = h.dt_beta; t.dt_prob_expo = (RT)h.dt_prob_expo;
+    t.use_coarse_delta_cv = h.use_coarse_delta_cv; t.use_antithetic_risk = h.use_antithetic_risk;
+    t.use_milstein = h.use_milstein;
     t.fast = nullptr;
     if constexpr (sizeof(RT) == 4) {
         // packed FP32 records (nmlmc_bs.cuh): per-option constants folded in double, rounded once;
         // only for unit work estimates (every option of the BS method costs one evaluation)
         bool unit = true;
         for (uint32_t j = 0; j < P; j++) unit = unit && h.W_est[j] == 1.0;
-        if (unit) {
+        if (unit && !h.mixed()) {
             std::vector<FastOption> fo(P);
             const double disc = h.discount ? exp(-h.r * h.tau) : 1.0;
             for (uint32_t j = 0; j < P; j++) {
@@ -428,6 +444,7 @@ int sample_core(nmlmc_ctx* c, uint32_t ell, uint64_t M, nmlmc_level_result* out)
     memcpy(out->inner_stats, c->h_pin + 16, 6 * sizeof(uint64_t));
     out->seconds = ms * 1e-3;
     c->trace_host = nullptr;
+    if (c->h_pin[9] != 0) return set_err(NMLMC_ERR_LIMIT);   // a sample exceeded kMaxPathSteps
     return NMLMC_OK;
 }
 
@@ -525,6 +542,7 @@ const char* nmlmc_error_string(int s) {
     case NMLMC_ERR_STATE: return "call out of order";
     case NMLMC_ERR_NOMEM: return "out of memory";
     case NMLMC_ERR_TIMEOUT: return "bounded device wait gave up";
+    case NMLMC_ERR_LIMIT: return "a path-simulated inner sample exceeded NMLMC_MAX_PATH_STEPS";
     default: return "unknown status";
     }
 }
@@ -627,13 +645,17 @@ int nmlmc_set_model(nmlmc_ctx* c, int32_t kind, double tau, double max_loss) {
     return NMLMC_OK;
 }
 
-int nmlmc_set_portfolio(nmlmc_ctx* c, const nmlmc_portfolio* p, double* out_start, double* out_delta) {
+static int set_portfolio_impl(nmlmc_ctx* c, const nmlmc_portfolio* p, const nmlmc_path_methods* pm,
+                              double* out_start, double* out_delta) {
     if (!c || !p || !c->configured) return set_err(!c || !p ? NMLMC_ERR_ARG : NMLMC_ERR_STATE);
     if (p->Q == 0 || p->P == 0 || !p->S0 || !p->mu || !p->sigma || !p->strike || !p->maturity || !p->w ||
         !p->stock_ind || !p->type)
         return set_err(NMLMC_ERR_ARG);
     if (p->subsample != NMLMC_SUB_NONE && p->subsample != NMLMC_SUB_RANDOM && p->subsample != NMLMC_SUB_UNIFORM)
         return set_err(NMLMC_ERR_ARG);
+    const int32_t* method = pm ? pm->method : nullptr;
+    if (pm && (pm->dt_h0inv == 0 || pm->dt_beta < 2 || !(pm->dt_prob_expo < 0)))
+        return set_err(NMLMC_ERR_ARG);                     // portfolio_sampler.cpp:525
     HostPortfolio& h = c->pf;
     h = HostPortfolio{};
     h.Q = p->Q;
@@ -641,35 +663,62 @@ int nmlmc_set_portfolio(nmlmc_ctx* c, const nmlmc_portfolio* p, double* out_star
     h.S0.assign(p->S0, p->S0 + p->Q);
     h.mu.assign(p->mu, p->mu + p->Q);
     h.sigma.assign(p->sigma, p->sigma + p->Q);
-    h.strike.assign(p->strike, p->strike + p->P);
-    h.maturity.assign(p->maturity, p->maturity + p->P);
-    h.w.assign(p->w, p->w + p->P);
-    h.prob.assign(p->P, 1.0);
-    if (p->prob) h.prob.assign(p->prob, p->prob + p->P);
+    // stored order: grouped by compute method, the caller's order within a method
+    for (int m = 0; m < 3; m++)
+        for (uint32_t j = 0; j < p->P; j++) {
+            const int32_t mj = method ? method[j] : 0;
+            if (mj < 0 || mj > 2) return set_err(NMLMC_ERR_ARG);
+            if (mj == m) { h.order.push_back(j); h.m_n[m]++; }
+        }
+    const bool f32 = c->cfg.precision != NMLMC_PREC_FP64;
+    double prev = INFINITY;
+    h.type.resize(p->P);
+    for (uint32_t k = 0; k < p->P; k++) {
+        const uint32_t j = h.order[k];
+        if (k == h.m_n[0] || k == h.m_n[0] + h.m_n[1]) prev = INFINITY;
+        if (p->stock_ind[j] >= p->Q || (p->type[j] != 1 && p->type[j] != -1)) return set_err(NMLMC_ERR_ARG);
+        const double pj = p->prob ? p->prob[j] : 1.0;
+        const double pr = f32 ? (double)(float)pj : pj;
+        if (!(pr > 0) || !(prev >= pr)) return set_err(NMLMC_ERR_ARG);   // portfolio_sampler.cpp:654
+        prev = pr;
+        h.strike.push_back(p->strike[j]);
+        h.maturity.push_back(p->maturity[j]);
+        h.w.push_back(p->w[j]);
+        h.prob.push_back(pj);
+        h.stock_ind.push_back(p->stock_ind[j]);
+        h.type[k] = (int8_t)p->type[j];
+    }
     h.W_est.assign(p->P, 1.0);
     h.start.assign(p->P, 0.0);
     h.delta_est.assign(p->P, 0.0);
-    h.stock_ind.assign(p->stock_ind, p->stock_ind + p->P);
-    h.type.resize(p->P);
-    const bool f32 = c->cfg.precision != NMLMC_PREC_FP64;
-    double prev = INFINITY;
-    for (uint32_t j = 0; j < p->P; j++) {
-        if (h.stock_ind[j] >= p->Q || (p->type[j] != 1 && p->type[j] != -1)) return set_err(NMLMC_ERR_ARG);
-        double pr = f32 ? (double)(float)h.prob[j] : h.prob[j];
-        if (!(pr > 0) || !(prev >= pr)) return set_err(NMLMC_ERR_ARG);   // portfolio_sampler.cpp:654
-        prev = pr;
-        h.type[j] = (int8_t)p->type[j];
-    }
     h.r = p->r; h.rho = p->rho; h.max_loss = p->max_loss; h.tau = p->tau;
     h.subsample = p->subsample; h.use_delta_cv = p->use_delta_cv; h.discount = p->discount;
+    if (pm) {
+        h.dt_h0inv = pm->dt_h0inv; h.dt_beta = pm->dt_beta; h.dt_prob_expo = pm->dt_prob_expo;
+        h.use_coarse_delta_cv = pm->use_coarse_delta_cv != 0;
+        h.use_antithetic_risk = pm->use_antithetic_risk != 0;
+        h.use_milstein = pm->use_milstein != 0;
+    }
     h.own_params = true;
     if (f32) comp_params<float>(h); else comp_params<double>(h);
-    if (out_start) memcpy(out_start, h.start.data(), p->P * sizeof(double));
-    if (out_delta) memcpy(out_delta, h.delta_est.data(), p->P * sizeof(double));
+    for (uint32_t k = 0; k < p->P; k++) {
+        if (out_start) out_start[h.order[k]] = h.start[k];
+        if (out_delta) out_delta[h.order[k]] = h.delta_est[k];
+    }
     c->kind = KIND_PORTFOLIO;
     c->pf_prec = -1;
     cudaSetDevice(c->device);
     return ensure_portfolio(c);
+}
+
+int nmlmc_set_portfolio(nmlmc_ctx* c, const nmlmc_portfolio* p, double* out_start, double* out_delta) {
+    return set_portfolio_impl(c, p, nullptr, out_start, out_delta);
+}
+
+int nmlmc_set_portfolio_methods(nmlmc_ctx* c, const nmlmc_portfolio* p, const nmlmc_path_methods* pm,
+                                double* out_start, double* out_delta) {
+    if (!pm) return set_err(NMLMC_ERR_ARG);
+    return set_portfolio_impl(c, p, pm, out_start, out_delta);
 }
 
 int nmlmc_set_trace(nmlmc_ctx* c, nmlmc_trace_rec* host_buf, uint64_t cap) {
@@ -692,6 +741,8 @@ int nmlmc_sample(nmlmc_ctx* c, uint32_t ell, uint64_t M, nmlmc_level_result* out
     cudaSetDevice(c->device);
     int rc = ensure_portfolio(c);
     if (rc) return rc;
+    // path-simulated compute methods are defined on the reference's CORE streams only
+    if (c->kind == KIND_PORTFOLIO && c->pf.mixed() && k.streams != NMLMC_STREAMS_CORE) return set_err(NMLMC_ERR_ARG);
     if ((rc = ensure_trace(c, M))) return rc;
     const bool f64 = k.precision == NMLMC_PREC_FP64;
     if (k.streams == NMLMC_STREAMS_CORE) {
@@ -877,31 +928,47 @@ void model_sample(uint32_t ell, uint64_t M, sample_output* out) {
 }
 
 static int portfolio_from_ref(const portfolio_data* d) {
-    if (d->options[1].size || d->options[2].size) return NMLMC_ERR_ARG;   // BS options only
     if (d->phi_type != 0) return NMLMC_ERR_ARG;                          // Indicator only
-    const nmlmc_options_span& o = d->options[0];
     const nmlmc_stocks_span& s = d->stocks;
-    if (!o.size || !s.size || !o.data || !s.data) return NMLMC_ERR_ARG;
+    size_t P = 0;
+    for (int m = 0; m < 3; m++) {
+        if (d->options[m].size && !d->options[m].data) return NMLMC_ERR_ARG;
+        P += d->options[m].size;
+    }
+    if (!P || !s.size || !s.data) return NMLMC_ERR_ARG;
+    if (d->options[1].size + d->options[2].size &&
+        (d->dt_h0inv == 0 || d->dt_beta < 2 || !(d->dt_prob_expo < 0)))
+        return NMLMC_ERR_ARG;                                            // portfolio_sampler.cpp:525
     HostPortfolio& h = g_ctx->pf;
     h = HostPortfolio{};
     h.Q = (uint32_t)s.size;
-    h.P = (uint32_t)o.size;
+    h.P = (uint32_t)P;
     for (size_t i = 0; i < s.size; i++) {
         h.S0.push_back(s.data[i].S0); h.mu.push_back(s.data[i].mu); h.sigma.push_back(s.data[i].sigma);
     }
-    float prev = INFINITY;
-    for (size_t j = 0; j < o.size; j++) {
-        const option_params& op = o.data[j];
-        if (op.stock_ind >= s.size || !(op.prob > 0) || !(prev >= op.prob)) return NMLMC_ERR_ARG;
-        prev = op.prob;
-        h.strike.push_back(op.strike); h.maturity.push_back(op.maturity); h.w.push_back(op.w);
-        h.prob.push_back(op.prob); h.W_est.push_back(op.W_est); h.start.push_back(op.start);
-        h.delta_est.push_back(op.delta_est); h.stock_ind.push_back(op.stock_ind);
-        h.type.push_back((int8_t)(op.type > 0 ? 1 : -1));
+    // options[m] in order, as portfolio_update_data stores them (portfolio_sampler.cpp:647-668)
+    for (int m = 0; m < 3; m++) {
+        const nmlmc_options_span& o = d->options[m];
+        float prev = INFINITY;
+        for (size_t j = 0; j < o.size; j++) {
+            const option_params& op = o.data[j];
+            if (op.stock_ind >= s.size || !(op.prob > 0) || !(prev >= op.prob)) return NMLMC_ERR_ARG;
+            prev = op.prob;
+            h.strike.push_back(op.strike); h.maturity.push_back(op.maturity); h.w.push_back(op.w);
+            h.prob.push_back(op.prob); h.W_est.push_back(op.W_est); h.start.push_back(op.start);
+            h.delta_est.push_back(op.delta_est); h.stock_ind.push_back(op.stock_ind);
+            h.type.push_back((int8_t)(op.type > 0 ? 1 : -1));
+            h.order.push_back((uint32_t)h.order.size());
+        }
+        h.m_n[m] = (uint32_t)o.size;
     }
     h.r = d->r; h.rho = d->rho; h.s1_rho2 = d->s1_rho2; h.s1_rho2_given = true;
     h.max_loss = d->max_loss; h.tau = d->tau;
     h.subsample = d->subsample; h.use_delta_cv = d->use_delta_cv ? 1 : 0; h.discount = 1;
+    h.dt_h0inv = d->dt_h0inv; h.dt_beta = d->dt_beta; h.dt_prob_expo = d->dt_prob_expo;
+    h.use_coarse_delta_cv = d->use_coarse_delta_cv ? 1 : 0;
+    h.use_antithetic_risk = d->use_antithetic_risk ? 1 : 0;
+    h.use_milstein = d->use_milstein ? 1 : 0;
     g_ctx->kind = KIND_PORTFOLIO;
     g_ctx->pf_prec = -1;
     return ensure_portfolio(g_ctx);

@@ -30,7 +30,15 @@ struct CountParams {
 enum Kind : int { KIND_REF_MODEL = 0, KIND_SHIFT_MODEL = 1, KIND_PORTFOLIO = 2 };
 enum Sub : int { SUB_NONE = 0, SUB_RANDOM = 1, SUB_UNIFORM = -1 };
 
-// Option table in HBM, structure of arrays (one entry per option, ComputeMethod::BS).
+enum Method : int { METHOD_BS = 0, METHOD_EXACT = 1, METHOD_UNBIASED = 2 };
+
+// Time steps one path-simulated inner sample may take (h0 beta^L of the Unbiased method); a
+// draw above it stops the call with NMLMC_ERR_LIMIT instead of running unbounded.
+constexpr uint64_t kMaxPathSteps = 1ull << 24;
+
+// Option table in HBM, structure of arrays.  Options are grouped by compute method
+// (portfolio::data::options[3], portfolio_sampler.cpp:62-92): method m occupies
+// [m_off[m], m_off[m] + m_n[m]) and its CDF restarts at 0.
 template <class RT>
 struct OptionTable {
     const RT* strike;
@@ -51,6 +59,13 @@ struct OptionTable {
     uint32_t P, Q;
     RT r, rho, s1_rho2, max_loss, tau, stau, prob_norm, compute_prob0, inv_count_prob;
     int subsample, use_delta_cv, discount;
+    // compute methods and the path-simulated inner values (portfolio_sampler.cpp:74-87)
+    uint32_t m_off[3], m_n[3];
+    RT compute_prob[3];
+    int mixed;                       // an Exact or Unbiased option is present
+    uint32_t dt_h0inv, dt_beta;
+    RT dt_prob_expo;
+    int use_coarse_delta_cv, use_antithetic_risk, use_milstein;
 };
 
 template <class RT>

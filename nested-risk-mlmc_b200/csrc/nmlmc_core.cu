@@ -109,6 +109,7 @@ struct CoreCtx {
     CoreStream sync, inner;     // warp-uniform copies
     RT* Rt;                     // portfolio: per-warp R_tau in shared memory
     RT Y, constant;
+    int err;                    // a path-simulated sample exceeded kMaxPathSteps
 };
 
 template <class RT>
@@ -130,6 +131,218 @@ __device__ __forceinline__ RT portfolio_bs_value(const OptionTable<RT>& ot, cons
     return xadd(val, cv);
 }
 
+template <class RT>
+__device__ __forceinline__ RT u01_rt(uint64_t w) {
+    if constexpr (sizeof(RT) == 4) return u01_f(w); else return u01_d(w);
+}
+
+// ---- path-simulated inner values (portfolio_sampler.cpp:212-225, 470-604; gbm_approx.hpp) ----
+
+// Normals of one inner sample, drawn in order from the inner CORE stream: a pending second
+// normal of an earlier pair when `have`, then fresh pairs from word position w.
+template <class RT>
+struct SeqNormals {
+    TfKey key;
+    uint64_t w;
+    bool have;
+    RT y;
+    __device__ __forceinline__ RT next() {
+        if (have) {
+            have = false;
+            return y;
+        }
+        RT x;
+        core_pair<RT>(key, w, x, y);
+        w += 2;
+        have = true;
+        return x;
+    }
+};
+
+template <class RT>
+__device__ __forceinline__ RT opt_diff_stock(const OptionTable<RT>& ot, uint32_t j, RT S0_T, RT St_T) {
+    // option_diff_from_stock (portfolio_sampler.cpp:212-219)
+    const RT mod = (RT)ot.type[j], K = ot.strike[j];
+    const RT a = xmul(mod, xsub(S0_T, K)), b = xmul(mod, xsub(St_T, K));
+    const RT start = a > (RT)0 ? a : (RT)0, finish = b > (RT)0 ? b : (RT)0;
+    return xmul(xmul(ot.w[j], xexp(xmul(-ot.r, ot.maturity[j]))), xsub(start, finish));
+}
+
+template <class RT>
+__device__ __forceinline__ RT opt_derv_stock(const OptionTable<RT>& ot, uint32_t j, RT St_T, RT S0) {
+    // option_derv_from_stock (portfolio_sampler.cpp:221-225)
+    const RT df = (RT)((ot.type[j] == 1 ? 1 : 0) - (St_T < ot.strike[j] ? 1 : 0));
+    return xmul(xmul(xmul(ot.w[j], xdiv(St_T, S0)), xexp(xmul(-ot.r, ot.maturity[j]))), df);
+}
+
+// simulate_stock_dt<with_coarse> (gbm_approx.hpp:18-57) on the three paths S[0..3) of
+// sample_inner_approx, plus (with_coarse) the coupled coarse paths S[3..6) stepping every
+// coarse_step fine steps on the summed increments.  States in double, increments in real_t.
+template <class RT>
+__device__ void stock_dt(SeqNormals<RT>& nz, double* S, uint64_t N, RT mu, RT sigma, RT t, bool milstein,
+                         bool with_coarse, uint32_t coarse_step) {
+    const RT dt = xdiv(t, (RT)N);
+    const RT sqrt_dt = xsqrt(dt);
+    const RT dt_c = xdiv(t, (RT)(N / coarse_step));
+    const double hs2 = __dmul_rn(0.5, (double)xmul(sigma, sigma));
+    const RT mudt = xmul(mu, dt), mudt_c = xmul(mu, dt_c);
+    RT dW_c = (RT)0;
+    for (uint64_t n = 0; n < N; n++) {
+        const RT dW = xmul(sqrt_dt, nz.next());
+        const RT m = milstein ? to_rt<RT>(__dmul_rn(hs2, (double)xsub(xmul(dW, dW), dt))) : (RT)0;
+        const double inc = (double)xadd(xadd(mudt, xmul(sigma, dW)), m);
+#pragma unroll
+        for (int i = 0; i < 3; i++) S[i] = __dadd_rn(S[i], __dmul_rn(S[i], inc));
+        if (with_coarse) {
+            dW_c = xadd(dW_c, dW);
+            if ((n + 1) % coarse_step == 0) {
+                const RT mc = milstein ? to_rt<RT>(__dmul_rn(hs2, (double)xsub(xmul(dW_c, dW_c), dt_c))) : (RT)0;
+                const double incc = (double)xadd(xadd(mudt_c, xmul(sigma, dW_c)), mc);
+#pragma unroll
+                for (int i = 3; i < 6; i++) S[i] = __dadd_rn(S[i], __dmul_rn(S[i], incc));
+                dW_c = (RT)0;
+            }
+        }
+    }
+}
+
+// sample_inner_exact (portfolio_sampler.cpp:470-519): exact GBM from tau to maturity for the
+// antithetic pair started at S0 and for the path started at R_tau.
+template <class RT>
+__device__ RT inner_exact(const OptionTable<RT>& ot, const RT* Rt, uint32_t j, SeqNormals<RT>& nz, double& work) {
+    const bool anti = ot.use_antithetic_risk != 0;
+    work += (double)ot.W_est[j];
+    const uint32_t s = ot.stock_ind[j];
+    const RT S0 = ot.S0[s], sg = ot.sigma[s], r = ot.r, tau = ot.tau;
+    const RT Tr = xsub(ot.maturity[j], tau);
+    const RT dW_0_tau = xmul(ot.stau, nz.next());
+    const RT dW_tau_T = xmul(xsqrt(Tr), nz.next());
+    const RT S0_t_1 = simulate_stock_ref<RT>(S0, r, sg, tau, dW_0_tau);
+    const RT S0_T_1 = simulate_stock_ref<RT>(S0_t_1, r, sg, Tr, dW_tau_T);
+    RT S0_T_2 = (RT)0;
+    if (anti) {
+        const RT S0_t_2 = simulate_stock_ref<RT>(S0, r, sg, tau, -dW_0_tau);
+        S0_T_2 = simulate_stock_ref<RT>(S0_t_2, r, sg, Tr, dW_tau_T);
+    }
+    const RT St_T = simulate_stock_ref<RT>(Rt[s], r, sg, Tr, dW_tau_T);
+    const RT v1 = opt_diff_stock(ot, j, S0_T_1, St_T);
+    const RT v2 = anti ? opt_diff_stock(ot, j, S0_T_2, St_T) : v1;
+    RT d1 = (RT)0, d2 = (RT)0;
+    if (ot.use_delta_cv) {
+        const RT diff = xsub(Rt[s], S0);
+        d1 = xmul(diff, opt_derv_stock(ot, j, S0_T_1, S0));
+        d2 = anti ? xmul(diff, opt_derv_stock(ot, j, S0_T_2, S0)) : d1;
+    }
+    return to_rt<RT>(__dmul_rn(0.5, (double)xadd(xadd(xadd(v1, v2), d1), d2)));
+}
+
+// sample_inner_approx (portfolio_sampler.cpp:539-604): fine level L with N = h0 beta^L steps
+// and, for L > 0, the coupled coarse level; payoff differences of the antithetic pair.
+template <class RT>
+__device__ RT inner_approx(const OptionTable<RT>& ot, const RT* Rt, uint32_t j, SeqNormals<RT>& nz, double& work,
+                           uint32_t L, uint64_t N_l) {
+    const uint32_t s = ot.stock_ind[j];
+    const RT S0 = ot.S0[s], sg = ot.sigma[s], r = ot.r, tau = ot.tau;
+    const RT dW = xmul(ot.stau, nz.next());
+    const RT S0_t_1 = simulate_stock_ref<RT>(S0, r, sg, tau, dW);
+    const RT S0_t_2 = simulate_stock_ref<RT>(S0, r, sg, tau, -dW);
+    const uint64_t N = (uint64_t)ot.dt_h0inv * N_l;
+    work += (double)xmul((RT)N_l, ot.W_est[j]);
+    double S[6] = {(double)S0_t_1, (double)Rt[s], (double)S0_t_2, (double)S0_t_1, (double)Rt[s], (double)S0_t_2};
+    const RT Tr = xsub(ot.maturity[j], tau);
+    if (L) {
+        stock_dt<RT>(nz, S, N, r, sg, Tr, ot.use_milstein != 0, true, ot.dt_beta);
+        work += (double)xmul((RT)(N_l / ot.dt_beta), ot.W_est[j]);
+    } else {
+        stock_dt<RT>(nz, S, N, r, sg, Tr, ot.use_milstein != 0, false, 2);
+    }
+    const bool anti = ot.use_antithetic_risk != 0;
+    const RT m = anti ? (RT)0.5 : (RT)1;
+    const RT diff = xsub(Rt[s], S0);
+    const bool do_d_f = ot.use_delta_cv && (ot.use_coarse_delta_cv || L == 0);
+    const bool do_d_c = ot.use_delta_cv && ot.use_coarse_delta_cv;
+    RT vf = 0, vc = 0, vdf = 0, vdc = 0;
+    for (int i = 0; i < (anti ? 2 : 1); i++) {
+        const int ic = 2 * i;
+        vf = xadd(vf, xmul(m, opt_diff_stock(ot, j, to_rt<RT>(S[ic]), to_rt<RT>(S[1]))));
+        if (do_d_f) vdf = xadd(vdf, xmul(m, opt_derv_stock(ot, j, to_rt<RT>(S[ic]), S0)));
+        if (L == 0) continue;
+        vc = xadd(vc, xmul(m, opt_diff_stock(ot, j, to_rt<RT>(S[ic + 3]), to_rt<RT>(S[4]))));
+        if (do_d_c) vdc = xadd(vdc, xmul(m, opt_derv_stock(ot, j, to_rt<RT>(S[ic + 3]), S0)));
+    }
+    return xadd(xsub(vf, vc), xmul(diff, xsub(vdf, vdc)));
+}
+
+// Level of sample_inner_unbiased (portfolio_sampler.cpp:521-537) from its randu_sync word:
+// L = floor(log u / (log beta * e)), P(L) proportional to beta^(e L).  Returns false (and
+// n_steps = 0) when h0 beta^L exceeds NMLMC_MAX_PATH_STEPS.
+template <class RT>
+__device__ __forceinline__ bool unbiased_level(const OptionTable<RT>& ot, uint64_t word, uint32_t& L, uint64_t& N_l) {
+    const RT e = ot.dt_prob_expo, x = (RT)ot.dt_beta;
+    const RT q = xdiv(xlog(u01_rt<RT>(word)), xmul(xlog(x), e));
+    const RT fl = sizeof(RT) == 4 ? (RT)floorf((float)q) : (RT)floor((double)q);
+    L = (uint32_t)fl;
+    N_l = 1;
+    for (uint32_t i = 0; i < L; i++) {
+        N_l *= ot.dt_beta;
+        if (N_l * ot.dt_h0inv > kMaxPathSteps) return false;
+    }
+    return N_l * ot.dt_h0inv <= kMaxPathSteps;
+}
+
+template <class RT>
+__device__ __forceinline__ RT inner_unbiased(const OptionTable<RT>& ot, const RT* Rt, uint32_t j, SeqNormals<RT>& nz,
+                                             double& work, uint32_t L, uint64_t N_l) {
+    const RT ret = inner_approx<RT>(ot, Rt, j, nz, work, L, N_l);
+    const RT e = ot.dt_prob_expo, x = (RT)ot.dt_beta;
+    const RT Lp = to_rt<RT>(__ddiv_rn((double)xpow(x, xmul(-e, (RT)L)), __dsub_rn(1.0, (double)xpow(x, e))));
+    return xmul(ret, Lp);
+}
+
+// rand_int_pdf over compute_prob (common.hpp:178-195), as sample_inner_random_option_ind
+// picks the compute method (portfolio_sampler.cpp:350-352).
+template <class RT>
+__device__ __forceinline__ uint32_t pick_method(const OptionTable<RT>& ot, RT uc) {
+    const RT u = xmul(uc, ot.prob_norm);
+    RT p = 0;
+    uint32_t ret = 0;
+    for (uint32_t i = 0; i < 3; i++) {
+        const RT cpi = ot.compute_prob[i];
+        if (cpi <= (RT)0) continue;
+        p = xadd(p, cpi);
+        ret = i;
+        if (u <= p) break;
+    }
+    return ret;
+}
+
+// Option within method m from the inner randu (portfolio_sampler.cpp:353-369): uniform
+// ceil(u n) - 1 with prob 1 / options_count, or rand_int_cdf on the method's CDF.
+template <class RT>
+__device__ __forceinline__ uint32_t pick_option(const OptionTable<RT>& ot, uint32_t m, RT u, RT& prob) {
+    const uint32_t nm = ot.m_n[m], off = ot.m_off[m];
+    if (ot.subsample == SUB_UNIFORM) {
+        prob = ot.inv_count_prob;
+        return off + (uint32_t)(xceil(xmul(u, (RT)nm)) - (RT)1);
+    }
+    const RT uu = xmul(u, ot.compute_prob[m]);
+    uint32_t pos0 = 0, pos1 = nm;
+    if (nm > 1) {
+        const uint32_t steps = 32 - __clz(nm - 1);
+        for (uint32_t t = 0; t < steps; t++) {
+            const uint32_t mid = (pos0 + pos1) / 2;
+            if (mid > 0 && uu < ot.cdf[off + mid]) pos1 = mid; else pos0 = mid;
+        }
+    }
+    prob = xdiv(ot.prob[off + pos0], ot.prob_norm);
+    return off + pos0;
+}
+
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t n) {   // 32 when absent
+    for (uint32_t i = 0; i < n && m; i++) m &= m - 1;
+    return m ? (uint32_t)(__ffs(m) - 1) : 32u;
+}
+
 // init_inner_sampler: start value (model: -max_loss; portfolio: Y.constant, plus the full
 // deterministic BS sum when Subsampling::None).  Warp-cooperative, result in every lane.
 template <class RT, int KIND>
@@ -137,10 +350,164 @@ __device__ RT core_init_inner(CoreCtx<RT, KIND>& c, double& work, int lane) {
     if (KIND != KIND_PORTFOLIO) return -c.mp.max_loss;
     if (c.ot.subsample != SUB_NONE) return c.constant;
     double det = 0, w = 0;
-    for (uint32_t j = lane; j < c.ot.P; j += 32) det += (double)portfolio_bs_value<RT>(c.ot, c.Rt, j, w);
+    for (uint32_t j = lane; j < c.ot.m_n[METHOD_BS]; j += 32) det += (double)portfolio_bs_value<RT>(c.ot, c.Rt, j, w);
     det = warp_sum(det);
     work += warp_sum(w);             // warp total, identical in every lane
     return xadd(to_rt<RT>(det), c.constant);
+}
+
+// Inner phase of a portfolio with Exact / Unbiased options on the CORE streams.  A sample draws
+// a variable number of words: on the sync stream the method word (sub-sampled modes) and one
+// level word per Unbiased evaluation; on the inner stream the option-index word (sub-sampled
+// modes) and the normals of its paths.  Windows of up to 32 samples, one per lane: the sync
+// words of a window are parsed first (a word is a method word unless the previous method word
+// chose Unbiased), the normal counts are prefix-summed over the lanes, and every lane then
+// addresses its own words directly — a normal pair's words sit after the index words of the
+// samples up to the one that drew it — so the draws equal the reference's sequential ones.
+template <class RT>
+__device__ void core_phase_paths(CoreCtx<RT, KIND_PORTFOLIO>& c, uint64_t count, bool want_s2, double& a1,
+                                 double& a2, double& w, uint64_t& nu, uint64_t& nn, int lane, bool& err) {
+    const OptionTable<RT>& ot = c.ot;
+    const bool none = ot.subsample == SUB_NONE;
+    const uint64_t r_in = none ? 0 : 1;                 // inner-stream index words per sample
+    const uint32_t n_exact = ot.m_n[METHOD_EXACT], n_unb = ot.m_n[METHOD_UNBIASED];
+    uint64_t done = 0;
+    while (done < count) {
+        const uint64_t rem = count - done;
+        uint32_t nsamp;
+        uint64_t sync_used;
+        uint32_t my_m = METHOD_BS;
+        uint64_t my_lword = 0;                          // sub-sampled: the Unbiased level word
+        uint64_t n_norm = 0;                            // normals this lane's sample draws
+        bool ok = true;
+        if (!none) {
+            const uint64_t sw = core_word(c.key, c.sync.wpos + (uint64_t)lane);
+            const uint32_t mth = pick_method<RT>(ot, u01_rt<RT>(sw));
+            const uint32_t U = __ballot_sync(0xffffffffu, mth == METHOD_UNBIASED);
+            uint32_t mask = 0, pos = 0;
+            nsamp = 0;
+            while (pos < 32 && nsamp < rem) {
+                mask |= 1u << pos;
+                nsamp++;
+                pos += 1 + ((U >> pos) & 1u);
+            }
+            sync_used = pos;
+            const uint32_t q = nth_set_bit(mask, (uint32_t)lane);
+            const uint32_t qm = __shfl_sync(0xffffffffu, mth, q & 31);
+            uint64_t lw = __shfl_sync(0xffffffffu, (unsigned long long)sw, (q + 1) & 31);
+            if ((uint32_t)lane < nsamp) {
+                my_m = qm;
+                if (my_m == METHOD_UNBIASED) {
+                    if (q + 1 >= 32) lw = core_word(c.key, c.sync.wpos + q + 1);
+                    my_lword = lw;
+                    uint32_t L;
+                    uint64_t N_l;
+                    ok = unbiased_level<RT>(ot, lw, L, N_l);
+                    n_norm = ok ? 1 + (uint64_t)ot.dt_h0inv * N_l : 0;
+                } else if (my_m == METHOD_EXACT) {
+                    n_norm = 2;
+                }
+            }
+        } else {
+            // sample_inner_all_options (portfolio_sampler.cpp:336-344): every Exact option, then
+            // every Unbiased one, each of the latter with its own level word
+            nsamp = (uint32_t)(rem < 32 ? rem : 32);
+            sync_used = (uint64_t)nsamp * n_unb;
+            if ((uint32_t)lane < nsamp) {
+                n_norm = 2ull * n_exact;
+                const uint64_t w0 = c.sync.wpos + (uint64_t)lane * n_unb;
+                for (uint32_t k = 0; k < n_unb && ok; k++) {
+                    uint32_t L;
+                    uint64_t N_l;
+                    ok = unbiased_level<RT>(ot, core_word(c.key, w0 + k), L, N_l);
+                    n_norm += ok ? 1 + (uint64_t)ot.dt_h0inv * N_l : 0;
+                }
+            }
+        }
+        if (!ok) err = true;
+        // exclusive prefix of the normal counts over the lanes
+        uint64_t incl = n_norm;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint64_t t = __shfl_up_sync(0xffffffffu, (unsigned long long)incl, d);
+            if (lane >= d) incl += t;
+        }
+        const uint64_t C = incl - n_norm;
+        const uint64_t C_tot = __shfl_sync(0xffffffffu, (unsigned long long)incl, 31);
+        const uint32_t nz_mask = __ballot_sync(0xffffffffu, n_norm > 0);
+        const uint64_t wpos_w = c.inner.wpos;
+        const uint64_t s0 = c.inner.saved ? 1 : 0;
+        // pairs drawn for the first C normals of the window: ceil((C - s0) / 2)
+        const uint64_t pairs_before = (C + 1 - s0) >> 1;
+        if ((uint32_t)lane < nsamp && ok) {
+            SeqNormals<RT> nz;
+            nz.key = c.key;
+            nz.w = wpos_w + r_in * ((uint64_t)lane + 1) + 2 * pairs_before;
+            nz.have = ((s0 ^ (C & 1)) != 0);
+            nz.y = (RT)0;
+            if (nz.have && n_norm > 0) {
+                if (C == 0) {
+                    nz.y = (RT)c.inner.sval;
+                } else {
+                    // the pending normal is the second one of the pair the last earlier lane
+                    // with normals drew
+                    const uint32_t prior = nz_mask & ((1u << lane) - 1u);
+                    const uint32_t l = 31 - __clz(prior);
+                    RT x;
+                    core_pair<RT>(c.key, wpos_w + r_in * ((uint64_t)l + 1) + 2 * (pairs_before - 1), x, nz.y);
+                }
+            }
+            double wk = 0;
+            RT v;
+            RT prob = (RT)1;
+            if (!none) {
+                const uint64_t iw = core_word(c.key, wpos_w + (uint64_t)lane + 2 * pairs_before);
+                const uint32_t j = pick_option<RT>(ot, my_m, u01_rt<RT>(iw), prob);
+                if (my_m == METHOD_BS) {
+                    v = portfolio_bs_value<RT>(ot, c.Rt, j, wk);
+                } else if (my_m == METHOD_EXACT) {
+                    v = inner_exact<RT>(ot, c.Rt, j, nz, wk);
+                } else {
+                    uint32_t L;
+                    uint64_t N_l;
+                    unbiased_level<RT>(ot, my_lword, L, N_l);
+                    v = inner_unbiased<RT>(ot, c.Rt, j, nz, wk, L, N_l);
+                }
+                v = xdiv(v, prob);
+            } else {
+                double acc = 0;
+                const uint32_t oe = ot.m_off[METHOD_EXACT], ou = ot.m_off[METHOD_UNBIASED];
+                for (uint32_t k = 0; k < n_exact; k++) acc += (double)inner_exact<RT>(ot, c.Rt, oe + k, nz, wk);
+                const uint64_t w0 = c.sync.wpos + (uint64_t)lane * n_unb;
+                for (uint32_t k = 0; k < n_unb; k++) {
+                    uint32_t L;
+                    uint64_t N_l;
+                    unbiased_level<RT>(ot, core_word(c.key, w0 + k), L, N_l);
+                    acc += (double)inner_unbiased<RT>(ot, c.Rt, ou + k, nz, wk, L, N_l);
+                }
+                v = to_rt<RT>(acc);
+            }
+            w += wk;
+            a1 += (double)v;
+            if (want_s2) a2 += (double)xmul(v, v);
+        }
+        __syncwarp();
+        // stream states after the window
+        const uint64_t pairs_tot = (C_tot + 1 - s0) >> 1;
+        const uint64_t s_end = s0 ^ (C_tot & 1);
+        if (C_tot > 0 && s_end) {
+            const uint32_t l_last = 31 - __clz(nz_mask);
+            RT x, y;
+            core_pair<RT>(c.key, wpos_w + r_in * ((uint64_t)l_last + 1) + 2 * (pairs_tot - 1), x, y);
+            c.inner.sval = (double)y;
+        }
+        c.inner.saved = (uint32_t)s_end;
+        c.inner.wpos = wpos_w + r_in * nsamp + 2 * pairs_tot;
+        c.sync.wpos += sync_used;
+        nu += sync_used + r_in * nsamp;
+        nn += C_tot;
+        done += nsamp;
+    }
 }
 
 // The inner phase: `count` inner samples split over the lanes; returns warp totals of s1 (and
@@ -172,6 +539,12 @@ __device__ void core_phase(CoreCtx<RT, KIND>& c, uint64_t count, bool want_s2, d
         __syncwarp();
         advance_normals<RT>(c.inner, c.key, per * count);
         nrandn += per * count;
+    } else if (c.ot.mixed) {
+        if constexpr (KIND == KIND_PORTFOLIO) {
+            bool err = false;
+            core_phase_paths<RT>(c, count, want_s2, a1, a2, w, nrandu, nrandn, lane, err);
+            if (__any_sync(0xffffffffu, err)) c.err = 1;
+        }
     } else if (c.ot.subsample != SUB_NONE) {
         // sample_inner_random_option(_ind) (portfolio_sampler.cpp:346-380): one randu_sync for
         // the method (rand_int_pdf over compute_prob) and one randu for the option index.
@@ -313,6 +686,7 @@ __global__ void __launch_bounds__(256) core_level_kernel(CoreLaunch<RT> L, CoreS
     c.Rt = reinterpret_cast<RT*>(smem_raw) + (size_t)warp_in_block * (L.ot.Q ? L.ot.Q : 1);
     c.Y = 0;
     c.constant = 0;
+    c.err = 0;
 
     const uint64_t q = L.M / L.cores, rem = L.M % L.cores;
     const uint64_t mcount = q + (core < rem ? 1 : 0);
@@ -405,7 +779,7 @@ __global__ void __launch_bounds__(256) core_level_kernel(CoreLaunch<RT> L, CoreS
         double* o = out_sums + (size_t)core * 10;
         for (int j = 0; j < 4; j++) { o[j] = f_sums[j]; o[4 + j] = d_sums[j]; }
         o[8] = work;
-        o[9] = 0;
+        o[9] = c.err ? 1.0 : 0.0;
         uint64_t* s = out_stats + (size_t)core * 6;
         for (int j = 0; j < 4; j++) s[j] = st[j];
         s[4] = nu;
@@ -416,27 +790,27 @@ __global__ void __launch_bounds__(256) core_level_kernel(CoreLaunch<RT> L, CoreS
 // Sums the per-core partials in core order (one block).
 __global__ void core_reduce_kernel(uint32_t cores, const double* in_sums, const uint64_t* in_stats,
                                    double* out_sums, uint64_t* out_stats) {
-    __shared__ double sd[256][9];
+    __shared__ double sd[256][10];
     __shared__ uint64_t su[256][6];
     const uint32_t t = threadIdx.x;
-    double a[9] = {0};
+    double a[10] = {0};
     uint64_t b[6] = {0};
     for (uint32_t c = t; c < cores; c += blockDim.x) {
-        for (int j = 0; j < 9; j++) a[j] += in_sums[(size_t)c * 10 + j];
+        for (int j = 0; j < 10; j++) a[j] += in_sums[(size_t)c * 10 + j];
         for (int j = 0; j < 6; j++) b[j] += in_stats[(size_t)c * 6 + j];
     }
-    for (int j = 0; j < 9; j++) sd[t][j] = a[j];
+    for (int j = 0; j < 10; j++) sd[t][j] = a[j];
     for (int j = 0; j < 6; j++) su[t][j] = b[j];
     __syncthreads();
     for (uint32_t s = blockDim.x / 2; s > 0; s >>= 1) {
         if (t < s) {
-            for (int j = 0; j < 9; j++) sd[t][j] += sd[t + s][j];
+            for (int j = 0; j < 10; j++) sd[t][j] += sd[t + s][j];
             for (int j = 0; j < 6; j++) su[t][j] += su[t + s][j];
         }
         __syncthreads();
     }
     if (t == 0) {
-        for (int j = 0; j < 9; j++) out_sums[j] = sd[0][j];
+        for (int j = 0; j < 10; j++) out_sums[j] = sd[0][j];
         for (int j = 0; j < 6; j++) out_stats[j] = su[0][j];
     }
 }

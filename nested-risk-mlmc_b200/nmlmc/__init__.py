@@ -17,7 +17,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libnmlmc.so")
 INCLUDE_H = os.path.join(os.path.dirname(os.path.dirname(HERE)), "include", "nmlmc.h")
 
-OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_NOMEM, ERR_TIMEOUT = range(6)
+OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_NOMEM, ERR_TIMEOUT, ERR_LIMIT = range(7)
+METHOD_BS, METHOD_EXACT, METHOD_UNBIASED = 0, 1, 2
+MAX_PATH_STEPS = 1 << 24
 PREC_REF32, PREC_FP64, PREC_FP32 = 0, 1, 2
 STREAMS_CORE, STREAMS_OUTER = 0, 1
 MODEL_REFERENCE, MODEL_SHIFT = 0, 1
@@ -110,6 +112,12 @@ class Portfolio(ctypes.Structure):
                 ("use_delta_cv", ctypes.c_int32), ("discount", ctypes.c_int32)]
 
 
+class PathMethods(ctypes.Structure):
+    _fields_ = [("method", _i32p), ("dt_h0inv", ctypes.c_uint32), ("dt_beta", ctypes.c_uint32),
+                ("dt_prob_expo", ctypes.c_double), ("use_coarse_delta_cv", ctypes.c_int32),
+                ("use_antithetic_risk", ctypes.c_int32), ("use_milstein", ctypes.c_int32)]
+
+
 class TraceRec(ctypes.Structure):
     _fields_ = [("count_f", ctypes.c_uint64), ("count_c", ctypes.c_uint64),
                 ("phi_f", ctypes.c_double), ("phi_c", ctypes.c_double),
@@ -177,7 +185,7 @@ EXPORTS = [
     "nmlmc_portfolio_full_loss", "nmlmc_mlmc_default_input", "nmlmc_mlmc_run",
     "nmlmc_mlmc_run_cb", "nmlmc_threefry_blocks", "nmlmc_outer_normals", "nmlmc_set_shard",
     "nmlmc_set_profiling", "nmlmc_phase_kernel_time", "nmlmc_kernel_launches",
-    "nmlmc_sample_level_noalloc", "nmlmc_portfolio_generate",
+    "nmlmc_sample_level_noalloc", "nmlmc_portfolio_generate", "nmlmc_set_portfolio_methods",
 ]
 
 
@@ -196,6 +204,8 @@ def lib() -> ctypes.CDLL:
     L.nmlmc_configure.argtypes = [ctypes.c_void_p, ctypes.POINTER(Config)]
     L.nmlmc_set_model.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_double, ctypes.c_double]
     L.nmlmc_set_portfolio.argtypes = [ctypes.c_void_p, ctypes.POINTER(Portfolio), _dp, _dp]
+    L.nmlmc_set_portfolio_methods.argtypes = [ctypes.c_void_p, ctypes.POINTER(Portfolio),
+                                              ctypes.POINTER(PathMethods), _dp, _dp]
     L.nmlmc_reset_streams.argtypes = [ctypes.c_void_p]
     L.nmlmc_sample.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(LevelResult)]
     L.nmlmc_sample_levels.argtypes = [ctypes.c_void_p, ctypes.c_uint32, _u32p, _u64p, ctypes.POINTER(LevelResult)]
@@ -288,7 +298,11 @@ class Sampler:
         _check(self.L.nmlmc_set_model(self.h, kind, tau, max_loss), "nmlmc_set_model")
 
     def set_portfolio(self, pf: dict, r=0.05, rho=0.0, max_loss=0.0, tau=1 / 52,
-                      subsample=SUB_UNIFORM, use_delta_cv=False, discount=True):
+                      subsample=SUB_UNIFORM, use_delta_cv=False, discount=True, methods=None):
+        """Portfolio of European options.  `methods` (optional): dict with `method` ([P] of
+        METHOD_BS / METHOD_EXACT / METHOD_UNBIASED) and the path-simulation parameters
+        dt_h0inv, dt_beta, dt_prob_expo, use_coarse_delta_cv, use_antithetic_risk,
+        use_milstein (defaults 8, 4, -1.5, False, True, True)."""
         d = {k: np.ascontiguousarray(pf[k], np.float64) for k in
              ("S0", "mu", "sigma", "strike", "maturity", "w", "prob")}
         si = np.ascontiguousarray(pf["stock_ind"], np.uint32)
@@ -300,8 +314,19 @@ class Sampler:
                        subsample, int(use_delta_cv), int(discount))
         start = np.zeros(P)
         delta = np.zeros(P)
-        _check(self.L.nmlmc_set_portfolio(self.h, ctypes.byref(st), _p(start, _dp), _p(delta, _dp)),
-               "nmlmc_set_portfolio")
+        if methods is None:
+            _check(self.L.nmlmc_set_portfolio(self.h, ctypes.byref(st), _p(start, _dp), _p(delta, _dp)),
+                   "nmlmc_set_portfolio")
+            return start, delta
+        me = np.ascontiguousarray(methods["method"], np.int32)
+        pm = PathMethods(_p(me, _i32p), int(methods.get("dt_h0inv", 8)), int(methods.get("dt_beta", 4)),
+                         float(methods.get("dt_prob_expo", -1.5)),
+                         int(bool(methods.get("use_coarse_delta_cv", False))),
+                         int(bool(methods.get("use_antithetic_risk", True))),
+                         int(bool(methods.get("use_milstein", True))))
+        _check(self.L.nmlmc_set_portfolio_methods(self.h, ctypes.byref(st), ctypes.byref(pm),
+                                                  _p(start, _dp), _p(delta, _dp)),
+               "nmlmc_set_portfolio_methods")
         return start, delta
 
     def reset_streams(self):
@@ -516,24 +541,34 @@ def norm_cdf_inv(p: float) -> float:
 
 
 def make_portfolio_data(pf: dict, r=0.05, rho=0.0, max_loss=0.0, tau=1 / 52,
-                        subsample=SUB_UNIFORM, use_delta_cv=False):
-    """Builds a reference-layout portfolio_data (BS options) from SoA arrays; returns the struct
-    and the arrays that back it (keep them alive while the struct is in use)."""
+                        subsample=SUB_UNIFORM, use_delta_cv=False, method=None,
+                        use_coarse_delta_cv=False, use_antithetic_risk=True, use_milstein=True,
+                        dt_h0inv=8, dt_beta=4, dt_prob_expo=-1.5):
+    """Builds a reference-layout portfolio_data from SoA arrays: option j goes to
+    options[method[j]] (all BS when `method` is None), in order.  Returns the struct and the
+    arrays that back it (keep them alive while the struct is in use)."""
     P, Q = len(pf["strike"]), len(pf["S0"])
-    opts = (OptionParams * P)()
-    for j in range(P):
-        o = opts[j]
-        o.strike, o.maturity, o.w = pf["strike"][j], pf["maturity"][j], pf["w"][j]
-        o.stock_ind, o.type, o.prob, o.W_est = int(pf["stock_ind"][j]), int(pf["type"][j]), pf["prob"][j], 1.0
+    meth = np.zeros(P, np.int32) if method is None else np.asarray(method, np.int32)
+    spans = []
+    for m in range(3):
+        idx = np.flatnonzero(meth == m)
+        opts = (OptionParams * max(len(idx), 1))()
+        for k, j in enumerate(idx):
+            o = opts[k]
+            o.strike, o.maturity, o.w = pf["strike"][j], pf["maturity"][j], pf["w"][j]
+            o.stock_ind, o.type, o.prob, o.W_est = int(pf["stock_ind"][j]), int(pf["type"][j]), pf["prob"][j], 1.0
+        spans.append((opts, len(idx)))
     stocks = (StockParams * Q)()
     for i in range(Q):
         stocks[i].S0, stocks[i].mu, stocks[i].sigma = pf["S0"][i], pf["mu"][i], pf["sigma"][i]
     d = PortfolioData()
-    d.options[0] = OptionsSpan(opts, P)
+    for m in range(3):
+        d.options[m] = OptionsSpan(spans[m][0], spans[m][1])
     d.stocks = StocksSpan(stocks, Q)
     d.r, d.rho, d.max_loss, d.tau = r, rho, max_loss, tau
     d.s1_rho2 = float(np.sqrt(np.float32(1) - np.float32(rho) * np.float32(rho)))
-    d.dt_h0inv, d.dt_beta, d.dt_prob_expo = 8, 4, -1.5
+    d.dt_h0inv, d.dt_beta, d.dt_prob_expo = dt_h0inv, dt_beta, dt_prob_expo
     d.phi_type, d._phi_size, d.subsample = 0, 1, subsample
-    d.use_delta_cv, d.use_coarse_delta_cv, d.use_antithetic_risk, d.use_milstein = use_delta_cv, False, True, True
-    return d, (opts, stocks)
+    d.use_delta_cv, d.use_coarse_delta_cv = use_delta_cv, use_coarse_delta_cv
+    d.use_antithetic_risk, d.use_milstein = use_antithetic_risk, use_milstein
+    return d, ([sp[0] for sp in spans], stocks)

@@ -70,6 +70,12 @@ def make_pair(case, o_prec, streams_o, streams_n, cores=None, seed=None):
         pf = O.synthetic_portfolio(**case["pf"])
         kw = dict(r=0.05, rho=case["rho"], max_loss=case["max_loss"], tau=1 / 52,
                   subsample=case["sub"], use_delta_cv=case["cv"])
+        if "methods" in case:
+            flags = dict(use_coarse_delta_cv=case["coarse_cv"], use_antithetic_risk=case["anti_risk"],
+                         use_milstein=case["milstein"])
+            s_o.set_portfolio_methods(pf, case["methods"], **kw, **flags)
+            s_g.set_portfolio(pf, **kw, methods=dict(method=case["methods"], **flags))
+            return s_o, s_g
         st_o, de_o = s_o.set_portfolio(pf, **kw)
         st_g, de_g = s_g.set_portfolio(pf, **kw)
         if case.get("gpu_prec", nm_prec(o_prec)) == nm_prec(o_prec):
@@ -171,6 +177,40 @@ def test_reference_named_portfolio_surface(nm, golden):
     finally:
         nm.portfolio_cleanup()
         nm.cleanup_nestedmc_sampler()
+
+
+def test_reference_named_portfolio_surface_methods(nm, golden):
+    """portfolio_init with options[1] (Exact) and options[2] (Unbiased): golden case J."""
+    meta, _ = golden
+    case = next(c for c in meta["engine"] if c["name"] == "J_pf_methods_cdf_cv")
+    res = case["results"]["f32"]
+    pf = O.synthetic_portfolio(**case["pf"])
+    p = nm.NestedSamplerParams(case["N0"], case["beta"], case["anti"], 4, 4, case["r"])
+    nm.init_nestedmc_sampler(case["cores"], p)
+    d, keep = nm.make_portfolio_data(pf, r=0.05, rho=case["rho"], max_loss=case["max_loss"],
+                                     tau=1 / 52, subsample=case["sub"], use_delta_cv=case["cv"],
+                                     method=case["methods"], use_coarse_delta_cv=case["coarse_cv"],
+                                     use_antithetic_risk=case["anti_risk"], use_milstein=case["milstein"])
+    nm.portfolio_comp_params(d)
+    nm.portfolio_init(d, case["seed"])
+    try:
+        for call in res["calls"]:
+            out = nm.portfolio_sample(call["ell"], 0, call["M"])
+            np.testing.assert_array_equal(out["fsums"], call["fsums"])
+            np.testing.assert_array_equal(out["diffsums"], call["diffsums"])
+            assert out["work"] == call["work"]
+    finally:
+        nm.portfolio_cleanup()
+        nm.cleanup_nestedmc_sampler()
+
+
+def test_methods_outer_layout_refused(nm):
+    """Path-simulated methods are defined on the CORE streams: the OUTER layout refuses them."""
+    s = nm.Sampler(precision=nm.PREC_FP64, streams=nm.STREAMS_OUTER, N0=32, beta=4, adaptive_r=1.5)
+    pf = O.synthetic_portfolio(2, 6, 3)
+    s.set_portfolio(pf, methods=dict(method=[0, 1, 2, 0, 1, 2]))
+    with pytest.raises(nm.NmlmcError):
+        s.sample(1, 10)
 
 
 OUTER_CASES = [
