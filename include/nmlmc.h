@@ -228,6 +228,45 @@ typedef struct nmlmc_path_methods {
 } nmlmc_path_methods;
 int nmlmc_set_portfolio_methods(nmlmc_ctx* ctx, const nmlmc_portfolio* pf, const nmlmc_path_methods* pm,
                                 double* out_start, double* out_delta_est);
+/* ---- path-simulated loss and its adjoint (no counterpart in the reference) --------------------
+ * A batch of n portfolios evaluated in one launch.  Portfolio p owns stocks
+ * [stock_off[p], stock_off[p+1]) and options [option_off[p], option_off[p+1]); stock_ind is the
+ * stock's index within its portfolio.  For outer sample m of portfolio p (OUTER-layout key
+ * (seed, ell<<56 | p<<32 | m): at p = 0 the outer draws of nmlmc_portfolio_full_loss):
+ *   L_m = sum_i w_i (V_i(0) - e^{-r tau} C_i(m)),
+ *   C_i(m) = e^{-r (T_i - tau)} (1/N) sum_n (pay(S+_n) + pay(S-_n)) / 2,
+ * S+-_n an antithetic pair of Milstein (or Euler) paths on 2^ell steps from (tau, R_tau) to T_i
+ * under the risk-neutral drift, N = inner_pairs.  Estimates per portfolio: E[L], the smoothed
+ * exceedance P_delta = E[1 / (1 + exp(-(L - K) / delta))] with delta = delta_rel |K| (delta_rel
+ * when K = 0), and the plain frequency of L > K.  Gradients (pathwise, inner draws recomputed from
+ * the counter RNG): dE[L]/dw_i, dP_delta/dw_i, dE[L]/dsigma_j, dP_delta/dsigma_j. */
+typedef struct nmlmc_portfolio_batch {
+    uint32_t n;
+    const uint32_t *stock_off, *option_off;        /* [n + 1]                                  */
+    const double *S0, *mu, *sigma;                 /* [stock_off[n]]                           */
+    const double *strike, *maturity, *w;           /* [option_off[n]]; maturity > tau          */
+    const uint32_t* stock_ind;                     /* [option_off[n]]                          */
+    const int32_t* type;                           /* [option_off[n]] +1 call / -1 put          */
+    const double* K;                               /* [n] loss thresholds                      */
+    double r, rho, tau;
+} nmlmc_portfolio_batch;
+typedef struct nmlmc_adjoint_config {
+    uint32_t ell;            /* 2^ell time steps from tau to maturity (ell <= 16)               */
+    uint32_t inner_pairs;    /* antithetic path pairs per option and outer sample               */
+    uint64_t M;              /* outer samples per portfolio (< 2^32)                            */
+    double delta_rel;        /* sigmoid width relative to |K|                                   */
+    int32_t precision;       /* NMLMC_PREC_FP32 (FP32 paths, FP64 sums) or NMLMC_PREC_FP64      */
+    int32_t milstein;        /* 1 Milstein, 0 Euler-Maruyama                                    */
+    uint64_t seed;
+} nmlmc_adjoint_config;
+typedef struct nmlmc_adjoint_result {
+    double EL, P_smooth, P_hard;
+} nmlmc_adjoint_result;
+/* res [n] required; gradients [options] / [stocks] and loss [n * M] may be NULL (all four
+ * gradient pointers NULL: the loss pass only).  seconds: device time of the kernels (may be NULL). */
+int nmlmc_path_adjoint(nmlmc_ctx* ctx, const nmlmc_portfolio_batch* batch, const nmlmc_adjoint_config* cfg,
+                       nmlmc_adjoint_result* res, double* grad_w_EL, double* grad_w_P,
+                       double* grad_sigma_EL, double* grad_sigma_P, double* loss, double* seconds);
 /* Restart every stream (CORE: random_state(seed, core) from counter 0; OUTER: outer indices
  * from 0). */
 int nmlmc_reset_streams(nmlmc_ctx* ctx);

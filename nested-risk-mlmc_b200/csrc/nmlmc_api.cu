@@ -721,6 +721,133 @@ int nmlmc_set_portfolio_methods(nmlmc_ctx* c, const nmlmc_portfolio* p, const nm
     return set_portfolio_impl(c, p, pm, out_start, out_delta);
 }
 
+// ---- path-simulated loss and its adjoint -------------------------------------------------------
+}  // extern "C"
+
+namespace {
+
+struct DevAlloc {                       // device buffers of one nmlmc_path_adjoint call
+    std::vector<void*> ptrs;
+    ~DevAlloc() { for (void* p : ptrs) cudaFree(p); }
+    template <class T>
+    T* get(size_t n) {
+        void* p = nullptr;
+        if (cudaMalloc(&p, (n ? n : 1) * sizeof(T)) != cudaSuccess) return nullptr;
+        ptrs.push_back(p);
+        return static_cast<T*>(p);
+    }
+    template <class T>
+    T* put(const std::vector<T>& h) {
+        T* d = get<T>(h.size());
+        if (d && !h.empty() && cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+            return nullptr;
+        return d;
+    }
+};
+
+template <class RT>
+int path_adjoint_t(nmlmc_ctx* c, const nmlmc_portfolio_batch* b, const nmlmc_adjoint_config* a,
+                   nmlmc_adjoint_result* res, double* gwE, double* gwP, double* gsE, double* gsP,
+                   double* loss, double* seconds) {
+    const uint32_t n = b->n, NS = b->stock_off[n], NO = b->option_off[n];
+    const bool grad = gwE || gwP || gsE || gsP;
+    DevAlloc D;
+    AdjLaunch<RT> A{};
+    A.n = n; A.ell = a->ell; A.pairs = a->inner_pairs; A.M = a->M; A.seed = a->seed;
+    A.milstein = a->milstein ? 1 : 0;
+    A.tile = (uint32_t)std::min<uint64_t>(kAdjMaxTile, a->M);
+    A.r = (RT)b->r; A.rho = (RT)b->rho; A.tau = (RT)b->tau;
+    A.s1_rho2 = (RT)sqrt(1 - b->rho * b->rho); A.stau = (RT)sqrt(b->tau); A.disc_tau = (RT)exp(-b->r * b->tau);
+    std::vector<uint32_t> so(b->stock_off, b->stock_off + n + 1), oo(b->option_off, b->option_off + n + 1);
+    std::vector<uint32_t> co(n + 1, 0);
+    uint32_t qmax = 0;
+    for (uint32_t p = 0; p < n; p++) {
+        co[p + 1] = co[p] + (oo[p + 1] - oo[p] + 127) / 128;
+        qmax = std::max(qmax, so[p + 1] - so[p]);
+    }
+    A.n_chunks = co[n];
+    A.q_max = qmax;
+    std::vector<RT> S0(NS), mu(NS), sg(NS), K(NO), T(NO), w(NO), V0(NO), vega(NO);
+    std::vector<int8_t> ty(NO);
+    std::vector<uint32_t> si(b->stock_ind, b->stock_ind + NO);
+    for (uint32_t j = 0; j < NS; j++) { S0[j] = (RT)b->S0[j]; mu[j] = (RT)b->mu[j]; sg[j] = (RT)b->sigma[j]; }
+    for (uint32_t p = 0; p < n; p++)
+        for (uint32_t i = oo[p]; i < oo[p + 1]; i++) {
+            const uint32_t s = so[p] + si[i];
+            const double Sd = b->S0[s], sd = b->sigma[s], Kd = b->strike[i], Td = b->maturity[i];
+            K[i] = (RT)Kd; T[i] = (RT)Td; w[i] = (RT)b->w[i]; ty[i] = (int8_t)b->type[i];
+            V0[i] = (RT)h_calc_bs<double>(b->type[i], Sd, Kd, b->r, Td, sd);
+            const double d1 = h_d1<double>(Sd, Kd, b->r, Td, sd);
+            vega[i] = (RT)(Sd * exp(-0.5 * d1 * d1) * 0.39894228040143268 * sqrt(Td));   // S0 phi(d1) sqrt(T)
+        }
+    std::vector<double> Kp(n), dl(n);
+    for (uint32_t p = 0; p < n; p++) {
+        Kp[p] = b->K[p];
+        dl[p] = b->K[p] != 0 ? a->delta_rel * fabs(b->K[p]) : a->delta_rel;
+    }
+    A.stock_off = D.put(so); A.option_off = D.put(oo); A.chunk_off = D.put(co);
+    A.S0 = D.put(S0); A.mu = D.put(mu); A.sigma = D.put(sg);
+    A.strike = D.put(K); A.maturity = D.put(T); A.w = D.put(w); A.V0 = D.put(V0); A.vega = D.put(vega);
+    A.stock_ind = D.put(si); A.type = D.put(ty); A.K = D.put(Kp); A.delta = D.put(dl);
+    A.R = D.get<RT>((size_t)NS * a->M); A.dR = D.get<RT>((size_t)NS * a->M);
+    A.L = D.get<double>((size_t)n * a->M); A.omega = D.get<double>((size_t)n * a->M);
+    A.est = D.get<double>(3 * n); A.wE = D.get<double>(n);
+    A.gw_E = D.get<double>(NO); A.gw_P = D.get<double>(NO); A.gs_E = D.get<double>(NS); A.gs_P = D.get<double>(NS);
+    if (!A.stock_off || !A.option_off || !A.chunk_off || !A.S0 || !A.mu || !A.sigma || !A.strike || !A.maturity ||
+        !A.w || !A.V0 || !A.vega || !A.stock_ind || !A.type || !A.K || !A.delta || !A.R || !A.dR || !A.L ||
+        !A.omega || !A.est || !A.wE || !A.gw_E || !A.gw_P || !A.gs_E || !A.gs_P)
+        return set_err(NMLMC_ERR_NOMEM);
+    NM_CUDA(cudaMemsetAsync(A.L, 0, (size_t)n * a->M * sizeof(double), c->stream), "memset");
+    NM_CUDA(cudaMemsetAsync(A.gw_E, 0, NO * sizeof(double), c->stream), "memset");
+    NM_CUDA(cudaMemsetAsync(A.gw_P, 0, NO * sizeof(double), c->stream), "memset");
+    NM_CUDA(cudaMemsetAsync(A.gs_E, 0, NS * sizeof(double), c->stream), "memset");
+    NM_CUDA(cudaMemsetAsync(A.gs_P, 0, NS * sizeof(double), c->stream), "memset");
+    NM_CUDA(cudaEventRecord(c->ev0, c->stream), "event");
+    NM_CUDA(launch_adjoint(A, grad, c->stream), "adjoint kernels");
+    NM_CUDA(cudaEventRecord(c->ev1, c->stream), "event");
+    std::vector<double> est(3 * n);
+    NM_CUDA(cudaMemcpyAsync(est.data(), A.est, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "d2h");
+    if (loss) NM_CUDA(cudaMemcpyAsync(loss, A.L, (size_t)n * a->M * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "d2h");
+    if (gwE) NM_CUDA(cudaMemcpyAsync(gwE, A.gw_E, NO * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "d2h");
+    if (gwP) NM_CUDA(cudaMemcpyAsync(gwP, A.gw_P, NO * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "d2h");
+    if (gsE) NM_CUDA(cudaMemcpyAsync(gsE, A.gs_E, NS * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "d2h");
+    if (gsP) NM_CUDA(cudaMemcpyAsync(gsP, A.gs_P, NS * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "d2h");
+    NM_CUDA(cudaStreamSynchronize(c->stream), "sync");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    if (seconds) *seconds = ms * 1e-3;
+    for (uint32_t p = 0; p < n; p++) res[p] = nmlmc_adjoint_result{est[3 * p], est[3 * p + 1], est[3 * p + 2]};
+    return NMLMC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int nmlmc_path_adjoint(nmlmc_ctx* c, const nmlmc_portfolio_batch* b, const nmlmc_adjoint_config* a,
+                       nmlmc_adjoint_result* res, double* gwE, double* gwP, double* gsE, double* gsP,
+                       double* loss, double* seconds) {
+    if (!c || !b || !a || !res || b->n == 0 || b->n >= (1u << 24) || !b->stock_off || !b->option_off ||
+        !b->S0 || !b->mu || !b->sigma || !b->strike || !b->maturity || !b->w || !b->stock_ind || !b->type || !b->K)
+        return set_err(NMLMC_ERR_ARG);
+    if (a->ell > 16 || a->inner_pairs == 0 || a->M == 0 || a->M >= (1ull << 32) || !(a->delta_rel > 0) ||
+        (a->precision != NMLMC_PREC_FP32 && a->precision != NMLMC_PREC_FP64) || !(b->tau > 0) ||
+        !(fabs(b->rho) < 1))
+        return set_err(NMLMC_ERR_ARG);
+    for (uint32_t p = 0; p < b->n; p++) {
+        const uint32_t Q = b->stock_off[p + 1] - b->stock_off[p], P = b->option_off[p + 1] - b->option_off[p];
+        if (b->stock_off[p + 1] <= b->stock_off[p] || b->option_off[p + 1] <= b->option_off[p]) return set_err(NMLMC_ERR_ARG);
+        for (uint32_t i = b->option_off[p]; i < b->option_off[p + 1]; i++)
+            if (b->stock_ind[i] >= Q || (b->type[i] != 1 && b->type[i] != -1) || !(b->maturity[i] > b->tau))
+                return set_err(NMLMC_ERR_ARG);
+        (void)P;
+    }
+    if (b->stock_off[0] != 0 || b->option_off[0] != 0) return set_err(NMLMC_ERR_ARG);
+    cudaSetDevice(c->device);
+    return a->precision == NMLMC_PREC_FP64 ? path_adjoint_t<double>(c, b, a, res, gwE, gwP, gsE, gsP, loss, seconds)
+                                           : path_adjoint_t<float>(c, b, a, res, gwE, gwP, gsE, gsP, loss, seconds);
+}
+
 int nmlmc_set_trace(nmlmc_ctx* c, nmlmc_trace_rec* host_buf, uint64_t cap) {
     if (!c) return set_err(NMLMC_ERR_ARG);
     c->trace_host = host_buf;

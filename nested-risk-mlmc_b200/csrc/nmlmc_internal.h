@@ -86,6 +86,29 @@ template <class RT>
 cudaError_t outer_full_loss(const OuterLevel<RT>& L, int prec, OuterBuffers& B, double* d_loss,
                             cudaStream_t stream);
 
+// ---- path-simulated loss and its adjoint (nmlmc_adjoint.cu) --------------------------------
+constexpr uint32_t kAdjMaxTile = 64;     // outer samples per CTA of the path kernels
+
+template <class RT>
+struct AdjLaunch {
+    uint32_t n, n_chunks, q_max;          // portfolios, option chunks of 128, max stocks per portfolio
+    uint32_t ell, pairs, tile;            // 2^ell steps, antithetic pairs, outer samples per CTA
+    uint64_t M, seed;
+    int milstein;
+    RT r, rho, s1_rho2, tau, stau, disc_tau;
+    const uint32_t *stock_off, *option_off, *chunk_off;   // [n + 1]
+    const RT *S0, *mu, *sigma;                             // [stocks]
+    const RT *strike, *maturity, *w, *V0, *vega;           // [options]
+    const uint32_t* stock_ind;                             // [options], within the portfolio
+    const int8_t* type;
+    const double *K, *delta;                               // [n]
+    RT *R, *dR;                                            // [stocks * M], row (p, m) of Q_p values
+    double *L, *omega, *est, *wE;                          // [n * M], [n * M], [3 n], [n]
+    double *gw_E, *gw_P, *gs_E, *gs_P;                     // [options], [stocks]
+};
+cudaError_t launch_adjoint(const AdjLaunch<float>& A, bool grad, cudaStream_t stream);
+cudaError_t launch_adjoint(const AdjLaunch<double>& A, bool grad, cudaStream_t stream);
+
 cudaError_t launch_threefry_blocks(const uint64_t* ctr, const uint64_t* key, uint64_t* out, uint64_t n,
                                    cudaStream_t s);
 cudaError_t launch_outer_normals(int prec, uint64_t seed, uint64_t stream, uint32_t tag, uint64_t n,

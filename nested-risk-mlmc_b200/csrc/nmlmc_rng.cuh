@@ -142,6 +142,7 @@ enum : uint32_t {
     PH_COARSE = 64,        // coarse pilot k     -> 64 + k
     PH_FINAL = 128,        // final phi (antithetic groups, fine-only, non-antithetic fine)
     PH_FINAL_C = 129,      // non-antithetic coarse phi
+    PH_ADJOINT = 200,      // inner paths of the path-simulated loss (option index in bits 32..63)
 };
 
 }  // namespace nmlmc

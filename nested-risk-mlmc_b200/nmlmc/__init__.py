@@ -118,6 +118,23 @@ class PathMethods(ctypes.Structure):
                 ("use_antithetic_risk", ctypes.c_int32), ("use_milstein", ctypes.c_int32)]
 
 
+class PortfolioBatch(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint32), ("stock_off", _u32p), ("option_off", _u32p),
+                ("S0", _dp), ("mu", _dp), ("sigma", _dp), ("strike", _dp), ("maturity", _dp),
+                ("w", _dp), ("stock_ind", _u32p), ("type", _i32p), ("K", _dp),
+                ("r", ctypes.c_double), ("rho", ctypes.c_double), ("tau", ctypes.c_double)]
+
+
+class AdjointConfig(ctypes.Structure):
+    _fields_ = [("ell", ctypes.c_uint32), ("inner_pairs", ctypes.c_uint32), ("M", ctypes.c_uint64),
+                ("delta_rel", ctypes.c_double), ("precision", ctypes.c_int32),
+                ("milstein", ctypes.c_int32), ("seed", ctypes.c_uint64)]
+
+
+class AdjointResult(ctypes.Structure):
+    _fields_ = [("EL", ctypes.c_double), ("P_smooth", ctypes.c_double), ("P_hard", ctypes.c_double)]
+
+
 class TraceRec(ctypes.Structure):
     _fields_ = [("count_f", ctypes.c_uint64), ("count_c", ctypes.c_uint64),
                 ("phi_f", ctypes.c_double), ("phi_c", ctypes.c_double),
@@ -186,6 +203,7 @@ EXPORTS = [
     "nmlmc_mlmc_run_cb", "nmlmc_threefry_blocks", "nmlmc_outer_normals", "nmlmc_set_shard",
     "nmlmc_set_profiling", "nmlmc_phase_kernel_time", "nmlmc_kernel_launches",
     "nmlmc_sample_level_noalloc", "nmlmc_portfolio_generate", "nmlmc_set_portfolio_methods",
+    "nmlmc_path_adjoint",
 ]
 
 
@@ -204,6 +222,9 @@ def lib() -> ctypes.CDLL:
     L.nmlmc_configure.argtypes = [ctypes.c_void_p, ctypes.POINTER(Config)]
     L.nmlmc_set_model.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_double, ctypes.c_double]
     L.nmlmc_set_portfolio.argtypes = [ctypes.c_void_p, ctypes.POINTER(Portfolio), _dp, _dp]
+    L.nmlmc_path_adjoint.argtypes = [ctypes.c_void_p, ctypes.POINTER(PortfolioBatch),
+                                     ctypes.POINTER(AdjointConfig), ctypes.POINTER(AdjointResult),
+                                     _dp, _dp, _dp, _dp, _dp, _dp]
     L.nmlmc_set_portfolio_methods.argtypes = [ctypes.c_void_p, ctypes.POINTER(Portfolio),
                                               ctypes.POINTER(PathMethods), _dp, _dp]
     L.nmlmc_reset_streams.argtypes = [ctypes.c_void_p]
@@ -328,6 +349,42 @@ class Sampler:
                                                   _p(start, _dp), _p(delta, _dp)),
                "nmlmc_set_portfolio_methods")
         return start, delta
+
+    def path_adjoint(self, batch: dict, ell: int, pairs: int, M: int, delta_rel: float = 0.01,
+                     precision: int = PREC_FP64, seed: int = 0, milstein: bool = True,
+                     grads: bool = True, loss: bool = False) -> dict:
+        """Path-simulated loss of a portfolio batch (make_batch) with the adjoint gradients of
+        E[L] and of the sigmoid-smoothed P(L > K); see nmlmc_path_adjoint."""
+        so = np.ascontiguousarray(batch["stock_off"], np.uint32)
+        oo = np.ascontiguousarray(batch["option_off"], np.uint32)
+        d = {k: np.ascontiguousarray(batch[k], np.float64) for k in
+             ("S0", "mu", "sigma", "strike", "maturity", "w", "K")}
+        si = np.ascontiguousarray(batch["stock_ind"], np.uint32)
+        ty = np.ascontiguousarray(batch["type"], np.int32)
+        n, NS, NO = len(so) - 1, int(so[-1]), int(oo[-1])
+        b = PortfolioBatch(n, _p(so, _u32p), _p(oo, _u32p), _p(d["S0"], _dp), _p(d["mu"], _dp),
+                           _p(d["sigma"], _dp), _p(d["strike"], _dp), _p(d["maturity"], _dp),
+                           _p(d["w"], _dp), _p(si, _u32p), _p(ty, _i32p), _p(d["K"], _dp),
+                           batch["r"], batch["rho"], batch["tau"])
+        cfg = AdjointConfig(ell, pairs, M, delta_rel, precision, int(milstein), seed)
+        res = (AdjointResult * n)()
+        out = {}
+        g = [np.zeros(NO), np.zeros(NO), np.zeros(NS), np.zeros(NS)] if grads else [None] * 4
+        lo = np.zeros(n * M) if loss else None
+        sec = ctypes.c_double(0)
+        _check(self.L.nmlmc_path_adjoint(self.h, ctypes.byref(b), ctypes.byref(cfg), res,
+                                         *[_p(x, _dp) if x is not None else None for x in g],
+                                         _p(lo, _dp) if lo is not None else None, ctypes.byref(sec)),
+               "nmlmc_path_adjoint")
+        out["EL"] = np.array([r.EL for r in res])
+        out["P_smooth"] = np.array([r.P_smooth for r in res])
+        out["P_hard"] = np.array([r.P_hard for r in res])
+        out["seconds"] = sec.value
+        if grads:
+            out["grad_w_EL"], out["grad_w_P"], out["grad_sigma_EL"], out["grad_sigma_P"] = g
+        if loss:
+            out["loss"] = lo.reshape(n, M)
+        return out
 
     def reset_streams(self):
         _check(self.L.nmlmc_reset_streams(self.h), "nmlmc_reset_streams")
@@ -572,3 +629,19 @@ def make_portfolio_data(pf: dict, r=0.05, rho=0.0, max_loss=0.0, tau=1 / 52,
     d.use_delta_cv, d.use_coarse_delta_cv = use_delta_cv, use_coarse_delta_cv
     d.use_antithetic_risk, d.use_milstein = use_antithetic_risk, use_milstein
     return d, ([sp[0] for sp in spans], stocks)
+
+
+def make_batch(portfolios: list, K, r: float = 0.05, rho: float = 0.0, tau: float = TAU_WEEK) -> dict:
+    """Concatenates portfolios (dicts of SoA arrays: S0, mu, sigma per stock; strike, maturity, w,
+    stock_ind, type per option) into the batch layout of nmlmc_path_adjoint."""
+    so, oo = [0], [0]
+    cat = {k: [] for k in ("S0", "mu", "sigma", "strike", "maturity", "w", "stock_ind", "type")}
+    for pf in portfolios:
+        for k in cat:
+            cat[k].append(np.asarray(pf[k]))
+        so.append(so[-1] + len(pf["S0"]))
+        oo.append(oo[-1] + len(pf["strike"]))
+    out = {k: np.concatenate(v) for k, v in cat.items()}
+    out.update(stock_off=np.array(so, np.uint32), option_off=np.array(oo, np.uint32),
+               K=np.asarray(K, np.float64).reshape(-1), r=r, rho=rho, tau=tau)
+    return out

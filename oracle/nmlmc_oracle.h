@@ -88,6 +88,13 @@ void o_portfolio_full_loss(o_ctx *, uint32_t ell, uint64_t first, uint64_t n, do
 
 double o_norm_cdf_inv(double p, int prec);    /* common.cpp:53-86 */
 
+/* Path-simulated portfolio loss of a batch of portfolios (adjoint_oracle.c): L[p * M + m]. */
+void o_adj_loss(uint32_t n, const uint32_t *stock_off, const uint32_t *option_off, const double *S0,
+                const double *mu, const double *sigma, const double *strike, const double *maturity,
+                const double *w, const uint32_t *stock_ind, const int32_t *type, double r, double rho,
+                double tau, uint32_t ell, uint32_t pairs, uint64_t M, uint64_t seed, int milstein,
+                double *L);
+
 #ifdef __cplusplus
 }
 #endif

@@ -96,7 +96,7 @@ def lib():
 def _stale() -> bool:
     so = os.path.getmtime(ORACLE_SO)
     return any(os.path.getmtime(os.path.join(HERE, f)) > so
-               for f in ("nmlmc_oracle.c", "nmlmc_oracle.h", "nmlmc_oracle_body.inc"))
+               for f in ("nmlmc_oracle.c", "nmlmc_oracle.h", "nmlmc_oracle_body.inc", "adjoint_oracle.c"))
 
 
 def threefry(ctr: np.ndarray, key: np.ndarray) -> np.ndarray:
@@ -435,3 +435,27 @@ def _methods_bind():
             ctypes.c_uint32, ctypes.c_double]
         L._methods_bound = True
     return L
+
+
+def adj_loss(batch: dict, ell: int, pairs: int, M: int, seed: int, milstein: bool = True) -> np.ndarray:
+    """Path-simulated loss L[p, m] of a portfolio batch (see adjoint_oracle.c)."""
+    L = lib()
+    if not getattr(L, "_adj_bound", False):
+        L.o_adj_loss.argtypes = [ctypes.c_uint32, _u32p, _u32p, _dp, _dp, _dp, _dp, _dp, _dp, _u32p,
+                                 _i32p, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                 ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64,
+                                 ctypes.c_int, _dp]
+        L._adj_bound = True
+    so = np.ascontiguousarray(batch["stock_off"], np.uint32)
+    oo = np.ascontiguousarray(batch["option_off"], np.uint32)
+    d = {k: np.ascontiguousarray(batch[k], np.float64) for k in
+         ("S0", "mu", "sigma", "strike", "maturity", "w")}
+    si = np.ascontiguousarray(batch["stock_ind"], np.uint32)
+    ty = np.ascontiguousarray(batch["type"], np.int32)
+    n = len(so) - 1
+    out = np.zeros(n * M)
+    L.o_adj_loss(n, _p(so, _u32p), _p(oo, _u32p), _p(d["S0"], _dp), _p(d["mu"], _dp),
+                 _p(d["sigma"], _dp), _p(d["strike"], _dp), _p(d["maturity"], _dp), _p(d["w"], _dp),
+                 _p(si, _u32p), _p(ty, _i32p), batch["r"], batch["rho"], batch["tau"], ell, pairs, M,
+                 seed, int(milstein), _p(out, _dp))
+    return out.reshape(n, M)

@@ -169,3 +169,20 @@ def test_live_reference_methods_case():
         np.testing.assert_array_equal(a["events"][1], b["events"][1])
         np.testing.assert_array_equal(a["fsums"], b["fsums"])
         assert a["work"] == b["work"]
+
+
+def test_adj_oracle_risk_neutral_mean():
+    """Path-simulated loss oracle: with mu = r the discounted inner value is a martingale, so E[L]
+    vanishes up to the time-step bias and the sampling error."""
+    g = np.random.default_rng(3)
+    Q, P = 2, 10
+    S0 = np.array([100.0, 95.0])
+    si = g.integers(0, Q, P).astype(np.uint32)
+    b = dict(stock_off=np.array([0, Q], np.uint32), option_off=np.array([0, P], np.uint32),
+             S0=S0, mu=np.full(Q, 0.05), sigma=np.array([0.2, 0.3]), stock_ind=si,
+             type=np.where(g.random(P) < 0.5, 1, -1).astype(np.int32),
+             maturity=0.5 + g.random(P), w=g.standard_normal(P), r=0.05, rho=0.3, tau=1 / 52)
+    b["strike"] = S0[si] * (0.9 + 0.2 * g.random(P))
+    L = O.adj_loss(b, 4, 32, 400, 7, True)[0]
+    se = L.std() / np.sqrt(L.size)
+    assert abs(L.mean()) < 4 * se + 5e-3 * np.abs(b["w"]).sum(), (L.mean(), se)
