@@ -221,6 +221,80 @@ def small_case():
         print(f"level {ell} M {M}: {r['seconds'] * 1e3:.3f} ms, {r['stats'][0] / r['seconds']:.3e} inner/s")
 
 
+# Lane operations per inner time step of an antithetic Milstein pair on the FP32 path (one normal):
+#   Threefry2x64-20 block / 4 = 35, SFU Box-Muller pair / 2 = 11, the Milstein update of both
+#   paths (dW, dW^2 - h, correction, two growth factors, two products) = 9, loop and select = 3;
+#   the adjoint pass adds the sigma-tangent of both paths (8).
+C4_OPS_LOSS = 35 + 11 + 9 + 3
+C4_OPS_GRAD = C4_OPS_LOSS + 8
+
+
+def c4_batch(nm, sizes, d, seed):
+    """Portfolios of the path-simulated workload: d GBM stocks (S0 = 100, mu = r = 0.05,
+    sigma ~ U[0.1, 0.4]); options on uniformly chosen stocks, 50/50 call/put, strike ~
+    U[0.8, 1.2] S0, maturity ~ U[0.25, 2], position ~ N(0, 1); numpy PCG64 seeded per portfolio."""
+    import numpy as np
+    pfs = []
+    for k, P in enumerate(sizes):
+        g = np.random.default_rng(seed + k)
+        si = g.integers(0, d, P).astype(np.uint32)
+        pfs.append(dict(S0=np.full(d, 100.0), mu=np.full(d, 0.05), sigma=0.1 + 0.3 * g.random(d),
+                        stock_ind=si, type=np.where(g.random(P) < 0.5, 1, -1).astype(np.int32),
+                        strike=100.0 * (0.8 + 0.4 * g.random(P)), maturity=0.25 + 1.75 * g.random(P),
+                        w=g.standard_normal(P)))
+    return nm.make_batch(pfs, [0.0] * len(sizes), r=0.05, rho=0.2, tau=1 / 52)
+
+
+def c4_case(args, small=False):
+    """Path-simulated loss with adjoint gradients (FP32 paths, FP64 sums): one portfolio of
+    P = 1e5 options on d = 50 stocks, and 64 portfolios with sizes log-uniform in [1e3, 1e5]
+    in one launch; Milstein on 2^ell steps from tau to maturity.  Thresholds K: the median loss
+    of a first loss-only pass; sigmoid width delta = 0.01 |K|."""
+    import numpy as np
+    sys.path.insert(0, PKG)
+    import nmlmc as nm
+    s = nm.Sampler(precision=nm.PREC_FP32)
+    g = np.random.default_rng(2026)
+    runs = [("single", [20_000 if small else 100_000], 64 if small else 256)]
+    if not small:
+        runs.append(("batch64", [int(x) for x in np.exp(g.uniform(np.log(1e3), np.log(1e5), 64))], 64))
+    ell, pairs = 4, 4
+    for name, sizes, M in runs:
+        b = c4_batch(nm, sizes, 50, 7)
+        kw = dict(ell=ell, pairs=pairs, M=M, seed=1, delta_rel=0.01)
+        b["K"] = np.median(s.path_adjoint(b, grads=False, loss=True, **kw)["loss"], axis=1)
+        for _ in range(max(args.warmup, 1)):
+            s.path_adjoint(b, **kw)
+        t_loss, t_all = [], []
+        cs = ClockSampler(0)
+        cs.start()
+        for _ in range(args.steps):
+            t_loss.append(s.path_adjoint(b, grads=False, **kw)["seconds"])
+            t_all.append(s.path_adjoint(b, **kw)["seconds"])
+        clk = cs.stop()
+        sm_mhz = clk.get("sm_mhz") or 1965.0
+        peak = 148 * 128 * sm_mhz * 1e6 / 1e12
+        P_tot = int(b["option_off"][-1])
+        normals = P_tot * M * pairs * (1 << ell)          # antithetic pair steps per pass
+        tl, ta = statistics.median(t_loss), statistics.median(t_all)
+        tg = ta - tl
+        ops = normals * C4_OPS_LOSS / tl
+        line = {"metric": f"path-simulated loss + adjoint, {name}", "value": 2 * normals * 2 / ta,
+                "unit": "path-steps/s (loss + adjoint passes)", "n_gpus": 1, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ta * 1e3, "higher_is_better": True,
+                "dtype": "f32 paths, f64 sums", "data": "synthetic",
+                "config": {"workload": name, "portfolios": len(sizes), "options": P_tot, "stocks_per_portfolio": 50,
+                           "ell": ell, "steps_per_path": 1 << ell, "inner_pairs": pairs, "M": M,
+                           "method": "Milstein", "delta_rel": 0.01},
+                "loss_pass_s": tl, "adjoint_pass_s": tg,
+                "roofline": {"bound": "alu", "achieved": ops / 1e12, "peak": peak, "unit": "Tops/s",
+                             "frac": ops / 1e12 / peak, "traffic": None,
+                             "ops_per_pair_step": C4_OPS_LOSS, "kernel": "k_adj_paths (loss pass)",
+                             "peak_source": "issue-slot peak 148 SM x 128 lanes x sampled SM clock"},
+                "clocks": clk, "vs_baseline": None}
+        print(json.dumps(line))
+
+
 # ---------------------------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
@@ -231,13 +305,16 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=20.0, help="CPU seconds of reference sampling")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison runs")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--case", default=None, choices=["small"],
-                    help="small: a few fixed level calls of the FP32 sampler (profiling case)")
+    ap.add_argument("--case", default=None, choices=["small", "c4", "c4-small"],
+                    help="small: a few fixed level calls of the FP32 sampler (profiling case); "
+                         "c4: the path-simulated loss with adjoint; c4-small: its profiling case")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
     if args.case == "small":
         return small_case()
+    if args.case in ("c4", "c4-small"):
+        return c4_case(args, small=args.case == "c4-small")
 
     sys.path.insert(0, PKG)
     import nmlmc as nm

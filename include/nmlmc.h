@@ -272,9 +272,15 @@ int nmlmc_path_adjoint(nmlmc_ctx* ctx, const nmlmc_portfolio_batch* batch, const
 int nmlmc_reset_streams(nmlmc_ctx* ctx);
 /* One level: M outer samples at level ell. */
 int nmlmc_sample(nmlmc_ctx* ctx, uint32_t ell, uint64_t M, nmlmc_level_result* out);
-/* Several levels in one submission (OUTER layout: one CUDA graph, levels run concurrently). */
+/* Several levels in one submission.  OUTER layout: the levels' launch sequences are captured
+ * into one CUDA graph (kept and updated in place while the topology repeats), each level summing
+ * into its own slot, one device->host copy and one synchronisation for the round; levels run one
+ * after another inside the graph.  Up to 64 levels; with tracing or phase profiling armed, or on
+ * the CORE layout, the levels run as consecutive nmlmc_sample calls. */
 int nmlmc_sample_levels(nmlmc_ctx* ctx, uint32_t n, const uint32_t* ells, const uint64_t* Ms,
                         nmlmc_level_result* outs);
+/* CUDA graphs of nmlmc_sample_levels: instantiated, updated in place, launched. */
+int nmlmc_graph_stats(nmlmc_ctx* ctx, uint64_t* instantiations, uint64_t* updates, uint64_t* launches);
 /* Arms a host buffer of `cap` records for the next nmlmc_sample call (M <= cap). */
 int nmlmc_set_trace(nmlmc_ctx* ctx, nmlmc_trace_rec* host_buf, uint64_t cap);
 /* Full portfolio loss L(Y) for outer samples [first, first + n) of level `ell` (OUTER layout

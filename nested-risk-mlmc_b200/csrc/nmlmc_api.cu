@@ -1,4 +1,5 @@
 // C ABI of the level sampler: contexts, the reference-named surface and host-side set-up.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -84,6 +85,9 @@ RT h_norm_cdf_inv(RT p) {
            (((((b[0] * r + b[1]) * r + b[2]) * r + b[3]) * r + b[4]) * r + 1);
 }
 
+// Levels one nmlmc_sample_levels submission may hold (accumulator slots of the OUTER buffers).
+constexpr uint32_t kMaxSubmit = 64;
+
 // Portfolio as handed to the sampler, kept on the host in double (the values are the real_t
 // ones when the context computes in float).
 struct HostPortfolio {
@@ -146,6 +150,11 @@ struct nmlmc_ctx {
     uint64_t next_outer[NMLMC_MAX_LEVELS] = {};
     // pinned staging
     double* h_pin = nullptr;          // 32 doubles
+    // one-submission level rounds (nmlmc_sample_levels on the OUTER layout)
+    double* h_lev = nullptr;          // pinned [kMaxSubmit][16] sums, then [kMaxSubmit][2] stamps
+    uint64_t* d_stamps = nullptr;     // device [kMaxSubmit][2] level begin / end (ns)
+    cudaGraphExec_t gexec = nullptr;  // executable graph of the last submission
+    uint64_t graph_instantiations = 0, graph_updates = 0, graph_launches = 0;
     // trace
     nmlmc_trace_rec* trace_host = nullptr;
     uint64_t trace_cap = 0;
@@ -378,7 +387,7 @@ int alloc_outer(nmlmc_ctx* c) {
               cudaMalloc(&B.class_items, cap * sizeof(uint32_t)) == cudaSuccess &&
               cudaMalloc(&B.counters, 256 * sizeof(uint32_t)) == cudaSuccess &&
               cudaMalloc(&B.block_sums, (size_t)B.grid * 16 * sizeof(double)) == cudaSuccess &&
-              cudaMalloc(&B.level_acc, 16 * sizeof(double)) == cudaSuccess;
+              cudaMalloc(&B.level_acc, kMaxSubmit * 16 * sizeof(double)) == cudaSuccess;
     if (!ok) return set_err(NMLMC_ERR_NOMEM);
     cudaMemset(B.counters, 0, 256 * sizeof(uint32_t));
     c->ob_alloc = true;
@@ -469,45 +478,7 @@ void prof_collect(nmlmc_ctx* c) {
     c->pn = 0;
 }
 
-template <class RT>
-int sample_outer(nmlmc_ctx* c, uint32_t ell, uint64_t Mtotal, nmlmc_level_result* out) {
-    // this rank's static share of the call's outer samples (all of them when world = 1)
-    const uint64_t q = Mtotal / c->shard_world, rem = Mtotal % c->shard_world;
-    const uint64_t lo = q * c->shard_rank + (c->shard_rank < rem ? c->shard_rank : rem);
-    const uint64_t M = q + (c->shard_rank < rem ? 1 : 0);
-    OuterLevel<RT> L{};
-    L.ell = ell;
-    L.M = M;
-    L.first_index = c->next_outer[ell] + lo;
-    L.seed = c->cfg.seed;
-    L.fine_only = ell == 0;
-    L.antithetic = c->cfg.antithetic != 0;
-    L.N0 = c->cfg.N0;
-    L.chunk = c->cfg.N0 >= 32 ? 32 : c->cfg.N0;
-    L.adaptive_r = (RT)c->cfg.adaptive_r;
-    L.cf = count_params(c->cfg, ell);
-    L.cc = count_params(c->cfg, ell == 0 ? 0 : ell - 1);
-    const bool adapt = is_adaptive(c->cfg, c->cfg.adaptive_r);
-    L.adaptive_f = adapt && L.cf.max_count > 2 * L.cf.base_count;
-    L.adaptive_c = !L.fine_only && adapt && L.cc.max_count > 2 * L.cc.base_count;
-    L.mp = model_params<RT>(c);
-    if (c->kind == KIND_PORTFOLIO) {
-        if constexpr (sizeof(RT) == 4) L.ot = c->dpf32.table; else L.ot = c->dpf64.table;
-    }
-    TraceRec* tr = c->trace_host ? c->d_trace : nullptr;
-    c->ob.prof_mark = c->prof ? prof_mark : nullptr;
-    c->ob.prof_user = c;
-    NM_CUDA(cudaEventRecord(c->ev0, c->stream), "event");
-    NM_CUDA(outer_level_begin(c->ob, c->stream), "level begin");
-    if (M) NM_CUDA(outer_sample_level<RT>(L, c->kind, c->cfg.precision, c->ob, tr, c->stream), "outer level kernels");
-    NM_CUDA(cudaEventRecord(c->ev1, c->stream), "event");
-    NM_CUDA(cudaMemcpyAsync(c->h_pin, c->ob.level_acc, 16 * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "d2h");
-    if (tr && M) NM_CUDA(cudaMemcpyAsync(c->trace_host, tr, M * sizeof(TraceRec), cudaMemcpyDeviceToHost, c->stream), "d2h");
-    NM_CUDA(cudaStreamSynchronize(c->stream), "sync");
-    if (c->prof) prof_collect(c);
-    float ms = 0;
-    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-    const double* a = c->h_pin;
+void fill_outer_result(const nmlmc_ctx* c, const double* a, uint64_t M, double seconds, nmlmc_level_result* out) {
     for (int j = 0; j < 4; j++) { out->fsums[j] = a[j]; out->diffsums[j] = a[4 + j]; }
     out->total_work = a[8];
     out->M = M;
@@ -523,9 +494,134 @@ int sample_outer(nmlmc_ctx* c, uint32_t ell, uint64_t Mtotal, nmlmc_level_result
         out->inner_stats[4] = 0;
         out->inner_stats[5] = M + inner * (c->kind == KIND_REF_MODEL ? 2 : 1);
     }
-    out->seconds = ms * 1e-3;
+    out->seconds = seconds;
+}
+
+template <class RT>
+OuterLevel<RT> outer_level_params(const nmlmc_ctx* c, uint32_t ell, uint64_t M, uint64_t first_index) {
+    OuterLevel<RT> L{};
+    L.ell = ell;
+    L.M = M;
+    L.first_index = first_index;
+    L.seed = c->cfg.seed;
+    L.fine_only = ell == 0;
+    L.antithetic = c->cfg.antithetic != 0;
+    L.N0 = c->cfg.N0;
+    L.chunk = c->cfg.N0 >= 32 ? 32 : c->cfg.N0;
+    L.adaptive_r = (RT)c->cfg.adaptive_r;
+    L.cf = count_params(c->cfg, ell);
+    L.cc = count_params(c->cfg, ell == 0 ? 0 : ell - 1);
+    const bool adapt = is_adaptive(c->cfg, c->cfg.adaptive_r);
+    L.adaptive_f = adapt && L.cf.max_count > 2 * L.cf.base_count;
+    L.adaptive_c = !L.fine_only && adapt && L.cc.max_count > 2 * L.cc.base_count;
+    L.mp = model_params<RT>(c);
+    if (c->kind == KIND_PORTFOLIO) {
+        if constexpr (sizeof(RT) == 4) L.ot = c->dpf32.table; else L.ot = c->dpf64.table;
+    }
+    return L;
+}
+
+template <class RT>
+int sample_outer(nmlmc_ctx* c, uint32_t ell, uint64_t Mtotal, nmlmc_level_result* out) {
+    // this rank's static share of the call's outer samples (all of them when world = 1)
+    const uint64_t q = Mtotal / c->shard_world, rem = Mtotal % c->shard_world;
+    const uint64_t lo = q * c->shard_rank + (c->shard_rank < rem ? c->shard_rank : rem);
+    const uint64_t M = q + (c->shard_rank < rem ? 1 : 0);
+    OuterLevel<RT> L = outer_level_params<RT>(c, ell, M, c->next_outer[ell] + lo);
+    TraceRec* tr = c->trace_host ? c->d_trace : nullptr;
+    c->ob.prof_mark = c->prof ? prof_mark : nullptr;
+    c->ob.prof_user = c;
+    NM_CUDA(cudaEventRecord(c->ev0, c->stream), "event");
+    NM_CUDA(outer_level_begin(c->ob, c->stream), "level begin");
+    if (M) NM_CUDA(outer_sample_level<RT>(L, c->kind, c->cfg.precision, c->ob, tr, c->stream), "outer level kernels");
+    NM_CUDA(cudaEventRecord(c->ev1, c->stream), "event");
+    NM_CUDA(cudaMemcpyAsync(c->h_pin, c->ob.level_acc, 16 * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "d2h");
+    if (tr && M) NM_CUDA(cudaMemcpyAsync(c->trace_host, tr, M * sizeof(TraceRec), cudaMemcpyDeviceToHost, c->stream), "d2h");
+    NM_CUDA(cudaStreamSynchronize(c->stream), "sync");
+    if (c->prof) prof_collect(c);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    fill_outer_result(c, c->h_pin, M, ms * 1e-3, out);
     c->next_outer[ell] += Mtotal;
     c->trace_host = nullptr;
+    return NMLMC_OK;
+}
+
+// This rank's share [lo, lo + M) of a call's Mtotal outer samples.
+void shard_range(const nmlmc_ctx* c, uint64_t Mtotal, uint64_t& lo, uint64_t& M) {
+    const uint64_t q = Mtotal / c->shard_world, rem = Mtotal % c->shard_world;
+    lo = q * c->shard_rank + (c->shard_rank < rem ? c->shard_rank : rem);
+    M = q + (c->shard_rank < rem ? 1 : 0);
+}
+
+// All levels of one MLMC round in one submission: the level sequences are captured from the
+// stream into a CUDA graph (no host round trip inside: device counters size every phase), each
+// level accumulating into its own slot; one copy of the slots and one synchronisation per round.
+// The executable graph is kept and updated in place (cudaGraphExecUpdate) while later rounds
+// have the same topology (the same levels and batch counts), re-instantiated otherwise.
+template <class RT>
+int sample_outer_levels(nmlmc_ctx* c, uint32_t n, const uint32_t* ells, const uint64_t* Mtot,
+                        nmlmc_level_result* outs) {
+    uint64_t next[NMLMC_MAX_LEVELS];
+    memcpy(next, c->next_outer, sizeof(next));
+    std::vector<uint64_t> Ms(n);
+    NM_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    cudaError_t err = cudaSuccess;
+    for (uint32_t i = 0; i < n && err == cudaSuccess; i++) {
+        const uint32_t ell = ells[i];
+        uint64_t lo, M;
+        shard_range(c, Mtot[i], lo, M);
+        Ms[i] = M;
+        OuterLevel<RT> L = outer_level_params<RT>(c, ell, M, next[ell] + lo);
+        next[ell] += Mtot[i];
+        OuterBuffers B = c->ob;
+        B.level_acc = c->ob.level_acc + 16 * (size_t)i;
+        B.prof_mark = nullptr;
+        err = launch_stamp(c->d_stamps + 2 * i, c->stream);
+        if (err == cudaSuccess) err = outer_level_begin(B, c->stream);
+        if (err == cudaSuccess && M) err = outer_sample_level<RT>(L, c->kind, c->cfg.precision, B, nullptr, c->stream);
+        if (err == cudaSuccess) err = launch_stamp(c->d_stamps + 2 * i + 1, c->stream);
+    }
+    uint64_t* h_st = reinterpret_cast<uint64_t*>(c->h_lev + kMaxSubmit * 16);
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(c->h_lev, c->ob.level_acc, (size_t)n * 16 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(h_st, c->d_stamps, (size_t)n * 2 * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(c->stream, &graph);
+    if (err == cudaSuccess) err = e2;
+    if (err != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return cuda_status(err, "capture level round");
+    }
+    if (c->gexec) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(c->gexec, graph, &info) == cudaSuccess) {
+            c->graph_updates++;
+        } else {
+            cudaGetLastError();
+            cudaGraphExecDestroy(c->gexec);
+            c->gexec = nullptr;
+        }
+    }
+    if (!c->gexec) {
+        err = cudaGraphInstantiate(&c->gexec, graph, 0);
+        if (err != cudaSuccess) {
+            c->gexec = nullptr;
+            cudaGraphDestroy(graph);
+            return cuda_status(err, "instantiate level round");
+        }
+        c->graph_instantiations++;
+    }
+    cudaGraphDestroy(graph);
+    NM_CUDA(cudaGraphLaunch(c->gexec, c->stream), "graph launch");
+    c->graph_launches++;
+    NM_CUDA(cudaStreamSynchronize(c->stream), "sync");
+    for (uint32_t i = 0; i < n; i++) {
+        const double sec = (double)(h_st[2 * i + 1] - h_st[2 * i]) * 1e-9;
+        fill_outer_result(c, c->h_lev + 16 * (size_t)i, Ms[i], sec, &outs[i]);
+        c->next_outer[ells[i]] += Mtot[i];
+    }
     return NMLMC_OK;
 }
 
@@ -589,6 +685,9 @@ int nmlmc_destroy(nmlmc_ctx* c) {
         cudaFree(B.level_acc);
     }
     for (cudaEvent_t e : c->pev) cudaEventDestroy(e);
+    dfree(c->d_stamps);
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    if (c->h_lev) cudaFreeHost(c->h_lev);
     if (c->h_pin) cudaFreeHost(c->h_pin);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -755,7 +854,7 @@ int path_adjoint_t(nmlmc_ctx* c, const nmlmc_portfolio_batch* b, const nmlmc_adj
     AdjLaunch<RT> A{};
     A.n = n; A.ell = a->ell; A.pairs = a->inner_pairs; A.M = a->M; A.seed = a->seed;
     A.milstein = a->milstein ? 1 : 0;
-    A.tile = (uint32_t)std::min<uint64_t>(kAdjMaxTile, a->M);
+    A.tile = 0;
     A.r = (RT)b->r; A.rho = (RT)b->rho; A.tau = (RT)b->tau;
     A.s1_rho2 = (RT)sqrt(1 - b->rho * b->rho); A.stau = (RT)sqrt(b->tau); A.disc_tau = (RT)exp(-b->r * b->tau);
     std::vector<uint32_t> so(b->stock_off, b->stock_off + n + 1), oo(b->option_off, b->option_off + n + 1);
@@ -767,6 +866,14 @@ int path_adjoint_t(nmlmc_ctx* c, const nmlmc_portfolio_batch* b, const nmlmc_adj
     }
     A.n_chunks = co[n];
     A.q_max = qmax;
+    // outer samples per CTA: at most kAdjMaxTile, and small enough for about 32 CTAs of four
+    // warps per SM (two waves at full occupancy) when the option chunks alone are too few
+    {
+        const uint64_t want = 148ull * 32;
+        const uint64_t rows = (want + A.n_chunks - 1) / A.n_chunks;
+        const uint64_t t = (a->M + rows - 1) / rows;
+        A.tile = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>({kAdjMaxTile, a->M, t}));
+    }
     std::vector<RT> S0(NS), mu(NS), sg(NS), K(NO), T(NO), w(NO), V0(NO), vega(NO);
     std::vector<int8_t> ty(NO);
     std::vector<uint32_t> si(b->stock_ind, b->stock_ind + NO);
@@ -883,6 +990,26 @@ int nmlmc_sample(nmlmc_ctx* c, uint32_t ell, uint64_t M, nmlmc_level_result* out
 int nmlmc_sample_levels(nmlmc_ctx* c, uint32_t n, const uint32_t* ells, const uint64_t* Ms,
                         nmlmc_level_result* outs) {
     if (!c || (n && (!ells || !Ms || !outs))) return set_err(NMLMC_ERR_ARG);
+    if (!c->configured || c->kind < 0) return set_err(NMLMC_ERR_STATE);
+    const nmlmc_config& k = c->cfg;
+    bool one_submission = n > 0 && n <= kMaxSubmit && k.streams == NMLMC_STREAMS_OUTER && !c->prof &&
+                          !c->trace_host && !(c->kind == KIND_PORTFOLIO && c->pf.mixed());
+    for (uint32_t i = 0; i < n && one_submission; i++) {
+        if (ells[i] >= NMLMC_MAX_LEVELS || (double)k.N0 * pow((double)k.beta, (double)ells[i]) > 4.0e9)
+            return set_err(NMLMC_ERR_ARG);
+    }
+    if (one_submission) {
+        cudaSetDevice(c->device);
+        int rc = ensure_portfolio(c);
+        if (rc || (rc = alloc_outer(c))) return rc;
+        if (!c->h_lev && cudaMallocHost(&c->h_lev, kMaxSubmit * 18 * sizeof(double)) != cudaSuccess)
+            return set_err(NMLMC_ERR_NOMEM);
+        if (!c->d_stamps && cudaMalloc(&c->d_stamps, kMaxSubmit * 2 * sizeof(uint64_t)) != cudaSuccess)
+            return set_err(NMLMC_ERR_NOMEM);
+        for (uint32_t i = 0; i < n; i++) memset(&outs[i], 0, sizeof(outs[i]));
+        return k.precision == NMLMC_PREC_FP64 ? sample_outer_levels<double>(c, n, ells, Ms, outs)
+                                              : sample_outer_levels<float>(c, n, ells, Ms, outs);
+    }
     for (uint32_t i = 0; i < n; i++) {
         int rc = nmlmc_sample(c, ells[i], Ms[i], &outs[i]);
         if (rc) return rc;
@@ -915,6 +1042,14 @@ int nmlmc_phase_kernel_time(nmlmc_ctx* c, uint64_t* launches, double* seconds) {
 }
 
 uint64_t nmlmc_kernel_launches(void) { return launches_total(); }
+
+int nmlmc_graph_stats(nmlmc_ctx* c, uint64_t* instantiations, uint64_t* updates, uint64_t* launches) {
+    if (!c || !instantiations || !updates || !launches) return set_err(NMLMC_ERR_ARG);
+    *instantiations = c->graph_instantiations;
+    *updates = c->graph_updates;
+    *launches = c->graph_launches;
+    return NMLMC_OK;
+}
 
 int nmlmc_portfolio_full_loss(nmlmc_ctx* c, uint32_t ell, uint64_t first, uint64_t n, double* host_loss) {
     if (!c || !host_loss) return set_err(NMLMC_ERR_ARG);

@@ -80,6 +80,7 @@ template <class RT>
 cudaError_t outer_sample_level(const OuterLevel<RT>& L, int kind, int prec, OuterBuffers& B,
                                TraceRec* trace, cudaStream_t stream);
 cudaError_t outer_level_begin(OuterBuffers& B, cudaStream_t stream);
+cudaError_t launch_stamp(uint64_t* slot, cudaStream_t stream);   // %globaltimer -> *slot
 
 // Portfolio loss sweep L(Y) over all options (K-quantile precompute).
 template <class RT>

@@ -683,6 +683,20 @@ __global__ void k_reduce_blocks(const double* block_sums, int grid, double* leve
     }
 }
 
+// Device timestamp (%globaltimer, nanoseconds): marks level boundaries inside a CUDA graph,
+// where event-record nodes carry no elapsed time.
+__global__ void k_stamp(uint64_t* slot) {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    *slot = t;
+}
+
+cudaError_t launch_stamp(uint64_t* slot, cudaStream_t stream) {
+    k_stamp<<<1, 1, 0, stream>>>(slot);
+    count_launch();
+    return cudaGetLastError();
+}
+
 // ---- host orchestration ----------------------------------------------------------------------
 static std::atomic<uint64_t> g_launches{0};
 void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }

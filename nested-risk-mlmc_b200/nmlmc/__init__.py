@@ -203,7 +203,7 @@ EXPORTS = [
     "nmlmc_mlmc_run_cb", "nmlmc_threefry_blocks", "nmlmc_outer_normals", "nmlmc_set_shard",
     "nmlmc_set_profiling", "nmlmc_phase_kernel_time", "nmlmc_kernel_launches",
     "nmlmc_sample_level_noalloc", "nmlmc_portfolio_generate", "nmlmc_set_portfolio_methods",
-    "nmlmc_path_adjoint",
+    "nmlmc_path_adjoint", "nmlmc_graph_stats",
 ]
 
 
@@ -351,10 +351,13 @@ class Sampler:
         return start, delta
 
     def path_adjoint(self, batch: dict, ell: int, pairs: int, M: int, delta_rel: float = 0.01,
-                     precision: int = PREC_FP64, seed: int = 0, milstein: bool = True,
+                     precision: int | None = None, seed: int = 0, milstein: bool = True,
                      grads: bool = True, loss: bool = False) -> dict:
         """Path-simulated loss of a portfolio batch (make_batch) with the adjoint gradients of
-        E[L] and of the sigmoid-smoothed P(L > K); see nmlmc_path_adjoint."""
+        E[L] and of the sigmoid-smoothed P(L > K); see nmlmc_path_adjoint.  precision: the
+        sampler's own unless given (PREC_REF32 runs the FP32 paths)."""
+        if precision is None:
+            precision = PREC_FP64 if self.cfg.precision == PREC_FP64 else PREC_FP32
         so = np.ascontiguousarray(batch["stock_off"], np.uint32)
         oo = np.ascontiguousarray(batch["option_off"], np.uint32)
         d = {k: np.ascontiguousarray(batch[k], np.float64) for k in
@@ -385,6 +388,12 @@ class Sampler:
         if loss:
             out["loss"] = lo.reshape(n, M)
         return out
+
+    def graph_stats(self) -> dict:
+        a, b, c = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        _check(self.L.nmlmc_graph_stats(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
+               "nmlmc_graph_stats")
+        return dict(instantiations=a.value, updates=b.value, launches=c.value)
 
     def reset_streams(self):
         _check(self.L.nmlmc_reset_streams(self.h), "nmlmc_reset_streams")
