@@ -295,6 +295,68 @@ def c4_case(args, small=False):
         print(json.dumps(line))
 
 
+def c3_case(args):
+    """Large portfolio: d = 200 stocks, P = 1e6 options (generator seed 1), K = the 99 % quantile
+    of the full loss over 1e5 outer samples; P(L > K) by continuation MLMC with the reference's
+    default importance sub-sampling (prob proportional to |w_i|, options sorted by |w_i|) and the
+    delta control variate, N0 = 64, beta = 2, adaptive r = 1.5.  The batched FP32 sampler (OUTER
+    streams, one CUDA graph per MLMC round) against the plain FP64 drop-in (reference stream
+    layout, 2048 virtual cores, one synchronous call per level) on the same GPU, both to the same
+    eps, and a direct estimate from 2e5 full evaluations as the accuracy check."""
+    import numpy as np
+    sys.path.insert(0, PKG)
+    import nmlmc as nm
+    eps = args.eps if args.eps else 1e-3
+    pf = nm.generate_portfolio(nm.PORTFOLIO_C3, 1)
+    order = np.argsort(-np.abs(pf["w"]), kind="stable")
+    for k in ("strike", "maturity", "w", "stock_ind", "type"):
+        pf[k] = pf[k][order]
+    pfw = dict(pf, prob=np.abs(pf["w"]))
+
+    def mk(prec, streams, K, seed, cores=0, sub=nm.SUB_RANDOM):
+        s = nm.Sampler(0, cores=cores or 2048, N0=64, beta=2, adaptive_r=1.5, precision=prec,
+                       streams=streams, seed=seed)
+        s.set_portfolio(pfw, r=0.05, rho=0.0, max_loss=K, tau=nm.TAU_WEEK, subsample=sub,
+                        use_delta_cv=True, discount=False)
+        return s
+
+    q = mk(nm.PREC_FP32, nm.STREAMS_OUTER, 0.0, seed=1)
+    K = nm.loss_quantile(q, 0.99, 100_000)
+    Ld = q.full_loss(62, 0, 200_000)
+    p_direct = float(np.mean(Ld > K))
+    sd = float(np.sqrt(p_direct * (1 - p_direct) / len(Ld)))
+    # warm-up: one MLMC run at a looser tolerance (module load, graph instantiation, allocations)
+    mk(nm.PREC_FP32, nm.STREAMS_OUTER, K, seed=4).mlmc_run(targetTOL=max(eps, 3e-3), M0=1024, batched=True)
+    runs = {}
+    cs = ClockSampler(0)
+    cs.start()
+    for name, prec, streams, cores, batched in (("fp32_batched", nm.PREC_FP32, nm.STREAMS_OUTER, 0, True),
+                                                 ("fp64_dropin", nm.PREC_FP64, nm.STREAMS_CORE, 2048, False)):
+        s = mk(prec, streams, K, seed=5, cores=cores)
+        t = time.perf_counter()
+        out = s.mlmc_run(targetTOL=eps, M0=1024, batched=batched)
+        wall = time.perf_counter() - t
+        runs[name] = dict(value=float(out["level_time"].sum()), e2e=wall, Eg=out["Eg"],
+                          levels=int(out["nlevels"]), starting_level=int(out["starting_level"]),
+                          level_M=[int(x) for x in out["level_M"]])
+    clk = cs.stop()
+    a, b = runs["fp32_batched"], runs["fp64_dropin"]
+    line = {"metric": f"time-to-eps (s) for MLMC P(L>K), large portfolio, eps={eps:g} absolute",
+            "value": a["value"], "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 1,
+            "ms_per_step": a["value"] * 1e3, "higher_is_better": False, "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded generator)",
+            "config": {"workload": "large portfolio d=200, P=1e6, K = 99% loss quantile",
+                       "sub_sampling": "random, prob ~ |w|, delta CV", "N0": 64, "beta": 2,
+                       "adaptive_r": 1.5, "eps": eps, "K": K,
+                       "eps_note": ("eps = 1e-4 needs starting level ~12 and an estimated 10 min on this "
+                                    "path (hours for the FP64 drop-in); not run in the default bench")},
+            "e2e": {"value": a["e2e"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": None},
+            "runs": runs, "p_direct": p_direct, "p_direct_sd": sd,
+            "speedup_vs_fp64_dropin": {"value": b["value"] / a["value"], "e2e": b["e2e"] / a["e2e"]},
+            "clocks": clk}
+    print(json.dumps(line))
+
+
 # ---------------------------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
@@ -305,7 +367,8 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=20.0, help="CPU seconds of reference sampling")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison runs")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--case", default=None, choices=["small", "c4", "c4-small"],
+    ap.add_argument("--eps", type=float, default=None, help="--case c3: target RMSE (default 1e-3)")
+    ap.add_argument("--case", default=None, choices=["small", "c3", "c4", "c4-small"],
                     help="small: a few fixed level calls of the FP32 sampler (profiling case); "
                          "c4: the path-simulated loss with adjoint; c4-small: its profiling case")
     args = ap.parse_args()
@@ -313,6 +376,8 @@ def main():
         return reference_arm(args)
     if args.case == "small":
         return small_case()
+    if args.case == "c3":
+        return c3_case(args)
     if args.case in ("c4", "c4-small"):
         return c4_case(args, small=args.case == "c4-small")
 

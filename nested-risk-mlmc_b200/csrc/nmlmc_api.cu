@@ -118,6 +118,9 @@ struct DevPortfolio {
     uint32_t* stock_ind = nullptr;
     int8_t* type = nullptr;
     FastOption* fast = nullptr;       // packed records of the FP32 path
+    FastOption* fast_s = nullptr;     // the same, scaled by 1 / sampling probability
+    uint2* alias = nullptr;           // alias table (OUTER, Subsampling::Random)
+    RT* phat = nullptr;
     OptionTable<RT> table{};
 };
 
@@ -201,7 +204,7 @@ template <class RT>
 void free_dev_portfolio(DevPortfolio<RT>& d) {
     dfree(d.strike); dfree(d.maturity); dfree(d.start); dfree(d.w); dfree(d.prob); dfree(d.W_est);
     dfree(d.cdf); dfree(d.S0); dfree(d.mu); dfree(d.sigma); dfree(d.delta_coalesce);
-    dfree(d.stock_ind); dfree(d.type); dfree(d.fast);
+    dfree(d.stock_ind); dfree(d.type); dfree(d.fast); dfree(d.fast_s); dfree(d.alias); dfree(d.phat);
     d.table = OptionTable<RT>{};
 }
 
@@ -229,6 +232,48 @@ void comp_params(HostPortfolio& h) {
         h.start[j] = (double)h_calc_bs<RT>(h.type[j], (RT)h.S0[s], (RT)h.strike[j], (RT)h.r, (RT)h.maturity[j], (RT)h.sigma[s]);
         h.delta_est[j] = (double)h_calc_delta<RT>(h.type[j], (RT)h.S0[s], (RT)h.strike[j], (RT)h.r, (RT)h.maturity[j], (RT)h.sigma[s]);
     }
+}
+
+// Alias table of the OUTER layout's importance sub-sampling (Walker's method in Vose's
+// construction, on integers).  The masses W_j = round(p_j / sum p * P 2^32), with the rounding
+// residue given to the largest, sum exactly to P 2^32; column j keeps threshold thr_j < 2^32 of
+// its own mass and hands the rest to alias_j.  One 64-bit draw v picks column floor(v P / 2^64)
+// and the coin (v P mod 2^64) >> 32, so option j is drawn with probability exactly
+// phat_j = W_j / (P 2^32), the weight the estimator divides by.  Full columns carry
+// thr = 2^32 - 1 and alias = themselves.
+void build_alias(uint32_t P, const std::vector<double>& p, std::vector<uint2>& tab, std::vector<double>& phat) {
+    double S = 0;
+    for (uint32_t j = 0; j < P; j++) S += p[j];
+    const uint64_t unit = 1ull << 32, total = (uint64_t)P << 32;
+    std::vector<uint64_t> W(P);
+    uint64_t sum = 0;
+    uint32_t jmax = 0;
+    for (uint32_t j = 0; j < P; j++) {
+        W[j] = (uint64_t)llround(p[j] / S * (double)total);
+        sum += W[j];
+        if (W[j] > W[jmax]) jmax = j;
+    }
+    if (sum > total) W[jmax] -= sum - total; else W[jmax] += total - sum;
+    phat.resize(P);
+    for (uint32_t j = 0; j < P; j++) phat[j] = (double)W[j] / (double)total;
+    tab.assign(P, uint2{0xffffffffu, 0});
+    std::vector<uint32_t> small, large;
+    for (uint32_t j = 0; j < P; j++) {
+        tab[j].y = j;
+        (W[j] < unit ? small : large).push_back(j);
+    }
+    while (!small.empty() && !large.empty()) {
+        const uint32_t sj = small.back(), lj = large.back();
+        small.pop_back();
+        tab[sj].x = (uint32_t)W[sj];
+        tab[sj].y = lj;
+        W[lj] -= unit - W[sj];
+        if (W[lj] < unit) {
+            large.pop_back();
+            small.push_back(lj);
+        }
+    }
+    for (uint32_t j : small) tab[j].x = (uint32_t)std::min<uint64_t>(W[j], 0xffffffffull);   // == unit: exact sums
 }
 
 // portfolio_comp_params + portfolio_update_data (portfolio_sampler.cpp:631-700) in real_t.
@@ -281,6 +326,21 @@ int build_dev_portfolio(nmlmc_ctx* c, DevPortfolio<RT>& d) {
     t.use_coarse_delta_cv = h.use_coarse_delta_cv; t.use_antithetic_risk = h.use_antithetic_risk;
     t.use_milstein = h.use_milstein;
     t.fast = nullptr;
+    t.fast_s = nullptr;
+    t.alias = nullptr;
+    t.phat = nullptr;
+    std::vector<double> phat;
+    if (h.subsample == SUB_RANDOM && !h.mixed()) {
+        std::vector<double> pr(P);
+        for (uint32_t j = 0; j < P; j++) pr[j] = (double)prob[j];
+        std::vector<uint2> tab;
+        build_alias(P, pr, tab, phat);
+        std::vector<RT> ph(P);
+        for (uint32_t j = 0; j < P; j++) ph[j] = (RT)phat[j];
+        if ((rc = upload(d.alias, tab)) || (rc = upload(d.phat, ph))) return rc;
+        t.alias = d.alias;
+        t.phat = d.phat;
+    }
     if constexpr (sizeof(RT) == 4) {
         // packed FP32 records (nmlmc_bs.cuh): per-option constants folded in double, rounded once;
         // only for unit work estimates (every option of the BS method costs one evaluation)
@@ -307,6 +367,23 @@ int build_dev_portfolio(nmlmc_ctx* c, DevPortfolio<RT>& d) {
             }
             if ((rc = upload(d.fast, fo))) return rc;
             t.fast = d.fast;
+            if (h.subsample != SUB_NONE) {
+                // sampler records: the inner value X = loss_j / phat_j folded into the weights
+                for (uint32_t j = 0; j < P; j++) {
+                    const double sc = h.subsample == SUB_UNIFORM ? (double)P : (phat[j] > 0 ? 1.0 / phat[j] : 0.0);
+                    const uint32_t s = h.stock_ind[j];
+                    const double sg = h.sigma[s], K = h.strike[j], T = h.maturity[j], Tr = T - h.tau;
+                    const double m = h.type[j] > 0 ? 1.0 : -1.0;
+                    const double V0 = h_calc_bs<double>(h.type[j], h.S0[s], K, h.r, T, sg);
+                    const double disc = h.discount ? exp(-h.r * h.tau) : 1.0;
+                    fo[j].wR = (float)(-sc * h.w[j] * disc * m);
+                    fo[j].wK = (float)(sc * h.w[j] * disc * m * K * exp(-h.r * Tr));
+                    fo[j].wV0 = (float)(sc * h.w[j] * V0);
+                    fo[j].cv = h.use_delta_cv ? (float)(sc * h.w[j] * h_calc_delta<double>(h.type[j], h.S0[s], K, h.r, T, sg)) : 0.f;
+                }
+                if ((rc = upload(d.fast_s, fo))) return rc;
+                t.fast_s = d.fast_s;
+            }
         }
     }
     return NMLMC_OK;

@@ -56,6 +56,9 @@ struct OptionTable {
     const RT* sigma;
     const RT* delta_coalesce;
     const struct FastOption* fast;   // FP32 path: packed records (nmlmc_bs.cuh), else nullptr
+    const struct FastOption* fast_s; // the same records scaled by 1 / (sampling probability)
+    const uint2* alias;              // OUTER Subsampling::Random: alias table {threshold, alias}
+    const RT* phat;                  // sampling probability of each option under the alias table
     uint32_t P, Q;
     RT r, rho, s1_rho2, max_loss, tau, stau, prob_norm, compute_prob0, inv_count_prob;
     int subsample, use_delta_cv, discount;

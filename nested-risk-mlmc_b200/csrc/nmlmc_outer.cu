@@ -152,27 +152,24 @@ __device__ __forceinline__ RT pf_value(const OptionTable<RT>& ot, const RT* Rrow
     return val;
 }
 
-// option index and its probability (sample_inner_random_option_ind, 346-370) from one 64-bit
-// value of the OUTER layout: uniform sub-sampling takes the exact integer floor(v * P / 2^64)
-// (identical in every precision); the CDF search uses u01<real_t>(v) as the reference does.
+// Option index of one inner sample from one 64-bit value of the OUTER layout (the draw of
+// sample_inner_random_option_ind, 346-370, with its own addressing): column j = floor(v P / 2^64),
+// exact in every precision.  Uniform sub-sampling takes j (prob 1 / P); importance sub-sampling
+// (Subsampling::Random) flips the column's alias coin (v P mod 2^64) >> 32 — O(1) instead of the
+// reference's CDF binary search, the distribution of the table's exact masses phat.
+__device__ __forceinline__ uint32_t pf_index(const uint2* alias, uint32_t P, uint64_t v) {
+    const uint32_t j = (uint32_t)__umul64hi(v, (uint64_t)P);
+    if (!alias) return j;
+    const uint32_t coin = (uint32_t)((v * (uint64_t)P) >> 32);
+    const uint2 e = alias[j];
+    return coin < e.x ? j : e.y;
+}
+
 template <class RT>
 __device__ __forceinline__ uint32_t pf_pick(const OptionTable<RT>& ot, uint64_t v, RT& prob) {
-    if (ot.subsample == SUB_UNIFORM) {
-        prob = ot.inv_count_prob;
-        return (uint32_t)__umul64hi(v, (uint64_t)ot.P);
-    }
-    RT u = sizeof(RT) == 4 ? (RT)u01_f(v) : (RT)u01_d(v);
-    RT uu = xmul(u, ot.compute_prob0);
-    uint32_t pos0 = 0, pos1 = ot.P;
-    if (ot.P > 1) {
-        uint32_t steps = 32 - __clz(ot.P - 1);
-        for (uint32_t s = 0; s < steps; s++) {
-            uint32_t mid = (pos0 + pos1) / 2;
-            if (mid > 0 && uu < ot.cdf[mid]) pos1 = mid; else pos0 = mid;
-        }
-    }
-    prob = xdiv(ot.prob[pos0], ot.prob_norm);
-    return pos0;
+    const uint32_t j = pf_index(ot.subsample == SUB_UNIFORM ? nullptr : ot.alias, ot.P, v);
+    prob = ot.subsample == SUB_UNIFORM ? ot.inv_count_prob : ot.phat[j];
+    return j;
 }
 
 // ---- one chunk: inner samples [s0, s0 + C) of phase `tag` of outer sample `item` ----------
@@ -222,23 +219,24 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
             }
         }
         work += (double)C;
-    } else if (PREC == PREC_FP32 && L.ot.fast && L.ot.subsample == SUB_UNIFORM) {
-        // portfolio, FP32: packed records and the SFU Black-Scholes (nmlmc_bs.cuh); X = P * loss_i
+    } else if (PREC == PREC_FP32 && L.ot.fast_s) {
+        // portfolio, FP32: packed records scaled by 1 / (sampling probability), the SFU
+        // Black-Scholes (nmlmc_bs.cuh); X = loss_j / phat_j
         const OptionTable<RT>& ot = L.ot;
         const float* Rrow = reinterpret_cast<const float*>(D.B.Rt) + (size_t)item * ot.Q;
-        const float Pf = (float)ot.P;
+        const uint2* alias = ot.subsample == SUB_UNIFORM ? nullptr : ot.alias;
 #pragma unroll 2
         for (uint32_t b = 0; b < C / 2; b++) {
             uint64_t v[2];
             threefry2x64((s0 >> 1) + b, tag, key, v[0], v[1]);
 #pragma unroll
             for (int q = 0; q < 2; q++) {
-                const uint32_t j = (uint32_t)__umul64hi(v[q], (uint64_t)ot.P);
-                const FastOption o = ot.fast[j];
+                const uint32_t j = pf_index(alias, ot.P, v[q]);
+                const FastOption o = ot.fast_s[j];
                 const uint32_t st = o.asset_type & 0x7fffffffu;
                 const float R = Rrow[st];
                 const float S0 = o.cv != 0.f ? (float)ot.S0[st] : 0.f;
-                const float d = Pf * option_loss_fast(o, R, __logf(R), S0);
+                const float d = option_loss_fast(o, R, __logf(R), S0);
                 a1.add((RT)d);
                 if (want_s2) a2.add((RT)(d * d));
             }

@@ -136,6 +136,9 @@ struct o_ctx {
     int use_coarse_delta_cv, use_antithetic_risk, use_milstein;
     uint32_t dt_h0inv, dt_beta;
     double dt_prob_expo;
+    /* OUTER layout, Subsampling::Random: alias table of the exact masses (o_build_alias) */
+    uint32_t *alias_thr, *alias_idx;
+    double *phat;
     /* CORE layout: persistent per-core streams */
     o_rs *rs_sync, *rs_inner;
     /* OUTER layout: next outer index per level, shard */
@@ -166,7 +169,49 @@ o_ctx *o_create(int prec, int streams, uint32_t cores, uint32_t N0, uint32_t bet
 
 static void free_portfolio(o_ctx *c) {
     free(c->S0); free(c->mu); free(c->sigma); free(c->cdf); free(c->delta_coalesce); free(c->opt);
+    free(c->alias_thr); free(c->alias_idx); free(c->phat);
     c->S0 = c->mu = c->sigma = c->cdf = c->delta_coalesce = NULL; c->opt = NULL;
+    c->alias_thr = c->alias_idx = NULL; c->phat = NULL;
+}
+
+/* Alias table of the OUTER layout's importance sub-sampling (the batched path's own addressing;
+ * the reference draws with rand_int_cdf, common.hpp:160-176, which the CORE layout keeps).
+ * Walker's method in Vose's construction on integers: masses W_j = round(p_j / sum p * P 2^32),
+ * the rounding residue to the largest, sum exactly P 2^32; column j keeps thr_j of its own mass
+ * and hands the rest to alias_j; full columns keep thr = 2^32 - 1 and alias themselves.  Option j
+ * is drawn with probability exactly phat_j = W_j / (P 2^32). */
+void o_build_alias(uint32_t P, const double *p, uint32_t *thr, uint32_t *alias, double *phat) {
+    double S = 0;
+    for (uint32_t j = 0; j < P; j++) S += p[j];
+    const uint64_t unit = 1ull << 32, total = (uint64_t)P << 32;
+    uint64_t *W = (uint64_t *)malloc(P * sizeof(uint64_t));
+    uint32_t *small = (uint32_t *)malloc(P * sizeof(uint32_t)), *large = (uint32_t *)malloc(P * sizeof(uint32_t));
+    uint64_t sum = 0;
+    uint32_t jmax = 0, ns = 0, nl = 0;
+    for (uint32_t j = 0; j < P; j++) {
+        W[j] = (uint64_t)llround(p[j] / S * (double)total);
+        sum += W[j];
+        if (W[j] > W[jmax]) jmax = j;
+    }
+    if (sum > total) W[jmax] -= sum - total; else W[jmax] += total - sum;
+    for (uint32_t j = 0; j < P; j++) {
+        phat[j] = (double)W[j] / (double)total;
+        thr[j] = 0xffffffffu;
+        alias[j] = j;
+        if (W[j] < unit) small[ns++] = j; else large[nl++] = j;
+    }
+    while (ns > 0 && nl > 0) {
+        const uint32_t sj = small[--ns], lj = large[nl - 1];
+        thr[sj] = (uint32_t)W[sj];
+        alias[sj] = lj;
+        W[lj] -= unit - W[sj];
+        if (W[lj] < unit) {
+            nl--;
+            small[ns++] = lj;
+        }
+    }
+    for (uint32_t q = 0; q < ns; q++) thr[small[q]] = W[small[q]] < 0xffffffffull ? (uint32_t)W[small[q]] : 0xffffffffu;
+    free(W); free(small); free(large);
 }
 
 void o_destroy(o_ctx *c) {

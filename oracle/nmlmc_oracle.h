@@ -78,6 +78,8 @@ int o_set_portfolio_methods(o_ctx *, uint32_t Q, const double *S0, const double 
                             int use_delta_cv, int use_coarse_delta_cv, int use_antithetic_risk,
                             int use_milstein, uint32_t dt_h0inv, uint32_t dt_beta,
                             double dt_prob_expo);
+/* Alias table of the OUTER layout's importance sub-sampling (see nmlmc_oracle.c). */
+void o_build_alias(uint32_t P, const double *p, uint32_t *thr, uint32_t *alias, double *phat);
 /* One sample(ell, M) call (nested_sampler.hpp:646-694).  trace (M records) and events may be
  * NULL.  Returns 0, or -1 if the events buffer is too small. */
 int o_sample(o_ctx *, uint32_t ell, uint64_t M, double fsums[4], double diffsums[4],

@@ -459,3 +459,18 @@ def adj_loss(batch: dict, ell: int, pairs: int, M: int, seed: int, milstein: boo
                  _p(si, _u32p), _p(ty, _i32p), batch["r"], batch["rho"], batch["tau"], ell, pairs, M,
                  seed, int(milstein), _p(out, _dp))
     return out.reshape(n, M)
+
+
+def build_alias(p) -> tuple:
+    """Alias table (thr, alias, phat) of the OUTER layout's importance sub-sampling."""
+    L = lib()
+    if not getattr(L, "_alias_bound", False):
+        L.o_build_alias.argtypes = [ctypes.c_uint32, _dp, _u32p, _u32p, _dp]
+        L._alias_bound = True
+    p = np.ascontiguousarray(p, np.float64)
+    P = len(p)
+    thr = np.zeros(P, np.uint32)
+    al = np.zeros(P, np.uint32)
+    ph = np.zeros(P)
+    L.o_build_alias(P, _p(p, _dp), _p(thr, _u32p), _p(al, _u32p), _p(ph, _dp))
+    return thr, al, ph

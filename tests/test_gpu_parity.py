@@ -246,7 +246,7 @@ def test_outer_layout_matches_oracle(nm, case, o_prec):
             assert gg["stats"][0] == go["stats"][0]
 
 
-@pytest.mark.parametrize("case", OUTER_CASES[:5], ids=[c["name"] for c in OUTER_CASES[:5]])
+@pytest.mark.parametrize("case", OUTER_CASES, ids=[c["name"] for c in OUTER_CASES])
 def test_fp32_against_fp64_same_streams(nm, case):
     """Batched FP32 (SFU Box-Muller, Kahan sums) against all-FP64 on the same OUTER streams."""
     c32 = dict(case, gpu_prec=nm.PREC_FP32)

@@ -186,3 +186,39 @@ def test_adj_oracle_risk_neutral_mean():
     L = O.adj_loss(b, 4, 32, 400, 7, True)[0]
     se = L.std() / np.sqrt(L.size)
     assert abs(L.mean()) < 4 * se + 5e-3 * np.abs(b["w"]).sum(), (L.mean(), se)
+
+
+@pytest.mark.parametrize("P", [1, 2, 7, 1000, 4096])
+def test_alias_table_exact_masses(P):
+    """Every option's mass in the alias table equals W_j = phat_j P 2^32 exactly, the masses sum
+    to P 2^32, and phat is within one mass unit of the requested probabilities."""
+    g = np.random.default_rng(P)
+    p = np.abs(g.standard_normal(P)) ** 3
+    p[: max(1, P // 10)] *= 1e-9                       # some nearly-zero masses
+    thr, al, ph = O.build_alias(p)
+    unit = 1 << 32
+    mass = np.zeros(P, dtype=object)
+    for j in range(P):
+        mass[j] += int(thr[j])
+        mass[int(al[j])] += unit - int(thr[j])
+    W = [int(round(x * P * unit)) for x in ph]
+    assert list(mass) == W
+    assert sum(W) == P * unit
+    # rounding: half a unit per option, the summed residue (at most P/2 units) on the largest
+    np.testing.assert_allclose(ph, p / p.sum(), rtol=0, atol=(P / 2 + 1) / (P * unit) + 1e-16)
+
+
+def test_alias_draw_distribution():
+    """The OUTER draw (column floor(v P / 2^64), coin (v P mod 2^64) >> 32) reproduces phat."""
+    g = np.random.default_rng(1)
+    p = np.array([5.0, 1.0, 0.25, 3.0, 0.75])
+    thr, al, ph = O.build_alias(p)
+    P = len(p)
+    n = 200_000
+    idx = np.empty(n, np.int64)
+    for t, v in enumerate(int(x) for x in g.integers(0, 2**64, n, dtype=np.uint64, endpoint=False)):
+        col = (v * P) >> 64
+        coin = ((v * P) & (2**64 - 1)) >> 32
+        idx[t] = col if coin < int(thr[col]) else int(al[col])
+    freq = np.bincount(idx, minlength=P) / n
+    assert np.all(np.abs(freq - ph) <= 4 * np.sqrt(ph * (1 - ph) / n)), (freq, ph)
