@@ -454,7 +454,7 @@ int alloc_outer(nmlmc_ctx* c) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
     B.cap = cap;
     B.Q = Q;
-    B.grid = sms * 4;
+    B.grid = sms * 4;            // partial-sum slots; the phase kernel runs its resident CTAs (<= grid)
     bool ok = cudaMalloc(&B.Yv, cap * sizeof(double)) == cudaSuccess &&
               cudaMalloc(&B.Rt, (Q ? cap * Q : 1) * sizeof(double)) == cudaSuccess &&
               cudaMalloc(&B.cnt_f, cap * sizeof(uint32_t)) == cudaSuccess &&

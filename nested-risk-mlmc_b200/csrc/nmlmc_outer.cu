@@ -40,8 +40,10 @@ enum : int {
     CNT_LIST = 0,        // [4]: fine list size (ping-pong slots 0/1), coarse list size (2/3)
     CNT_CLASS = 8,       // [64]: outer samples per final class
     CNT_FILL = 72,       // [64]: scatter fill per class
-    CNT_TOTAL = 144
+    CNT_TOTAL = 144,
+    CNT_QUEUE = 192      // [kMaxSegs]: tile tickets of the phase kernel's work queue, per segment
 };
+static_assert(CNT_QUEUE + kMaxSegs <= 256, "counter slots");
 
 // ---- accumulators -------------------------------------------------------------------------
 // FP32: compensated pair (hi + lo) — Kahan accumulation inside a thread, TwoSum merging across
@@ -381,6 +383,7 @@ __global__ void __launch_bounds__(kTile) k_phase(DevLevel<RT> D, SegSet S, Trace
     __shared__ Acc<PREC> sm_a2[kWarps];
     __shared__ float sm_ind[kWarps];
     __shared__ double sm_acc[kWarps][16];
+    __shared__ uint64_t sm_ticket;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const uint32_t C = D.L.chunk;
     uint32_t* counters = D.B.counters;
@@ -403,11 +406,20 @@ __global__ void __launch_bounds__(kTile) k_phase(DevLevel<RT> D, SegSet S, Trace
         const bool pilot = g.mode != 2;
         if (pilot && blockIdx.x == 0 && t == 0) sm_acc[0][9] += (double)n_items * (double)g.count;
 
+        // The grid is persistent (the CTAs resident at once) and claims the segment's tiles from a
+        // device work queue: one ticket per tile, so no CTA waits for a second wave and uneven
+        // tiles balance themselves.  Which CTA evaluates a tile does not change any result.
+        uint32_t* queue = counters + CNT_QUEUE + si;
         if (nch <= (uint32_t)kTile) {
             // ---- a tile holds kTile / nch whole items ----
             const uint32_t per_tile = kTile / nch;
             const uint64_t tiles = ((uint64_t)n_items + per_tile - 1) / per_tile;
-            for (uint64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+            for (;;) {
+                if (t == 0) sm_ticket = atomicAdd(queue, 1u);
+                __syncthreads();
+                const uint64_t tile = sm_ticket;
+                __syncthreads();
+                if (tile >= tiles) break;
                 const uint64_t lin = tile * per_tile + (t >> g.nch_log2);
                 const uint32_t j = t & (nch - 1);
                 const bool valid = lin < n_items;
@@ -492,7 +504,12 @@ __global__ void __launch_bounds__(kTile) k_phase(DevLevel<RT> D, SegSet S, Trace
         } else {
             // ---- one CTA walks an item tile by tile ----
             const uint32_t tiles_per_item = nch / kTile;
-            for (uint64_t it = blockIdx.x; it < n_items; it += gridDim.x) {
+            for (;;) {
+                if (t == 0) sm_ticket = atomicAdd(queue, 1u);
+                __syncthreads();
+                const uint64_t it = sm_ticket;
+                __syncthreads();
+                if (it >= n_items) break;
                 const uint32_t item = list ? list[it] : (uint32_t)it;
                 uint32_t gs = nch;
                 uint64_t csmall = g.count;
@@ -700,10 +717,28 @@ static std::atomic<uint64_t> g_launches{0};
 void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 uint64_t launches_total() { return g_launches.load(std::memory_order_relaxed); }
 
+// Persistent grid of the phase kernel: the CTAs that are resident at once (occupancy x SMs),
+// at most the grid the partial-sum buffer was sized for.
+template <class RT, int KIND, int PREC>
+static int phase_grid(int cap) {
+    static int g = 0;
+    if (g == 0) {
+        int dev = 0, sms = 148, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_phase<RT, KIND, PREC>, kTile, 0) != cudaSuccess ||
+            per_sm < 1)
+            per_sm = 1;
+        g = per_sm * sms;
+    }
+    return g < cap ? g : cap;
+}
+
 template <class RT, int KIND, int PREC>
 static void launch_phase(const DevLevel<RT>& D, const SegSet& S, TraceRec* trace, cudaStream_t stream) {
+    cudaMemsetAsync(D.B.counters + CNT_QUEUE, 0, kMaxSegs * sizeof(uint32_t), stream);
     if (D.B.prof_mark) D.B.prof_mark(D.B.prof_user, 0, stream);
-    k_phase<RT, KIND, PREC><<<D.B.grid, kTile, 0, stream>>>(D, S, trace);
+    k_phase<RT, KIND, PREC><<<phase_grid<RT, KIND, PREC>(D.B.grid), kTile, 0, stream>>>(D, S, trace);
     if (D.B.prof_mark) D.B.prof_mark(D.B.prof_user, 1, stream);
     count_launch();
 }
