@@ -295,6 +295,30 @@ def c4_case(args, small=False):
         print(json.dumps(line))
 
 
+def c3_portfolio(nm):
+    """The large-portfolio configuration: generator seed 1, options sorted by |w| (prob ~ |w|)."""
+    import numpy as np
+    pf = nm.generate_portfolio(nm.PORTFOLIO_C3, 1)
+    order = np.argsort(-np.abs(pf["w"]), kind="stable")
+    for k in ("strike", "maturity", "w", "stock_ind", "type"):
+        pf[k] = pf[k][order]
+    return dict(pf, prob=np.abs(pf["w"]))
+
+
+def c3_level_case():
+    """Profiling case of the large-portfolio phase kernel: two level-10 calls of 8192 outer
+    samples (9 adaptive pilot phases and the final phase each) with K = 4726.3 (the 99 % loss
+    quantile of the bench's c3 case)."""
+    sys.path.insert(0, PKG)
+    import nmlmc as nm
+    s = nm.Sampler(0, N0=64, beta=2, adaptive_r=1.5, precision=nm.PREC_FP32, streams=nm.STREAMS_OUTER, seed=5)
+    s.set_portfolio(c3_portfolio(nm), r=0.05, rho=0.0, max_loss=4726.308348894119, tau=nm.TAU_WEEK,
+                    subsample=nm.SUB_RANDOM, use_delta_cv=True, discount=False)
+    for ell, M in ((10, 8192), (10, 8192)):
+        r = s.sample(ell, M)
+        print(f"level {ell} M {M}: {r['seconds'] * 1e3:.3f} ms, {r['stats'][0] / r['seconds']:.3e} inner/s")
+
+
 def c3_case(args):
     """Large portfolio: d = 200 stocks, P = 1e6 options (generator seed 1), K = the 99 % quantile
     of the full loss over 1e5 outer samples; P(L > K) by continuation MLMC with the reference's
@@ -307,11 +331,7 @@ def c3_case(args):
     sys.path.insert(0, PKG)
     import nmlmc as nm
     eps = args.eps if args.eps else 1e-3
-    pf = nm.generate_portfolio(nm.PORTFOLIO_C3, 1)
-    order = np.argsort(-np.abs(pf["w"]), kind="stable")
-    for k in ("strike", "maturity", "w", "stock_ind", "type"):
-        pf[k] = pf[k][order]
-    pfw = dict(pf, prob=np.abs(pf["w"]))
+    pfw = c3_portfolio(nm)
 
     def mk(prec, streams, K, seed, cores=0, sub=nm.SUB_RANDOM):
         s = nm.Sampler(0, cores=cores or 2048, N0=64, beta=2, adaptive_r=1.5, precision=prec,
@@ -368,7 +388,7 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison runs")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--eps", type=float, default=None, help="--case c3: target RMSE (default 1e-3)")
-    ap.add_argument("--case", default=None, choices=["small", "c3", "c4", "c4-small"],
+    ap.add_argument("--case", default=None, choices=["small", "c3", "c3-level", "c4", "c4-small"],
                     help="small: a few fixed level calls of the FP32 sampler (profiling case); "
                          "c4: the path-simulated loss with adjoint; c4-small: its profiling case")
     args = ap.parse_args()
@@ -378,6 +398,8 @@ def main():
         return small_case()
     if args.case == "c3":
         return c3_case(args)
+    if args.case == "c3-level":
+        return c3_level_case()
     if args.case in ("c4", "c4-small"):
         return c4_case(args, small=args.case == "c4-small")
 
