@@ -310,8 +310,9 @@ int nmlmc_outer_normals(int32_t precision, uint64_t seed, uint64_t stream, uint3
 
 /* ---- allocation-free level call ------------------------------------------------------------
  * No counterpart in the reference.  For callers that may not allocate device memory: code that
- * runs while a framework owns the device memory pool, code replayed inside a captured CUDA
- * graph, hosts that reserve all device memory up front.  One level call of the model problem
+ * runs while a framework owns the device memory pool, latency-critical code that cannot afford
+ * cudaMalloc's implicit device-wide synchronisation, hosts that reserve all device memory up
+ * front.  One level call of the model problem
  * (kind NMLMC_MODEL_REFERENCE or NMLMC_MODEL_SHIFT; the OUTER stream layout, precision
  * NMLMC_PREC_FP32 or NMLMC_PREC_FP64, antithetic) over outer samples [first_index,
  * first_index + M) of level `ell`, on `stream` (a cudaStream_t; NULL = the default stream) of the

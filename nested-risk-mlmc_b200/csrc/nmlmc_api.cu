@@ -445,7 +445,7 @@ int alloc_outer(nmlmc_ctx* c) {
     if (c->ob_alloc && c->ob.cap == cap && c->ob.Q >= Q) return NMLMC_OK;
     OuterBuffers& B = c->ob;
     if (c->ob_alloc) {
-        cudaFree(B.Yv); cudaFree(B.Rt); cudaFree(B.cnt_f); cudaFree(B.cnt_c); cudaFree(B.pil);
+        cudaFree(B.Yv); cudaFree(B.Rt); cudaFree(B.cnt_f); cudaFree(B.cnt_c);
         cudaFree(B.lists); cudaFree(B.class_items); cudaFree(B.counters); cudaFree(B.block_sums);
         cudaFree(B.level_acc);
         c->ob_alloc = false;
@@ -459,7 +459,6 @@ int alloc_outer(nmlmc_ctx* c) {
               cudaMalloc(&B.Rt, (Q ? cap * Q : 1) * sizeof(double)) == cudaSuccess &&
               cudaMalloc(&B.cnt_f, cap * sizeof(uint32_t)) == cudaSuccess &&
               cudaMalloc(&B.cnt_c, cap * sizeof(uint32_t)) == cudaSuccess &&
-              cudaMalloc(&B.pil, cap * sizeof(uint32_t)) == cudaSuccess &&
               cudaMalloc(&B.lists, 4 * cap * sizeof(uint32_t)) == cudaSuccess &&
               cudaMalloc(&B.class_items, cap * sizeof(uint32_t)) == cudaSuccess &&
               cudaMalloc(&B.counters, 256 * sizeof(uint32_t)) == cudaSuccess &&
@@ -757,7 +756,7 @@ int nmlmc_destroy(nmlmc_ctx* c) {
     dfree(c->d_out_sums); dfree(c->d_out_stats); dfree(c->d_trace);
     if (c->ob_alloc) {
         OuterBuffers& B = c->ob;
-        cudaFree(B.Yv); cudaFree(B.Rt); cudaFree(B.cnt_f); cudaFree(B.cnt_c); cudaFree(B.pil);
+        cudaFree(B.Yv); cudaFree(B.Rt); cudaFree(B.cnt_f); cudaFree(B.cnt_c);
         cudaFree(B.lists); cudaFree(B.class_items); cudaFree(B.counters); cudaFree(B.block_sums);
         cudaFree(B.level_acc);
     }

@@ -60,7 +60,6 @@ struct OuterBuffers {
     void* Rt;                // RT[cap * Q]   portfolio R_tau rows
     uint32_t* cnt_f;         // final fine count / chunk size (0 = undecided)
     uint32_t* cnt_c;
-    uint32_t* pil;           // pilots taken (trace)
     uint32_t* lists;         // 4 * cap: fine/coarse round lists, ping-pong
     uint32_t* class_items;   // cap: items sorted by final class
     uint32_t* counters;      // device counters (see nmlmc_outer.cu)

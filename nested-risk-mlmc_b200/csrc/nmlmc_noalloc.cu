@@ -3,8 +3,8 @@
 //
 // Who needs it: callers that may not allocate device memory themselves — code that runs while
 // a framework owns the device memory pool (a cudaMalloc behind its back fragments the pool or
-// blocks on its allocator), code replayed inside a captured CUDA graph (cudaMalloc is not
-// allowed during capture), and hosts that cap device memory and reserve it up front.  They pass
+// blocks on its allocator), latency-critical code for which cudaMalloc's implicit device-wide
+// synchronisation is not acceptable, and hosts that cap device memory and reserve it up front.  They pass
 // scalars in and a device buffer for the result out; nothing is allocated per call.
 //
 // The array below is reserved in every process that loads this library, on every GPU it touches,
@@ -58,7 +58,6 @@ bool carve(unsigned char* base, int grid, OuterBuffers& B) {
     B.Rt = nullptr;                                          // models only: no R_tau rows
     B.cnt_f = reinterpret_cast<uint32_t*>(take(kMaxOuter * sizeof(uint32_t)));
     B.cnt_c = reinterpret_cast<uint32_t*>(take(kMaxOuter * sizeof(uint32_t)));
-    B.pil = reinterpret_cast<uint32_t*>(take(kMaxOuter * sizeof(uint32_t)));
     B.lists = reinterpret_cast<uint32_t*>(take(4 * kMaxOuter * sizeof(uint32_t)));
     B.class_items = reinterpret_cast<uint32_t*>(take(kMaxOuter * sizeof(uint32_t)));
     B.counters = reinterpret_cast<uint32_t*>(take(256 * sizeof(uint32_t)));

@@ -99,10 +99,22 @@ struct DevLevel {
 };
 
 // inner mean start + s1 / count (sample_inner_mean, nested_sampler.hpp:112-119)
+// s / count; a power-of-two count multiplies by its exact reciprocal, which gives the same
+// correctly rounded quotient without the division sequence.
+__device__ __forceinline__ float div_count(float s, uint64_t count) {
+    if ((count & (count - 1)) == 0) return __fmul_rn(s, __int_as_float((127 - (63 - __clzll((long long)count))) << 23));
+    return __fdiv_rn(s, (float)count);
+}
+__device__ __forceinline__ double div_count(double s, uint64_t count) {
+    if ((count & (count - 1)) == 0)
+        return __dmul_rn(s, __longlong_as_double((long long)(1023 - (63 - __clzll((long long)count))) << 52));
+    return __ddiv_rn(s, (double)count);
+}
+
 template <class RT, int PREC>
 __device__ __forceinline__ RT inner_mean(RT start, const Acc<PREC>& s1, uint64_t count) {
-    if (PREC == PREC_FP32) return __fadd_rn((float)start, __fdiv_rn((float)s1.value(), (float)count));
-    return to_rt<RT>(__dadd_rn((double)start, __ddiv_rn((double)s1.value(), (double)count)));
+    if (PREC == PREC_FP32) return __fadd_rn((float)start, div_count((float)s1.value(), count));
+    return to_rt<RT>(__dadd_rn((double)start, div_count((double)s1.value(), count)));
 }
 
 // Box-Muller pair from two OUTER words at the context precision.
@@ -177,10 +189,9 @@ __device__ __forceinline__ uint32_t pf_pick(const OptionTable<RT>& ot, uint64_t 
 // ---- one chunk: inner samples [s0, s0 + C) of phase `tag` of outer sample `item` ----------
 // C (inner samples per chunk) is a compile-time constant so the independent Threefry blocks of a
 // chunk can be interleaved (two at a time) for instruction-level parallelism.
-template <class RT, int KIND, int PREC, uint32_t C>
+template <class RT, int KIND, int PREC, uint32_t C, bool S2>
 __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t item, uint32_t tag,
-                                             uint64_t s0, bool want_s2, Acc<PREC>& a1,
-                                             Acc<PREC>& a2, double& work) {
+                                             uint64_t s0, Acc<PREC>& a1, Acc<PREC>& a2, double& work) {
     const OuterLevel<RT>& L = D.L;
     const TfKey key = tf_key(L.seed, outer_stream_id(L.ell, L.first_index + item));
     const RT* Yv = reinterpret_cast<const RT*>(D.B.Yv);
@@ -197,7 +208,7 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
             for (int q = 0; q < 4; q++) {
                 RT d = (PREC == PREC_FP32) ? (RT)(Y + z[q]) : xadd(Y, z[q]);
                 a1.add(d);
-                if (want_s2) a2.add((PREC == PREC_FP32) ? (RT)(d * d) : xmul(d, d));
+                if (S2) a2.add((PREC == PREC_FP32) ? (RT)(d * d) : xmul(d, d));
             }
         }
         work += (double)C;
@@ -217,7 +228,7 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
                 RT c = xadd(xmul(st, Y2[q]), xmul(s1t, X[q]));
                 RT d = xsub(xmul(a, a), xmul(c, c));
                 a1.add(d);
-                if (want_s2) a2.add(xmul(d, d));
+                if (S2) a2.add(xmul(d, d));
             }
         }
         work += (double)C;
@@ -240,7 +251,7 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
                 const float S0 = o.cv != 0.f ? (float)ot.S0[st] : 0.f;
                 const float d = option_loss_fast(o, R, __logf(R), S0);
                 a1.add((RT)d);
-                if (want_s2) a2.add((RT)(d * d));
+                if (S2) a2.add((RT)(d * d));
             }
         }
         work += (double)C;
@@ -258,22 +269,32 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
                 RT d = xdiv(pf_value<RT>(ot, Rrow, j), prob);
                 work += (double)ot.W_est[j];
                 a1.add(d);
-                if (want_s2) a2.add(xmul(d, d));
+                if (S2) a2.add(xmul(d, d));
             }
         }
     }
 }
 
+template <class RT, int KIND, int PREC, bool S2>
+__device__ __forceinline__ void eval_chunk_s(const DevLevel<RT>& D, uint32_t item, uint32_t tag,
+                                             uint64_t s0, uint32_t C, Acc<PREC>& a1, Acc<PREC>& a2,
+                                             double& work) {
+    switch (C) {
+    case 32: eval_chunk_c<RT, KIND, PREC, 32, S2>(D, item, tag, s0, a1, a2, work); break;
+    case 16: eval_chunk_c<RT, KIND, PREC, 16, S2>(D, item, tag, s0, a1, a2, work); break;
+    case 8: eval_chunk_c<RT, KIND, PREC, 8, S2>(D, item, tag, s0, a1, a2, work); break;
+    default: eval_chunk_c<RT, KIND, PREC, 4, S2>(D, item, tag, s0, a1, a2, work); break;
+    }
+}
+
+// want_s2 (pilots: the sum of squares for the variance) is resolved once per chunk, so the
+// inner loop carries no per-sample test.
 template <class RT, int KIND, int PREC>
 __device__ __forceinline__ void eval_chunk(const DevLevel<RT>& D, uint32_t item, uint32_t tag,
                                            uint64_t s0, uint32_t C, bool want_s2, Acc<PREC>& a1,
                                            Acc<PREC>& a2, double& work) {
-    switch (C) {
-    case 32: eval_chunk_c<RT, KIND, PREC, 32>(D, item, tag, s0, want_s2, a1, a2, work); break;
-    case 16: eval_chunk_c<RT, KIND, PREC, 16>(D, item, tag, s0, want_s2, a1, a2, work); break;
-    case 8: eval_chunk_c<RT, KIND, PREC, 8>(D, item, tag, s0, want_s2, a1, a2, work); break;
-    default: eval_chunk_c<RT, KIND, PREC, 4>(D, item, tag, s0, want_s2, a1, a2, work); break;
-    }
+    if (want_s2) eval_chunk_s<RT, KIND, PREC, true>(D, item, tag, s0, C, a1, a2, work);
+    else eval_chunk_s<RT, KIND, PREC, false>(D, item, tag, s0, C, a1, a2, work);
 }
 
 // ---- segments of uniform chunk count ------------------------------------------------------
@@ -296,17 +317,18 @@ struct SegSet {
 };
 
 // Adaptive decision after a pilot of `cur` samples (get_samples_count, 240-273, with
-// sample_inner_delta2, 120-129).
+// sample_inner_delta2, 120-129).  Writes the final count of a decided item; returns true when
+// the item goes on to the next pilot round.
 template <class RT, int PREC>
-__device__ __forceinline__ void pilot_done(const DevLevel<RT>& D, const Seg& g, uint32_t item, RT start,
-                                           const Acc<PREC>& a1, const Acc<PREC>& a2, uint32_t* counters) {
+__device__ __forceinline__ bool pilot_decide(const DevLevel<RT>& D, const Seg& g, uint32_t item, RT start,
+                                             const Acc<PREC>& a1, const Acc<PREC>& a2) {
     const OuterLevel<RT>& L = D.L;
     const CountParams& cp = (g.mode == 0) ? L.cf : L.cc;
     const uint64_t cur = g.count;
     RT delta2;
     if (PREC == PREC_FP32) {
         float s1 = (float)a1.value(), s2 = (float)a2.value(), n = (float)cur;
-        float mean_d = __fdiv_rn(s1, n);
+        float mean_d = div_count(s1, cur);
         float var = __fdiv_rn(__fsub_rn(s2, __fmul_rn(s1, mean_d)), n - 1.0f);
         float dist = __fadd_rn((float)start, mean_d);
         delta2 = (RT)__fdiv_rn(__fmul_rn(dist, dist), var);
@@ -314,44 +336,73 @@ __device__ __forceinline__ void pilot_done(const DevLevel<RT>& D, const Seg& g, 
         double s1 = (double)a1.value(), s2 = (double)a2.value();
         RT out_var = to_rt<RT>(__dsub_rn(__ddiv_rn(s2, (double)(cur - 1)),
                                          __ddiv_rn(__dmul_rn(s1, s1), (double)(cur * (cur - 1)))));
-        RT dist = xadd(start, to_rt<RT>(__ddiv_rn(s1, (double)cur)));
+        RT dist = xadd(start, to_rt<RT>(div_count(s1, cur)));
         delta2 = xdiv(xmul(dist, dist), out_var);
     }
     RT newc;
     if (L.adaptive_r == (RT)2) newc = xdiv((RT)cp.tmp, delta2);
     else newc = xmul(xpow(delta2, xdiv(-L.adaptive_r, (RT)2)), (RT)cp.tmp);
     uint32_t* cnt = (g.mode == 0) ? D.B.cnt_f : D.B.cnt_c;
-    atomicAdd(&D.B.pil[item], 1u);
-    if (newc <= (RT)cur) { cnt[item] = (uint32_t)cur; return; }
+    if (newc <= (RT)cur) { cnt[item] = (uint32_t)cur; return false; }
     const uint64_t nxt = cur * 2;
-    if (cp.max_count <= 2 * nxt) { cnt[item] = (uint32_t)cp.max_count; return; }
-    uint32_t pos = atomicAdd(&counters[g.next_slot], 1u);
-    g.next_list[pos] = item;
+    if (cp.max_count <= 2 * nxt) { cnt[item] = (uint32_t)cp.max_count; return false; }
+    return true;
 }
 
-// Per-item completion of the final phase: phi_f, phi_c, the 4 + 4 moments, statistics and the
-// trace record.  c[0..3] += phi_f^k, c[4..7] += (phi_f - phi_c)^k, c[8] inner samples,
-// c[9] hit the maximum count, c[10] stayed at the base count.
+// Appends the warp's surviving items to the next round's list: one atomic per warp (all 32
+// lanes call it).
+__device__ __forceinline__ void warp_append(bool surv, uint32_t item, uint32_t* count, uint32_t* list, int lane) {
+    const unsigned bal = __ballot_sync(0xffffffffu, surv);
+    if (!bal) return;
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(count, (uint32_t)__popc(bal));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (surv) list[base + __popc(bal & ((1u << lane) - 1u))] = item;
+}
+
+// Pilot rounds an item went through on one side, recovered from its final count: a count below
+// the maximum was fixed by the pilot of that size (rounds 0..r), the maximum is reached after
+// every round of the side (get_samples_count, 240-273).
+__device__ __forceinline__ uint32_t pilots_taken(uint32_t cnt, const CountParams& cp, bool adaptive) {
+    if (!adaptive) return 0;
+    uint32_t r = 0;
+    if (cnt == (uint32_t)cp.max_count) {
+        for (uint64_t c = cp.base_count; cp.max_count > 2 * c; c *= 2) r++;
+        return r;
+    }
+    for (uint64_t c = cp.base_count; c < cnt; c *= 2) r++;
+    return r + 1;
+}
+
+// Per-item completion of the final phase: phi_f, phi_c; their moments go into this thread's
+// moment slots mom[q * kTile] (q = 0..3 phi_f^k, 4..7 (phi_f - phi_c)^k; a zero phi adds
+// nothing and touches no slot), the counts of items that hit the maximum / stayed at the base
+// count, and the trace record.
 template <class RT>
-__device__ __forceinline__ void final_contrib(const DevLevel<RT>& D, const Seg& g, uint32_t item,
-                                              RT mean_big, RT phi_small, bool fine_big, double* c,
-                                              TraceRec* trace) {
+__device__ __forceinline__ void final_item(const DevLevel<RT>& D, uint32_t item, RT mean_big, RT phi_small,
+                                           bool fine_big, double* mom, uint32_t& n_max, uint32_t& n_base,
+                                           TraceRec* trace) {
     RT phi_big = (mean_big >= (RT)0) ? (RT)1 : (RT)0;
     RT f_phi, c_phi;
     if (D.L.fine_only) { f_phi = phi_big; c_phi = 0; }
     else if (fine_big) { f_phi = phi_big; c_phi = phi_small; }
     else { f_phi = phi_small; c_phi = phi_big; }
-    RT p = 1;
-    for (int q = 0; q < 4; q++) { p = xmul(p, f_phi); c[q] = (double)p; }
-    if (!D.L.fine_only) {
-        RT dphi = xsub(f_phi, c_phi);
-        p = 1;
-        for (int q = 0; q < 4; q++) { p = xmul(p, dphi); c[4 + q] = (double)p; }
+    if (f_phi != (RT)0) {
+        RT p = 1;
+#pragma unroll
+        for (int q = 0; q < 4; q++) { p = xmul(p, f_phi); mom[q * kTile] += (double)p; }
     }
-    c[8] = (double)g.count;
+    if (!D.L.fine_only) {
+        const RT dphi = xsub(f_phi, c_phi);
+        if (dphi != (RT)0) {
+            RT p = 1;
+#pragma unroll
+            for (int q = 0; q < 4; q++) { p = xmul(p, dphi); mom[(4 + q) * kTile] += (double)p; }
+        }
+    }
     const uint32_t cf = D.B.cnt_f[item];
-    c[9] = (cf == (uint32_t)D.L.cf.max_count) ? 1.0 : 0.0;
-    c[10] = (cf == (uint32_t)D.L.cf.base_count) ? 1.0 : 0.0;
+    n_max += (cf == (uint32_t)D.L.cf.max_count) ? 1u : 0u;
+    n_base += (cf == (uint32_t)D.L.cf.base_count) ? 1u : 0u;
     if (trace) {
         TraceRec tr;
         tr.count_f = cf;
@@ -361,33 +412,30 @@ __device__ __forceinline__ void final_contrib(const DevLevel<RT>& D, const Seg& 
         tr.mean_big = (double)mean_big;
         tr.min_abs_small = INFINITY;
         tr.core = 0;
-        tr.pilots = D.B.pil[item];
+        tr.pilots = pilots_taken(cf, D.L.cf, D.L.adaptive_f) +
+                    (D.L.fine_only ? 0u : pilots_taken((uint32_t)tr.count_c, D.L.cc, D.L.adaptive_c));
         trace[item] = tr;
     }
 }
 
-// Per-warp accumulators, written only by lane 0 of the warp (no atomics): [0..3] phi_f
-// moments, [4..7] difference moments, [8] work, [9] inner samples, [10] hit max, [11] stayed at
-// base (the layout of OuterBuffers::block_sums).
-__device__ __forceinline__ void add_contrib(double* slot, const double* c) {
-#pragma unroll
-    for (int q = 0; q < 8; q++) slot[q] += c[q];
-    slot[9] += c[8];
-    slot[10] += c[9];
-    slot[11] += c[10];
-}
-
+// Block partial sums (OuterBuffers::block_sums layout): [0..3] phi_f moments, [4..7] difference
+// moments, [8] work, [9] inner samples, [10] hit the maximum count, [11] stayed at the base count.
 template <class RT, int KIND, int PREC>
 __global__ void __launch_bounds__(kTile) k_phase(DevLevel<RT> D, SegSet S, TraceRec* trace) {
     __shared__ Acc<PREC> sm_a1[kWarps];
     __shared__ Acc<PREC> sm_a2[kWarps];
     __shared__ float sm_ind[kWarps];
+    __shared__ double sm_mom[8 * kTile];        // per-thread moment slots [q][thread]
     __shared__ double sm_acc[kWarps][16];
-    __shared__ uint64_t sm_ticket;
+    __shared__ uint32_t sm_ticket;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const uint32_t C = D.L.chunk;
     uint32_t* counters = D.B.counters;
     double wsum = 0;                                     // work of this thread's chunks
+    uint32_t n_max = 0, n_base = 0;
+    double* mom = sm_mom + t;
+#pragma unroll
+    for (int q = 0; q < 8; q++) mom[q * kTile] = 0;
     if (lane < 16) sm_acc[warp][lane] = 0;
     __syncthreads();
     const RT* Yv = reinterpret_cast<const RT*>(D.B.Yv);
@@ -404,23 +452,26 @@ __global__ void __launch_bounds__(kTile) k_phase(DevLevel<RT> D, SegSet S, Trace
         if (n_items == 0) continue;
         const uint32_t nch = 1u << g.nch_log2;
         const bool pilot = g.mode != 2;
-        if (pilot && blockIdx.x == 0 && t == 0) sm_acc[0][9] += (double)n_items * (double)g.count;
+        if (blockIdx.x == 0 && t == 0) sm_acc[0][9] += (double)n_items * (double)g.count;
 
         // The grid is persistent (the CTAs resident at once) and claims the segment's tiles from a
         // device work queue: one ticket per tile, so no CTA waits for a second wave and uneven
-        // tiles balance themselves.  Which CTA evaluates a tile does not change any result.
+        // tiles balance themselves.  The next ticket is claimed while the current tile is
+        // evaluated.  Which CTA evaluates a tile does not change any result.
         uint32_t* queue = counters + CNT_QUEUE + si;
+        if (t == 0) sm_ticket = atomicAdd(queue, 1u);
+        __syncthreads();
+        uint64_t ticket = sm_ticket;
         if (nch <= (uint32_t)kTile) {
             // ---- a tile holds kTile / nch whole items ----
             const uint32_t per_tile = kTile / nch;
             const uint64_t tiles = ((uint64_t)n_items + per_tile - 1) / per_tile;
             for (;;) {
-                if (t == 0) sm_ticket = atomicAdd(queue, 1u);
-                __syncthreads();
-                const uint64_t tile = sm_ticket;
-                __syncthreads();
-                if (tile >= tiles) break;
-                const uint64_t lin = tile * per_tile + (t >> g.nch_log2);
+                __syncthreads();                         // every thread has read the ticket
+                if (ticket >= tiles) break;
+                uint32_t next = 0;
+                if (t == 0) next = atomicAdd(queue, 1u);
+                const uint64_t lin = ticket * per_tile + (t >> g.nch_log2);
                 const uint32_t j = t & (nch - 1);
                 const bool valid = lin < n_items;
                 const uint32_t item = valid ? (list ? list[lin] : (uint32_t)lin) : 0;
@@ -483,34 +534,25 @@ __global__ void __launch_bounds__(kTile) k_phase(DevLevel<RT> D, SegSet S, Trace
                     __syncthreads();
                 }
                 if (pilot) {
-                    if (leader) pilot_done<RT, PREC>(D, g, item, start, a1, a2, counters);
-                } else {
-                    double c[11];
-#pragma unroll
-                    for (int q = 0; q < 11; q++) c[q] = 0;
-                    if (leader) final_contrib<RT>(D, g, item, inner_mean<RT, PREC>(start, a1, g.count), (RT)ind,
-                                                  fine_big, c, trace);
-                    if (nch < 32) {
-                        // several items per warp: reduce the warp's contributions first
-#pragma unroll
-                        for (int q = 0; q < 11; q++)
-                            for (int m = 16; m > 0; m >>= 1) c[q] += __shfl_down_sync(0xffffffffu, c[q], m);
-                        if (lane == 0) add_contrib(sm_acc[warp], c);
-                    } else if (leader) {
-                        add_contrib(sm_acc[warp], c);   // the leader is lane 0 of its warp
-                    }
+                    const bool surv = leader && pilot_decide<RT, PREC>(D, g, item, start, a1, a2);
+                    warp_append(surv, item, counters + g.next_slot, g.next_list, lane);
+                } else if (leader) {
+                    final_item<RT>(D, item, inner_mean<RT, PREC>(start, a1, g.count), (RT)ind, fine_big, mom,
+                                   n_max, n_base, trace);
                 }
+                if (t == 0) sm_ticket = next;
+                __syncthreads();
+                ticket = sm_ticket;
             }
         } else {
             // ---- one CTA walks an item tile by tile ----
             const uint32_t tiles_per_item = nch / kTile;
             for (;;) {
-                if (t == 0) sm_ticket = atomicAdd(queue, 1u);
-                __syncthreads();
-                const uint64_t it = sm_ticket;
-                __syncthreads();
-                if (it >= n_items) break;
-                const uint32_t item = list ? list[it] : (uint32_t)it;
+                __syncthreads();                         // every thread has read the ticket
+                if (ticket >= n_items) break;
+                uint32_t next = 0;
+                if (t == 0) next = atomicAdd(queue, 1u);
+                const uint32_t item = list ? list[ticket] : (uint32_t)ticket;
                 uint32_t gs = nch;
                 uint64_t csmall = g.count;
                 bool fine_big = true;
@@ -577,21 +619,38 @@ __global__ void __launch_bounds__(kTile) k_phase(DevLevel<RT> D, SegSet S, Trace
                 }
                 if (t == 0) {
                     if (pilot) {
-                        pilot_done<RT, PREC>(D, g, item, start, tot1, tot2, counters);
+                        if (pilot_decide<RT, PREC>(D, g, item, start, tot1, tot2))
+                            g.next_list[atomicAdd(&counters[g.next_slot], 1u)] = item;
                     } else {
-                        double c[11];
-                        for (int q = 0; q < 11; q++) c[q] = 0;
-                        final_contrib<RT>(D, g, item, inner_mean<RT, PREC>(start, tot1, g.count), (RT)tind,
-                                          fine_big, c, trace);
-                        add_contrib(sm_acc[0], c);
+                        final_item<RT>(D, item, inner_mean<RT, PREC>(start, tot1, g.count), (RT)tind, fine_big, mom,
+                                       n_max, n_base, trace);
                     }
+                    sm_ticket = next;
                 }
+                __syncthreads();
+                ticket = sm_ticket;
             }
         }
     }
-    // work of the block's chunks, then the block totals into this CTA's partial-sum slot
-    for (int m = 16; m > 0; m >>= 1) wsum += __shfl_down_sync(0xffffffffu, wsum, m);
-    if (lane == 0) sm_acc[warp][8] += wsum;
+    // this thread's work, moments and counts -> per-warp sums -> this CTA's partial-sum slot
+    for (int m = 16; m > 0; m >>= 1) {
+        wsum += __shfl_down_sync(0xffffffffu, wsum, m);
+        n_max += __shfl_down_sync(0xffffffffu, n_max, m);
+        n_base += __shfl_down_sync(0xffffffffu, n_base, m);
+    }
+    double mv[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        mv[q] = mom[q * kTile];
+        for (int m = 16; m > 0; m >>= 1) mv[q] += __shfl_down_sync(0xffffffffu, mv[q], m);
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < 8; q++) sm_acc[warp][q] += mv[q];
+        sm_acc[warp][8] += wsum;
+        sm_acc[warp][10] += (double)n_max;
+        sm_acc[warp][11] += (double)n_base;
+    }
     __syncthreads();
     if (t < 16) {
         double v = 0;
@@ -607,7 +666,6 @@ __global__ void __launch_bounds__(kTile) k_outer(DevLevel<RT> D, uint32_t nb) {
     RT* Yv = reinterpret_cast<RT*>(D.B.Yv);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
         const TfKey key = tf_key(L.seed, outer_stream_id(L.ell, L.first_index + i));
-        D.B.pil[i] = 0;
         D.B.cnt_f[i] = L.adaptive_f ? 0u : (uint32_t)L.cf.max_count;
         D.B.cnt_c[i] = L.adaptive_c ? 0u : (uint32_t)L.cc.max_count;
         if (KIND != KIND_PORTFOLIO) {

@@ -46,6 +46,7 @@ def compare_traces(gpu, ora, bound, per_core=False, max_frac=0.0):
             if per_core:
                 stopped.add(core)
             continue
+        assert g["pilots"] == o["pilots"], (m, g, o)    # equal counts: the same pilot rounds
         if g["phi_f"] != o["phi_f"] or g["phi_c"] != o["phi_c"]:
             near = min(abs(o["mean_big"]), o["min_abs_small"])
             assert near < bound, (m, g, o)

@@ -1,8 +1,8 @@
 """The allocation-free level call (nmlmc_sample_level_noalloc) against the regular entry point.
 
 Who it is for: callers that may not allocate device memory — code running while a framework
-owns the device memory pool, code replayed inside a captured CUDA graph, hosts that reserve all
-device memory up front.  It keeps its scratch in one fixed device array, so this test calls it
+owns the device memory pool, latency-critical code that cannot afford cudaMalloc's implicit
+device-wide synchronisation, hosts that reserve all device memory up front.  It keeps its scratch in one fixed device array, so this test calls it
 through the C ABI twice in a row (the second call must not see the first call's leftovers) and
 compares each result with nmlmc_sample on the same outer samples (same streams, so the sums are
 equal; the tolerance is exact equality, the same rule as the other same-stream tests).
