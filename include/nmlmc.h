@@ -153,7 +153,8 @@ typedef struct nmlmc_config {
     int32_t precision;         /* NMLMC_PREC_*                                                   */
     int32_t streams;           /* NMLMC_STREAMS_*                                                */
     uint64_t seed;
-    uint64_t batch;            /* OUTER layout: outer samples held per batch (0 -> 1<<20)        */
+    uint64_t batch;            /* OUTER layout: outer samples per batch (0 -> 1<<22; portfolios:
+                                  at most 1 GiB of R_tau rows)                                  */
 } nmlmc_config;
 
 typedef struct nmlmc_level_result {
@@ -279,6 +280,34 @@ int nmlmc_sample(nmlmc_ctx* ctx, uint32_t ell, uint64_t M, nmlmc_level_result* o
  * the CORE layout, the levels run as consecutive nmlmc_sample calls. */
 int nmlmc_sample_levels(nmlmc_ctx* ctx, uint32_t n, const uint32_t* ells, const uint64_t* Ms,
                         nmlmc_level_result* outs);
+/* ---- phase-kernel autotuner (batched FP32 path) ----------------------------------------------
+ * No counterpart in the reference (its CUDA build has one fixed launch shape).  The phase kernel
+ * of the OUTER layout has three register/occupancy variants (0: up to 255 registers per thread,
+ * 1: two resident CTAs of 256 threads per SM guaranteed, 2: four) and a chunk length (inner
+ * samples per thread; power of two in [4, 64] dividing N0; a level's items of n inner samples
+ * take n / chunk threads, so it also sets the outer samples per warp).  With autotuning on, the
+ * first nmlmc_sample / nmlmc_sample_levels call of a level with enough work times the
+ * candidates on a probe of the level's own parameters whose outer stream indices start at 2^55
+ * (no result changes) and keeps the fastest for that level in the context.  Mode 1 (the
+ * default) tunes the variant only; the variants give identical results.  Mode 2 also tries half
+ * and double the chunk length; another chunk length regroups the FP32 compensated inner sums
+ * (last-bit differences of inner means), so pin the configuration to make such runs reproducible
+ * across processes.  Changing the model, portfolio or configuration drops the tuned (not the
+ * pinned) choices.  Tuning applies to NMLMC_PREC_FP32 only. */
+typedef struct nmlmc_phase_config {
+    uint32_t variant;          /* 0, 1, 2 (above)                                                */
+    uint32_t chunk;            /* inner samples per thread                                       */
+    int32_t state;             /* get: 0 default, 1 autotuned, 2 pinned                          */
+    double probe_ms;           /* get: device time of the tuned choice on its probe              */
+} nmlmc_phase_config;
+int nmlmc_set_autotune(nmlmc_ctx* ctx, int32_t mode);   /* 0 off, 1 variants (default), 2 + chunk */
+int nmlmc_get_phase_config(nmlmc_ctx* ctx, uint32_t ell, nmlmc_phase_config* out);
+/* Pins level ell's configuration (cfg == NULL unpins it: default, tunable again). */
+int nmlmc_set_phase_config(nmlmc_ctx* ctx, uint32_t ell, const nmlmc_phase_config* cfg);
+/* Tunes level ell now, variant and chunk length, on a probe of min(M, batch) outer samples
+ * (replaces a tuned or pinned choice). */
+int nmlmc_autotune_level(nmlmc_ctx* ctx, uint32_t ell, uint64_t M);
+
 /* CUDA graphs of nmlmc_sample_levels: instantiated, updated in place, launched. */
 int nmlmc_graph_stats(nmlmc_ctx* ctx, uint64_t* instantiations, uint64_t* updates, uint64_t* launches);
 /* Arms a host buffer of `cap` records for the next nmlmc_sample call (M <= cap). */

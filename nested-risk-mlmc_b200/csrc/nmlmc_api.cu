@@ -126,6 +126,13 @@ struct DevPortfolio {
 
 }  // namespace
 
+// Phase-kernel configuration of one level: register/occupancy variant and chunk length.
+struct PhaseChoice {
+    int32_t state = 0;        // 0 default, 1 tuned, 2 pinned by the caller
+    uint32_t variant = 0, chunk = 0;
+    double probe_ms = 0;      // device time of the chosen configuration on the tuning probe
+};
+
 struct nmlmc_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -165,6 +172,10 @@ struct nmlmc_ctx {
     uint64_t d_trace_cap = 0;
     // sharding over ranks (OUTER layout)
     uint32_t shard_rank = 0, shard_world = 1;
+    // phase-kernel configuration per level on the batched FP32 path (autotuned or pinned)
+    int32_t autotune = 1;             // 0 off, 1 variants, 2 variants and chunk length
+    bool batch_default = true;        // cfg.batch was 0: the library chose the batch size
+    PhaseChoice phase[NMLMC_MAX_LEVELS];
     // phase-kernel timing
     bool prof = false;
     std::vector<cudaEvent_t> pev;
@@ -440,8 +451,13 @@ int alloc_core(nmlmc_ctx* c) {
 }
 
 int alloc_outer(nmlmc_ctx* c) {
-    const uint64_t cap = c->cfg.batch;
     const uint32_t Q = c->kind == KIND_PORTFOLIO ? c->pf.Q : 0;
+    uint64_t cap = c->cfg.batch;
+    if (c->batch_default && Q) {            // default batch: at most 1 GiB of R_tau rows
+        const uint64_t lim = (1ull << 30) / ((uint64_t)Q * sizeof(double));
+        const uint64_t lo = 1ull << 16;
+        if (cap > lim) cap = lim > lo ? lim : lo;
+    }
     if (c->ob_alloc && c->ob.cap == cap && c->ob.Q >= Q) return NMLMC_OK;
     OuterBuffers& B = c->ob;
     if (c->ob_alloc) {
@@ -573,6 +589,35 @@ void fill_outer_result(const nmlmc_ctx* c, const double* a, uint64_t M, double s
     out->seconds = seconds;
 }
 
+// Default phase configuration: up to 255 registers for the models (their inner loop is ALU-bound
+// and gains nothing from more warps), four CTAs per SM for the FP32 portfolio (its option-table
+// gathers need the warps to hide L2 latency), chunks of min(N0, 32) inner samples.
+PhaseChoice default_phase(const nmlmc_ctx* c) {
+    PhaseChoice p;
+    p.variant = (c->cfg.precision == NMLMC_PREC_FP32 && c->kind == KIND_PORTFOLIO) ? 2u : 0u;
+    p.chunk = c->cfg.N0 >= 32 ? 32u : c->cfg.N0;
+    return p;
+}
+
+bool valid_chunk(const nmlmc_config& k, uint32_t ch);
+
+// The level's tuned or pinned choice; a pinned chunk that no longer divides N0 falls back to the
+// default.
+PhaseChoice phase_choice(const nmlmc_ctx* c, uint32_t ell) {
+    const PhaseChoice& p = c->phase[ell];
+    return (p.state && valid_chunk(c->cfg, p.chunk)) ? p : default_phase(c);
+}
+
+void reset_phase(nmlmc_ctx* c) {
+    for (auto& p : c->phase) {
+        if (p.state != 2) p = PhaseChoice{};
+    }
+}
+
+bool valid_chunk(const nmlmc_config& k, uint32_t ch) {
+    return ch >= 4 && ch <= 64 && (ch & (ch - 1)) == 0 && (k.N0 % ch) == 0;
+}
+
 template <class RT>
 OuterLevel<RT> outer_level_params(const nmlmc_ctx* c, uint32_t ell, uint64_t M, uint64_t first_index) {
     OuterLevel<RT> L{};
@@ -583,7 +628,9 @@ OuterLevel<RT> outer_level_params(const nmlmc_ctx* c, uint32_t ell, uint64_t M, 
     L.fine_only = ell == 0;
     L.antithetic = c->cfg.antithetic != 0;
     L.N0 = c->cfg.N0;
-    L.chunk = c->cfg.N0 >= 32 ? 32 : c->cfg.N0;
+    const PhaseChoice pc = phase_choice(c, ell);
+    L.chunk = pc.chunk;
+    L.variant = pc.variant;
     L.adaptive_r = (RT)c->cfg.adaptive_r;
     L.cf = count_params(c->cfg, ell);
     L.cc = count_params(c->cfg, ell == 0 ? 0 : ell - 1);
@@ -597,12 +644,86 @@ OuterLevel<RT> outer_level_params(const nmlmc_ctx* c, uint32_t ell, uint64_t M, 
     return L;
 }
 
+// ---- phase-kernel autotuner (batched FP32 path) ---------------------------------------------
+// The first call of a level that carries enough work to time (>= 4096 outer samples and ~8e6
+// inner samples in one batch) times candidate configurations on a probe — the level's own
+// parameters on min(M, batch) outer samples whose stream indices start at 2^55, far from any
+// real index, so the probe changes no result — and keeps the fastest for the level:
+//   1. the register/occupancy variants 0, 1, 2 at the default chunk length;
+//   2. (mode 2, or an explicit nmlmc_autotune_level) half and double the chunk length at the
+//      best variant, taken only if > 3 % faster.
+// The variants compute identically, so mode 1 never changes a result; the chunk length changes
+// the grouping of the FP32 compensated inner sums (last-bit differences of inner means).
+// Pinned levels are not tuned.
+constexpr uint64_t kProbeIndex = 1ull << 55;
+
+template <class RT>
+cudaError_t time_phase_config(nmlmc_ctx* c, uint32_t ell, uint64_t Mp, const PhaseChoice& pc, double& ms_out) {
+    OuterLevel<RT> L = outer_level_params<RT>(c, ell, Mp, kProbeIndex);
+    L.chunk = pc.chunk;
+    L.variant = pc.variant;
+    OuterBuffers B = c->ob;
+    B.prof_mark = nullptr;
+    cudaError_t e = cudaSuccess;
+    float ms = 0;
+    for (int rep = 0; rep < 2 && e == cudaSuccess; rep++) {       // the first run warms up
+        e = cudaEventRecord(c->ev0, c->stream);
+        if (e == cudaSuccess) e = outer_level_begin(B, c->stream);
+        if (e == cudaSuccess) e = outer_sample_level<RT>(L, c->kind, c->cfg.precision, B, nullptr, c->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(c->ev1, c->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(c->ev1);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    }
+    ms_out = ms;
+    return e;
+}
+
+template <class RT>
+int tune_level(nmlmc_ctx* c, uint32_t ell, uint64_t M, bool chunks) {
+    const uint64_t Mp = M < c->ob.cap ? M : c->ob.cap;
+    PhaseChoice best = default_phase(c);
+    best.state = 1;
+    double best_ms = INFINITY;
+    for (uint32_t v = 0; v < 3; v++) {
+        PhaseChoice pc = best;
+        pc.variant = v;
+        double ms;
+        NM_CUDA(time_phase_config<RT>(c, ell, Mp, pc, ms), "autotune probe");
+        if (ms < best_ms) { best_ms = ms; best.variant = v; }
+    }
+    const uint32_t c0 = best.chunk;
+    for (uint32_t ch : {c0 / 2, c0 * 2}) {
+        if (!chunks || !valid_chunk(c->cfg, ch)) continue;
+        PhaseChoice pc = best;
+        pc.chunk = ch;
+        double ms;
+        NM_CUDA(time_phase_config<RT>(c, ell, Mp, pc, ms), "autotune probe");
+        if (ms < 0.97 * best_ms) { best_ms = ms; best.chunk = ch; }
+    }
+    best.probe_ms = best_ms;
+    c->phase[ell] = best;
+    return NMLMC_OK;
+}
+
+// Tunes `ell` if autotuning is on, the level is still on its default configuration and this
+// call (M outer samples on this rank) is large enough to time.
+template <class RT>
+int ensure_tuned(nmlmc_ctx* c, uint32_t ell, uint64_t M) {
+    if (!c->autotune || c->cfg.precision != NMLMC_PREC_FP32 || c->phase[ell].state != 0) return NMLMC_OK;
+    const uint64_t Mp = M < c->ob.cap ? M : c->ob.cap;
+    const CountParams cf = count_params(c->cfg, ell);
+    if (Mp < 4096 || (double)Mp * (double)cf.base_count * (double)(ell + 1) < 8.0e6) return NMLMC_OK;
+    return tune_level<RT>(c, ell, M, c->autotune == 2);
+}
+
 template <class RT>
 int sample_outer(nmlmc_ctx* c, uint32_t ell, uint64_t Mtotal, nmlmc_level_result* out) {
     // this rank's static share of the call's outer samples (all of them when world = 1)
     const uint64_t q = Mtotal / c->shard_world, rem = Mtotal % c->shard_world;
     const uint64_t lo = q * c->shard_rank + (c->shard_rank < rem ? c->shard_rank : rem);
     const uint64_t M = q + (c->shard_rank < rem ? 1 : 0);
+    int rc = ensure_tuned<RT>(c, ell, M);
+    if (rc) return rc;
     OuterLevel<RT> L = outer_level_params<RT>(c, ell, M, c->next_outer[ell] + lo);
     TraceRec* tr = c->trace_host ? c->d_trace : nullptr;
     c->ob.prof_mark = c->prof ? prof_mark : nullptr;
@@ -641,6 +762,12 @@ int sample_outer_levels(nmlmc_ctx* c, uint32_t n, const uint32_t* ells, const ui
     uint64_t next[NMLMC_MAX_LEVELS];
     memcpy(next, c->next_outer, sizeof(next));
     std::vector<uint64_t> Ms(n);
+    for (uint32_t i = 0; i < n; i++) {             // tuning probes run before the capture
+        uint64_t lo, M;
+        shard_range(c, Mtot[i], lo, M);
+        int rc = ensure_tuned<RT>(c, ells[i], M);
+        if (rc) return rc;
+    }
     NM_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
     cudaError_t err = cudaSuccess;
     for (uint32_t i = 0; i < n && err == cudaSuccess; i++) {
@@ -775,8 +902,9 @@ int nmlmc_destroy(nmlmc_ctx* c) {
 int nmlmc_configure(nmlmc_ctx* c, const nmlmc_config* cfg) {
     if (!c || !cfg) return set_err(NMLMC_ERR_ARG);
     nmlmc_config k = *cfg;
+    c->batch_default = k.batch == 0;
     if (k.cores == 0) k.cores = 2048;
-    if (k.batch == 0) k.batch = 1u << 20;
+    if (k.batch == 0) k.batch = 1u << 22;
     // beta: a power of two >= 2 (the adaptive base count N0 * (beta/2)^ell is 0 for beta = 1)
     if (k.N0 == 0 || k.beta < 2 || (k.beta & (k.beta - 1)) != 0) return set_err(NMLMC_ERR_ARG);
     if (k.precision < NMLMC_PREC_REF32 || k.precision > NMLMC_PREC_FP32) return set_err(NMLMC_ERR_ARG);
@@ -791,9 +919,16 @@ int nmlmc_configure(nmlmc_ctx* c, const nmlmc_config* cfg) {
     }
     cudaSetDevice(c->device);
     const bool prec_changed = c->cfg.precision != k.precision;
+    // a new seed keeps the tuned phase configurations; any other change drops them
+    const nmlmc_config& a = c->cfg;
+    const bool retune = !c->configured || a.cores != k.cores || a.N0 != k.N0 || a.beta != k.beta ||
+                        a.adaptive_r != k.adaptive_r || a.antithetic != k.antithetic ||
+                        a.adaptive_incl_r2 != k.adaptive_incl_r2 || a.precision != k.precision ||
+                        a.streams != k.streams || a.batch != k.batch;
     c->cfg = k;
     c->configured = true;
     if (prec_changed) c->pf_prec = -1;
+    if (retune) reset_phase(c);
     return nmlmc_reset_streams(c);
 }
 
@@ -817,6 +952,7 @@ int nmlmc_set_model(nmlmc_ctx* c, int32_t kind, double tau, double max_loss) {
     c->tau = tau;
     c->max_loss = max_loss;
     c->stau_given = false;
+    reset_phase(c);
     return NMLMC_OK;
 }
 
@@ -882,6 +1018,7 @@ static int set_portfolio_impl(nmlmc_ctx* c, const nmlmc_portfolio* p, const nmlm
     }
     c->kind = KIND_PORTFOLIO;
     c->pf_prec = -1;
+    reset_phase(c);
     cudaSetDevice(c->device);
     return ensure_portfolio(c);
 }
@@ -1118,6 +1255,51 @@ int nmlmc_phase_kernel_time(nmlmc_ctx* c, uint64_t* launches, double* seconds) {
 }
 
 uint64_t nmlmc_kernel_launches(void) { return launches_total(); }
+
+int nmlmc_set_autotune(nmlmc_ctx* c, int32_t mode) {
+    if (!c || mode < 0 || mode > 2) return set_err(NMLMC_ERR_ARG);
+    c->autotune = mode;
+    return NMLMC_OK;
+}
+
+int nmlmc_get_phase_config(nmlmc_ctx* c, uint32_t ell, nmlmc_phase_config* out) {
+    if (!c || !out || ell >= NMLMC_MAX_LEVELS) return set_err(NMLMC_ERR_ARG);
+    if (!c->configured) return set_err(NMLMC_ERR_STATE);
+    const PhaseChoice p = phase_choice(c, ell);
+    out->variant = p.variant;
+    out->chunk = p.chunk;
+    out->state = c->phase[ell].state;
+    out->probe_ms = p.probe_ms;
+    return NMLMC_OK;
+}
+
+int nmlmc_set_phase_config(nmlmc_ctx* c, uint32_t ell, const nmlmc_phase_config* cfg) {
+    if (!c || ell >= NMLMC_MAX_LEVELS) return set_err(NMLMC_ERR_ARG);
+    if (!c->configured) return set_err(NMLMC_ERR_STATE);
+    if (!cfg) {                                   // unpin: back to the default, tunable again
+        c->phase[ell] = PhaseChoice{};
+        return NMLMC_OK;
+    }
+    if (cfg->variant > 2 || !valid_chunk(c->cfg, cfg->chunk)) return set_err(NMLMC_ERR_ARG);
+    PhaseChoice p;
+    p.state = 2;
+    p.variant = cfg->variant;
+    p.chunk = cfg->chunk;
+    c->phase[ell] = p;
+    return NMLMC_OK;
+}
+
+int nmlmc_autotune_level(nmlmc_ctx* c, uint32_t ell, uint64_t M) {
+    if (!c || ell >= NMLMC_MAX_LEVELS || M == 0) return set_err(NMLMC_ERR_ARG);
+    if (!c->configured || c->kind < 0) return set_err(NMLMC_ERR_STATE);
+    if (c->cfg.streams != NMLMC_STREAMS_OUTER || c->cfg.precision != NMLMC_PREC_FP32) return set_err(NMLMC_ERR_ARG);
+    if ((double)c->cfg.N0 * pow((double)c->cfg.beta, (double)ell) > 4.0e9) return set_err(NMLMC_ERR_ARG);
+    cudaSetDevice(c->device);
+    int rc = ensure_portfolio(c);
+    if (rc || (rc = alloc_outer(c))) return rc;
+    if (c->kind == KIND_PORTFOLIO && c->pf.mixed()) return set_err(NMLMC_ERR_ARG);
+    return tune_level<float>(c, ell, M, true);
+}
 
 int nmlmc_graph_stats(nmlmc_ctx* c, uint64_t* instantiations, uint64_t* updates, uint64_t* launches) {
     if (!c || !instantiations || !updates || !launches) return set_err(NMLMC_ERR_ARG);

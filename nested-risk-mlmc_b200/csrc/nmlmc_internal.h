@@ -46,6 +46,7 @@ struct OuterLevel {
     uint64_t seed;
     bool fine_only, antithetic, adaptive_f, adaptive_c;
     uint32_t N0, chunk;     // chunk = inner samples per thread (power of two dividing all counts)
+    uint32_t variant;       // phase-kernel register/occupancy variant (FP32 path: 0, 1, 2)
     RT adaptive_r;
     CountParams cf, cc;
     ModelParams<RT> mp;

@@ -1,0 +1,922 @@
+#pragma once
+// OUTER-layout (batched) level sampler: kernels and the per-level launch sequence.
+//
+// Included by nmlmc_outer.cu (dispatch, full-loss sweep, utilities) and by nmlmc_outer_kind.cu,
+// which is compiled once per sampler kind (NMLMC_OUTER_KIND) so the kernel instantiations build
+// in parallel.
+//
+// The reference walks each outer sample depth-first: pilots of doubling size until the
+// adaptive rule stops (get_samples_count, nested_sampler.hpp:240-273), then the antithetic
+// fine/coarse estimate (sample_phi_antithetic, 171-216).  Adaptive counts differ by up to 2^ell
+// between outer samples, so a warp per outer sample leaves most of the GPU idle behind the few
+// samples that refine to the maximum.  Here every outer sample has its own counter-based
+// stream (key = (seed, level<<56 | index), counter = (block, phase tag)), which makes each
+// inner sample addressable, and a level call runs breadth-first:
+//
+//   k_outer      one thread per outer sample: outer draws (Y, or R_tau row + constant)
+//   k_phase      pilot round r: every outer sample still refining, fine and coarse, as
+//                uniform-size segments; one thread per chunk of inner samples, block-segmented
+//                reduction, the adaptive decision fused in (survivors appended to the next
+//                round's list)
+//   k_classify   bucket outer samples by their final count (a power of two)
+//   k_phase      final: antithetic groups and the big-count mean, phi, 4 moments into per-CTA
+//                partial sums (fixed order, no atomics on the sums)
+//   k_reduce     per-CTA partials -> the level's sums
+//
+// Every thread does the same unit of work (one chunk), so the device stays full whatever the
+// spread of inner counts.  An item with more chunks than a CTA has threads is walked tile by
+// tile by one CTA.
+#include <cmath>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "nmlmc_common.cuh"
+#include "nmlmc_internal.h"
+
+namespace nmlmc {
+
+constexpr int kTile = 256;           // threads per CTA = chunks per tile
+constexpr int kWarps = kTile / 32;
+constexpr int kMaxSegs = 40;
+
+// device counter slots (uint32 each)
+enum : int {
+    CNT_LIST = 0,        // [4]: fine list size (ping-pong slots 0/1), coarse list size (2/3)
+    CNT_CLASS = 8,       // [64]: outer samples per final class
+    CNT_FILL = 72,       // [64]: scatter fill per class
+    CNT_TOTAL = 144,
+    CNT_QUEUE = 192      // [kMaxSegs]: tile tickets of the phase kernel's work queue, per segment
+};
+static_assert(CNT_QUEUE + kMaxSegs <= 256, "counter slots");
+
+// ---- accumulators -------------------------------------------------------------------------
+// FP32: compensated pair (hi + lo) — Kahan accumulation inside a thread, TwoSum merging across
+// threads.  FP64 and REF32: double, the reference's sum_t.
+template <int PREC> struct Acc;
+
+template <> struct Acc<PREC_FP32> {
+    float hi, lo;
+    __device__ __forceinline__ void zero() { hi = 0.f; lo = 0.f; }
+    __device__ __forceinline__ void add(float v) {
+        float y = __fadd_rn(v, lo);
+        float t = __fadd_rn(hi, y);
+        lo = __fsub_rn(y, __fsub_rn(t, hi));
+        hi = t;
+    }
+    __device__ __forceinline__ void merge(const Acc& o) {
+        float s = __fadd_rn(hi, o.hi);
+        float bp = __fsub_rn(s, hi);
+        float e = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bp)), __fsub_rn(o.hi, bp));
+        hi = s;
+        lo = __fadd_rn(__fadd_rn(lo, o.lo), e);
+    }
+    __device__ __forceinline__ Acc shfl_xor(int m) const {
+        Acc r;
+        r.hi = __shfl_xor_sync(0xffffffffu, hi, m);
+        r.lo = __shfl_xor_sync(0xffffffffu, lo, m);
+        return r;
+    }
+    __device__ __forceinline__ float value() const { return __fadd_rn(hi, lo); }
+};
+
+template <> struct Acc<PREC_FP64> {
+    double v;
+    __device__ __forceinline__ void zero() { v = 0; }
+    __device__ __forceinline__ void add(double x) { v = __dadd_rn(v, x); }
+    __device__ __forceinline__ void merge(const Acc& o) { v = __dadd_rn(v, o.v); }
+    __device__ __forceinline__ Acc shfl_xor(int m) const { Acc r; r.v = __shfl_xor_sync(0xffffffffu, v, m); return r; }
+    __device__ __forceinline__ double value() const { return v; }
+};
+template <> struct Acc<PREC_REF32> {
+    double v;
+    __device__ __forceinline__ void zero() { v = 0; }
+    __device__ __forceinline__ void add(double x) { v = __dadd_rn(v, x); }
+    __device__ __forceinline__ void merge(const Acc& o) { v = __dadd_rn(v, o.v); }
+    __device__ __forceinline__ Acc shfl_xor(int m) const { Acc r; r.v = __shfl_xor_sync(0xffffffffu, v, m); return r; }
+    __device__ __forceinline__ double value() const { return v; }
+};
+
+template <class RT>
+struct DevLevel {
+    OuterLevel<RT> L;
+    OuterBuffers B;
+};
+
+// inner mean start + s1 / count (sample_inner_mean, nested_sampler.hpp:112-119)
+// s / count; a power-of-two count multiplies by its exact reciprocal, which gives the same
+// correctly rounded quotient without the division sequence.
+__device__ __forceinline__ float div_count(float s, uint64_t count) {
+    if ((count & (count - 1)) == 0) return __fmul_rn(s, __int_as_float((127 - (63 - __clzll((long long)count))) << 23));
+    return __fdiv_rn(s, (float)count);
+}
+__device__ __forceinline__ double div_count(double s, uint64_t count) {
+    if ((count & (count - 1)) == 0)
+        return __dmul_rn(s, __longlong_as_double((long long)(1023 - (63 - __clzll((long long)count))) << 52));
+    return __ddiv_rn(s, (double)count);
+}
+
+template <class RT, int PREC>
+__device__ __forceinline__ RT inner_mean(RT start, const Acc<PREC>& s1, uint64_t count) {
+    if (PREC == PREC_FP32) return __fadd_rn((float)start, div_count((float)s1.value(), count));
+    return to_rt<RT>(__dadd_rn((double)start, div_count((double)s1.value(), count)));
+}
+
+// Box-Muller pair from two OUTER words at the context precision.
+template <int PREC, class RT>
+__device__ __forceinline__ void bm_pair(uint32_t u0, uint32_t u1, RT& x, RT& y) {
+    if (PREC == PREC_FP32) {
+        float fx, fy;
+        boxmuller32_f(u0, u1, fx, fy);
+        x = (RT)fx;
+        y = (RT)fy;
+    } else {
+        double dx, dy;
+        boxmuller32_d(u0, u1, dx, dy);
+        x = to_rt<RT>(dx);
+        y = to_rt<RT>(dy);
+    }
+}
+
+template <int PREC, class RT>
+__device__ __forceinline__ RT u01_word(uint32_t w) {
+    if (PREC == PREC_FP64) return (RT)__dadd_rn(__dmul_rn((double)w, 0x1p-32), 0x1p-33);
+    return (RT)__fadd_rn(__fmul_rn(__uint2float_rn(w), 0x1p-32f), 0x1p-33f);
+}
+
+// normal k of an OUTER phase (used for the outer draws)
+template <int PREC, class RT>
+__device__ __forceinline__ RT outer_normal_at(const TfKey& key, uint32_t tag, uint64_t k) {
+    uint64_t v0, v1;
+    threefry2x64(k >> 2, tag, key, v0, v1);
+    uint64_t e = ((k >> 1) & 1) ? v1 : v0;
+    RT x, y;
+    bm_pair<PREC, RT>((uint32_t)e, (uint32_t)(e >> 32), x, y);
+    return (k & 1) ? y : x;
+}
+
+// ---- portfolio inner value (BS path of portfolio::sampler) ----------------------------------
+template <class RT>
+__device__ __forceinline__ RT pf_value(const OptionTable<RT>& ot, const RT* Rrow, uint32_t j) {
+    uint32_t s = ot.stock_ind[j];
+    int type = ot.type[j];
+    RT sigma = ot.sigma[s];
+    RT bs = calc_bs_ref<RT>(type, Rrow[s], ot.strike[j], ot.r, xsub(ot.maturity[j], ot.tau), sigma);
+    RT finish = ot.discount ? xmul(xexp(xmul(-ot.r, ot.tau)), bs) : bs;
+    RT val = xmul(ot.w[j], xsub(ot.start[j], finish));
+    if (ot.use_delta_cv) {
+        RT derv = xmul(ot.w[j], calc_delta_ref<RT>(type, ot.S0[s], ot.strike[j], ot.r, ot.maturity[j], sigma));
+        val = xadd(val, xmul(xsub(Rrow[s], ot.S0[s]), derv));
+    }
+    return val;
+}
+
+// Option index of one inner sample from one 64-bit value of the OUTER layout (the draw of
+// sample_inner_random_option_ind, 346-370, with its own addressing): column j = floor(v P / 2^64),
+// exact in every precision.  Uniform sub-sampling takes j (prob 1 / P); importance sub-sampling
+// (Subsampling::Random) flips the column's alias coin (v P mod 2^64) >> 32 — O(1) instead of the
+// reference's CDF binary search, the distribution of the table's exact masses phat.
+__device__ __forceinline__ uint32_t pf_index(const uint2* alias, uint32_t P, uint64_t v) {
+    const uint32_t j = (uint32_t)__umul64hi(v, (uint64_t)P);
+    if (!alias) return j;
+    const uint32_t coin = (uint32_t)((v * (uint64_t)P) >> 32);
+    const uint2 e = alias[j];
+    return coin < e.x ? j : e.y;
+}
+
+template <class RT>
+__device__ __forceinline__ uint32_t pf_pick(const OptionTable<RT>& ot, uint64_t v, RT& prob) {
+    const uint32_t j = pf_index(ot.subsample == SUB_UNIFORM ? nullptr : ot.alias, ot.P, v);
+    prob = ot.subsample == SUB_UNIFORM ? ot.inv_count_prob : ot.phat[j];
+    return j;
+}
+
+// ---- one chunk: inner samples [s0, s0 + C) of phase `tag` of outer sample `item` ----------
+// C (inner samples per chunk) is a compile-time constant so the independent Threefry blocks of a
+// chunk can be interleaved (two at a time) for instruction-level parallelism.
+template <class RT, int KIND, int PREC, uint32_t C, bool S2>
+__device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t item, uint32_t tag,
+                                             uint64_t s0, Acc<PREC>& a1, Acc<PREC>& a2, double& work) {
+    const OuterLevel<RT>& L = D.L;
+    const TfKey key = tf_key(L.seed, outer_stream_id(L.ell, L.first_index + item));
+    const RT* Yv = reinterpret_cast<const RT*>(D.B.Yv);
+    if (KIND == KIND_SHIFT_MODEL) {              // X = Y + Z: one normal per inner sample
+        const RT Y = Yv[item];
+#pragma unroll 2
+        for (uint32_t b = 0; b < C / 4; b++) {
+            uint64_t v0, v1;
+            threefry2x64((s0 >> 2) + b, tag, key, v0, v1);
+            RT z[4];
+            bm_pair<PREC, RT>((uint32_t)v0, (uint32_t)(v0 >> 32), z[0], z[1]);
+            bm_pair<PREC, RT>((uint32_t)v1, (uint32_t)(v1 >> 32), z[2], z[3]);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                RT d = (PREC == PREC_FP32) ? (RT)(Y + z[q]) : xadd(Y, z[q]);
+                a1.add(d);
+                if (S2) a2.add((PREC == PREC_FP32) ? (RT)(d * d) : xmul(d, d));
+            }
+        }
+        work += (double)C;
+    } else if (KIND == KIND_REF_MODEL) {         // model_sampler.cpp:62-76: two normals
+        const RT Y = Yv[item];
+        const RT st = L.mp.stau, s1t = L.mp.s1tau;
+#pragma unroll 2
+        for (uint32_t b = 0; b < C / 2; b++) {   // one block = two inner samples
+            uint64_t v0, v1;
+            threefry2x64((s0 >> 1) + b, tag, key, v0, v1);
+            RT X[2], Y2[2];
+            bm_pair<PREC, RT>((uint32_t)v0, (uint32_t)(v0 >> 32), X[0], Y2[0]);
+            bm_pair<PREC, RT>((uint32_t)v1, (uint32_t)(v1 >> 32), X[1], Y2[1]);
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                RT a = xadd(xmul(st, Y), xmul(s1t, X[q]));
+                RT c = xadd(xmul(st, Y2[q]), xmul(s1t, X[q]));
+                RT d = xsub(xmul(a, a), xmul(c, c));
+                a1.add(d);
+                if (S2) a2.add(xmul(d, d));
+            }
+        }
+        work += (double)C;
+    } else if (PREC == PREC_FP32 && L.ot.fast_s) {
+        // portfolio, FP32: packed records scaled by 1 / (sampling probability), the SFU
+        // Black-Scholes (nmlmc_bs.cuh); X = loss_j / phat_j
+        const OptionTable<RT>& ot = L.ot;
+        const float* Rrow = reinterpret_cast<const float*>(D.B.Rt) + (size_t)item * ot.Q;
+        const uint2* alias = ot.subsample == SUB_UNIFORM ? nullptr : ot.alias;
+#pragma unroll 2
+        for (uint32_t b = 0; b < C / 2; b++) {
+            uint64_t v[2];
+            threefry2x64((s0 >> 1) + b, tag, key, v[0], v[1]);
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const uint32_t j = pf_index(alias, ot.P, v[q]);
+                const FastOption o = ot.fast_s[j];
+                const uint32_t st = o.asset_type & 0x7fffffffu;
+                const float R = Rrow[st];
+                const float S0 = o.cv != 0.f ? (float)ot.S0[st] : 0.f;
+                const float d = option_loss_fast(o, R, __logf(R), S0);
+                a1.add((RT)d);
+                if (S2) a2.add((RT)(d * d));
+            }
+        }
+        work += (double)C;
+    } else {                                     // portfolio: one 64-bit value per inner sample
+        const OptionTable<RT>& ot = L.ot;
+        const RT* Rrow = reinterpret_cast<const RT*>(D.B.Rt) + (size_t)item * ot.Q;
+#pragma unroll 2
+        for (uint32_t b = 0; b < C / 2; b++) {
+            uint64_t v[2];
+            threefry2x64((s0 >> 1) + b, tag, key, v[0], v[1]);
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                RT prob;
+                uint32_t j = pf_pick<RT>(ot, v[q], prob);
+                RT d = xdiv(pf_value<RT>(ot, Rrow, j), prob);
+                work += (double)ot.W_est[j];
+                a1.add(d);
+                if (S2) a2.add(xmul(d, d));
+            }
+        }
+    }
+}
+
+template <class RT, int KIND, int PREC, bool S2>
+__device__ __forceinline__ void eval_chunk_s(const DevLevel<RT>& D, uint32_t item, uint32_t tag,
+                                             uint64_t s0, uint32_t C, Acc<PREC>& a1, Acc<PREC>& a2,
+                                             double& work) {
+    switch (C) {
+    case 64: eval_chunk_c<RT, KIND, PREC, 64, S2>(D, item, tag, s0, a1, a2, work); break;
+    case 32: eval_chunk_c<RT, KIND, PREC, 32, S2>(D, item, tag, s0, a1, a2, work); break;
+    case 16: eval_chunk_c<RT, KIND, PREC, 16, S2>(D, item, tag, s0, a1, a2, work); break;
+    case 8: eval_chunk_c<RT, KIND, PREC, 8, S2>(D, item, tag, s0, a1, a2, work); break;
+    default: eval_chunk_c<RT, KIND, PREC, 4, S2>(D, item, tag, s0, a1, a2, work); break;
+    }
+}
+
+// want_s2 (pilots: the sum of squares for the variance) is resolved once per chunk, so the
+// inner loop carries no per-sample test.
+template <class RT, int KIND, int PREC>
+__device__ __forceinline__ void eval_chunk(const DevLevel<RT>& D, uint32_t item, uint32_t tag,
+                                           uint64_t s0, uint32_t C, bool want_s2, Acc<PREC>& a1,
+                                           Acc<PREC>& a2, double& work) {
+    if (want_s2) eval_chunk_s<RT, KIND, PREC, true>(D, item, tag, s0, C, a1, a2, work);
+    else eval_chunk_s<RT, KIND, PREC, false>(D, item, tag, s0, C, a1, a2, work);
+}
+
+// ---- segments of uniform chunk count ------------------------------------------------------
+struct Seg {
+    const uint32_t* list;    // item ids; nullptr: identity 0..n-1
+    uint32_t n_slot;         // counter slot with the item count (list != nullptr)
+    uint32_t n_host;         // item count (list == nullptr)
+    uint32_t nch_log2;       // chunks per item = 1 << nch_log2
+    uint32_t tag;            // OUTER phase tag
+    uint32_t mode;           // 0 fine pilot, 1 coarse pilot, 2 final
+    uint32_t class_k;        // final: class index (list offset = items of lower classes)
+    uint32_t next_slot;      // pilots: counter slot of the next round's list
+    uint32_t* next_list;
+    uint64_t count;          // inner samples per item in this segment
+};
+
+struct SegSet {
+    int n;
+    Seg s[kMaxSegs];
+};
+
+// Adaptive decision after a pilot of `cur` samples (get_samples_count, 240-273, with
+// sample_inner_delta2, 120-129).  Writes the final count of a decided item; returns true when
+// the item goes on to the next pilot round.
+template <class RT, int PREC>
+__device__ __forceinline__ bool pilot_decide(const DevLevel<RT>& D, const Seg& g, uint32_t item, RT start,
+                                             const Acc<PREC>& a1, const Acc<PREC>& a2) {
+    const OuterLevel<RT>& L = D.L;
+    const CountParams& cp = (g.mode == 0) ? L.cf : L.cc;
+    const uint64_t cur = g.count;
+    RT delta2;
+    if (PREC == PREC_FP32) {
+        float s1 = (float)a1.value(), s2 = (float)a2.value(), n = (float)cur;
+        float mean_d = div_count(s1, cur);
+        float var = __fdiv_rn(__fsub_rn(s2, __fmul_rn(s1, mean_d)), n - 1.0f);
+        float dist = __fadd_rn((float)start, mean_d);
+        delta2 = (RT)__fdiv_rn(__fmul_rn(dist, dist), var);
+    } else {
+        double s1 = (double)a1.value(), s2 = (double)a2.value();
+        RT out_var = to_rt<RT>(__dsub_rn(__ddiv_rn(s2, (double)(cur - 1)),
+                                         __ddiv_rn(__dmul_rn(s1, s1), (double)(cur * (cur - 1)))));
+        RT dist = xadd(start, to_rt<RT>(div_count(s1, cur)));
+        delta2 = xdiv(xmul(dist, dist), out_var);
+    }
+    RT newc;
+    if (L.adaptive_r == (RT)2) newc = xdiv((RT)cp.tmp, delta2);
+    else newc = xmul(xpow(delta2, xdiv(-L.adaptive_r, (RT)2)), (RT)cp.tmp);
+    uint32_t* cnt = (g.mode == 0) ? D.B.cnt_f : D.B.cnt_c;
+    if (newc <= (RT)cur) { cnt[item] = (uint32_t)cur; return false; }
+    const uint64_t nxt = cur * 2;
+    if (cp.max_count <= 2 * nxt) { cnt[item] = (uint32_t)cp.max_count; return false; }
+    return true;
+}
+
+// Appends the warp's surviving items to the next round's list: one atomic per warp (all 32
+// lanes call it).
+__device__ __forceinline__ void warp_append(bool surv, uint32_t item, uint32_t* count, uint32_t* list, int lane) {
+    const unsigned bal = __ballot_sync(0xffffffffu, surv);
+    if (!bal) return;
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(count, (uint32_t)__popc(bal));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (surv) list[base + __popc(bal & ((1u << lane) - 1u))] = item;
+}
+
+// Pilot rounds an item went through on one side, recovered from its final count: a count below
+// the maximum was fixed by the pilot of that size (rounds 0..r), the maximum is reached after
+// every round of the side (get_samples_count, 240-273).
+__device__ __forceinline__ uint32_t pilots_taken(uint32_t cnt, const CountParams& cp, bool adaptive) {
+    if (!adaptive) return 0;
+    uint32_t r = 0;
+    if (cnt == (uint32_t)cp.max_count) {
+        for (uint64_t c = cp.base_count; cp.max_count > 2 * c; c *= 2) r++;
+        return r;
+    }
+    for (uint64_t c = cp.base_count; c < cnt; c *= 2) r++;
+    return r + 1;
+}
+
+// Per-item completion of the final phase: phi_f, phi_c; their moments go into this thread's
+// moment slots mom[q * kTile] (q = 0..3 phi_f^k, 4..7 (phi_f - phi_c)^k; a zero phi adds
+// nothing and touches no slot), the counts of items that hit the maximum / stayed at the base
+// count, and the trace record.
+template <class RT>
+__device__ __forceinline__ void final_item(const DevLevel<RT>& D, uint32_t item, RT mean_big, RT phi_small,
+                                           bool fine_big, double* mom, uint32_t& n_max, uint32_t& n_base,
+                                           TraceRec* trace) {
+    RT phi_big = (mean_big >= (RT)0) ? (RT)1 : (RT)0;
+    RT f_phi, c_phi;
+    if (D.L.fine_only) { f_phi = phi_big; c_phi = 0; }
+    else if (fine_big) { f_phi = phi_big; c_phi = phi_small; }
+    else { f_phi = phi_small; c_phi = phi_big; }
+    if (f_phi != (RT)0) {
+        RT p = 1;
+#pragma unroll
+        for (int q = 0; q < 4; q++) { p = xmul(p, f_phi); mom[q * kTile] += (double)p; }
+    }
+    if (!D.L.fine_only) {
+        const RT dphi = xsub(f_phi, c_phi);
+        if (dphi != (RT)0) {
+            RT p = 1;
+#pragma unroll
+            for (int q = 0; q < 4; q++) { p = xmul(p, dphi); mom[(4 + q) * kTile] += (double)p; }
+        }
+    }
+    const uint32_t cf = D.B.cnt_f[item];
+    n_max += (cf == (uint32_t)D.L.cf.max_count) ? 1u : 0u;
+    n_base += (cf == (uint32_t)D.L.cf.base_count) ? 1u : 0u;
+    if (trace) {
+        TraceRec tr;
+        tr.count_f = cf;
+        tr.count_c = D.L.fine_only ? 0 : D.B.cnt_c[item];
+        tr.phi_f = (double)f_phi;
+        tr.phi_c = (double)c_phi;
+        tr.mean_big = (double)mean_big;
+        tr.min_abs_small = INFINITY;
+        tr.core = 0;
+        tr.pilots = pilots_taken(cf, D.L.cf, D.L.adaptive_f) +
+                    (D.L.fine_only ? 0u : pilots_taken((uint32_t)tr.count_c, D.L.cc, D.L.adaptive_c));
+        trace[item] = tr;
+    }
+}
+
+// Block partial sums (OuterBuffers::block_sums layout): [0..3] phi_f moments, [4..7] difference
+// moments, [8] work, [9] inner samples, [10] hit the maximum count, [11] stayed at the base count.
+// MINB = CTAs per SM the register allocation must allow (1: up to 255 registers per thread,
+// 2: 128, 4: 64) — the register/occupancy variants the autotuner chooses between.  The variants
+// run the same arithmetic in the same order, so their results are identical.
+template <class RT, int KIND, int PREC, int MINB>
+__global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet S, TraceRec* trace) {
+    __shared__ Acc<PREC> sm_a1[kWarps];
+    __shared__ Acc<PREC> sm_a2[kWarps];
+    __shared__ float sm_ind[kWarps];
+    __shared__ double sm_mom[8 * kTile];        // per-thread moment slots [q][thread]
+    __shared__ double sm_acc[kWarps][16];
+    __shared__ uint32_t sm_ticket;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const uint32_t C = D.L.chunk;
+    uint32_t* counters = D.B.counters;
+    double wsum = 0;                                     // work of this thread's chunks
+    uint32_t n_max = 0, n_base = 0;
+    double* mom = sm_mom + t;
+#pragma unroll
+    for (int q = 0; q < 8; q++) mom[q * kTile] = 0;
+    if (lane < 16) sm_acc[warp][lane] = 0;
+    __syncthreads();
+    const RT* Yv = reinterpret_cast<const RT*>(D.B.Yv);
+
+    for (int si = 0; si < S.n; si++) {
+        const Seg g = S.s[si];
+        const uint32_t* list = g.list;
+        uint32_t n_items = g.list ? counters[g.n_slot] : g.n_host;
+        if (g.mode == 2 && g.list) {
+            uint32_t off = 0;
+            for (uint32_t k = 0; k < g.class_k; k++) off += counters[CNT_CLASS + k];
+            list += off;
+        }
+        if (n_items == 0) continue;
+        const uint32_t nch = 1u << g.nch_log2;
+        const bool pilot = g.mode != 2;
+        if (blockIdx.x == 0 && t == 0) sm_acc[0][9] += (double)n_items * (double)g.count;
+
+        // The grid is persistent (the CTAs resident at once) and claims the segment's tiles from a
+        // device work queue: one ticket per tile, so no CTA waits for a second wave and uneven
+        // tiles balance themselves.  The next ticket is claimed while the current tile is
+        // evaluated.  Which CTA evaluates a tile does not change any result.
+        uint32_t* queue = counters + CNT_QUEUE + si;
+        if (t == 0) sm_ticket = atomicAdd(queue, 1u);
+        __syncthreads();
+        uint64_t ticket = sm_ticket;
+        if (nch <= (uint32_t)kTile) {
+            // ---- a tile holds kTile / nch whole items ----
+            const uint32_t per_tile = kTile / nch;
+            const uint64_t tiles = ((uint64_t)n_items + per_tile - 1) / per_tile;
+            for (;;) {
+                __syncthreads();                         // every thread has read the ticket
+                if (ticket >= tiles) break;
+                uint32_t next = 0;
+                if (t == 0) next = atomicAdd(queue, 1u);
+                const uint64_t lin = ticket * per_tile + (t >> g.nch_log2);
+                const uint32_t j = t & (nch - 1);
+                const bool valid = lin < n_items;
+                const uint32_t item = valid ? (list ? list[lin] : (uint32_t)lin) : 0;
+                uint32_t gs = nch;
+                uint64_t csmall = g.count;
+                bool fine_big = true;
+                if (!pilot && valid && !D.L.fine_only) {
+                    uint32_t cf = D.B.cnt_f[item], cc = D.B.cnt_c[item];
+                    csmall = cf < cc ? cf : cc;
+                    fine_big = cf > cc;
+                    gs = (uint32_t)(csmall / C);
+                }
+                const RT start = valid ? (D.L.ot.P ? Yv[item] : -D.L.mp.max_loss) : (RT)0;
+                Acc<PREC> a1, a2;
+                a1.zero();
+                a2.zero();
+                if (valid) eval_chunk<RT, KIND, PREC>(D, item, g.tag, (uint64_t)j * C, C, pilot, a1, a2, wsum);
+                const float coeff = (float)gs / (float)nch;     // 1 / groups (a power of two)
+                float ind = 0.f;
+                if (!pilot && gs == 1) ind = inner_mean<RT, PREC>(start, a1, csmall) >= (RT)0 ? coeff : 0.f;
+                const uint32_t wl = nch < 32 ? nch : 32;
+                for (uint32_t m = 1; m < wl; m <<= 1) {
+                    a1.merge(a1.shfl_xor(m));
+                    if (pilot) a2.merge(a2.shfl_xor(m));
+                    else {
+                        ind += __shfl_xor_sync(0xffffffffu, ind, m);
+                        if (2 * m == gs) ind = inner_mean<RT, PREC>(start, a1, csmall) >= (RT)0 ? coeff : 0.f;
+                    }
+                }
+                const bool leader = (j == 0) && valid;
+                if (nch > 32) {
+                    if (lane == 0) { sm_a1[warp] = a1; sm_a2[warp] = a2; sm_ind[warp] = ind; }
+                    __syncthreads();
+                    if (leader) {
+                        const uint32_t nw = nch / 32;
+                        Acc<PREC> t1, t2;
+                        t1.zero();
+                        t2.zero();
+                        float ti = 0.f;
+                        if (!pilot && gs > 32) {
+                            const uint32_t gw = gs / 32;
+                            for (uint32_t gq = 0; gq < nw / gw; gq++) {
+                                Acc<PREC> gsum;
+                                gsum.zero();
+                                for (uint32_t q = 0; q < gw; q++) gsum.merge(sm_a1[warp + gq * gw + q]);
+                                ti += inner_mean<RT, PREC>(start, gsum, csmall) >= (RT)0 ? coeff : 0.f;
+                                t1.merge(gsum);
+                            }
+                        } else {
+                            for (uint32_t q = 0; q < nw; q++) {
+                                t1.merge(sm_a1[warp + q]);
+                                if (pilot) t2.merge(sm_a2[warp + q]);
+                                ti += sm_ind[warp + q];
+                            }
+                        }
+                        a1 = t1;
+                        a2 = t2;
+                        ind = ti;
+                    }
+                    __syncthreads();
+                }
+                if (pilot) {
+                    const bool surv = leader && pilot_decide<RT, PREC>(D, g, item, start, a1, a2);
+                    warp_append(surv, item, counters + g.next_slot, g.next_list, lane);
+                } else if (leader) {
+                    final_item<RT>(D, item, inner_mean<RT, PREC>(start, a1, g.count), (RT)ind, fine_big, mom,
+                                   n_max, n_base, trace);
+                }
+                if (t == 0) sm_ticket = next;
+                __syncthreads();
+                ticket = sm_ticket;
+            }
+        } else {
+            // ---- one CTA walks an item tile by tile ----
+            const uint32_t tiles_per_item = nch / kTile;
+            for (;;) {
+                __syncthreads();                         // every thread has read the ticket
+                if (ticket >= n_items) break;
+                uint32_t next = 0;
+                if (t == 0) next = atomicAdd(queue, 1u);
+                const uint32_t item = list ? list[ticket] : (uint32_t)ticket;
+                uint32_t gs = nch;
+                uint64_t csmall = g.count;
+                bool fine_big = true;
+                if (!pilot && !D.L.fine_only) {
+                    uint32_t cf = D.B.cnt_f[item], cc = D.B.cnt_c[item];
+                    csmall = cf < cc ? cf : cc;
+                    fine_big = cf > cc;
+                    gs = (uint32_t)(csmall / C);
+                }
+                const RT start = D.L.ot.P ? Yv[item] : -D.L.mp.max_loss;
+                const float coeff = (float)gs / (float)nch;
+                Acc<PREC> tot1, tot2, gacc;
+                tot1.zero();
+                tot2.zero();
+                gacc.zero();
+                float tind = 0.f;
+                for (uint32_t tl = 0; tl < tiles_per_item; tl++) {
+                    const uint32_t j = tl * kTile + t;
+                    Acc<PREC> a1, a2;
+                    a1.zero();
+                    a2.zero();
+                    eval_chunk<RT, KIND, PREC>(D, item, g.tag, (uint64_t)j * C, C, pilot, a1, a2, wsum);
+                    float ind = 0.f;
+                    if (!pilot && gs == 1) ind = inner_mean<RT, PREC>(start, a1, csmall) >= (RT)0 ? coeff : 0.f;
+                    for (uint32_t m = 1; m < 32; m <<= 1) {
+                        a1.merge(a1.shfl_xor(m));
+                        if (pilot) a2.merge(a2.shfl_xor(m));
+                        else {
+                            ind += __shfl_xor_sync(0xffffffffu, ind, m);
+                            if (2 * m == gs) ind = inner_mean<RT, PREC>(start, a1, csmall) >= (RT)0 ? coeff : 0.f;
+                        }
+                    }
+                    if (lane == 0) { sm_a1[warp] = a1; sm_a2[warp] = a2; sm_ind[warp] = ind; }
+                    __syncthreads();
+                    if (t == 0) {
+                        if (!pilot && gs > 32 && gs < (uint32_t)kTile) {
+                            const uint32_t gw = gs / 32;
+                            for (uint32_t gq = 0; gq < (uint32_t)kWarps / gw; gq++) {
+                                Acc<PREC> gsum;
+                                gsum.zero();
+                                for (uint32_t q = 0; q < gw; q++) gsum.merge(sm_a1[gq * gw + q]);
+                                tind += inner_mean<RT, PREC>(start, gsum, csmall) >= (RT)0 ? coeff : 0.f;
+                                tot1.merge(gsum);
+                            }
+                        } else {
+                            Acc<PREC> t1;
+                            t1.zero();
+                            for (int q = 0; q < kWarps; q++) {
+                                t1.merge(sm_a1[q]);
+                                if (pilot) tot2.merge(sm_a2[q]);
+                                if (!pilot && gs <= 32) tind += sm_ind[q];
+                            }
+                            tot1.merge(t1);
+                            if (!pilot && gs >= (uint32_t)kTile) {
+                                gacc.merge(t1);
+                                if ((((uint64_t)tl + 1) * kTile) % gs == 0) {
+                                    tind += inner_mean<RT, PREC>(start, gacc, csmall) >= (RT)0 ? coeff : 0.f;
+                                    gacc.zero();
+                                }
+                            }
+                        }
+                    }
+                    __syncthreads();
+                }
+                if (t == 0) {
+                    if (pilot) {
+                        if (pilot_decide<RT, PREC>(D, g, item, start, tot1, tot2))
+                            g.next_list[atomicAdd(&counters[g.next_slot], 1u)] = item;
+                    } else {
+                        final_item<RT>(D, item, inner_mean<RT, PREC>(start, tot1, g.count), (RT)tind, fine_big, mom,
+                                       n_max, n_base, trace);
+                    }
+                    sm_ticket = next;
+                }
+                __syncthreads();
+                ticket = sm_ticket;
+            }
+        }
+    }
+    // this thread's work, moments and counts -> per-warp sums -> this CTA's partial-sum slot
+    for (int m = 16; m > 0; m >>= 1) {
+        wsum += __shfl_down_sync(0xffffffffu, wsum, m);
+        n_max += __shfl_down_sync(0xffffffffu, n_max, m);
+        n_base += __shfl_down_sync(0xffffffffu, n_base, m);
+    }
+    double mv[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        mv[q] = mom[q * kTile];
+        for (int m = 16; m > 0; m >>= 1) mv[q] += __shfl_down_sync(0xffffffffu, mv[q], m);
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < 8; q++) sm_acc[warp][q] += mv[q];
+        sm_acc[warp][8] += wsum;
+        sm_acc[warp][10] += (double)n_max;
+        sm_acc[warp][11] += (double)n_base;
+    }
+    __syncthreads();
+    if (t < 16) {
+        double v = 0;
+        for (int w = 0; w < kWarps; w++) v += sm_acc[w][t];
+        D.B.block_sums[(size_t)blockIdx.x * 16 + t] += v;
+    }
+}
+
+// ---- outer draws ---------------------------------------------------------------------------
+template <class RT, int KIND, int PREC>
+__global__ void __launch_bounds__(kTile) k_outer(DevLevel<RT> D, uint32_t nb) {
+    const OuterLevel<RT>& L = D.L;
+    RT* Yv = reinterpret_cast<RT*>(D.B.Yv);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
+        const TfKey key = tf_key(L.seed, outer_stream_id(L.ell, L.first_index + i));
+        D.B.cnt_f[i] = L.adaptive_f ? 0u : (uint32_t)L.cf.max_count;
+        D.B.cnt_c[i] = L.adaptive_c ? 0u : (uint32_t)L.cc.max_count;
+        if (KIND != KIND_PORTFOLIO) {
+            Yv[i] = outer_normal_at<PREC, RT>(key, PH_OUTER, 0);
+        } else {
+            // portfolio_sampler.cpp:293-311 on the OUTER layout: normal 0 systemic, 1 + s per stock
+            const OptionTable<RT>& ot = L.ot;
+            RT* Rrow = reinterpret_cast<RT*>(D.B.Rt) + (size_t)i * ot.Q;
+            RT dW_sys = 0, cv = (RT)0;
+            const uint32_t nnorm = ot.Q == 1 ? 1 : ot.Q + 1;
+            for (uint32_t b = 0; 4 * b < nnorm; b++) {          // four normals per block
+                uint64_t v0, v1;
+                threefry2x64(b, PH_OUTER, key, v0, v1);
+                RT z[4];
+                bm_pair<PREC, RT>((uint32_t)v0, (uint32_t)(v0 >> 32), z[0], z[1]);
+                bm_pair<PREC, RT>((uint32_t)v1, (uint32_t)(v1 >> 32), z[2], z[3]);
+                for (uint32_t q = 0; q < 4; q++) {
+                    const uint32_t k = 4 * b + q;
+                    if (k >= nnorm) break;
+                    if (k == 0) { dW_sys = xmul(ot.stau, z[0]); if (ot.Q > 1) continue; }
+                    const uint32_t s = ot.Q == 1 ? 0 : k - 1;
+                    RT W = ot.Q == 1 ? dW_sys : xadd(xmul(ot.rho, dW_sys), xmul(ot.s1_rho2, xmul(ot.stau, z[q])));
+                    RT R;
+                    if (PREC == PREC_FP32) {     // GBM at tau in float (expf), the fast path's R
+                        const float sg = (float)ot.sigma[s];
+                        R = (RT)((float)ot.S0[s] * expf(sg * (float)W + ((float)ot.mu[s] - 0.5f * sg * sg) * (float)ot.tau));
+                    } else {
+                        R = simulate_stock_ref<RT>(ot.S0[s], ot.mu[s], ot.sigma[s], ot.tau, W);
+                    }
+                    Rrow[s] = R;
+                    if (ot.use_delta_cv) cv = xadd(cv, xmul(xsub(R, ot.S0[s]), ot.delta_coalesce[s]));
+                }
+            }
+            Yv[i] = xsub(-ot.max_loss, cv);
+        }
+    }
+}
+
+// ---- bucket outer samples by final count (count_big = max(cnt_f, cnt_c)) ------------------
+// Pass 0 counts the outer samples of each class, pass 1 scatters their indices into class order.
+// Each CTA histograms a tile in shared memory first, so the global counters see one atomic per
+// class per tile instead of one per outer sample.
+template <class RT>
+__global__ void k_classify(DevLevel<RT> D, uint32_t nb, int pass) {
+    uint32_t* counters = D.B.counters;
+    const uint32_t C = D.L.chunk;
+    __shared__ uint32_t offs[64], hist[64], base[64];
+    if (pass == 1 && threadIdx.x == 0) {
+        uint32_t a = 0;
+        for (int k = 0; k < 64; k++) { offs[k] = a; a += counters[CNT_CLASS + k]; }
+    }
+    for (uint32_t t0 = blockIdx.x * blockDim.x; t0 < nb; t0 += gridDim.x * blockDim.x) {
+        if (threadIdx.x < 64) hist[threadIdx.x] = 0;
+        __syncthreads();
+        const uint32_t i = t0 + threadIdx.x;
+        const bool valid = i < nb;
+        uint32_t k = 0, rank = 0;
+        if (valid) {
+            uint32_t cf = D.B.cnt_f[i], cc = D.L.fine_only ? 0u : D.B.cnt_c[i];
+            uint32_t q = (cf > cc ? cf : cc) / C;
+            k = q ? 31 - __clz(q) : 0;
+            rank = atomicAdd(&hist[k], 1u);
+        }
+        __syncthreads();
+        if (threadIdx.x < 64 && hist[threadIdx.x]) {
+            if (pass == 0) atomicAdd(&counters[CNT_CLASS + threadIdx.x], hist[threadIdx.x]);
+            else base[threadIdx.x] = atomicAdd(&counters[CNT_FILL + threadIdx.x], hist[threadIdx.x]);
+        }
+        __syncthreads();
+        if (pass == 1 && valid) D.B.class_items[offs[k] + base[k] + rank] = i;
+        __syncthreads();
+    }
+}
+
+static __global__ void k_reduce_blocks(const double* block_sums, int grid, double* level_acc) {
+    __shared__ double sm[256];
+    for (int q = 0; q < 16; q++) {
+        double v = 0;
+        for (int b = threadIdx.x; b < grid; b += blockDim.x) v += block_sums[(size_t)b * 16 + q];
+        sm[threadIdx.x] = v;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+            if ((int)threadIdx.x < s) sm[threadIdx.x] += sm[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) level_acc[q] += sm[0];
+        __syncthreads();
+    }
+}
+
+// Persistent grid of the phase kernel: the CTAs that are resident at once (occupancy x SMs),
+// at most the grid the partial-sum buffer was sized for.
+template <class RT, int KIND, int PREC, int MINB>
+static int phase_grid(int cap) {
+    static int g = 0;
+    if (g == 0) {
+        int dev = 0, sms = 148, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_phase<RT, KIND, PREC, MINB>, kTile, 0) != cudaSuccess ||
+            per_sm < 1)
+            per_sm = 1;
+        g = per_sm * sms;
+    }
+    return g < cap ? g : cap;
+}
+
+template <class RT, int KIND, int PREC, int MINB>
+static void launch_phase_v(const DevLevel<RT>& D, const SegSet& S, TraceRec* trace, cudaStream_t stream) {
+    cudaMemsetAsync(D.B.counters + CNT_QUEUE, 0, kMaxSegs * sizeof(uint32_t), stream);
+    if (D.B.prof_mark) D.B.prof_mark(D.B.prof_user, 0, stream);
+    k_phase<RT, KIND, PREC, MINB><<<phase_grid<RT, KIND, PREC, MINB>(D.B.grid), kTile, 0, stream>>>(D, S, trace);
+    if (D.B.prof_mark) D.B.prof_mark(D.B.prof_user, 1, stream);
+    count_launch();
+}
+
+// The FP32 path has three register/occupancy variants (OuterLevel::variant 0, 1, 2 -> 1, 2, 4
+// resident CTAs per SM guaranteed); the parity precisions run variant 0.
+template <class RT, int KIND, int PREC>
+static void launch_phase(const DevLevel<RT>& D, const SegSet& S, TraceRec* trace, cudaStream_t stream) {
+    if constexpr (PREC == PREC_FP32) {
+        if (D.L.variant == 1) return launch_phase_v<RT, KIND, PREC, 2>(D, S, trace, stream);
+        if (D.L.variant == 2) return launch_phase_v<RT, KIND, PREC, 4>(D, S, trace, stream);
+    }
+    launch_phase_v<RT, KIND, PREC, 1>(D, S, trace, stream);
+}
+
+static inline uint32_t ilog2_u64(uint64_t v) {
+    uint32_t r = 0;
+    while ((1ull << (r + 1)) <= v) r++;
+    return r;
+}
+
+template <class RT, int KIND, int PREC>
+static cudaError_t run_batch(DevLevel<RT>& D, uint32_t nb, TraceRec* trace, cudaStream_t stream) {
+    const OuterLevel<RT>& L = D.L;
+    OuterBuffers& B = D.B;
+    const uint32_t C = L.chunk;
+    const int grid = B.grid;
+    cudaError_t e;
+    int og = (int)((nb + kTile - 1) / kTile);
+    if (og > grid) og = grid;
+    if (og < 1) og = 1;
+    k_outer<RT, KIND, PREC><<<og, kTile, 0, stream>>>(D, nb);
+    count_launch();
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+
+    if (L.adaptive_f || L.adaptive_c) {
+        uint32_t rounds_f = 0, rounds_c = 0;
+        if (L.adaptive_f) for (uint64_t c = L.cf.base_count; L.cf.max_count > 2 * c; c *= 2) rounds_f++;
+        if (L.adaptive_c) for (uint64_t c = L.cc.base_count; L.cc.max_count > 2 * c; c *= 2) rounds_c++;
+        const uint32_t rounds = rounds_f > rounds_c ? rounds_f : rounds_c;
+        uint32_t* listF[2] = {B.lists, B.lists + B.cap};
+        uint32_t* listC[2] = {B.lists + 2 * B.cap, B.lists + 3 * B.cap};
+        for (uint32_t r = 0; r < rounds; r++) {
+            const int cur = r & 1, nxt = cur ^ 1;
+            e = cudaMemsetAsync(B.counters + CNT_LIST + nxt, 0, sizeof(uint32_t), stream);
+            if (e == cudaSuccess) e = cudaMemsetAsync(B.counters + CNT_LIST + 2 + nxt, 0, sizeof(uint32_t), stream);
+            if (e != cudaSuccess) return e;
+            SegSet S;
+            S.n = 0;
+            for (int which = 0; which < 2; which++) {
+                const bool fine = which == 0;
+                if (fine ? (r >= rounds_f) : (r >= rounds_c)) continue;
+                const CountParams& cp = fine ? L.cf : L.cc;
+                Seg& g = S.s[S.n++];
+                g.list = (r == 0) ? nullptr : (fine ? listF[cur] : listC[cur]);
+                g.n_slot = CNT_LIST + (fine ? 0 : 2) + cur;
+                g.n_host = nb;
+                g.count = cp.base_count << r;
+                g.nch_log2 = ilog2_u64(g.count / C);
+                g.tag = (fine ? PH_FINE : PH_COARSE) + r;
+                g.mode = fine ? 0 : 1;
+                g.class_k = 0;
+                g.next_slot = CNT_LIST + (fine ? 0 : 2) + nxt;
+                g.next_list = fine ? listF[nxt] : listC[nxt];
+            }
+            if (S.n == 0) continue;
+            launch_phase<RT, KIND, PREC>(D, S, nullptr, stream);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
+        e = cudaMemsetAsync(B.counters + CNT_CLASS, 0, 128 * sizeof(uint32_t), stream);
+        if (e != cudaSuccess) return e;
+        k_classify<RT><<<og, kTile, 0, stream>>>(D, nb, 0);
+        k_classify<RT><<<og, kTile, 0, stream>>>(D, nb, 1);
+        count_launch(2);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        const uint64_t maxc = L.cf.max_count > L.cc.max_count ? L.cf.max_count : L.cc.max_count;
+        const uint32_t kmax = ilog2_u64(maxc / C);
+        SegSet S;
+        S.n = 0;
+        for (uint32_t k = 0; k <= kmax && S.n < kMaxSegs; k++) {
+            Seg& g = S.s[S.n++];
+            g.list = B.class_items;
+            g.n_slot = CNT_CLASS + k;
+            g.n_host = 0;
+            g.count = (uint64_t)C << k;
+            g.nch_log2 = k;
+            g.tag = PH_FINAL;
+            g.mode = 2;
+            g.class_k = k;
+            g.next_slot = 0;
+            g.next_list = nullptr;
+        }
+        launch_phase<RT, KIND, PREC>(D, S, trace, stream);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    } else {
+        const uint64_t cbig = (L.fine_only || L.cf.max_count >= L.cc.max_count) ? L.cf.max_count : L.cc.max_count;
+        SegSet S;
+        S.n = 1;
+        Seg& g = S.s[0];
+        g.list = nullptr;
+        g.n_slot = 0;
+        g.n_host = nb;
+        g.count = cbig;
+        g.nch_log2 = ilog2_u64(cbig / C);
+        g.tag = PH_FINAL;
+        g.mode = 2;
+        g.class_k = 0;
+        g.next_slot = 0;
+        g.next_list = nullptr;
+        launch_phase<RT, KIND, PREC>(D, S, trace, stream);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+template <class RT, int KIND, int PREC>
+cudaError_t sample_level_t(const OuterLevel<RT>& L, OuterBuffers& B, TraceRec* trace,
+                                  cudaStream_t stream) {
+    DevLevel<RT> D;
+    D.L = L;
+    D.B = B;
+    for (uint64_t done = 0; done < L.M;) {
+        const uint64_t nb = (L.M - done) < B.cap ? (L.M - done) : B.cap;
+        D.L.first_index = L.first_index + done;
+        cudaError_t e = run_batch<RT, KIND, PREC>(D, (uint32_t)nb, trace ? trace + done : nullptr, stream);
+        if (e != cudaSuccess) return e;
+        done += nb;
+    }
+    k_reduce_blocks<<<1, 256, 0, stream>>>(B.block_sums, B.grid, B.level_acc);
+    count_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace nmlmc

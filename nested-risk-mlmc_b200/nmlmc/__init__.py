@@ -183,6 +183,14 @@ PORTFOLIO_C2 = dict(Q=20, P=10_000, S0=100.0, r=0.05, mu=0.05, sigma_lo=0.1, sig
 PORTFOLIO_C3 = dict(PORTFOLIO_C2, Q=200, P=1_000_000)
 TAU_WEEK = 1 / 52
 
+class PhaseConfig(ctypes.Structure):
+    """nmlmc_phase_config: phase-kernel variant and chunk length of one level."""
+    _fields_ = [("variant", ctypes.c_uint32), ("chunk", ctypes.c_uint32), ("state", ctypes.c_int32),
+                ("probe_ms", ctypes.c_double)]
+
+
+PHASE_DEFAULT, PHASE_TUNED, PHASE_PINNED = 0, 1, 2
+
 SAMPLE_LEVEL_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64,
                                    ctypes.POINTER(LevelResult))
 SAMPLE_LEVELS_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint32, _u32p, _u64p,
@@ -203,7 +211,8 @@ EXPORTS = [
     "nmlmc_mlmc_run_cb", "nmlmc_threefry_blocks", "nmlmc_outer_normals", "nmlmc_set_shard",
     "nmlmc_set_profiling", "nmlmc_phase_kernel_time", "nmlmc_kernel_launches",
     "nmlmc_sample_level_noalloc", "nmlmc_portfolio_generate", "nmlmc_set_portfolio_methods",
-    "nmlmc_path_adjoint", "nmlmc_graph_stats",
+    "nmlmc_path_adjoint", "nmlmc_graph_stats", "nmlmc_set_autotune", "nmlmc_get_phase_config",
+    "nmlmc_set_phase_config", "nmlmc_autotune_level",
 ]
 
 
@@ -243,6 +252,10 @@ def lib() -> ctypes.CDLL:
                                            _dp, _dp, _dp, _u32p, _i32p]
     L.nmlmc_set_shard.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32]
     L.nmlmc_set_profiling.argtypes = [ctypes.c_void_p, ctypes.c_int32]
+    L.nmlmc_set_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int32]
+    L.nmlmc_get_phase_config.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(PhaseConfig)]
+    L.nmlmc_set_phase_config.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(PhaseConfig)]
+    L.nmlmc_autotune_level.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64]
     L.nmlmc_phase_kernel_time.argtypes = [ctypes.c_void_p, _u64p, _dp]
     L.nmlmc_kernel_launches.restype = ctypes.c_uint64
     L.nmlmc_sample_level_noalloc.argtypes = [ctypes.c_int32, ctypes.c_double, ctypes.c_double,
@@ -394,6 +407,31 @@ class Sampler:
         _check(self.L.nmlmc_graph_stats(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
                "nmlmc_graph_stats")
         return dict(instantiations=a.value, updates=b.value, launches=c.value)
+
+    # ---- phase-kernel autotuner (batched FP32 path) ----
+    def set_autotune(self, mode: int):
+        """0 off, 1 register/occupancy variant per level (default), 2 variant and chunk length."""
+        _check(self.L.nmlmc_set_autotune(self.h, int(mode)), "nmlmc_set_autotune")
+
+    def phase_config(self, ell: int) -> dict:
+        """Level ell's phase-kernel configuration: variant, chunk, state (PHASE_*), probe_ms."""
+        p = PhaseConfig()
+        _check(self.L.nmlmc_get_phase_config(self.h, ell, ctypes.byref(p)), "nmlmc_get_phase_config")
+        return dict(variant=p.variant, chunk=p.chunk, state=p.state, probe_ms=p.probe_ms)
+
+    def set_phase_config(self, ell: int, variant=None, chunk=None):
+        """Pins level ell's configuration; with no arguments, unpins it."""
+        if variant is None and chunk is None:
+            _check(self.L.nmlmc_set_phase_config(self.h, ell, None), "nmlmc_set_phase_config")
+            return
+        cur = self.phase_config(ell)
+        p = PhaseConfig(cur["variant"] if variant is None else variant,
+                        cur["chunk"] if chunk is None else chunk, 0, 0.0)
+        _check(self.L.nmlmc_set_phase_config(self.h, ell, ctypes.byref(p)), "nmlmc_set_phase_config")
+
+    def autotune_level(self, ell: int, M: int) -> dict:
+        _check(self.L.nmlmc_autotune_level(self.h, ell, M), "nmlmc_autotune_level")
+        return self.phase_config(ell)
 
     def reset_streams(self):
         _check(self.L.nmlmc_reset_streams(self.h), "nmlmc_reset_streams")
