@@ -647,8 +647,9 @@ OuterLevel<RT> outer_level_params(const nmlmc_ctx* c, uint32_t ell, uint64_t M, 
 // ---- phase-kernel autotuner (batched FP32 path) ---------------------------------------------
 // The first call of a level that carries enough work to time (>= 4096 outer samples and ~8e6
 // inner samples in one batch) times candidate configurations on a probe — the level's own
-// parameters on min(M, batch) outer samples whose stream indices start at 2^55, far from any
-// real index, so the probe changes no result — and keeps the fastest for the level:
+// parameters on about 2^26 inner samples of pilot work (probe_size), from outer samples whose
+// stream indices start at 2^55, far from any real index, so the probe changes no result — and
+// keeps the fastest for the level:
 //   1. the register/occupancy variants 0, 1, 2 at the default chunk length;
 //   2. (mode 2, or an explicit nmlmc_autotune_level) half and double the chunk length at the
 //      best variant, taken only if > 3 % faster.
@@ -678,9 +679,20 @@ cudaError_t time_phase_config(nmlmc_ctx* c, uint32_t ell, uint64_t Mp, const Pha
     return e;
 }
 
+// Probe size: about 2^26 inner samples of pilot work (~1 ms), at least 4096 outer samples, at
+// most the call's M and one batch.
+uint64_t probe_size(const nmlmc_ctx* c, uint32_t ell, uint64_t M) {
+    const CountParams cf = count_params(c->cfg, ell);
+    uint64_t Mp = (1ull << 26) / (cf.base_count * (uint64_t)(ell + 1));
+    if (Mp < 4096) Mp = 4096;
+    if (Mp > M) Mp = M;
+    if (Mp > c->ob.cap) Mp = c->ob.cap;
+    return Mp;
+}
+
 template <class RT>
 int tune_level(nmlmc_ctx* c, uint32_t ell, uint64_t M, bool chunks) {
-    const uint64_t Mp = M < c->ob.cap ? M : c->ob.cap;
+    const uint64_t Mp = probe_size(c, ell, M);
     PhaseChoice best = default_phase(c);
     best.state = 1;
     double best_ms = INFINITY;

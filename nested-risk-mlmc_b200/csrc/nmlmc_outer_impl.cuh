@@ -102,7 +102,6 @@ struct DevLevel {
     OuterBuffers B;
 };
 
-// inner mean start + s1 / count (sample_inner_mean, nested_sampler.hpp:112-119)
 // s / count; a power-of-two count multiplies by its exact reciprocal, which gives the same
 // correctly rounded quotient without the division sequence.
 __device__ __forceinline__ float div_count(float s, uint64_t count) {
@@ -115,6 +114,7 @@ __device__ __forceinline__ double div_count(double s, uint64_t count) {
     return __ddiv_rn(s, (double)count);
 }
 
+// inner mean start + s1 / count (sample_inner_mean, nested_sampler.hpp:112-119)
 template <class RT, int PREC>
 __device__ __forceinline__ RT inner_mean(RT start, const Acc<PREC>& s1, uint64_t count) {
     if (PREC == PREC_FP32) return __fadd_rn((float)start, div_count((float)s1.value(), count));
