@@ -373,6 +373,8 @@ typedef struct nmlmc_mlmc_input {
     int32_t verbose;               /* print the reference's "# Sampling" lines and tables */
     uint32_t max_levels;           /* 0 = unbounded                                       */
     int32_t batched;               /* 1: one nmlmc_sample_levels submission per round      */
+    uint32_t max_iterations;       /* stop after this many completed TOL iterations (0: run
+                                      to targetTOL); with a checkpoint, resume later        */
 } nmlmc_mlmc_input;
 
 #define NMLMC_MAX_LEVELS 64
@@ -386,6 +388,8 @@ typedef struct nmlmc_mlmc_output {
     double level_diffsums[NMLMC_MAX_LEVELS][4];
     double level_work[NMLMC_MAX_LEVELS];
     double level_time[NMLMC_MAX_LEVELS];
+    uint32_t iterations_done;               /* TOL iterations completed, resumed ones included */
+    uint32_t complete;                      /* 1: targetTOL reached; 0: stopped by max_iterations */
 } nmlmc_mlmc_output;
 
 typedef void (*nmlmc_sample_level_fn)(void* user, uint32_t ell, uint64_t M,
@@ -402,6 +406,40 @@ int nmlmc_mlmc_run(nmlmc_ctx* ctx, const nmlmc_mlmc_input* in, nmlmc_mlmc_output
 int nmlmc_mlmc_run_cb(const nmlmc_mlmc_input* in, nmlmc_sample_level_fn level_fn,
                       nmlmc_sample_levels_fn levels_fn, void* user, nmlmc_mlmc_output* out,
                       char* table, size_t table_cap);
+
+/* ---- checkpoint / resume of the driver ----------------------------------------------------
+ * No counterpart in the reference (its mlmc_t::run keeps the state in memory only).  After
+ * every completed TOL iteration the driver writes `path` (atomically: a temporary file renamed
+ * over it): the input parameters, the iteration state (next iteration, TOL, starting level,
+ * calls) and every level's FP64 sums (M, sum phi_f^k, sum dphi^k, work, time), followed by the
+ * sampler's state (`save`; for nmlmc_mlmc_run_ckpt the context's stream positions).  With
+ * `resume` set and `path` present, a run whose input parameters (targetTOL, startTOL, theta,
+ * starting_level_coeff, Ca, M0) equal the saved ones continues at the saved iteration with the
+ * saved sums and sampler state, and ends exactly as the uninterrupted run would; otherwise it
+ * warm-starts: the saved level sums seed a run of the new parameters from its first iteration.
+ * The file is little-endian: "NMLMCCK1", u32 version = 1, u32 header bytes, then the fields in
+ * the order above (nmlmc/checkpoint.py reads it). */
+typedef size_t (*nmlmc_state_save_fn)(void* user, void* buf, size_t cap);   /* bytes needed  */
+typedef int (*nmlmc_state_load_fn)(void* user, const void* buf, size_t size);
+typedef struct nmlmc_checkpoint_io {
+    const char* path;              /* NULL: no checkpoint                                   */
+    int32_t resume;                /* 1: start from `path` when it exists                    */
+    nmlmc_state_save_fn save;      /* optional sampler state stored in the checkpoint        */
+    nmlmc_state_load_fn load;
+} nmlmc_checkpoint_io;
+int nmlmc_mlmc_run_cb_ckpt(const nmlmc_mlmc_input* in, nmlmc_sample_level_fn level_fn,
+                           nmlmc_sample_levels_fn levels_fn, void* user, const nmlmc_checkpoint_io* io,
+                           nmlmc_mlmc_output* out, char* table, size_t table_cap);
+/* The GPU driver with checkpoints: the sampler state saved is the context's (below). */
+int nmlmc_mlmc_run_ckpt(nmlmc_ctx* ctx, const nmlmc_mlmc_input* in, const char* path, int32_t resume,
+                        nmlmc_mlmc_output* out, char* table, size_t table_cap);
+
+/* Sampler state of a context: its configuration (checked on restore), the OUTER layout's next
+ * outer-sample index per level and, on the CORE layout, every virtual core's two stream states.
+ * nmlmc_get_sampler_state writes at most `cap` bytes and reports the size needed in *size
+ * (buf may be NULL to query it). */
+int nmlmc_get_sampler_state(nmlmc_ctx* ctx, void* buf, size_t cap, size_t* size);
+int nmlmc_set_sampler_state(nmlmc_ctx* ctx, const void* buf, size_t size);
 
 #ifdef __cplusplus
 }

@@ -1242,6 +1242,84 @@ int nmlmc_sample_levels(nmlmc_ctx* c, uint32_t n, const uint32_t* ells, const ui
     return NMLMC_OK;
 }
 
+// ---- sampler state (checkpoints of the MLMC driver) --------------------------------------------
+// Blob: SamplerStateHeader, then (CORE layout) cores x 2 CoreStream records as on the device.
+namespace {
+struct SamplerStateHeader {
+    char magic[8];
+    uint32_t streams, cores;
+    uint64_t seed;
+    uint32_t N0, beta;
+    double adaptive_r;
+    int32_t precision, antithetic;
+    uint32_t shard_rank, shard_world;
+    uint64_t next_outer[NMLMC_MAX_LEVELS];
+    uint64_t core_bytes;
+};
+constexpr char kStateMagic[8] = {'N', 'M', 'L', 'M', 'C', 'S', 'S', '1'};
+}  // namespace
+
+int nmlmc_get_sampler_state(nmlmc_ctx* c, void* buf, size_t cap, size_t* size) {
+    if (!c || !size) return set_err(NMLMC_ERR_ARG);
+    if (!c->configured) return set_err(NMLMC_ERR_STATE);
+    const bool core = c->cfg.streams == NMLMC_STREAMS_CORE;
+    const uint64_t core_bytes = core ? (uint64_t)c->cfg.cores * 2 * sizeof(CoreStream) : 0;
+    *size = sizeof(SamplerStateHeader) + core_bytes;
+    if (!buf) return NMLMC_OK;
+    if (cap < *size) return set_err(NMLMC_ERR_ARG);
+    SamplerStateHeader h;
+    memset(&h, 0, sizeof h);
+    memcpy(h.magic, kStateMagic, 8);
+    h.streams = (uint32_t)c->cfg.streams;
+    h.cores = c->cfg.cores;
+    h.seed = c->cfg.seed;
+    h.N0 = c->cfg.N0;
+    h.beta = c->cfg.beta;
+    h.adaptive_r = c->cfg.adaptive_r;
+    h.precision = c->cfg.precision;
+    h.antithetic = c->cfg.antithetic;
+    h.shard_rank = c->shard_rank;
+    h.shard_world = c->shard_world;
+    memcpy(h.next_outer, c->next_outer, sizeof(h.next_outer));
+    h.core_bytes = core_bytes;
+    memcpy(buf, &h, sizeof h);
+    if (core_bytes) {
+        cudaSetDevice(c->device);
+        int rc = alloc_core(c);
+        if (rc) return rc;
+        NM_CUDA(cudaStreamSynchronize(c->stream), "sync");
+        NM_CUDA(cudaMemcpy(static_cast<char*>(buf) + sizeof h, c->d_states, core_bytes, cudaMemcpyDeviceToHost),
+                "sampler state d2h");
+    }
+    return NMLMC_OK;
+}
+
+int nmlmc_set_sampler_state(nmlmc_ctx* c, const void* buf, size_t size) {
+    if (!c || !buf || size < sizeof(SamplerStateHeader)) return set_err(NMLMC_ERR_ARG);
+    if (!c->configured) return set_err(NMLMC_ERR_STATE);
+    SamplerStateHeader h;
+    memcpy(&h, buf, sizeof h);
+    if (memcmp(h.magic, kStateMagic, 8) != 0) return set_err(NMLMC_ERR_ARG);
+    // the state belongs to the same streams: layout, cores, seed, counts and precision
+    if (h.streams != (uint32_t)c->cfg.streams || h.cores != c->cfg.cores || h.seed != c->cfg.seed ||
+        h.N0 != c->cfg.N0 || h.beta != c->cfg.beta || h.adaptive_r != c->cfg.adaptive_r ||
+        h.precision != c->cfg.precision || h.antithetic != c->cfg.antithetic ||
+        h.shard_rank != c->shard_rank || h.shard_world != c->shard_world)
+        return set_err(NMLMC_ERR_ARG);
+    const uint64_t core_bytes = c->cfg.streams == NMLMC_STREAMS_CORE ? (uint64_t)c->cfg.cores * 2 * sizeof(CoreStream) : 0;
+    if (h.core_bytes != core_bytes || size != sizeof h + core_bytes) return set_err(NMLMC_ERR_ARG);
+    memcpy(c->next_outer, h.next_outer, sizeof(c->next_outer));
+    if (core_bytes) {
+        cudaSetDevice(c->device);
+        int rc = alloc_core(c);
+        if (rc) return rc;
+        NM_CUDA(cudaStreamSynchronize(c->stream), "sync");
+        NM_CUDA(cudaMemcpy(c->d_states, static_cast<const char*>(buf) + sizeof h, core_bytes, cudaMemcpyHostToDevice),
+                "sampler state h2d");
+    }
+    return NMLMC_OK;
+}
+
 int nmlmc_set_shard(nmlmc_ctx* c, uint32_t rank, uint32_t world) {
     if (!c || world == 0 || rank >= world) return set_err(NMLMC_ERR_ARG);
     if (world > 1 && c->cfg.streams != NMLMC_STREAMS_OUTER) return set_err(NMLMC_ERR_ARG);

@@ -12,6 +12,11 @@
 // With `batched`, the missing samples of all levels in one round are requested in a single
 // submission (nmlmc_sample_levels) instead of one synchronous call per level; on the OUTER
 // stream layout the results are identical because every outer sample owns its stream.
+//
+// Checkpoints (no counterpart in the reference): after every completed TOL iteration the state
+// of the loop — the level sums in FP64, the iteration, TOL and starting level — and the
+// sampler's stream state are written to a file; a run resumed from it with the same parameters
+// continues at that iteration and ends exactly as the uninterrupted run.
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -211,8 +216,105 @@ Level from_result(const nmlmc_level_result& r) {
     return o;
 }
 
+// ---- checkpoints ---------------------------------------------------------------------------
+// Little-endian file: "NMLMCCK1", u32 version, u32 bytes of the fixed part (up to the levels),
+// the input parameters (targetTOL, startTOL, theta, starting_level_coeff, Ca: f64; M0: u64), the
+// iteration state (next iteration, total iterations, levels, starting level: u32; calls: u64;
+// TOL, bias_est, stat_error, elapsed seconds: f64), per level M (u64), the 4 + 4 FP64 sums, work
+// and time (f64), then the sampler state (u64 size + bytes).
+constexpr char kCkptMagic[8] = {'N', 'M', 'L', 'M', 'C', 'C', 'K', '1'};
+constexpr uint32_t kCkptVersion = 1;
+
+struct Checkpoint {
+    double targetTOL = 0, startTOL = 0, theta = 0, coeff = 0, Ca = 0;
+    uint64_t M0 = 0;
+    uint32_t itr_next = 0, total_itrs = 0, starting_level = 0;
+    uint64_t calls = 0;
+    double TOL = 0, bias_est = 0, stat_error = 0, elapsed = 0;
+    std::vector<Level> levels;
+    std::string sampler;
+};
+
+template <class T>
+void put(std::string& b, const T& v) { b.append(reinterpret_cast<const char*>(&v), sizeof(T)); }
+
+template <class T>
+bool get(const std::string& b, size_t& o, T& v) {
+    if (o + sizeof(T) > b.size()) return false;
+    memcpy(&v, b.data() + o, sizeof(T));
+    o += sizeof(T);
+    return true;
+}
+
+int write_checkpoint(const char* path, const Checkpoint& k) {
+    std::string b;
+    b.append(kCkptMagic, 8);
+    put(b, kCkptVersion);
+    const uint32_t fixed = 8 + 4 + 4 + 5 * 8 + 8 + 4 * 4 + 8 + 4 * 8;
+    put(b, fixed);
+    put(b, k.targetTOL); put(b, k.startTOL); put(b, k.theta); put(b, k.coeff); put(b, k.Ca); put(b, k.M0);
+    put(b, k.itr_next); put(b, k.total_itrs); put(b, (uint32_t)k.levels.size()); put(b, k.starting_level);
+    put(b, k.calls); put(b, k.TOL); put(b, k.bias_est); put(b, k.stat_error); put(b, k.elapsed);
+    for (const Level& l : k.levels) {
+        put(b, l.M);
+        for (int j = 0; j < 4; j++) put(b, l.f[j]);
+        for (int j = 0; j < 4; j++) put(b, l.d[j]);
+        put(b, l.work);
+        put(b, l.time);
+    }
+    put(b, (uint64_t)k.sampler.size());
+    b += k.sampler;
+    const std::string tmp = std::string(path) + ".tmp";
+    FILE* fp = fopen(tmp.c_str(), "wb");
+    if (!fp) return NMLMC_ERR_STATE;
+    const bool ok = fwrite(b.data(), 1, b.size(), fp) == b.size();
+    if (fclose(fp) != 0 || !ok || rename(tmp.c_str(), path) != 0) {
+        remove(tmp.c_str());
+        return NMLMC_ERR_STATE;
+    }
+    return NMLMC_OK;
+}
+
+constexpr int kNoCheckpoint = -1;
+
+// kNoCheckpoint: no file at `path`; NMLMC_ERR_ARG: not a readable checkpoint.
+int read_checkpoint(const char* path, Checkpoint& k) {
+    FILE* fp = fopen(path, "rb");
+    if (!fp) return kNoCheckpoint;
+    std::string b;
+    char chunk[1 << 16];
+    size_t n;
+    while ((n = fread(chunk, 1, sizeof chunk, fp)) > 0) b.append(chunk, n);
+    fclose(fp);
+    size_t o = 8;
+    uint32_t version = 0, fixed = 0, nlev = 0;
+    if (b.size() < 8 || memcmp(b.data(), kCkptMagic, 8) != 0) return NMLMC_ERR_ARG;
+    if (!get(b, o, version) || version != kCkptVersion || !get(b, o, fixed)) return NMLMC_ERR_ARG;
+    bool ok = get(b, o, k.targetTOL) && get(b, o, k.startTOL) && get(b, o, k.theta) && get(b, o, k.coeff) &&
+              get(b, o, k.Ca) && get(b, o, k.M0) && get(b, o, k.itr_next) && get(b, o, k.total_itrs) &&
+              get(b, o, nlev) && get(b, o, k.starting_level) && get(b, o, k.calls) && get(b, o, k.TOL) &&
+              get(b, o, k.bias_est) && get(b, o, k.stat_error) && get(b, o, k.elapsed);
+    if (!ok || o != fixed || nlev == 0 || nlev > NMLMC_MAX_LEVELS || k.starting_level >= nlev) return NMLMC_ERR_ARG;
+    k.levels.resize(nlev);
+    for (Level& l : k.levels) {
+        ok = ok && get(b, o, l.M);
+        for (int j = 0; j < 4; j++) ok = ok && get(b, o, l.f[j]);
+        for (int j = 0; j < 4; j++) ok = ok && get(b, o, l.d[j]);
+        ok = ok && get(b, o, l.work) && get(b, o, l.time);
+    }
+    uint64_t ns = 0;
+    if (!ok || !get(b, o, ns) || o + ns != b.size()) return NMLMC_ERR_ARG;
+    k.sampler.assign(b.data() + o, ns);
+    return NMLMC_OK;
+}
+
+bool same_inputs(const Checkpoint& k, const nmlmc_mlmc_input& in) {
+    return k.targetTOL == in.targetTOL && k.startTOL == in.startTOL && k.theta == in.theta &&
+           k.coeff == in.starting_level_coeff && k.Ca == in.Ca && k.M0 == in.M0;
+}
+
 int run(const nmlmc_mlmc_input& in, nmlmc_sample_level_fn level_fn, nmlmc_sample_levels_fn levels_fn,
-        void* user, nmlmc_mlmc_output* res, char* table, size_t table_cap) {
+        void* user, const nmlmc_checkpoint_io* io, nmlmc_mlmc_output* res, char* table, size_t table_cap) {
     const auto t0 = std::chrono::steady_clock::now();
     Output out;
     const double sqrt_2_inv = 1. / std::sqrt(2);
@@ -222,7 +324,50 @@ int run(const nmlmc_mlmc_input& in, nmlmc_sample_level_fn level_fn, nmlmc_sample
     out.levels.resize(1);
     std::vector<uint64_t> Ml(out.levels.size());
     uint64_t calls = 0;
-    for (uint32_t itr = 0; itr <= total_itrs; itr++) {
+    uint32_t itr0 = 0;
+    double elapsed0 = 0;
+    const bool ckpt = io && io->path;
+    if (ckpt && io->resume) {
+        Checkpoint k;
+        const int rc = read_checkpoint(io->path, k);
+        if (rc == NMLMC_ERR_ARG) return rc;
+        if (rc == NMLMC_OK) {
+            // the saved level sums come from the sampler's streams up to the saved positions: both
+            // an exact resume and a warm start continue from there
+            if (!k.sampler.empty()) {
+                if (!io->load || io->load(user, k.sampler.data(), k.sampler.size()) != NMLMC_OK) return NMLMC_ERR_STATE;
+            }
+            out.levels = k.levels;
+            out.starting_level = k.starting_level;
+            if (same_inputs(k, in) && k.total_itrs == total_itrs) {   // continue the same run
+                itr0 = k.itr_next;
+                out.TOL = k.TOL;
+                out.bias_est = k.bias_est;
+                out.stat_error = k.stat_error;
+                calls = k.calls;
+                elapsed0 = k.elapsed;
+            }
+        }
+    }
+    auto save = [&](uint32_t itr_next) -> int {
+        Checkpoint k;
+        k.targetTOL = in.targetTOL; k.startTOL = in.startTOL; k.theta = in.theta;
+        k.coeff = in.starting_level_coeff; k.Ca = in.Ca; k.M0 = in.M0;
+        k.itr_next = itr_next; k.total_itrs = total_itrs; k.starting_level = out.starting_level;
+        k.calls = calls; k.TOL = out.TOL; k.bias_est = out.bias_est; k.stat_error = out.stat_error;
+        k.elapsed = elapsed0 + std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        k.levels = out.levels;
+        if (io->save) {
+            const size_t need = io->save(user, nullptr, 0);
+            k.sampler.resize(need);
+            if (need && io->save(user, &k.sampler[0], need) != need) return NMLMC_ERR_STATE;
+        }
+        return write_checkpoint(io->path, k);
+    };
+    uint32_t done_here = 0;
+    bool complete = true;
+    uint32_t itr_end = itr0;
+    for (uint32_t itr = itr0; itr <= total_itrs; itr++) {
         out.starting_level = better_starting_level(out, in.starting_level_coeff);
         while (true) {
             optimal_Ml(in.theta * sq(out.TOL) / in.Ca, in.M0, out, Ml);
@@ -271,8 +416,17 @@ int run(const nmlmc_mlmc_input& in, nmlmc_sample_level_fn level_fn, nmlmc_sample
             break;
         }
         out.TOL *= sqrt_2_inv;
+        itr_end = itr + 1;
+        if (ckpt) {
+            const int rc = save(itr + 1);
+            if (rc) return rc;
+        }
+        if (in.max_iterations && ++done_here >= in.max_iterations && itr < total_itrs) {
+            complete = false;
+            break;
+        }
     }
-    const double total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    const double total = elapsed0 + std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (in.verbose) std::cout << "# Total time taken: " << total << " seconds." << std::endl;
     if (res) {
         memset(res, 0, sizeof(*res));
@@ -293,6 +447,8 @@ int run(const nmlmc_mlmc_input& in, nmlmc_sample_level_fn level_fn, nmlmc_sample
             res->level_time[l] = out.levels[l].time;
             res->total_work += out.levels[l].work;
         }
+        res->iterations_done = itr_end;
+        res->complete = complete ? 1u : 0u;
     }
     if (table && table_cap) {
         std::string s = to_string(out);
@@ -319,6 +475,19 @@ void gpu_levels(void* u, uint32_t n, const uint32_t* ells, const uint64_t* Ms, n
     if (rc) { g->status = rc; for (uint32_t i = 0; i < n; i++) outs[i].M = 0; }
 }
 
+size_t gpu_save_state(void* u, void* buf, size_t cap) {
+    GpuUser* g = static_cast<GpuUser*>(u);
+    size_t need = 0;
+    if (nmlmc_get_sampler_state(g->ctx, nullptr, 0, &need) != NMLMC_OK) return 0;
+    if (!buf) return need;
+    if (cap < need || nmlmc_get_sampler_state(g->ctx, buf, cap, &need) != NMLMC_OK) return 0;
+    return need;
+}
+int gpu_load_state(void* u, const void* buf, size_t size) {
+    GpuUser* g = static_cast<GpuUser*>(u);
+    return nmlmc_set_sampler_state(g->ctx, buf, size);
+}
+
 }  // namespace
 
 extern "C" {
@@ -334,6 +503,7 @@ nmlmc_mlmc_input nmlmc_mlmc_default_input(void) {
     in.verbose = 1;
     in.max_levels = 0;
     in.batched = 0;
+    in.max_iterations = 0;
     return in;
 }
 
@@ -341,7 +511,14 @@ int nmlmc_mlmc_run_cb(const nmlmc_mlmc_input* in, nmlmc_sample_level_fn level_fn
                       nmlmc_sample_levels_fn levels_fn, void* user, nmlmc_mlmc_output* out,
                       char* table, size_t table_cap) {
     if (!in || !level_fn || !(in->targetTOL > 0) || !(in->startTOL >= in->targetTOL)) return NMLMC_ERR_ARG;
-    return run(*in, level_fn, levels_fn, user, out, table, table_cap);
+    return run(*in, level_fn, levels_fn, user, nullptr, out, table, table_cap);
+}
+
+int nmlmc_mlmc_run_cb_ckpt(const nmlmc_mlmc_input* in, nmlmc_sample_level_fn level_fn,
+                           nmlmc_sample_levels_fn levels_fn, void* user, const nmlmc_checkpoint_io* io,
+                           nmlmc_mlmc_output* out, char* table, size_t table_cap) {
+    if (!in || !level_fn || !(in->targetTOL > 0) || !(in->startTOL >= in->targetTOL)) return NMLMC_ERR_ARG;
+    return run(*in, level_fn, levels_fn, user, io, out, table, table_cap);
 }
 
 int nmlmc_mlmc_run(nmlmc_ctx* ctx, const nmlmc_mlmc_input* in, nmlmc_mlmc_output* out, char* table,
@@ -349,6 +526,15 @@ int nmlmc_mlmc_run(nmlmc_ctx* ctx, const nmlmc_mlmc_input* in, nmlmc_mlmc_output
     if (!ctx || !in) return NMLMC_ERR_ARG;
     GpuUser u{ctx, NMLMC_OK};
     int rc = nmlmc_mlmc_run_cb(in, gpu_level, gpu_levels, &u, out, table, table_cap);
+    return u.status ? u.status : rc;
+}
+
+int nmlmc_mlmc_run_ckpt(nmlmc_ctx* ctx, const nmlmc_mlmc_input* in, const char* path, int32_t resume,
+                        nmlmc_mlmc_output* out, char* table, size_t table_cap) {
+    if (!ctx || !in || !path) return NMLMC_ERR_ARG;
+    GpuUser u{ctx, NMLMC_OK};
+    nmlmc_checkpoint_io io{path, resume, gpu_save_state, gpu_load_state};
+    int rc = nmlmc_mlmc_run_cb_ckpt(in, gpu_level, gpu_levels, &u, &io, out, table, table_cap);
     return u.status ? u.status : rc;
 }
 

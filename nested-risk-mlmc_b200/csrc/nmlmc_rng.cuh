@@ -123,8 +123,8 @@ __device__ __forceinline__ void boxmuller32_f(uint32_t u0, uint32_t u1, float& x
     p = fmaf(q, p, 0.5f);
     p = fmaf(q, p, 1.0f);
     float t_ser = 2.0f * q * p;
-    float t = (q < 0.015625f) ? t_ser : t_log;   // -2 ln u  (>= 0)
-    float r = t * rsqrtf(fmaxf(t, 1e-30f));
+    float t = (q < 0.015625f) ? t_ser : t_log;   // -2 ln u > 0: t_ser >= 2q >= 2^-32, t_log > 0.03
+    float r = t * rsqrtf(t);
     x = s * r;
     y = c * r;
 }

@@ -151,7 +151,8 @@ class MlmcInput(ctypes.Structure):
     _fields_ = [("targetTOL", ctypes.c_double), ("startTOL", ctypes.c_double),
                 ("theta", ctypes.c_double), ("starting_level_coeff", ctypes.c_double),
                 ("Ca", ctypes.c_double), ("M0", ctypes.c_uint64), ("verbose", ctypes.c_int32),
-                ("max_levels", ctypes.c_uint32), ("batched", ctypes.c_int32)]
+                ("max_levels", ctypes.c_uint32), ("batched", ctypes.c_int32),
+                ("max_iterations", ctypes.c_uint32)]
 
 
 class MlmcOutput(ctypes.Structure):
@@ -164,7 +165,8 @@ class MlmcOutput(ctypes.Structure):
                 ("level_fsums", (ctypes.c_double * 4) * MAX_LEVELS),
                 ("level_diffsums", (ctypes.c_double * 4) * MAX_LEVELS),
                 ("level_work", ctypes.c_double * MAX_LEVELS),
-                ("level_time", ctypes.c_double * MAX_LEVELS)]
+                ("level_time", ctypes.c_double * MAX_LEVELS),
+                ("iterations_done", ctypes.c_uint32), ("complete", ctypes.c_uint32)]
 
 
 class PortfolioSpec(ctypes.Structure):
@@ -193,6 +195,14 @@ PHASE_DEFAULT, PHASE_TUNED, PHASE_PINNED = 0, 1, 2
 
 SAMPLE_LEVEL_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64,
                                    ctypes.POINTER(LevelResult))
+STATE_SAVE_FN = ctypes.CFUNCTYPE(ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t)
+STATE_LOAD_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t)
+
+
+class CheckpointIO(ctypes.Structure):
+    """nmlmc_checkpoint_io: checkpoint file of the MLMC driver and the sampler-state hooks."""
+    _fields_ = [("path", ctypes.c_char_p), ("resume", ctypes.c_int32), ("save", STATE_SAVE_FN),
+                ("load", STATE_LOAD_FN)]
 SAMPLE_LEVELS_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint32, _u32p, _u64p,
                                     ctypes.POINTER(LevelResult))
 
@@ -212,7 +222,8 @@ EXPORTS = [
     "nmlmc_set_profiling", "nmlmc_phase_kernel_time", "nmlmc_kernel_launches",
     "nmlmc_sample_level_noalloc", "nmlmc_portfolio_generate", "nmlmc_set_portfolio_methods",
     "nmlmc_path_adjoint", "nmlmc_graph_stats", "nmlmc_set_autotune", "nmlmc_get_phase_config",
-    "nmlmc_set_phase_config", "nmlmc_autotune_level",
+    "nmlmc_set_phase_config", "nmlmc_autotune_level", "nmlmc_mlmc_run_cb_ckpt", "nmlmc_mlmc_run_ckpt",
+    "nmlmc_get_sampler_state", "nmlmc_set_sampler_state",
 ]
 
 
@@ -248,6 +259,15 @@ def lib() -> ctypes.CDLL:
     L.nmlmc_mlmc_run_cb.argtypes = [ctypes.POINTER(MlmcInput), SAMPLE_LEVEL_FN, SAMPLE_LEVELS_FN,
                                     ctypes.c_void_p, ctypes.POINTER(MlmcOutput), ctypes.c_char_p,
                                     ctypes.c_size_t]
+    L.nmlmc_mlmc_run_cb_ckpt.argtypes = [ctypes.POINTER(MlmcInput), SAMPLE_LEVEL_FN, SAMPLE_LEVELS_FN,
+                                         ctypes.c_void_p, ctypes.POINTER(CheckpointIO),
+                                         ctypes.POINTER(MlmcOutput), ctypes.c_char_p, ctypes.c_size_t]
+    L.nmlmc_mlmc_run_ckpt.argtypes = [ctypes.c_void_p, ctypes.POINTER(MlmcInput), ctypes.c_char_p,
+                                      ctypes.c_int32, ctypes.POINTER(MlmcOutput), ctypes.c_char_p,
+                                      ctypes.c_size_t]
+    L.nmlmc_get_sampler_state.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                          ctypes.POINTER(ctypes.c_size_t)]
+    L.nmlmc_set_sampler_state.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]
     L.nmlmc_portfolio_generate.argtypes = [ctypes.POINTER(PortfolioSpec), ctypes.c_uint64, _dp, _dp, _dp,
                                            _dp, _dp, _dp, _u32p, _i32p]
     L.nmlmc_set_shard.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32]
@@ -473,7 +493,10 @@ class Sampler:
         return out
 
     def mlmc_run(self, targetTOL=1e-3, M0=100, verbose=False, batched=False, max_levels=0,
-                 **kw) -> dict:
+                 checkpoint=None, resume=False, **kw) -> dict:
+        """Continuation MLMC to targetTOL.  With `checkpoint` (a path) the driver writes its state
+        after every TOL iteration; `resume` continues from that file (max_iterations=k in kw
+        stops after k iterations)."""
         inp = self.L.nmlmc_mlmc_default_input()
         inp.targetTOL, inp.M0, inp.verbose = targetTOL, M0, int(verbose)
         inp.batched, inp.max_levels = int(batched), max_levels
@@ -481,9 +504,24 @@ class Sampler:
             setattr(inp, k, v)
         out = MlmcOutput()
         buf = ctypes.create_string_buffer(1 << 16)
-        _check(self.L.nmlmc_mlmc_run(self.h, ctypes.byref(inp), ctypes.byref(out), buf, len(buf)),
-               "nmlmc_mlmc_run")
+        if checkpoint is None:
+            _check(self.L.nmlmc_mlmc_run(self.h, ctypes.byref(inp), ctypes.byref(out), buf, len(buf)),
+                   "nmlmc_mlmc_run")
+        else:
+            _check(self.L.nmlmc_mlmc_run_ckpt(self.h, ctypes.byref(inp), os.fsencode(checkpoint), int(resume),
+                                              ctypes.byref(out), buf, len(buf)), "nmlmc_mlmc_run_ckpt")
         return mlmc_output_dict(out, buf.value.decode())
+
+    def sampler_state(self) -> bytes:
+        """The context's stream state (nmlmc_get_sampler_state)."""
+        n = ctypes.c_size_t()
+        _check(self.L.nmlmc_get_sampler_state(self.h, None, 0, ctypes.byref(n)), "nmlmc_get_sampler_state")
+        b = ctypes.create_string_buffer(n.value)
+        _check(self.L.nmlmc_get_sampler_state(self.h, b, n.value, ctypes.byref(n)), "nmlmc_get_sampler_state")
+        return b.raw[:n.value]
+
+    def set_sampler_state(self, state: bytes):
+        _check(self.L.nmlmc_set_sampler_state(self.h, state, len(state)), "nmlmc_set_sampler_state")
 
 
 def mlmc_output_dict(out: MlmcOutput, table: str) -> dict:
@@ -495,13 +533,16 @@ def mlmc_output_dict(out: MlmcOutput, table: str) -> dict:
                 level_fsums=np.array([out.level_fsums[i][:] for i in range(n)]),
                 level_diffsums=np.array([out.level_diffsums[i][:] for i in range(n)]),
                 level_work=np.array(out.level_work[:n]), level_time=np.array(out.level_time[:n]),
-                table=table)
+                iterations_done=out.iterations_done, complete=bool(out.complete), table=table)
 
 
 def mlmc_run_cb(sample_level, sample_levels=None, *, targetTOL=1e-3, M0=100, verbose=False,
-                batched=False, **kw) -> dict:
+                batched=False, checkpoint=None, resume=False, state=None, **kw) -> dict:
     """The host MLMC driver over a Python level sampler: sample_level(ell, M) -> dict with
-    fsums, diffsums, work (and optionally seconds)."""
+    fsums, diffsums, work (and optionally seconds).  A sampler that fails leaves the result's M
+    at 0 and the driver stops with an error.  With `checkpoint` (a path) the driver writes its
+    state after every TOL iteration, `resume` continues from it, and `state` = (save, load)
+    stores the sampler's own state in the file: save() -> bytes, load(bytes)."""
     L = lib()
 
     def fill(res, d, M):
@@ -513,11 +554,18 @@ def mlmc_run_cb(sample_level, sample_levels=None, *, targetTOL=1e-3, M0=100, ver
         res.seconds = float(d.get("seconds", 0.0))
 
     def _one(user, ell, M, out):
-        fill(out.contents, sample_level(int(ell), int(M)), int(M))
+        try:
+            fill(out.contents, sample_level(int(ell), int(M)), int(M))
+        except Exception:          # a failed sampler: M stays 0 and the driver stops
+            out.contents.M = 0
 
     def _many(user, n, ells, Ms, outs):
-        for i in range(n):
-            fill(outs[i], sample_levels_or_one(int(ells[i]), int(Ms[i])), int(Ms[i]))
+        try:
+            for i in range(n):
+                fill(outs[i], sample_levels_or_one(int(ells[i]), int(Ms[i])), int(Ms[i]))
+        except Exception:
+            for i in range(n):
+                outs[i].M = 0
 
     def sample_levels_or_one(ell, M):
         return sample_level(ell, M)
@@ -530,8 +578,31 @@ def mlmc_run_cb(sample_level, sample_levels=None, *, targetTOL=1e-3, M0=100, ver
         setattr(inp, k, v)
     out = MlmcOutput()
     buf = ctypes.create_string_buffer(1 << 16)
-    _check(L.nmlmc_mlmc_run_cb(ctypes.byref(inp), f1, f2, None, ctypes.byref(out), buf, len(buf)),
-           "nmlmc_mlmc_run_cb")
+    if checkpoint is None:
+        _check(L.nmlmc_mlmc_run_cb(ctypes.byref(inp), f1, f2, None, ctypes.byref(out), buf, len(buf)),
+               "nmlmc_mlmc_run_cb")
+        return mlmc_output_dict(out, buf.value.decode())
+
+    def _save(user, p, cap):
+        b = state[0]()
+        if p:
+            if cap < len(b):
+                return 0
+            ctypes.memmove(p, b, len(b))
+        return len(b)
+
+    def _load(user, p, n):
+        try:
+            state[1](ctypes.string_at(p, n))
+            return OK
+        except Exception:
+            return ERR_STATE
+
+    fs = STATE_SAVE_FN(_save) if state else STATE_SAVE_FN()
+    fl = STATE_LOAD_FN(_load) if state else STATE_LOAD_FN()
+    io = CheckpointIO(os.fsencode(checkpoint), int(resume), fs, fl)
+    _check(L.nmlmc_mlmc_run_cb_ckpt(ctypes.byref(inp), f1, f2, None, ctypes.byref(io), ctypes.byref(out),
+                                    buf, len(buf)), "nmlmc_mlmc_run_cb_ckpt")
     return mlmc_output_dict(out, buf.value.decode())
 
 
@@ -692,3 +763,6 @@ def make_batch(portfolios: list, K, r: float = 0.05, rho: float = 0.0, tau: floa
     out.update(stock_off=np.array(so, np.uint32), option_off=np.array(oo, np.uint32),
                K=np.asarray(K, np.float64).reshape(-1), r=r, rho=rho, tau=tau)
     return out
+
+
+from . import checkpoint, tables  # noqa: E402  (file readers: checkpoints, printed reports)
