@@ -283,7 +283,7 @@ int nmlmc_sample_levels(nmlmc_ctx* ctx, uint32_t n, const uint32_t* ells, const 
 /* ---- phase-kernel autotuner (batched FP32 path) ----------------------------------------------
  * No counterpart in the reference (its CUDA build has one fixed launch shape).  The phase kernel
  * of the OUTER layout has three register/occupancy variants (0: up to 255 registers per thread,
- * 1: two resident CTAs of 256 threads per SM guaranteed, 2: four) and a chunk length (inner
+ * 1: three resident CTAs of 256 threads per SM guaranteed, 2: four) and a chunk length (inner
  * samples per thread; power of two in [4, 64] dividing N0; a level's items of n inner samples
  * take n / chunk threads, so it also sets the outer samples per warp).  With autotuning on, the
  * first nmlmc_sample / nmlmc_sample_levels call of a level with enough work times the

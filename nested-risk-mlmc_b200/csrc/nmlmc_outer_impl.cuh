@@ -426,7 +426,7 @@ __device__ __forceinline__ void final_item(const DevLevel<RT>& D, uint32_t item,
 // Block partial sums (OuterBuffers::block_sums layout): [0..3] phi_f moments, [4..7] difference
 // moments, [8] work, [9] inner samples, [10] hit the maximum count, [11] stayed at the base count.
 // MINB = CTAs per SM the register allocation must allow (1: up to 255 registers per thread,
-// 2: 128, 4: 64) — the register/occupancy variants the autotuner chooses between.  The variants
+// 3: 80, 4: 64) — the register/occupancy variants the autotuner chooses between.  The variants
 // run the same arithmetic in the same order, so their results are identical.
 template <class RT, int KIND, int PREC, int MINB>
 __global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet S, TraceRec* trace) {
@@ -790,12 +790,12 @@ static void launch_phase_v(const DevLevel<RT>& D, const SegSet& S, TraceRec* tra
     count_launch();
 }
 
-// The FP32 path has three register/occupancy variants (OuterLevel::variant 0, 1, 2 -> 1, 2, 4
+// The FP32 path has three register/occupancy variants (OuterLevel::variant 0, 1, 2 -> 1, 3, 4
 // resident CTAs per SM guaranteed); the parity precisions run variant 0.
 template <class RT, int KIND, int PREC>
 static void launch_phase(const DevLevel<RT>& D, const SegSet& S, TraceRec* trace, cudaStream_t stream) {
     if constexpr (PREC == PREC_FP32) {
-        if (D.L.variant == 1) return launch_phase_v<RT, KIND, PREC, 2>(D, S, trace, stream);
+        if (D.L.variant == 1) return launch_phase_v<RT, KIND, PREC, 3>(D, S, trace, stream);
         if (D.L.variant == 2) return launch_phase_v<RT, KIND, PREC, 4>(D, S, trace, stream);
     }
     launch_phase_v<RT, KIND, PREC, 1>(D, S, trace, stream);
