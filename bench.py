@@ -351,6 +351,31 @@ def dropin_extrapolated(s, level_M, budget_s=60.0):
                        " outer samples] x the level counts of the FP32 run")
 
 
+def c3_table_case():
+    """Profiling case: the large-portfolio phase kernel with option tables of 1e6, 1e4, 1e3 and
+    100 options (generator seed 1, d = 200, prob ~ |w|), importance and uniform sub-sampling,
+    non-adaptive level 6 (4096 inner samples per outer sample) on 2^14 outer samples: how much of
+    the time the table's memory latency takes."""
+    import numpy as np
+    sys.path.insert(0, PKG)
+    import nmlmc as nm
+    for P in (1_000_000, 10_000, 1_000, 100):
+        pf = nm.generate_portfolio(dict(nm.PORTFOLIO_C3, P=P), 1)
+        order = np.argsort(-np.abs(pf["w"]), kind="stable")
+        for k in ("strike", "maturity", "w", "stock_ind", "type"):
+            pf[k] = pf[k][order]
+        pf = dict(pf, prob=np.abs(pf["w"]))
+        for sub, name in ((nm.SUB_RANDOM, "importance"), (nm.SUB_UNIFORM, "uniform")):
+            s = nm.Sampler(0, N0=64, beta=2, adaptive_r=0.0, precision=nm.PREC_FP32,
+                           streams=nm.STREAMS_OUTER, seed=5)
+            s.set_portfolio(pf, r=0.05, rho=0.0, max_loss=4726.3, tau=nm.TAU_WEEK, subsample=sub,
+                            use_delta_cv=True, discount=False)
+            s.set_autotune(0)
+            for _ in range(3):
+                r = s.sample(6, 1 << 14)
+            print(f"P {P} {name}: {r['seconds'] * 1e3:.3f} ms, {r['stats'][0] / r['seconds']:.3e} inner/s")
+
+
 def c3_case(args):
     """Large portfolio: d = 200 stocks, P = 1e6 options (generator seed 1), K = the 99 % quantile
     of the full loss over 1e5 outer samples; P(L > K) by continuation MLMC with the reference's
@@ -436,7 +461,7 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison runs")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--eps", type=float, default=None, help="--case c3: target RMSE (default 1e-3)")
-    ap.add_argument("--case", default=None, choices=["small", "c3", "c3-level", "c4", "c4-small"],
+    ap.add_argument("--case", default=None, choices=["small", "c3", "c3-level", "c3-table", "c4", "c4-small"],
                     help="small: a few fixed level calls of the FP32 sampler (profiling case); "
                          "c4: the path-simulated loss with adjoint; c4-small: its profiling case")
     args = ap.parse_args()
@@ -448,6 +473,8 @@ def main():
         return c3_case(args)
     if args.case == "c3-level":
         return c3_level_case()
+    if args.case == "c3-table":
+        return c3_table_case()
     if args.case in ("c4", "c4-small"):
         return c4_case(args, small=args.case == "c4-small")
 

@@ -336,6 +336,8 @@ int nmlmc_threefry_blocks(const uint64_t* ctr, const uint64_t* key, uint64_t* ou
  * computed on the GPU at `precision` (NMLMC_PREC_FP64 or NMLMC_PREC_FP32), widened to double. */
 int nmlmc_outer_normals(int32_t precision, uint64_t seed, uint64_t stream, uint32_t tag, uint64_t n,
                         double* out);
+/* Phi(x) of the FP32 Black-Scholes path (rational erfc on the SFU) at n points (host buffers). */
+int nmlmc_norm_cdf_fast(const float* x, float* out, uint64_t n);
 
 /* ---- allocation-free level call ------------------------------------------------------------
  * No counterpart in the reference.  For callers that may not allocate device memory: code that

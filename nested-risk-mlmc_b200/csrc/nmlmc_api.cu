@@ -1449,6 +1449,18 @@ int nmlmc_outer_normals(int32_t precision, uint64_t seed, uint64_t stream, uint3
     return cuda_status(e, "outer normals");
 }
 
+int nmlmc_norm_cdf_fast(const float* x, float* out, uint64_t n) {
+    if (!x || !out) return set_err(NMLMC_ERR_ARG);
+    if (n == 0) return NMLMC_OK;
+    float* d = nullptr;
+    if (cudaMalloc(&d, 2 * n * sizeof(float)) != cudaSuccess) return set_err(NMLMC_ERR_NOMEM);
+    cudaError_t e = cudaMemcpy(d, x, n * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = launch_norm_cdf_fast(d, d + n, n, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(out, d + n, n * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return cuda_status(e, "norm_cdf_fast");
+}
+
 // ---- reference-named surface (one process-wide sampler, like g_p_nestedmc_data) --------------
 static nmlmc_ctx* g_ctx = nullptr;
 static int32_t g_default_prec = NMLMC_PREC_REF32, g_default_streams = NMLMC_STREAMS_CORE;

@@ -14,8 +14,10 @@
 // Phi(x) = erfc(-x/sqrt 2) / 2 with the rational-Chebyshev erfc of Numerical Recipes in C
 // (2nd ed., §6.2, "erfcc": fractional error below 1.2e-7 for all arguments), its exponential and
 // reciprocal on MUFU (__expf, __frcp_rn).  Measured against double erfc over |x| <= 10 the
-// composite Phi has relative error <= 4e-7 (tests/test_gpu_portfolio.py); the loss of one option
-// is then within 1e-6 * (|wV0| + |wR R| + |wK|) of the double-precision value.
+// composite Phi has absolute error <= 1.8e-7 and, where Phi >= 1e-20, relative error <= 8e-6: in
+// the far tail the FP32 rounding of the exponent -z^2 (up to ~43) dominates, not the erfc fit
+// (tests/test_gpu_portfolio.py, bounds 2.5e-7 and 1e-5).  The loss of one option is then within
+// 1e-6 * (|wV0| + |wR R| + |wK|) of the double-precision value.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>

@@ -112,6 +112,7 @@ cudaError_t launch_adjoint(const AdjLaunch<double>& A, bool grad, cudaStream_t s
 
 cudaError_t launch_threefry_blocks(const uint64_t* ctr, const uint64_t* key, uint64_t* out, uint64_t n,
                                    cudaStream_t s);
+cudaError_t launch_norm_cdf_fast(const float* x, float* out, uint64_t n, cudaStream_t s);
 cudaError_t launch_outer_normals(int prec, uint64_t seed, uint64_t stream, uint32_t tag, uint64_t n,
                                  double* out, cudaStream_t s);
 

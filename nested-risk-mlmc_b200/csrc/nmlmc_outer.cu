@@ -221,6 +221,17 @@ cudaError_t launch_threefry_blocks(const uint64_t* ctr, const uint64_t* key, uin
     return cudaGetLastError();
 }
 
+// Phi(x) of the FP32 Black-Scholes path (norm_cdf_fast, nmlmc_bs.cuh) on n points.
+__global__ void k_norm_cdf_fast(const float* x, float* out, uint64_t n) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = norm_cdf_fast(x[i]);
+}
+
+cudaError_t launch_norm_cdf_fast(const float* x, float* out, uint64_t n, cudaStream_t s) {
+    k_norm_cdf_fast<<<256, 256, 0, s>>>(x, out, n);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_outer_normals(int prec, uint64_t seed, uint64_t stream, uint32_t tag, uint64_t n,
                                  double* out, cudaStream_t s) {
     if (prec == PREC_FP32) k_outer_normals<PREC_FP32><<<256, 256, 0, s>>>(seed, stream, tag, n, out);

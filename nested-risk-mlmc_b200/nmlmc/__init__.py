@@ -223,7 +223,7 @@ EXPORTS = [
     "nmlmc_sample_level_noalloc", "nmlmc_portfolio_generate", "nmlmc_set_portfolio_methods",
     "nmlmc_path_adjoint", "nmlmc_graph_stats", "nmlmc_set_autotune", "nmlmc_get_phase_config",
     "nmlmc_set_phase_config", "nmlmc_autotune_level", "nmlmc_mlmc_run_cb_ckpt", "nmlmc_mlmc_run_ckpt",
-    "nmlmc_get_sampler_state", "nmlmc_set_sampler_state",
+    "nmlmc_get_sampler_state", "nmlmc_set_sampler_state", "nmlmc_norm_cdf_fast",
 ]
 
 
@@ -284,6 +284,8 @@ def lib() -> ctypes.CDLL:
                                              ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64,
                                              ctypes.c_void_p, ctypes.c_void_p]
     L.nmlmc_threefry_blocks.argtypes = [_u64p, _u64p, _u64p, ctypes.c_uint64]
+    L.nmlmc_norm_cdf_fast.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                                      ctypes.c_uint64]
     L.nmlmc_outer_normals.argtypes = [ctypes.c_int32, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32,
                                       ctypes.c_uint64, _dp]
     # reference surface
@@ -604,6 +606,15 @@ def mlmc_run_cb(sample_level, sample_levels=None, *, targetTOL=1e-3, M0=100, ver
     _check(L.nmlmc_mlmc_run_cb_ckpt(ctypes.byref(inp), f1, f2, None, ctypes.byref(io), ctypes.byref(out),
                                     buf, len(buf)), "nmlmc_mlmc_run_cb_ckpt")
     return mlmc_output_dict(out, buf.value.decode())
+
+
+def norm_cdf_fast(x) -> np.ndarray:
+    """Phi(x) as the FP32 Black-Scholes path computes it on the GPU (float32 in and out)."""
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.empty_like(x)
+    fp = ctypes.POINTER(ctypes.c_float)
+    _check(lib().nmlmc_norm_cdf_fast(x.ctypes.data_as(fp), out.ctypes.data_as(fp), x.size), "nmlmc_norm_cdf_fast")
+    return out
 
 
 def generate_portfolio(spec: dict, seed: int) -> dict:

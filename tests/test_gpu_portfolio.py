@@ -32,6 +32,21 @@ def sampler(nm, prec, pf, seed=0, **kw):
     return s
 
 
+def test_fast_norm_cdf_bound(nm):
+    """Phi of the FP32 Black-Scholes (rational erfc, SFU exponential and reciprocal) against the
+    double-precision Phi over |x| <= 10: absolute error <= 2.5e-7; relative error <= 1e-5 where
+    Phi >= 1e-20 (measured 1.8e-7 and 8e-6; the FP32 exponent -z^2 limits the far tail)."""
+    from math import erfc, sqrt
+    x = np.concatenate([np.linspace(-10, 10, 200001), np.random.default_rng(1).uniform(-10, 10, 100000)])
+    x = x.astype(np.float32)
+    got = nm.norm_cdf_fast(x).astype(np.float64)
+    ref = np.array([0.5 * erfc(-float(v) / sqrt(2.0)) for v in x])
+    assert np.max(np.abs(got - ref)) <= 2.5e-7
+    m = ref >= 1e-20
+    rel = np.abs(got[m] - ref[m]) / ref[m]
+    assert rel.max() <= 1e-5, (rel.max(), x[m][np.argmax(rel)])
+
+
 def test_generator_deterministic(nm):
     a = nm.generate_portfolio(nm.PORTFOLIO_C2, 7)
     b = nm.generate_portfolio(nm.PORTFOLIO_C2, 7)
