@@ -55,6 +55,13 @@ WORKLOAD = dict(workload="model problem X=Y+Z, K=1, adaptive inner sampling, lev
 #   Box-Muller pair ~ 22 FP32/ALU + 4 SFU ops shared by 2 normals -> 13;
 #   X = Y + Z (1) and a Kahan update of the inner sum (4) -> 5.
 OPS_PER_INNER = 35 + 13 + 5
+# Algorithmic lane operations per inner sample of the large portfolio on the FP32 path:
+#   half a Threefry2x64-20 block (70); the option draw: column floor(vP/2^64), coin, alias
+#   compare and select (5); the Black-Scholes loss: ln R (2), call/put sign (1), d1 and d2 (3),
+#   two Phi = rational erfc (|x| scale 2, reciprocal 1, 10 FMA, exponential 2, product and
+#   half 2, reflection 2: 19 each), the position-weighted value (4), delta control variate (2);
+#   Kahan update (4).
+C3_OPS_PER_INNER = 70 + 5 + (2 + 1 + 3 + 2 * 19 + 4 + 2) + 4
 
 
 def exact_p():
@@ -148,6 +155,28 @@ def run_once(nm, s, batched, dist=None):
     t0 = time.perf_counter()
     out = sharded_mlmc_run(s, device=dev, targetTOL=EPS, M0=WORKLOAD["M0"])
     return out, time.perf_counter() - t0
+
+
+def per_level_error(nm, device, nlevels, M=1 << 16):
+    """Each level's FP32 estimate against the all-FP64 one on the same OUTER streams (M outer
+    samples): mean of phi_f and of phi_f - phi_c, the outer samples whose phi differs, and the
+    largest |inner mean - K| among them (the FP32 flip bound is 2e-5)."""
+    import numpy as np
+    out = []
+    for ell in range(nlevels):
+        a = make_sampler(nm, device, nm.PREC_FP32, nm.STREAMS_OUTER, seed=11)
+        b = make_sampler(nm, device, nm.PREC_FP64, nm.STREAMS_OUTER, seed=11)
+        a.set_autotune(0)
+        ra, rb = a.sample(ell, M, trace=True), b.sample(ell, M, trace=True)
+        ta, tb = ra["trace"], rb["trace"]
+        flip = (ta["phi_f"] != tb["phi_f"]) | (ta["phi_c"] != tb["phi_c"])
+        out.append({"level": ell, "M": M,
+                    "fEl_fp32_minus_fp64": (ra["fsums"][0] - rb["fsums"][0]) / M,
+                    "dEl_fp32_minus_fp64": (ra["diffsums"][0] - rb["diffsums"][0]) / M,
+                    "phi_flips": int(flip.sum()),
+                    "max_abs_mean_at_flip": (max(abs(float(x)) for x in np.minimum(
+                        np.abs(tb["mean_big"][flip]), tb["min_abs_small"][flip])) if flip.any() else None)})
+    return out
 
 
 # ---------------------------------------------------------------------------------------------
@@ -351,6 +380,22 @@ def dropin_extrapolated(s, level_M, budget_s=60.0):
                        " outer samples] x the level counts of the FP32 run")
 
 
+def c3_sweep_case():
+    """Profiling case of the full-portfolio loss sweep (the K-quantile precompute): the large
+    portfolio (d = 200, P = 1e6 packed FP32 records), L(Y) for 8192 outer samples, twice."""
+    sys.path.insert(0, PKG)
+    import nmlmc as nm
+    s = nm.Sampler(0, N0=64, beta=2, precision=nm.PREC_FP32, streams=nm.STREAMS_OUTER, seed=1)
+    s.set_portfolio(c3_portfolio(nm), r=0.05, rho=0.0, max_loss=0.0, tau=nm.TAU_WEEK,
+                    subsample=nm.SUB_RANDOM, use_delta_cv=True, discount=False)
+    for _ in range(2):
+        t = time.perf_counter()
+        L = s.full_loss(62, 0, 8192)
+        dt = time.perf_counter() - t
+        print(f"sweep 8192 x 1e6 options: {dt * 1e3:.3f} ms (wall), {8192 * 1e6 / dt:.3e} evaluations/s, "
+              f"mean loss {L.mean():.3f}")
+
+
 def c3_table_case():
     """Profiling case: the large-portfolio phase kernel with option tables of 1e6, 1e4, 1e3 and
     100 options (generator seed 1, d = 200, prob ~ |w|), importance and uniform sub-sampling,
@@ -399,7 +444,16 @@ def c3_case(args):
 
     q = mk(nm.PREC_FP32, nm.STREAMS_OUTER, 0.0, seed=1)
     K = nm.loss_quantile(q, 0.99, 100_000)
+    t = time.perf_counter()
     Ld = q.full_loss(62, 0, 200_000)
+    t_sweep = time.perf_counter() - t
+    # the full-loss sweep streams the packed 32-byte records once per tile of 32 outer samples
+    P = len(pfw["w"])
+    sweep = {"outer_samples": len(Ld), "options": P, "seconds": t_sweep,
+             "option_evaluations_per_s": len(Ld) * P / t_sweep,
+             "table_bytes_per_s": P * 32 * -(-len(Ld) // 32) / t_sweep,
+             "note": "wall time of nmlmc_portfolio_full_loss (outer draws, sweep, 1.6 MB copy back); "
+                     "the 32 MB table is L2-resident, so the sweep streams it from L2"}
     p_direct = float(np.mean(Ld > K))
     sd = float(np.sqrt(p_direct * (1 - p_direct) / len(Ld)))
     # warm-up of the FP32 sampler on another seed (module load, graph instantiation,
@@ -432,6 +486,26 @@ def c3_case(args):
         if prec == nm.PREC_FP32:
             runs[name]["phase_config"] = phase_choices(s, int(out["nlevels"]))
     clk = cs.stop()
+    # phase-kernel roofline: CUDA events around every phase-kernel launch while the FP32 sampler
+    # repeats one call per active level of its run (at most 8192 outer samples each)
+    a = runs["fp32_batched"]
+    s32.set_profiling(True)
+    inner = 0.0
+    for ell, M in enumerate(a["level_M"]):
+        if ell >= a["starting_level"] and M > 0:
+            inner += float(s32.sample(ell, min(M, 8192))["stats"][0])
+    n_phase, t_phase = s32.phase_kernel_time()
+    s32.set_profiling(False)
+    sm_mhz = clk.get("sm_mhz") or 1965.0
+    peak = 148 * 128 * sm_mhz * 1e6 / 1e12
+    ach = inner * C3_OPS_PER_INNER / t_phase / 1e12
+    roof = {"bound": "alu", "achieved": ach, "peak": peak, "unit": "Tops/s", "frac": ach / peak,
+            "traffic": None, "kernel": "k_phase (FP32, portfolio)", "launches": n_phase,
+            "kernel_seconds": t_phase, "inner_samples": inner, "ops_per_inner_sample": C3_OPS_PER_INNER,
+            "peak_source": "issue-slot peak 148 SM x 128 lanes x sampled SM clock",
+            "timing": "CUDA events around each phase-kernel launch of one call per active level "
+                      "(<= 8192 outer samples) after the timed runs",
+            "note": "latency-bound: dependent option-table gathers and the per-sample arithmetic chain"}
     a, b = runs["fp32_batched"], runs["fp64_dropin"]
     line = {"metric": f"time-to-eps (s) for MLMC P(L>K), large portfolio, eps={eps:g} absolute",
             "value": a["value"], "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 1,
@@ -446,6 +520,7 @@ def c3_case(args):
             "runs": runs, "p_direct": p_direct, "p_direct_sd": sd,
             "speedup_vs_fp64_dropin": {"value": b["value"] / a["value"],
                                        "e2e": (b["e2e"] / a["e2e"]) if b.get("e2e") else None},
+            "roofline": roof, "full_loss_sweep": sweep,
             "clocks": clk}
     print(json.dumps(line))
 
@@ -461,7 +536,8 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison runs")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--eps", type=float, default=None, help="--case c3: target RMSE (default 1e-3)")
-    ap.add_argument("--case", default=None, choices=["small", "c3", "c3-level", "c3-table", "c4", "c4-small"],
+    ap.add_argument("--case", default=None, choices=["small", "c3", "c3-level", "c3-table", "c3-sweep", "c4",
+                                                      "c4-small"],
                     help="small: a few fixed level calls of the FP32 sampler (profiling case); "
                          "c4: the path-simulated loss with adjoint; c4-small: its profiling case")
     args = ap.parse_args()
@@ -475,6 +551,8 @@ def main():
         return c3_level_case()
     if args.case == "c3-table":
         return c3_table_case()
+    if args.case == "c3-sweep":
+        return c3_sweep_case()
     if args.case in ("c4", "c4-small"):
         return c4_case(args, small=args.case == "c4-small")
 
@@ -505,7 +583,6 @@ def main():
 
     clocks = ClockSampler(local)
     clocks.start()
-    s.set_profiling(True)
     launches0 = nm.kernel_launches()
     barrier()
     dev_times, walls, outs = [], [], []
@@ -519,9 +596,18 @@ def main():
     barrier()
     region = time.perf_counter() - t_region
     launches = nm.kernel_launches() - launches0
+    clk = clocks.stop()
+    # The phase kernel's own time: a profiled repeat of the timed runs (same seeds) with CUDA
+    # events around every phase-kernel launch; profiling submits the levels one call at a time
+    # (event pairs have no elapsed time inside a graph), so it stays out of the timed region.
+    s.set_profiling(True)
+    inner_prof = 0.0
+    for k in range(args.steps):
+        s.configure(seed=k)
+        o, _ = run_once(nm, s, batched=True, dist=dist)
+        inner_prof += float(o["total_work"])
     n_phase, t_phase = s.phase_kernel_time()
     s.set_profiling(False)
-    clk = clocks.stop()
 
     dev_t = sum(dev_times) / len(dev_times)
     wall_t = sum(walls) / len(walls)
@@ -549,12 +635,16 @@ def main():
     # roofline of the phase kernel (the dominant kernel): lane-ops per inner sample x inner
     # samples / its CUDA-event time; peak = issue slots at the sampled SM clock
     sm_mhz = clk.get("sm_mhz") or 1965.0
-    achieved = inner * OPS_PER_INNER / t_phase / 1e9 if t_phase > 0 else None
+    achieved = inner_prof * OPS_PER_INNER / t_phase / 1e9 if t_phase > 0 else None
     peak = 148 * 128 * sm_mhz * 1e6 / 1e9
     roof = {"bound": "alu", "achieved": achieved, "peak": peak, "unit": "Gop/s",
             "frac": (achieved / peak) if achieved else None, "traffic": None,
             "kernel": "k_phase (FP32, X=Y+Z)", "launches": n_phase,
             "kernel_seconds": t_phase, "ops_per_inner_sample": OPS_PER_INNER,
+            "timing": "CUDA events around every phase-kernel launch in a profiled repeat of the timed "
+                      "runs (same seeds, levels submitted one call at a time)",
+            "traffic_note": "DRAM bytes per level-0 launch (ncu): 8 B per outer sample (Y and counts); "
+                            "no input data, so no HBM roofline applies",
             "peak_source": "issue-slot peak 148 SM x 4 SMSP x 32 lanes x sampled SM clock "
                            "(not in the measured-peaks file, which holds HBM and bf16 GEMM)"}
 
@@ -588,6 +678,7 @@ def main():
                                           "e2e": wd / wall_t}
         line["speedup_vs_fp64_same_streams"] = {"value": line["fp64_same_streams"]["value"] / dev_t,
                                                 "e2e": w64 / wall_t}
+        line["fp32_vs_fp64_per_level"] = per_level_error(nm, local, int(ref["nlevels"]))
     if world == 1 and not args.no_cpu:
         v, kind, cores, desc = cpu_reference_time(schedule, budget_s=args.ref_budget)
         line["cpu_baseline"] = {"value": v, "unit": "s", "cores": cores, "kind": kind, "sample": desc}
