@@ -486,6 +486,23 @@ def c3_case(args):
         if prec == nm.PREC_FP32:
             runs[name]["phase_config"] = phase_choices(s, int(out["nlevels"]))
     clk = cs.stop()
+    # each active level's FP32 estimate against the all-FP64 batched sampler on the same OUTER
+    # streams (at most 4096 outer samples per level)
+    per_level = []
+    for ell, M in enumerate(runs["fp32_batched"]["level_M"]):
+        if ell < runs["fp32_batched"]["starting_level"] or M == 0:
+            continue
+        m = min(M, 4096)
+        x, y = mk(nm.PREC_FP32, nm.STREAMS_OUTER, K, seed=17), mk(nm.PREC_FP64, nm.STREAMS_OUTER, K, seed=17)
+        x.set_autotune(0)
+        rx, ry = x.sample(ell, m, trace=True), y.sample(ell, m, trace=True)
+        tx, ty = rx["trace"], ry["trace"]
+        flip = (tx["phi_f"] != ty["phi_f"]) | (tx["phi_c"] != ty["phi_c"])
+        per_level.append({"level": ell, "M": m,
+                          "fEl_fp32_minus_fp64": (rx["fsums"][0] - ry["fsums"][0]) / m,
+                          "dEl_fp32_minus_fp64": (rx["diffsums"][0] - ry["diffsums"][0]) / m,
+                          "phi_flips": int(flip.sum()),
+                          "count_mismatches": int(((tx["count_f"] != ty["count_f"]) | (tx["count_c"] != ty["count_c"])).sum())})
     # phase-kernel roofline: CUDA events around every phase-kernel launch while the FP32 sampler
     # repeats one call per active level of its run (at most 8192 outer samples each)
     a = runs["fp32_batched"]
@@ -520,7 +537,7 @@ def c3_case(args):
             "runs": runs, "p_direct": p_direct, "p_direct_sd": sd,
             "speedup_vs_fp64_dropin": {"value": b["value"] / a["value"],
                                        "e2e": (b["e2e"] / a["e2e"]) if b.get("e2e") else None},
-            "roofline": roof, "full_loss_sweep": sweep,
+            "roofline": roof, "full_loss_sweep": sweep, "fp32_vs_fp64_per_level": per_level,
             "clocks": clk}
     print(json.dumps(line))
 
