@@ -153,7 +153,7 @@ def run_once(nm, s, batched, dist=None):
     from nmlmc.distributed import sharded_mlmc_run
     _, dev = dist
     t0 = time.perf_counter()
-    out = sharded_mlmc_run(s, device=dev, targetTOL=EPS, M0=WORKLOAD["M0"])
+    out = sharded_mlmc_run(s, device=dev, targetTOL=EPS, M0=WORKLOAD["M0"], batched=batched)
     return out, time.perf_counter() - t0
 
 

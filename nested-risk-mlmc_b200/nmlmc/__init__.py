@@ -541,7 +541,8 @@ def mlmc_output_dict(out: MlmcOutput, table: str) -> dict:
 def mlmc_run_cb(sample_level, sample_levels=None, *, targetTOL=1e-3, M0=100, verbose=False,
                 batched=False, checkpoint=None, resume=False, state=None, **kw) -> dict:
     """The host MLMC driver over a Python level sampler: sample_level(ell, M) -> dict with
-    fsums, diffsums, work (and optionally seconds).  A sampler that fails leaves the result's M
+    fsums, diffsums, work (and optionally seconds); with `batched`, sample_levels(ells, Ms) (if
+    given) takes all levels of a round at once.  A sampler that fails leaves the result's M
     at 0 and the driver stops with an error.  With `checkpoint` (a path) the driver writes its
     state after every TOL iteration, `resume` continues from it, and `state` = (save, load)
     stores the sampler's own state in the file: save() -> bytes, load(bytes)."""
@@ -563,14 +564,14 @@ def mlmc_run_cb(sample_level, sample_levels=None, *, targetTOL=1e-3, M0=100, ver
 
     def _many(user, n, ells, Ms, outs):
         try:
+            el = [int(ells[i]) for i in range(n)]
+            ms = [int(Ms[i]) for i in range(n)]
+            rs = sample_levels(el, ms) if sample_levels else [sample_level(e, m) for e, m in zip(el, ms)]
             for i in range(n):
-                fill(outs[i], sample_levels_or_one(int(ells[i]), int(Ms[i])), int(Ms[i]))
+                fill(outs[i], rs[i], ms[i])
         except Exception:
             for i in range(n):
                 outs[i].M = 0
-
-    def sample_levels_or_one(ell, M):
-        return sample_level(ell, M)
 
     f1 = SAMPLE_LEVEL_FN(_one)
     f2 = SAMPLE_LEVELS_FN(_many)

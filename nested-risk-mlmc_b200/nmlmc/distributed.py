@@ -5,7 +5,9 @@ share [r*M/W ...] of each sample_level(ell, M) call (nmlmc_set_shard) and the 16
 results are summed over ranks with one all_reduce per call (NCCL on GPUs, gloo on CPU).  All ranks
 then hold the single-device result, run the same host driver and take the same decisions; no
 data-path collective exists.  The sampler is any object with set_shard(rank, world) and
-sample(ell, M) -> dict (fsums, diffsums, work, seconds) — nmlmc.Sampler on GPUs.
+sample(ell, M) -> dict (fsums, diffsums, work, seconds) — nmlmc.Sampler on GPUs.  With `batched`
+and a sampler that has sample_levels(ells, Ms), every MLMC round is one submission per rank (one
+CUDA graph on GPUs) and one all_reduce of all its levels.
 """
 from __future__ import annotations
 
@@ -35,7 +37,11 @@ def sharded_mlmc_run(sampler, group=None, device=None, *, targetTOL=1e-3, M0=100
     def one(ell, M):
         return reduce([sampler.sample(ell, M)])[0]
 
-    out = mlmc_run_cb(one, targetTOL=targetTOL, M0=M0, batched=batched, **kw)
+    def many(ells, Ms):
+        return reduce(sampler.sample_levels(ells, Ms))
+
+    levels_fn = many if batched and hasattr(sampler, "sample_levels") else None
+    out = mlmc_run_cb(one, levels_fn, targetTOL=targetTOL, M0=M0, batched=batched, **kw)
     sampler.set_shard(0, 1)
     return out
 

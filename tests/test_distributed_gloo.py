@@ -30,6 +30,10 @@ class OracleShardSampler:
         r = self.s.sample(ell, M)
         return dict(fsums=r["fsums"], diffsums=r["diffsums"], work=r["work"], seconds=0.0)
 
+    def sample_levels(self, ells, Ms):
+        self.batches = getattr(self, "batches", 0) + 1
+        return [self.sample(e, m) for e, m in zip(ells, Ms)]
+
 
 def _free_port():
     with socket.socket() as s:
@@ -37,7 +41,7 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _worker(rank, world, port, q):
+def _worker(rank, world, port, q, batched=False):
     for p in (ROOT, PKG, os.path.join(ROOT, "oracle")):
         if p not in sys.path:
             sys.path.insert(0, p)
@@ -47,20 +51,26 @@ def _worker(rank, world, port, q):
     from nmlmc.distributed import sharded_mlmc_run
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
     try:
-        out = sharded_mlmc_run(OracleShardSampler(), targetTOL=CFG["tol"], M0=CFG["M0"])
+        smp = OracleShardSampler()
+        out = sharded_mlmc_run(smp, targetTOL=CFG["tol"], M0=CFG["M0"], batched=batched)
         q.put((rank, [int(x) for x in out["level_M"]], out["Eg"], out["level_fsums"].tolist(),
-               out["level_diffsums"].tolist(), out["calls"]))
+               out["level_diffsums"].tolist(), out["calls"], getattr(smp, "batches", 0)))
     finally:
         dist.destroy_process_group()
 
 
-def test_two_gloo_ranks_reproduce_single_process(nm):
+import pytest
+
+
+@pytest.mark.parametrize("batched", [False, True])
+def test_two_gloo_ranks_reproduce_single_process(nm, batched):
+    """Per-level calls, or one submission and one all_reduce per MLMC round (batched)."""
     import multiprocessing as mp
     single = nm.mlmc_run_cb(OracleShardSampler().sample, targetTOL=CFG["tol"], M0=CFG["M0"])
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q, batched)) for r in range(2)]
     for p in procs:
         p.start()
     res = [q.get(timeout=300) for _ in procs]
@@ -68,7 +78,8 @@ def test_two_gloo_ranks_reproduce_single_process(nm):
         p.join(timeout=60)
         assert p.exitcode == 0
     res.sort()
-    for rank, level_M, Eg, fs, ds, calls in res:
+    for rank, level_M, Eg, fs, ds, calls, batches in res:
+        assert (batches > 0) == batched
         assert level_M == [int(x) for x in single["level_M"]]
         assert Eg == single["Eg"]
         np.testing.assert_array_equal(np.array(fs), single["level_fsums"])
