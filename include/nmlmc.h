@@ -421,7 +421,10 @@ int nmlmc_mlmc_run_cb(const nmlmc_mlmc_input* in, nmlmc_sample_level_fn level_fn
  * warm-starts: the saved level sums seed a run of the new parameters from its first iteration.
  * The file is little-endian: "NMLMCCK1", u32 version = 1, u32 header bytes, then the fields in
  * the order above (nmlmc/checkpoint.py reads it). */
-typedef size_t (*nmlmc_state_save_fn)(void* user, void* buf, size_t cap);   /* bytes needed  */
+/* save(user, NULL, 0) returns the bytes needed, save(user, buf, cap) writes them and returns
+ * the count; (size_t)-1 reports a failure (the run stops with NMLMC_ERR_STATE).  load returns
+ * NMLMC_OK or an error status. */
+typedef size_t (*nmlmc_state_save_fn)(void* user, void* buf, size_t cap);
 typedef int (*nmlmc_state_load_fn)(void* user, const void* buf, size_t size);
 typedef struct nmlmc_checkpoint_io {
     const char* path;              /* NULL: no checkpoint                                   */

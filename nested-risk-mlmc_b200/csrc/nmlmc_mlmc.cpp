@@ -223,6 +223,7 @@ Level from_result(const nmlmc_level_result& r) {
 // TOL, bias_est, stat_error, elapsed seconds: f64), per level M (u64), the 4 + 4 FP64 sums, work
 // and time (f64), then the sampler state (u64 size + bytes).
 constexpr char kCkptMagic[8] = {'N', 'M', 'L', 'M', 'C', 'C', 'K', '1'};
+constexpr size_t kStateError = (size_t)-1;     // a state hook's failure (nmlmc_state_save_fn)
 constexpr uint32_t kCkptVersion = 1;
 
 struct Checkpoint {
@@ -359,6 +360,7 @@ int run(const nmlmc_mlmc_input& in, nmlmc_sample_level_fn level_fn, nmlmc_sample
         k.levels = out.levels;
         if (io->save) {
             const size_t need = io->save(user, nullptr, 0);
+            if (need == kStateError) return NMLMC_ERR_STATE;
             k.sampler.resize(need);
             if (need && io->save(user, &k.sampler[0], need) != need) return NMLMC_ERR_STATE;
         }
@@ -478,9 +480,9 @@ void gpu_levels(void* u, uint32_t n, const uint32_t* ells, const uint64_t* Ms, n
 size_t gpu_save_state(void* u, void* buf, size_t cap) {
     GpuUser* g = static_cast<GpuUser*>(u);
     size_t need = 0;
-    if (nmlmc_get_sampler_state(g->ctx, nullptr, 0, &need) != NMLMC_OK) return 0;
+    if (nmlmc_get_sampler_state(g->ctx, nullptr, 0, &need) != NMLMC_OK) return kStateError;
     if (!buf) return need;
-    if (cap < need || nmlmc_get_sampler_state(g->ctx, buf, cap, &need) != NMLMC_OK) return 0;
+    if (cap < need || nmlmc_get_sampler_state(g->ctx, buf, cap, &need) != NMLMC_OK) return kStateError;
     return need;
 }
 int gpu_load_state(void* u, const void* buf, size_t size) {

@@ -587,12 +587,15 @@ def mlmc_run_cb(sample_level, sample_levels=None, *, targetTOL=1e-3, M0=100, ver
         return mlmc_output_dict(out, buf.value.decode())
 
     def _save(user, p, cap):
-        b = state[0]()
-        if p:
-            if cap < len(b):
-                return 0
-            ctypes.memmove(p, b, len(b))
-        return len(b)
+        try:
+            b = state[0]()
+            if p:
+                if cap < len(b):
+                    return ctypes.c_size_t(-1).value
+                ctypes.memmove(p, b, len(b))
+            return len(b)
+        except Exception:          # the run stops with NMLMC_ERR_STATE
+            return ctypes.c_size_t(-1).value
 
     def _load(user, p, n):
         try:

@@ -130,6 +130,19 @@ def test_resume_without_a_file_starts_fresh_and_bad_files_are_errors(nm, golden,
     assert not os.path.exists(path + ".tmp")
 
 
+def test_failing_state_hook_stops_the_run(nm, golden, tmp_path):
+    """A sampler whose state cannot be saved must not leave a checkpoint without it."""
+    kw, sa = _args(golden)
+
+    def bad_save():
+        raise RuntimeError("state unavailable")
+
+    with pytest.raises(nm.NmlmcError):
+        nm.mlmc_run_cb(Synthetic(*sa), targetTOL=kw["tol"], M0=kw["M0"], checkpoint=str(tmp_path / "x.ckpt"),
+                       state=(bad_save, lambda b: None))
+    assert not os.path.exists(str(tmp_path / "x.ckpt"))
+
+
 def test_report_reader(nm, golden):
     """The reports' text (identical to the reference's to_string) read back: the final report
     of each golden run against the driver's numbers."""
