@@ -153,8 +153,8 @@ typedef struct nmlmc_config {
     int32_t precision;         /* NMLMC_PREC_*                                                   */
     int32_t streams;           /* NMLMC_STREAMS_*                                                */
     uint64_t seed;
-    uint64_t batch;            /* OUTER layout: outer samples per batch (0 -> 1<<22; portfolios:
-                                  at most 1 GiB of R_tau rows)                                  */
+    uint64_t batch;            /* OUTER layout: outer samples per batch (0: grows with the calls
+                                  up to 1<<24; portfolios: at most 1 GiB of R_tau rows)        */
 } nmlmc_config;
 
 typedef struct nmlmc_level_result {

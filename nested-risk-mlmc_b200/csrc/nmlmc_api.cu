@@ -126,6 +126,15 @@ struct DevPortfolio {
 
 }  // namespace
 
+// An executable graph of one submission topology: the levels of the round and their batch
+// counts (the launch sequence of a level follows from its level and batch count).
+struct GraphSlot {
+    std::vector<uint64_t> key;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t last_use = 0;
+};
+constexpr size_t kGraphCache = 16;
+
 // Phase-kernel configuration of one level: register/occupancy variant and chunk length.
 struct PhaseChoice {
     int32_t state = 0;        // 0 default, 1 tuned, 2 pinned by the caller
@@ -163,7 +172,8 @@ struct nmlmc_ctx {
     // one-submission level rounds (nmlmc_sample_levels on the OUTER layout)
     double* h_lev = nullptr;          // pinned [kMaxSubmit][16] sums, then [kMaxSubmit][2] stamps
     uint64_t* d_stamps = nullptr;     // device [kMaxSubmit][2] level begin / end (ns)
-    cudaGraphExec_t gexec = nullptr;  // executable graph of the last submission
+    std::vector<GraphSlot> graphs;    // executable graphs of recent submissions, by topology
+    uint64_t graph_clock = 0;
     uint64_t graph_instantiations = 0, graph_updates = 0, graph_launches = 0;
     // trace
     nmlmc_trace_rec* trace_host = nullptr;
@@ -450,16 +460,35 @@ int alloc_core(nmlmc_ctx* c) {
     return NMLMC_OK;
 }
 
-int alloc_outer(nmlmc_ctx* c) {
+void drop_graphs(nmlmc_ctx* c) {
+    for (GraphSlot& g : c->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    c->graphs.clear();
+}
+
+// Batch buffers for calls of up to `want` outer samples per rank.  An explicit cfg.batch is the
+// batch size; the default grows on demand in powers of two from 2^16 up to the default maximum
+// (2^24 outer samples, portfolios at most 1 GiB of R_tau rows), so small users stay small.
+int alloc_outer(nmlmc_ctx* c, uint64_t want) {
     const uint32_t Q = c->kind == KIND_PORTFOLIO ? c->pf.Q : 0;
     uint64_t cap = c->cfg.batch;
-    if (c->batch_default && Q) {            // default batch: at most 1 GiB of R_tau rows
-        const uint64_t lim = (1ull << 30) / ((uint64_t)Q * sizeof(double));
-        const uint64_t lo = 1ull << 16;
-        if (cap > lim) cap = lim > lo ? lim : lo;
+    if (c->batch_default) {
+        uint64_t cap_max = cap;
+        if (Q) {
+            const uint64_t lim = (1ull << 30) / ((uint64_t)Q * sizeof(double));
+            const uint64_t lo = 1ull << 16;
+            if (cap_max > lim) cap_max = lim > lo ? lim : lo;
+        }
+        cap = 1ull << 16;
+        while (cap < want && cap < cap_max) cap <<= 1;
+        if (cap > cap_max) cap = cap_max;
+        if (c->ob_alloc && c->ob.cap >= cap && c->ob.Q >= Q) return NMLMC_OK;
+        if (c->ob_alloc && c->ob.cap > cap) cap = c->ob.cap;      // never shrink
+    } else if (c->ob_alloc && c->ob.cap == cap && c->ob.Q >= Q) {
+        return NMLMC_OK;
     }
-    if (c->ob_alloc && c->ob.cap == cap && c->ob.Q >= Q) return NMLMC_OK;
     OuterBuffers& B = c->ob;
+    drop_graphs(c);                       // their nodes hold the old buffers
     if (c->ob_alloc) {
         cudaFree(B.Yv); cudaFree(B.Rt); cudaFree(B.cnt_f); cudaFree(B.cnt_c);
         cudaFree(B.lists); cudaFree(B.class_items); cudaFree(B.counters); cudaFree(B.block_sums);
@@ -809,27 +838,49 @@ int sample_outer_levels(nmlmc_ctx* c, uint32_t n, const uint32_t* ells, const ui
         if (graph) cudaGraphDestroy(graph);
         return cuda_status(err, "capture level round");
     }
-    if (c->gexec) {
+    // the executable graph of this topology, if a recent round had it: update it in place
+    std::vector<uint64_t> key;
+    for (uint32_t i = 0; i < n; i++) {
+        key.push_back(ells[i]);
+        key.push_back((Ms[i] + c->ob.cap - 1) / c->ob.cap);
+    }
+    GraphSlot* slot = nullptr;
+    for (GraphSlot& g : c->graphs)
+        if (g.key == key) slot = &g;
+    if (slot && slot->exec) {
         cudaGraphExecUpdateResultInfo info;
-        if (cudaGraphExecUpdate(c->gexec, graph, &info) == cudaSuccess) {
+        if (cudaGraphExecUpdate(slot->exec, graph, &info) == cudaSuccess) {
             c->graph_updates++;
         } else {
             cudaGetLastError();
-            cudaGraphExecDestroy(c->gexec);
-            c->gexec = nullptr;
+            cudaGraphExecDestroy(slot->exec);
+            slot->exec = nullptr;
         }
     }
-    if (!c->gexec) {
-        err = cudaGraphInstantiate(&c->gexec, graph, 0);
+    if (!slot || !slot->exec) {
+        cudaGraphExec_t exec = nullptr;
+        err = cudaGraphInstantiate(&exec, graph, 0);
         if (err != cudaSuccess) {
-            c->gexec = nullptr;
             cudaGraphDestroy(graph);
             return cuda_status(err, "instantiate level round");
         }
         c->graph_instantiations++;
+        if (!slot) {
+            if (c->graphs.size() >= kGraphCache) {        // evict the least recently used
+                size_t lru = 0;
+                for (size_t j = 1; j < c->graphs.size(); j++)
+                    if (c->graphs[j].last_use < c->graphs[lru].last_use) lru = j;
+                if (c->graphs[lru].exec) cudaGraphExecDestroy(c->graphs[lru].exec);
+                c->graphs.erase(c->graphs.begin() + lru);
+            }
+            c->graphs.push_back(GraphSlot{key, nullptr, 0});
+            slot = &c->graphs.back();
+        }
+        slot->exec = exec;
     }
+    slot->last_use = ++c->graph_clock;
     cudaGraphDestroy(graph);
-    NM_CUDA(cudaGraphLaunch(c->gexec, c->stream), "graph launch");
+    NM_CUDA(cudaGraphLaunch(slot->exec, c->stream), "graph launch");
     c->graph_launches++;
     NM_CUDA(cudaStreamSynchronize(c->stream), "sync");
     for (uint32_t i = 0; i < n; i++) {
@@ -901,7 +952,7 @@ int nmlmc_destroy(nmlmc_ctx* c) {
     }
     for (cudaEvent_t e : c->pev) cudaEventDestroy(e);
     dfree(c->d_stamps);
-    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    drop_graphs(c);
     if (c->h_lev) cudaFreeHost(c->h_lev);
     if (c->h_pin) cudaFreeHost(c->h_pin);
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -916,7 +967,7 @@ int nmlmc_configure(nmlmc_ctx* c, const nmlmc_config* cfg) {
     nmlmc_config k = *cfg;
     c->batch_default = k.batch == 0;
     if (k.cores == 0) k.cores = 2048;
-    if (k.batch == 0) k.batch = 1u << 22;
+    if (k.batch == 0) k.batch = 1u << 24;
     // beta: a power of two >= 2 (the adaptive base count N0 * (beta/2)^ell is 0 for beta = 1)
     if (k.N0 == 0 || k.beta < 2 || (k.beta & (k.beta - 1)) != 0) return set_err(NMLMC_ERR_ARG);
     if (k.precision < NMLMC_PREC_REF32 || k.precision > NMLMC_PREC_FP32) return set_err(NMLMC_ERR_ARG);
@@ -1208,7 +1259,7 @@ int nmlmc_sample(nmlmc_ctx* c, uint32_t ell, uint64_t M, nmlmc_level_result* out
         if ((rc = alloc_core(c))) return rc;
         return f64 ? sample_core<double>(c, ell, M, out) : sample_core<float>(c, ell, M, out);
     }
-    if ((rc = alloc_outer(c))) return rc;
+    if ((rc = alloc_outer(c, (M + c->shard_world - 1) / c->shard_world))) return rc;
     return f64 ? sample_outer<double>(c, ell, M, out) : sample_outer<float>(c, ell, M, out);
 }
 
@@ -1225,8 +1276,13 @@ int nmlmc_sample_levels(nmlmc_ctx* c, uint32_t n, const uint32_t* ells, const ui
     }
     if (one_submission) {
         cudaSetDevice(c->device);
+        uint64_t want = 0;
+        for (uint32_t i = 0; i < n; i++) {
+            const uint64_t m = (Ms[i] + c->shard_world - 1) / c->shard_world;
+            if (m > want) want = m;
+        }
         int rc = ensure_portfolio(c);
-        if (rc || (rc = alloc_outer(c))) return rc;
+        if (rc || (rc = alloc_outer(c, want))) return rc;
         if (!c->h_lev && cudaMallocHost(&c->h_lev, kMaxSubmit * 18 * sizeof(double)) != cudaSuccess)
             return set_err(NMLMC_ERR_NOMEM);
         if (!c->d_stamps && cudaMalloc(&c->d_stamps, kMaxSubmit * 2 * sizeof(uint64_t)) != cudaSuccess)
@@ -1386,7 +1442,7 @@ int nmlmc_autotune_level(nmlmc_ctx* c, uint32_t ell, uint64_t M) {
     if ((double)c->cfg.N0 * pow((double)c->cfg.beta, (double)ell) > 4.0e9) return set_err(NMLMC_ERR_ARG);
     cudaSetDevice(c->device);
     int rc = ensure_portfolio(c);
-    if (rc || (rc = alloc_outer(c))) return rc;
+    if (rc || (rc = alloc_outer(c, M))) return rc;
     if (c->kind == KIND_PORTFOLIO && c->pf.mixed()) return set_err(NMLMC_ERR_ARG);
     return tune_level<float>(c, ell, M, true);
 }
@@ -1405,7 +1461,7 @@ int nmlmc_portfolio_full_loss(nmlmc_ctx* c, uint32_t ell, uint64_t first, uint64
     if (n == 0) return NMLMC_OK;
     cudaSetDevice(c->device);
     int rc = ensure_portfolio(c);
-    if (rc || (rc = alloc_outer(c))) return rc;
+    if (rc || (rc = alloc_outer(c, n))) return rc;
     double* d_loss = nullptr;
     if (cudaMalloc(&d_loss, n * sizeof(double)) != cudaSuccess) return set_err(NMLMC_ERR_NOMEM);
     cudaError_t e;
