@@ -308,6 +308,11 @@ int nmlmc_set_phase_config(nmlmc_ctx* ctx, uint32_t ell, const nmlmc_phase_confi
  * (replaces a tuned or pinned choice). */
 int nmlmc_autotune_level(nmlmc_ctx* ctx, uint32_t ell, uint64_t M);
 
+/* Fault injection for tests (no counterpart in the reference): after `after` more successful
+ * device allocations by the library, the next one fails as if the device were out of memory;
+ * -1 switches it off.  The failing call returns NMLMC_ERR_NOMEM and the context stays usable. */
+int nmlmc_inject_alloc_failure(int32_t after);
+
 /* CUDA graphs of nmlmc_sample_levels: instantiated, updated in place, launched. */
 int nmlmc_graph_stats(nmlmc_ctx* ctx, uint64_t* instantiations, uint64_t* updates, uint64_t* launches);
 /* Arms a host buffer of `cap` records for the next nmlmc_sample call (M <= cap). */

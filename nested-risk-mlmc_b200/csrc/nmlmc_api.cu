@@ -1,6 +1,7 @@
 // C ABI of the level sampler: contexts, the reference-named surface and host-side set-up.
 #include <algorithm>
 #include <cmath>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -10,6 +11,7 @@
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "../../include/nmlmc.h"
 #include "nmlmc_internal.h"
@@ -198,6 +200,30 @@ namespace {
 
 thread_local int g_tls_error = NMLMC_OK;
 
+// NVTX range for profilers (nsys, ncu --nvtx): header-only NVTX v3, inert unless a tool attaches.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
+// Device allocations of the library go through dev_malloc so that tests can make one of them fail
+// (nmlmc_inject_alloc_failure): -1 = off, k >= 0 = k more allocations succeed, then one fails.
+std::atomic<int64_t> g_fail_alloc{-1};
+
+template <class T>
+cudaError_t dev_malloc(T** p, size_t bytes) {
+    const int64_t k = g_fail_alloc.load();
+    if (k == 0) {
+        g_fail_alloc.store(-1);
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    if (k > 0) g_fail_alloc.store(k - 1);
+    return cudaMalloc(p, bytes);
+}
+
 int set_err(int e) {
     g_tls_error = e;
     return e;
@@ -233,7 +259,7 @@ template <class T>
 int upload(T*& d, const std::vector<T>& h) {
     dfree(d);
     size_t n = h.size() ? h.size() : 1;
-    if (cudaMalloc(&d, n * sizeof(T)) != cudaSuccess) return set_err(NMLMC_ERR_NOMEM);
+    if (dev_malloc(&d, n * sizeof(T)) != cudaSuccess) return set_err(NMLMC_ERR_NOMEM);
     if (!h.empty()) NM_CUDA(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
     return NMLMC_OK;
 }
@@ -452,12 +478,29 @@ int alloc_core(nmlmc_ctx* c) {
     const uint32_t cores = c->cfg.cores;
     if (c->states_cores == cores && c->d_states) return NMLMC_OK;
     dfree(c->d_states); dfree(c->d_part_sums); dfree(c->d_part_stats);
-    if (cudaMalloc(&c->d_states, (size_t)cores * 2 * sizeof(CoreStream)) != cudaSuccess ||
-        cudaMalloc(&c->d_part_sums, (size_t)cores * 10 * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&c->d_part_stats, (size_t)cores * 6 * sizeof(uint64_t)) != cudaSuccess)
+    c->states_cores = 0;
+    if (dev_malloc(&c->d_states, (size_t)cores * 2 * sizeof(CoreStream)) != cudaSuccess ||
+        dev_malloc(&c->d_part_sums, (size_t)cores * 10 * sizeof(double)) != cudaSuccess ||
+        dev_malloc(&c->d_part_stats, (size_t)cores * 6 * sizeof(uint64_t)) != cudaSuccess) {
+        dfree(c->d_states); dfree(c->d_part_sums); dfree(c->d_part_stats);
         return set_err(NMLMC_ERR_NOMEM);
+    }
     c->states_cores = cores;
     return NMLMC_OK;
+}
+
+void free_outer(nmlmc_ctx* c) {
+    OuterBuffers& B = c->ob;
+    if (c->ob_alloc) {
+        cudaFree(B.Yv); cudaFree(B.Rt); cudaFree(B.cnt_f); cudaFree(B.cnt_c);
+        cudaFree(B.lists); cudaFree(B.class_items); cudaFree(B.counters); cudaFree(B.block_sums);
+        cudaFree(B.level_acc);
+    }
+    B.Yv = B.Rt = nullptr;
+    B.cnt_f = B.cnt_c = B.lists = B.class_items = B.counters = nullptr;
+    B.block_sums = B.level_acc = nullptr;
+    B.cap = 0;
+    c->ob_alloc = false;
 }
 
 void drop_graphs(nmlmc_ctx* c) {
@@ -489,29 +532,27 @@ int alloc_outer(nmlmc_ctx* c, uint64_t want) {
     }
     OuterBuffers& B = c->ob;
     drop_graphs(c);                       // their nodes hold the old buffers
-    if (c->ob_alloc) {
-        cudaFree(B.Yv); cudaFree(B.Rt); cudaFree(B.cnt_f); cudaFree(B.cnt_c);
-        cudaFree(B.lists); cudaFree(B.class_items); cudaFree(B.counters); cudaFree(B.block_sums);
-        cudaFree(B.level_acc);
-        c->ob_alloc = false;
-    }
+    free_outer(c);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
     B.cap = cap;
     B.Q = Q;
     B.grid = sms * 4;            // partial-sum slots; the phase kernel runs its resident CTAs (<= grid)
-    bool ok = cudaMalloc(&B.Yv, cap * sizeof(double)) == cudaSuccess &&
-              cudaMalloc(&B.Rt, (Q ? cap * Q : 1) * sizeof(double)) == cudaSuccess &&
-              cudaMalloc(&B.cnt_f, cap * sizeof(uint32_t)) == cudaSuccess &&
-              cudaMalloc(&B.cnt_c, cap * sizeof(uint32_t)) == cudaSuccess &&
-              cudaMalloc(&B.lists, 4 * cap * sizeof(uint32_t)) == cudaSuccess &&
-              cudaMalloc(&B.class_items, cap * sizeof(uint32_t)) == cudaSuccess &&
-              cudaMalloc(&B.counters, 256 * sizeof(uint32_t)) == cudaSuccess &&
-              cudaMalloc(&B.block_sums, (size_t)B.grid * 16 * sizeof(double)) == cudaSuccess &&
-              cudaMalloc(&B.level_acc, kMaxSubmit * 16 * sizeof(double)) == cudaSuccess;
-    if (!ok) return set_err(NMLMC_ERR_NOMEM);
+    bool ok = dev_malloc(&B.Yv, cap * sizeof(double)) == cudaSuccess &&
+              dev_malloc(&B.Rt, (Q ? cap * Q : 1) * sizeof(double)) == cudaSuccess &&
+              dev_malloc(&B.cnt_f, cap * sizeof(uint32_t)) == cudaSuccess &&
+              dev_malloc(&B.cnt_c, cap * sizeof(uint32_t)) == cudaSuccess &&
+              dev_malloc(&B.lists, 4 * cap * sizeof(uint32_t)) == cudaSuccess &&
+              dev_malloc(&B.class_items, cap * sizeof(uint32_t)) == cudaSuccess &&
+              dev_malloc(&B.counters, 256 * sizeof(uint32_t)) == cudaSuccess &&
+              dev_malloc(&B.block_sums, (size_t)B.grid * 16 * sizeof(double)) == cudaSuccess &&
+              dev_malloc(&B.level_acc, kMaxSubmit * 16 * sizeof(double)) == cudaSuccess;
+    c->ob_alloc = true;                   // free_outer releases a partial set too
+    if (!ok) {
+        free_outer(c);
+        return set_err(NMLMC_ERR_NOMEM);
+    }
     cudaMemset(B.counters, 0, 256 * sizeof(uint32_t));
-    c->ob_alloc = true;
     return NMLMC_OK;
 }
 
@@ -535,7 +576,7 @@ int ensure_trace(nmlmc_ctx* c, uint64_t M) {
     if (M > c->trace_cap) return set_err(NMLMC_ERR_ARG);
     if (c->d_trace_cap < M) {
         dfree(c->d_trace);
-        if (cudaMalloc(&c->d_trace, M * sizeof(TraceRec)) != cudaSuccess) return set_err(NMLMC_ERR_NOMEM);
+        if (dev_malloc(&c->d_trace, M * sizeof(TraceRec)) != cudaSuccess) return set_err(NMLMC_ERR_NOMEM);
         c->d_trace_cap = M;
     }
     return NMLMC_OK;
@@ -721,6 +762,7 @@ uint64_t probe_size(const nmlmc_ctx* c, uint32_t ell, uint64_t M) {
 
 template <class RT>
 int tune_level(nmlmc_ctx* c, uint32_t ell, uint64_t M, bool chunks) {
+    NvtxRange nv("nmlmc autotune level");
     const uint64_t Mp = probe_size(c, ell, M);
     PhaseChoice best = default_phase(c);
     best.state = 1;
@@ -763,6 +805,9 @@ int sample_outer(nmlmc_ctx* c, uint32_t ell, uint64_t Mtotal, nmlmc_level_result
     const uint64_t q = Mtotal / c->shard_world, rem = Mtotal % c->shard_world;
     const uint64_t lo = q * c->shard_rank + (c->shard_rank < rem ? c->shard_rank : rem);
     const uint64_t M = q + (c->shard_rank < rem ? 1 : 0);
+    char label[64];
+    snprintf(label, sizeof label, "nmlmc level %u M %llu", ell, (unsigned long long)Mtotal);
+    NvtxRange nv(label);
     int rc = ensure_tuned<RT>(c, ell, M);
     if (rc) return rc;
     OuterLevel<RT> L = outer_level_params<RT>(c, ell, M, c->next_outer[ell] + lo);
@@ -800,6 +845,7 @@ void shard_range(const nmlmc_ctx* c, uint64_t Mtotal, uint64_t& lo, uint64_t& M)
 template <class RT>
 int sample_outer_levels(nmlmc_ctx* c, uint32_t n, const uint32_t* ells, const uint64_t* Mtot,
                         nmlmc_level_result* outs) {
+    NvtxRange nv("nmlmc round submission");
     uint64_t next[NMLMC_MAX_LEVELS];
     memcpy(next, c->next_outer, sizeof(next));
     std::vector<uint64_t> Ms(n);
@@ -927,8 +973,8 @@ int nmlmc_create(nmlmc_ctx** out, int device) {
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
         cudaMallocHost(&c->h_pin, 64 * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&c->d_out_sums, 16 * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&c->d_out_stats, 8 * sizeof(uint64_t)) != cudaSuccess) {
+        dev_malloc(&c->d_out_sums, 16 * sizeof(double)) != cudaSuccess ||
+        dev_malloc(&c->d_out_stats, 8 * sizeof(uint64_t)) != cudaSuccess) {
         nmlmc_destroy(c);
         return set_err(NMLMC_ERR_CUDA);
     }
@@ -944,12 +990,7 @@ int nmlmc_destroy(nmlmc_ctx* c) {
     free_dev_portfolio(c->dpf64);
     dfree(c->d_states); dfree(c->d_part_sums); dfree(c->d_part_stats);
     dfree(c->d_out_sums); dfree(c->d_out_stats); dfree(c->d_trace);
-    if (c->ob_alloc) {
-        OuterBuffers& B = c->ob;
-        cudaFree(B.Yv); cudaFree(B.Rt); cudaFree(B.cnt_f); cudaFree(B.cnt_c);
-        cudaFree(B.lists); cudaFree(B.class_items); cudaFree(B.counters); cudaFree(B.block_sums);
-        cudaFree(B.level_acc);
-    }
+    free_outer(c);
     for (cudaEvent_t e : c->pev) cudaEventDestroy(e);
     dfree(c->d_stamps);
     drop_graphs(c);
@@ -1011,6 +1052,9 @@ int nmlmc_reset_streams(nmlmc_ctx* c) {
 int nmlmc_set_model(nmlmc_ctx* c, int32_t kind, double tau, double max_loss) {
     if (!c) return set_err(NMLMC_ERR_ARG);
     if (kind != NMLMC_MODEL_REFERENCE && kind != NMLMC_MODEL_SHIFT) return set_err(NMLMC_ERR_ARG);
+    // finite inputs; the reference model needs sqrt(tau) and sqrt(1 - tau) (model_sampler.cpp:21-39)
+    if (!std::isfinite(tau) || !std::isfinite(max_loss)) return set_err(NMLMC_ERR_ARG);
+    if (kind == NMLMC_MODEL_REFERENCE && !(tau >= 0 && tau <= 1)) return set_err(NMLMC_ERR_ARG);
     c->kind = kind;
     c->tau = tau;
     c->max_loss = max_loss;
@@ -1027,6 +1071,17 @@ static int set_portfolio_impl(nmlmc_ctx* c, const nmlmc_portfolio* p, const nmlm
         return set_err(NMLMC_ERR_ARG);
     if (p->subsample != NMLMC_SUB_NONE && p->subsample != NMLMC_SUB_RANDOM && p->subsample != NMLMC_SUB_UNIFORM)
         return set_err(NMLMC_ERR_ARG);
+    // finite inputs, positive prices and volatilities (a NaN would turn into phi = 0 silently)
+    if (!std::isfinite(p->r) || !std::isfinite(p->rho) || !std::isfinite(p->max_loss) || !std::isfinite(p->tau))
+        return set_err(NMLMC_ERR_ARG);
+    for (uint32_t s = 0; s < p->Q; s++)
+        if (!(p->S0[s] > 0) || !std::isfinite(p->S0[s]) || !std::isfinite(p->mu[s]) || !(p->sigma[s] > 0) ||
+            !std::isfinite(p->sigma[s]))
+            return set_err(NMLMC_ERR_ARG);
+    for (uint32_t j = 0; j < p->P; j++)
+        if (!(p->strike[j] > 0) || !std::isfinite(p->strike[j]) || !std::isfinite(p->maturity[j]) ||
+            !std::isfinite(p->w[j]) || (p->prob && !std::isfinite(p->prob[j])))
+            return set_err(NMLMC_ERR_ARG);
     const int32_t* method = pm ? pm->method : nullptr;
     if (pm && (pm->dt_h0inv == 0 || pm->dt_beta < 2 || !(pm->dt_prob_expo < 0)))
         return set_err(NMLMC_ERR_ARG);                     // portfolio_sampler.cpp:525
@@ -1107,7 +1162,7 @@ struct DevAlloc {                       // device buffers of one nmlmc_path_adjo
     template <class T>
     T* get(size_t n) {
         void* p = nullptr;
-        if (cudaMalloc(&p, (n ? n : 1) * sizeof(T)) != cudaSuccess) return nullptr;
+        if (dev_malloc(&p, (n ? n : 1) * sizeof(T)) != cudaSuccess) return nullptr;
         ptrs.push_back(p);
         return static_cast<T*>(p);
     }
@@ -1285,7 +1340,7 @@ int nmlmc_sample_levels(nmlmc_ctx* c, uint32_t n, const uint32_t* ells, const ui
         if (rc || (rc = alloc_outer(c, want))) return rc;
         if (!c->h_lev && cudaMallocHost(&c->h_lev, kMaxSubmit * 18 * sizeof(double)) != cudaSuccess)
             return set_err(NMLMC_ERR_NOMEM);
-        if (!c->d_stamps && cudaMalloc(&c->d_stamps, kMaxSubmit * 2 * sizeof(uint64_t)) != cudaSuccess)
+        if (!c->d_stamps && dev_malloc(&c->d_stamps, kMaxSubmit * 2 * sizeof(uint64_t)) != cudaSuccess)
             return set_err(NMLMC_ERR_NOMEM);
         for (uint32_t i = 0; i < n; i++) memset(&outs[i], 0, sizeof(outs[i]));
         return k.precision == NMLMC_PREC_FP64 ? sample_outer_levels<double>(c, n, ells, Ms, outs)
@@ -1447,6 +1502,12 @@ int nmlmc_autotune_level(nmlmc_ctx* c, uint32_t ell, uint64_t M) {
     return tune_level<float>(c, ell, M, true);
 }
 
+int nmlmc_inject_alloc_failure(int32_t after) {
+    if (after < -1) return set_err(NMLMC_ERR_ARG);
+    g_fail_alloc.store(after);
+    return NMLMC_OK;
+}
+
 int nmlmc_graph_stats(nmlmc_ctx* c, uint64_t* instantiations, uint64_t* updates, uint64_t* launches) {
     if (!c || !instantiations || !updates || !launches) return set_err(NMLMC_ERR_ARG);
     *instantiations = c->graph_instantiations;
@@ -1463,7 +1524,7 @@ int nmlmc_portfolio_full_loss(nmlmc_ctx* c, uint32_t ell, uint64_t first, uint64
     int rc = ensure_portfolio(c);
     if (rc || (rc = alloc_outer(c, n))) return rc;
     double* d_loss = nullptr;
-    if (cudaMalloc(&d_loss, n * sizeof(double)) != cudaSuccess) return set_err(NMLMC_ERR_NOMEM);
+    if (dev_malloc(&d_loss, n * sizeof(double)) != cudaSuccess) return set_err(NMLMC_ERR_NOMEM);
     cudaError_t e;
     if (c->cfg.precision == NMLMC_PREC_FP64) {
         OuterLevel<double> L{};
@@ -1484,7 +1545,7 @@ int nmlmc_threefry_blocks(const uint64_t* ctr, const uint64_t* key, uint64_t* ou
     if (!ctr || !key || !out) return set_err(NMLMC_ERR_ARG);
     if (n == 0) return NMLMC_OK;
     uint64_t* d = nullptr;
-    if (cudaMalloc(&d, 6 * n * sizeof(uint64_t)) != cudaSuccess) return set_err(NMLMC_ERR_NOMEM);
+    if (dev_malloc(&d, 6 * n * sizeof(uint64_t)) != cudaSuccess) return set_err(NMLMC_ERR_NOMEM);
     cudaError_t e = cudaMemcpy(d, ctr, 2 * n * sizeof(uint64_t), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(d + 2 * n, key, 2 * n * sizeof(uint64_t), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = launch_threefry_blocks(d, d + 2 * n, d + 4 * n, n, 0);
@@ -1498,7 +1559,7 @@ int nmlmc_outer_normals(int32_t precision, uint64_t seed, uint64_t stream, uint3
     if (!out || (precision != NMLMC_PREC_FP32 && precision != NMLMC_PREC_FP64)) return set_err(NMLMC_ERR_ARG);
     if (n == 0) return NMLMC_OK;
     double* d = nullptr;
-    if (cudaMalloc(&d, n * sizeof(double)) != cudaSuccess) return set_err(NMLMC_ERR_NOMEM);
+    if (dev_malloc(&d, n * sizeof(double)) != cudaSuccess) return set_err(NMLMC_ERR_NOMEM);
     cudaError_t e = launch_outer_normals(precision, seed, stream, tag, n, d, 0);
     if (e == cudaSuccess) e = cudaMemcpy(out, d, n * sizeof(double), cudaMemcpyDeviceToHost);
     cudaFree(d);
@@ -1509,7 +1570,7 @@ int nmlmc_norm_cdf_fast(const float* x, float* out, uint64_t n) {
     if (!x || !out) return set_err(NMLMC_ERR_ARG);
     if (n == 0) return NMLMC_OK;
     float* d = nullptr;
-    if (cudaMalloc(&d, 2 * n * sizeof(float)) != cudaSuccess) return set_err(NMLMC_ERR_NOMEM);
+    if (dev_malloc(&d, 2 * n * sizeof(float)) != cudaSuccess) return set_err(NMLMC_ERR_NOMEM);
     cudaError_t e = cudaMemcpy(d, x, n * sizeof(float), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = launch_norm_cdf_fast(d, d + n, n, 0);
     if (e == cudaSuccess) e = cudaMemcpy(out, d + n, n * sizeof(float), cudaMemcpyDeviceToHost);

@@ -30,11 +30,21 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/nmlmc.h"
 
 namespace {
 
 inline double sq(double x) { return x * x; }
+
+// Profiler range (NVTX v3, header-only; inert unless a tool such as nsys attaches).
+struct NvtxScope {
+    explicit NvtxScope(const char* name) { nvtxRangePushA(name); }
+    ~NvtxScope() { nvtxRangePop(); }
+    NvtxScope(const NvtxScope&) = delete;
+    NvtxScope& operator=(const NvtxScope&) = delete;
+};
 
 // mc_diff_output_t<double, 4> (mlmc.hpp:21-85)
 struct Level {
@@ -370,6 +380,9 @@ int run(const nmlmc_mlmc_input& in, nmlmc_sample_level_fn level_fn, nmlmc_sample
     bool complete = true;
     uint32_t itr_end = itr0;
     for (uint32_t itr = itr0; itr <= total_itrs; itr++) {
+        char label[48];
+        snprintf(label, sizeof label, "nmlmc TOL iteration %u", itr);
+        const NvtxScope nv(label);
         out.starting_level = better_starting_level(out, in.starting_level_coeff);
         while (true) {
             optimal_Ml(in.theta * sq(out.TOL) / in.Ca, in.M0, out, Ml);

@@ -224,6 +224,7 @@ EXPORTS = [
     "nmlmc_path_adjoint", "nmlmc_graph_stats", "nmlmc_set_autotune", "nmlmc_get_phase_config",
     "nmlmc_set_phase_config", "nmlmc_autotune_level", "nmlmc_mlmc_run_cb_ckpt", "nmlmc_mlmc_run_ckpt",
     "nmlmc_get_sampler_state", "nmlmc_set_sampler_state", "nmlmc_norm_cdf_fast",
+    "nmlmc_inject_alloc_failure",
 ]
 
 
@@ -273,6 +274,7 @@ def lib() -> ctypes.CDLL:
     L.nmlmc_set_shard.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32]
     L.nmlmc_set_profiling.argtypes = [ctypes.c_void_p, ctypes.c_int32]
     L.nmlmc_set_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int32]
+    L.nmlmc_inject_alloc_failure.argtypes = [ctypes.c_int32]
     L.nmlmc_get_phase_config.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(PhaseConfig)]
     L.nmlmc_set_phase_config.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(PhaseConfig)]
     L.nmlmc_autotune_level.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64]
