@@ -253,7 +253,7 @@ def reference_arm(args):
 def small_case():
     """Fixed level calls of the FP32 sampler (the profiling case): level 0 with 2^24 outer samples
     (fine only, 32 inner samples each) and level 8 with 2^16 (adaptive pilots and the antithetic
-    final phase).  Device memory: the 2^20-sample batch buffers (~40 MB)."""
+    final phase).  Device memory: the batch buffers, grown to 2^24 outer samples (~600 MB)."""
     sys.path.insert(0, PKG)
     import nmlmc as nm
     s = make_sampler(nm, 0, nm.PREC_FP32, nm.STREAMS_OUTER, seed=0)
