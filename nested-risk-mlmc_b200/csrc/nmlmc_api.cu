@@ -717,16 +717,18 @@ OuterLevel<RT> outer_level_params(const nmlmc_ctx* c, uint32_t ell, uint64_t M, 
 // ---- phase-kernel autotuner (batched FP32 path) ---------------------------------------------
 // The first call of a level that carries enough work to time (>= 4096 outer samples and ~8e6
 // inner samples in one batch) times candidate configurations on a probe — the level's own
-// parameters on about 2^26 inner samples of pilot work (probe_size), from outer samples whose
+// parameters on about 20 ms of work (probe_size), from outer samples whose
 // stream indices start at 2^55, far from any real index, so the probe changes no result — and
 // keeps the fastest for the level:
-//   1. the register/occupancy variants 0, 1, 2 at the default chunk length;
+//   1. the register/occupancy variants 0, 1, 2 at the default chunk length, another than the
+//      default taken only if > 3 % faster;
 //   2. (mode 2, or an explicit nmlmc_autotune_level) half and double the chunk length at the
 //      best variant, taken only if > 3 % faster.
 // The variants compute identically, so mode 1 never changes a result; the chunk length changes
 // the grouping of the FP32 compensated inner sums (last-bit differences of inner means).
 // Pinned levels are not tuned.
 constexpr uint64_t kProbeIndex = 1ull << 55;
+constexpr double kProbeMs = 20.0;       // device time of one tuning probe
 
 template <class RT>
 cudaError_t time_phase_config(nmlmc_ctx* c, uint32_t ell, uint64_t Mp, const PhaseChoice& pc, double& ms_out) {
@@ -749,30 +751,47 @@ cudaError_t time_phase_config(nmlmc_ctx* c, uint32_t ell, uint64_t Mp, const Pha
     return e;
 }
 
-// Probe size: about 2^26 inner samples of pilot work (~1 ms), at least 4096 outer samples, at
-// most the call's M and one batch.
-uint64_t probe_size(const nmlmc_ctx* c, uint32_t ell, uint64_t M) {
-    const CountParams cf = count_params(c->cfg, ell);
-    uint64_t Mp = (1ull << 26) / (cf.base_count * (uint64_t)(ell + 1));
-    if (Mp < 4096) Mp = 4096;
-    if (Mp > M) Mp = M;
-    if (Mp > c->ob.cap) Mp = c->ob.cap;
-    return Mp;
+// Probe size, measured: starting from min(4096, M, batch) outer samples, the default
+// configuration is timed on growing probes (at most 8x per step, launch overheads make small
+// probes look cheap) until one takes kProbeMs of device time or the probe reaches the call's M or
+// one batch.  Shorter probes mis-ranked the variants of the large-portfolio levels.  The work per outer sample ranges from the base count to the maximum count of the level,
+// too wide to predict from the configuration.
+template <class RT>
+cudaError_t probe_size(nmlmc_ctx* c, uint32_t ell, uint64_t M, uint64_t& Mp) {
+    const uint64_t lim = M < c->ob.cap ? M : c->ob.cap;
+    Mp = lim < 4096 ? lim : 4096;
+    for (;;) {
+        double ms = 0;
+        cudaError_t e = time_phase_config<RT>(c, ell, Mp, default_phase(c), ms);
+        if (e != cudaSuccess) return e;
+        if (ms >= kProbeMs || Mp >= lim) return cudaSuccess;
+        double grow = ms > 0 ? kProbeMs / ms : 8.0;
+        if (grow > 8.0) grow = 8.0;
+        if (grow < 2.0) grow = 2.0;
+        const double next = (double)Mp * grow;
+        Mp = next >= (double)lim ? lim : (uint64_t)next;
+    }
 }
 
 template <class RT>
 int tune_level(nmlmc_ctx* c, uint32_t ell, uint64_t M, bool chunks) {
     NvtxRange nv("nmlmc autotune level");
-    const uint64_t Mp = probe_size(c, ell, M);
+    uint64_t Mp = 0;
+    NM_CUDA(probe_size<RT>(c, ell, M, Mp), "autotune probe size");
+    // the default stays unless another candidate is more than 3 % faster on the probe (near-ties
+    // on a short probe are noise)
     PhaseChoice best = default_phase(c);
     best.state = 1;
-    double best_ms = INFINITY;
+    double best_ms;
+    NM_CUDA(time_phase_config<RT>(c, ell, Mp, best, best_ms), "autotune probe");
+    const uint32_t v0 = best.variant;
     for (uint32_t v = 0; v < 3; v++) {
+        if (v == v0) continue;
         PhaseChoice pc = best;
         pc.variant = v;
         double ms;
         NM_CUDA(time_phase_config<RT>(c, ell, Mp, pc, ms), "autotune probe");
-        if (ms < best_ms) { best_ms = ms; best.variant = v; }
+        if (ms < 0.97 * best_ms) { best_ms = ms; best.variant = v; }
     }
     const uint32_t c0 = best.chunk;
     for (uint32_t ch : {c0 / 2, c0 * 2}) {
