@@ -160,6 +160,23 @@ def test_report_reader(nm, golden):
         np.testing.assert_allclose(nm.tables.column(r, "Wl"), out["level_work"] / out["level_M"], rtol=1e-4)
 
 
+def test_report_reader_on_the_driver_stdout(nm, golden, capfd):
+    """The driver's verbose stdout (the reference's "# Sampling" lines and one report per TOL
+    iteration) read back: one report per completed iteration, TOL shrinking by sqrt(2), the last
+    report equal to the returned table."""
+    kw, sa = _args(golden)
+    out = nm.mlmc_run_cb(Synthetic(*sa), targetTOL=kw["tol"], M0=kw["M0"], verbose=True)
+    text = capfd.readouterr().out
+    assert "# Sampling" in text
+    reps = nm.tables.parse_reports(text)
+    assert len(reps) == out["iterations_done"]
+    tols = [r["TOL"] for r in reps]
+    np.testing.assert_allclose(np.array(tols[1:]) / np.array(tols[:-1]), 2 ** -0.5, rtol=1e-4)
+    last = nm.tables.parse_reports(out["table"])[0]
+    np.testing.assert_array_equal(last["data"], reps[-1]["data"])
+    assert last["starting_level"] == reps[-1]["starting_level"] == out["starting_level"]
+
+
 def test_report_reader_starred_levels(nm):
     text = """TOL: 0.001
 RMS: 0.0009 (0.0004, 0.0008)
