@@ -422,7 +422,9 @@ int nmlmc_mlmc_run_cb(const nmlmc_mlmc_input* in, nmlmc_sample_level_fn level_fn
  * sampler's state (`save`; for nmlmc_mlmc_run_ckpt the context's stream positions).  With
  * `resume` set and `path` present, a run whose input parameters (targetTOL, startTOL, theta,
  * starting_level_coeff, Ca, M0) equal the saved ones continues at the saved iteration with the
- * saved sums and sampler state, and ends exactly as the uninterrupted run would; otherwise it
+ * saved sums and sampler state, and ends exactly as the uninterrupted run would (on the FP32
+ * batched path: with autotuning in mode 0 or 1, or chunk lengths pinned, since a fresh context
+ * tunes again and another chunk length regroups the FP32 inner sums); otherwise it
  * warm-starts: the saved level sums seed a run of the new parameters from its first iteration.
  * The file is little-endian: "NMLMCCK1", u32 version = 1, u32 header bytes, then the fields in
  * the order above (nmlmc/checkpoint.py reads it). */
