@@ -748,19 +748,20 @@ __global__ void k_classify(DevLevel<RT> D, uint32_t nb, int pass) {
     }
 }
 
-static __global__ void k_reduce_blocks(const double* block_sums, int grid, double* level_acc) {
-    __shared__ double sm[256];
-    for (int q = 0; q < 16; q++) {
-        double v = 0;
-        for (int b = threadIdx.x; b < grid; b += blockDim.x) v += block_sums[(size_t)b * 16 + q];
-        sm[threadIdx.x] = v;
-        __syncthreads();
-        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-            if ((int)threadIdx.x < s) sm[threadIdx.x] += sm[threadIdx.x + s];
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) level_acc[q] += sm[0];
-        __syncthreads();
+// Per-CTA partials -> the level's 16 sums, one CTA of 256 threads: thread t adds sum q = t % 16 of
+// CTA slots t / 16, t / 16 + 16, ... (consecutive threads read consecutive doubles), then thread q
+// adds its 16 group sums in a fixed order.  Launch with 256 threads.
+static __global__ void __launch_bounds__(256) k_reduce_blocks(const double* block_sums, int grid, double* level_acc) {
+    __shared__ double sm[16][17];
+    const int t = threadIdx.x, q = t & 15, g = t >> 4;
+    double v = 0;
+    for (int b = g; b < grid; b += 16) v += block_sums[(size_t)b * 16 + q];
+    sm[g][q] = v;
+    __syncthreads();
+    if (t < 16) {
+        double s = 0;
+        for (int k = 0; k < 16; k++) s += sm[k][t];
+        level_acc[t] += s;
     }
 }
 
