@@ -553,6 +553,8 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison runs")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--eps", type=float, default=None, help="--case c3: target RMSE (default 1e-3)")
+    ap.add_argument("--schedule-out", default=None,
+                    help="write the run's outer samples per level (bench_schedule.json format) here")
     ap.add_argument("--case", default=None, choices=["small", "c3", "c3-level", "c3-table", "c3-sweep", "c4",
                                                       "c4-small"],
                     help="small: a few fixed level calls of the FP32 sampler (profiling case); "
@@ -645,9 +647,10 @@ def main():
     schedule = dict(eps=EPS, levels=list(range(int(ref["nlevels"]))),
                     M=[int(x) for x in ref["level_M"]],
                     note="outer samples per level of the eps run (seed 0) of the batched sampler")
-    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-    with open(os.path.join(ROOT, "gpurun_out", "bench_schedule.json"), "w") as f:
-        json.dump(schedule, f)
+    if args.schedule_out:          # the level counts of this run (the reference arm's schedule)
+        os.makedirs(os.path.dirname(os.path.abspath(args.schedule_out)), exist_ok=True)
+        with open(args.schedule_out, "w") as f:
+            json.dump(schedule, f)
 
     # roofline of the phase kernel (the dominant kernel): lane-ops per inner sample x inner
     # samples / its CUDA-event time; peak = issue slots at the sampled SM clock
