@@ -100,22 +100,29 @@ class ClockSampler:
             self.p.kill()
         self.f.flush()
         self.f.seek(0)
-        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        text = self.f.read()
         os.unlink(self.f.name)
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in rows:
-            r = [x.strip() for x in r]
-            try:
-                sm.append(float(r[1]))
-                smax = float(r[2])
-            except (ValueError, IndexError):
-                continue
-            for name, v in zip(names, r[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(name)
-        return dict(sm_mhz=statistics.median(sm) if sm else None, sm_max_mhz=smax,
-                    reasons=sorted(reasons), samples=len(sm))
+        return parse_clock_samples(text)
+
+
+def parse_clock_samples(text: str) -> dict:
+    """Median SM clock, maximum SM clock and the throttle reasons seen in nvidia-smi CSV rows of
+    ClockSampler.FIELDS (index, clocks.sm, clocks.max.sm, power.draw, active mask, then the four
+    reasons as Active / Not Active)."""
+    sm, smax, reasons = [], None, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in text.strip().splitlines():
+        r = [x.strip() for x in line.split(",")]
+        try:
+            sm.append(float(r[1]))
+            smax = float(r[2])
+        except (ValueError, IndexError):
+            continue
+        for name, v in zip(names, r[5:9]):
+            if v.lower().startswith("active"):
+                reasons.add(name)
+    return dict(sm_mhz=statistics.median(sm) if sm else None, sm_max_mhz=smax,
+                reasons=sorted(reasons), samples=len(sm))
 
 
 # ---------------------------------------------------------------------------------------------
