@@ -489,7 +489,7 @@ def c3_case(args):
         runs[name] = dict(value=float(out["level_time"].sum()), e2e=wall, Eg=out["Eg"],
                           levels=int(out["nlevels"]), starting_level=int(out["starting_level"]),
                           level_M=[int(x) for x in out["level_M"]],
-                          inner_samples=float(out["total_work"]))
+                          inner_samples=float(out["total_work"]), calls=int(out["calls"]))
         if prec == nm.PREC_FP32:
             runs[name]["phase_config"] = phase_choices(s, int(out["nlevels"]))
     clk = cs.stop()
@@ -540,7 +540,12 @@ def c3_case(args):
                        "adaptive_r": 1.5, "eps": eps, "K": K,
                        "eps_note": ("below 5e-4 the FP64 drop-in is timed per level on bounded samples and "
                                     "scaled by the FP32 run's level counts (extrapolated)")},
-            "e2e": {"value": a["e2e"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": None},
+            "e2e": {"value": a["e2e"], "unit": "s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": a["calls"] * (16 * 8 + 2 * 8),
+                    "h2d_note": "the portfolio's option records and alias table are uploaded by "
+                                "set_portfolio before the timed run and stay resident; each round's "
+                                "level counts travel as kernel arguments",
+                    "d2h_note": "per sampled level: 16 FP64 sums and two device clock stamps"},
             "runs": runs, "p_direct": p_direct, "p_direct_sd": sd,
             "speedup_vs_fp64_dropin": {"value": b["value"] / a["value"],
                                        "e2e": (b["e2e"] / a["e2e"]) if b.get("e2e") else None},
@@ -681,7 +686,10 @@ def main():
             "config": dict(WORKLOAD, parallelism=f"outer-sample shards x{world}",
                            phase_config=phase_choices(s, int(ref["nlevels"]))),
             "e2e": {"value": wall_t, "unit": "s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": int(calls / len(outs) * 16 * 8)},
+                    "d2h_bytes_per_step": int(calls / len(outs) * (16 * 8 + 2 * 8)),
+                    "h2d_note": "no input arrays: tau, K and each round's level counts travel as kernel "
+                                "arguments of the round's graph",
+                    "d2h_note": "per sampled level: 16 FP64 sums and two device clock stamps"},
             "roofline": roof, "clocks": clk, "gpu_launches": int(launches),
             "inner_samples_per_step": inner / len(outs),
             "inner_samples_per_s": inner / sum(dev_times),
