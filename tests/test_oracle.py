@@ -222,3 +222,43 @@ def test_alias_draw_distribution():
         idx[t] = col if coin < int(thr[col]) else int(al[col])
     freq = np.bincount(idx, minlength=P) / n
     assert np.all(np.abs(freq - ph) <= 4 * np.sqrt(ph * (1 - ph) / n)), (freq, ph)
+
+
+# cores, N0, beta, adaptive r, antithetic, model kind, tau, K, levels, M per call: the sampler's
+# parameters and edge sizes (M = 1, M below the core count so some cores get no outer sample,
+# non-adaptive r = 0, r close to 2, beta = 4, odd core counts, no antithetic estimator)
+LIVE_GRID = [
+    (1, 32, 2, 0.0, True, O.MODEL_SHIFT, 0.0, 1.0, (0, 2, 4), 17),
+    (3, 16, 2, 1.5, False, O.MODEL_SHIFT, 0.0, 0.7, (0, 1, 3), 11),
+    (4, 32, 4, 1.5, True, O.MODEL_REFERENCE, 0.02, 0.09, (0, 1, 2), 9),
+    (5, 64, 2, 1.9, True, O.MODEL_SHIFT, 0.0, 0.0, (0, 5), 3),
+    (2, 32, 2, 1.5, True, O.MODEL_SHIFT, 0.0, 1.0, (6, 1), 1),
+    (7, 32, 2, 1.5, True, O.MODEL_REFERENCE, 0.1, 0.2, (3, 0, 3), 20),
+    (6, 32, 2, 1.5, True, O.MODEL_SHIFT, 0.0, 0.3, (2, 4), 300),
+]
+
+
+@pytest.mark.parametrize("variant,prec", [("f32_lzcnt", O.PREC_REF32), ("f64_lzcnt", O.PREC_FP64)])
+@pytest.mark.parametrize("case", range(len(LIVE_GRID)))
+def test_live_reference_parameter_grid(variant, prec, case):
+    """Where the reference is compiled here: every event, level sum and inner statistic of the
+    oracle equals the reference's over a grid of sampler parameters, including calls that leave
+    cores without outer samples and repeated levels (streams persist across calls)."""
+    if not O.ref_available(variant):
+        pytest.skip("oracle/_ref not built on this host")
+    cores, N0, beta, r, anti, kind, tau, K, ells, M = LIVE_GRID[case]
+    seed = 1000 + case
+    ref = O.Reference(variant)
+    ref.init(cores, N0, beta, r, anti)
+    ref.model_init(kind, tau, K, seed, traced=True)
+    s = O.Sampler(prec, O.STREAMS_CORE, cores, N0, beta, r, anti, False, seed)
+    s.set_model(kind, tau, K)
+    for ell in ells:
+        a = ref.sample(ell, M, events_cap=2_000_000)
+        b = s.sample(ell, M, events_cap=2_000_000)
+        assert a["events"][0] == b["events"][0], (case, ell)
+        np.testing.assert_array_equal(a["events"][1], b["events"][1])
+        np.testing.assert_array_equal(a["fsums"], b["fsums"])
+        np.testing.assert_array_equal(a["diffsums"], b["diffsums"])
+        np.testing.assert_array_equal(a["stats"], b["stats"])
+        assert a["work"] == b["work"]
