@@ -262,3 +262,44 @@ def test_live_reference_parameter_grid(variant, prec, case):
         np.testing.assert_array_equal(a["diffsums"], b["diffsums"])
         np.testing.assert_array_equal(a["stats"], b["stats"])
         assert a["work"] == b["work"]
+
+
+# portfolio (BS options): Q stocks, P options, generator seed, option weights, sub-sampling, delta
+# CV, correlation, K, cores, N0, beta, r, levels, M per call
+LIVE_PF_GRID = [
+    (1, 7, 31, "uniform", O.SUB_UNIFORM, False, 0.0, 0.05, 2, 32, 2, 1.5, (0, 3, 1), 5),
+    (6, 90, 32, "w", O.SUB_RANDOM, True, 0.5, 0.2, 5, 32, 4, 1.5, (0, 2), 3),
+    (2, 9, 33, "w", O.SUB_NONE, True, 0.9, 0.3, 3, 16, 2, 0.0, (1, 2), 8),
+    (3, 40, 34, "uniform", O.SUB_RANDOM, False, 0.1, 0.15, 4, 64, 2, 1.9, (0, 1, 2, 1), 13),
+]
+
+
+@pytest.mark.parametrize("variant,prec", [("f32_lzcnt", O.PREC_REF32), ("f64_lzcnt", O.PREC_FP64)])
+@pytest.mark.parametrize("case", range(len(LIVE_PF_GRID)))
+def test_live_reference_portfolio_grid(variant, prec, case):
+    """Where the reference is compiled here: option start values, delta estimates and every
+    event and level sum of the portfolio sampler equal the reference's over a grid of portfolio
+    shapes, sub-sampling modes, delta CV, correlations and call sizes."""
+    if not O.ref_available(variant):
+        pytest.skip("oracle/_ref not built on this host")
+    Q, P, g, prob, sub, cv, rho, K, cores, N0, beta, r, ells, M = LIVE_PF_GRID[case]
+    pf = O.synthetic_portfolio(Q, P, g, prob=prob)
+    seed = 2000 + case
+    ref = O.Reference(variant)
+    ref.init(cores, N0, beta, r, True)
+    st_r, de_r = ref.portfolio_init(pf, r=0.05, rho=rho, max_loss=K, tau=1 / 52, subsample=sub,
+                                    use_delta_cv=cv, seed=seed, traced=True)
+    s = O.Sampler(prec, O.STREAMS_CORE, cores, N0, beta, r, True, False, seed)
+    st_o, de_o = s.set_portfolio(pf, r=0.05, rho=rho, max_loss=K, tau=1 / 52, subsample=sub,
+                                 use_delta_cv=cv)
+    np.testing.assert_array_equal(st_o, st_r)
+    np.testing.assert_array_equal(de_o, de_r)
+    for ell in ells:
+        a = ref.sample(ell, M, events_cap=2_000_000)
+        b = s.sample(ell, M, events_cap=2_000_000)
+        assert a["events"][0] == b["events"][0], (case, ell)
+        np.testing.assert_array_equal(a["events"][1], b["events"][1])
+        np.testing.assert_array_equal(a["events"][2], b["events"][2])
+        np.testing.assert_array_equal(a["fsums"], b["fsums"])
+        np.testing.assert_array_equal(a["diffsums"], b["diffsums"])
+        np.testing.assert_array_equal(a["stats"], b["stats"])
