@@ -66,3 +66,28 @@ def test_no_device_is_an_error_not_a_fallback(nm):
         pytest.skip("host has a GPU")
     with pytest.raises(nm.NmlmcError):
         nm.Sampler()
+
+
+def test_plain_c_caller_builds_links_and_runs(nm, tmp_path):
+    """The header is plain C (C99, -pedantic, no C++ or torch types): a C caller compiles, links
+    against libnmlmc.so and calls the functions that need no device."""
+    src = tmp_path / "caller.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <string.h>\n#include "nmlmc.h"\n'
+        "int main(void) {\n"
+        "    nmlmc_mlmc_input in = nmlmc_mlmc_default_input();\n"
+        "    if (nmlmc_version() <= 0) return 2;\n"
+        "    if (strlen(nmlmc_error_string(NMLMC_ERR_ARG)) == 0) return 3;\n"
+        "    printf(\"%d %g %u\\n\", nmlmc_version(), in.targetTOL, (unsigned)in.M0);\n"
+        "    return 0;\n}\n")
+    exe = tmp_path / "caller"
+    libdir = os.path.dirname(nm.LIB_PATH)
+    cc = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror",
+                         f"-I{os.path.join(ROOT, 'include')}", str(src), "-o", str(exe),
+                         f"-L{libdir}", "-lnmlmc", f"-Wl,-rpath,{libdir}"],
+                        capture_output=True, text=True)
+    assert cc.returncode == 0, cc.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert run.returncode == 0, run.stderr
+    v, tol, m0 = run.stdout.split()
+    assert int(v) == nm.lib().nmlmc_version()
