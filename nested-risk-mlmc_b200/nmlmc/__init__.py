@@ -547,8 +547,19 @@ def mlmc_run_cb(sample_level, sample_levels=None, *, targetTOL=1e-3, M0=100, ver
     given) takes all levels of a round at once.  A sampler that fails leaves the result's M
     at 0 and the driver stops with an error.  With `checkpoint` (a path) the driver writes its
     state after every TOL iteration, `resume` continues from it, and `state` = (save, load)
-    stores the sampler's own state in the file: save() -> bytes, load(bytes)."""
+    stores the sampler's own state in the file: save() -> bytes, load(bytes).  An exception
+    raised by a callback stops the run; it is re-raised as NmlmcError (status of the driver) with
+    the callback's exception as its cause."""
     L = lib()
+    failures = []              # exceptions raised inside the ctypes callbacks, first one first
+
+    def finish(rc, what):
+        if failures:
+            e = failures[0]
+            if rc == OK:
+                raise e
+            raise NmlmcError(rc, f"{what}: a callback raised {type(e).__name__}: {e}") from e
+        _check(rc, what)
 
     def fill(res, d, M):
         for j in range(4):
@@ -561,7 +572,8 @@ def mlmc_run_cb(sample_level, sample_levels=None, *, targetTOL=1e-3, M0=100, ver
     def _one(user, ell, M, out):
         try:
             fill(out.contents, sample_level(int(ell), int(M)), int(M))
-        except Exception:          # a failed sampler: M stays 0 and the driver stops
+        except Exception as e:     # a failed sampler: M stays 0 and the driver stops
+            failures.append(e)
             out.contents.M = 0
 
     def _many(user, n, ells, Ms, outs):
@@ -571,7 +583,8 @@ def mlmc_run_cb(sample_level, sample_levels=None, *, targetTOL=1e-3, M0=100, ver
             rs = sample_levels(el, ms) if sample_levels else [sample_level(e, m) for e, m in zip(el, ms)]
             for i in range(n):
                 fill(outs[i], rs[i], ms[i])
-        except Exception:
+        except Exception as e:
+            failures.append(e)
             for i in range(n):
                 outs[i].M = 0
 
@@ -584,7 +597,7 @@ def mlmc_run_cb(sample_level, sample_levels=None, *, targetTOL=1e-3, M0=100, ver
     out = MlmcOutput()
     buf = ctypes.create_string_buffer(1 << 16)
     if checkpoint is None:
-        _check(L.nmlmc_mlmc_run_cb(ctypes.byref(inp), f1, f2, None, ctypes.byref(out), buf, len(buf)),
+        finish(L.nmlmc_mlmc_run_cb(ctypes.byref(inp), f1, f2, None, ctypes.byref(out), buf, len(buf)),
                "nmlmc_mlmc_run_cb")
         return mlmc_output_dict(out, buf.value.decode())
 
@@ -596,20 +609,22 @@ def mlmc_run_cb(sample_level, sample_levels=None, *, targetTOL=1e-3, M0=100, ver
                     return ctypes.c_size_t(-1).value
                 ctypes.memmove(p, b, len(b))
             return len(b)
-        except Exception:          # the run stops with NMLMC_ERR_STATE
+        except Exception as e:     # the run stops with NMLMC_ERR_STATE
+            failures.append(e)
             return ctypes.c_size_t(-1).value
 
     def _load(user, p, n):
         try:
             state[1](ctypes.string_at(p, n))
             return OK
-        except Exception:
+        except Exception as e:
+            failures.append(e)
             return ERR_STATE
 
     fs = STATE_SAVE_FN(_save) if state else STATE_SAVE_FN()
     fl = STATE_LOAD_FN(_load) if state else STATE_LOAD_FN()
     io = CheckpointIO(os.fsencode(checkpoint), int(resume), fs, fl)
-    _check(L.nmlmc_mlmc_run_cb_ckpt(ctypes.byref(inp), f1, f2, None, ctypes.byref(io), ctypes.byref(out),
+    finish(L.nmlmc_mlmc_run_cb_ckpt(ctypes.byref(inp), f1, f2, None, ctypes.byref(io), ctypes.byref(out),
                                     buf, len(buf)), "nmlmc_mlmc_run_cb_ckpt")
     return mlmc_output_dict(out, buf.value.decode())
 

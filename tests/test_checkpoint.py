@@ -61,8 +61,9 @@ def test_resume_after_a_crash_equals_the_uninterrupted_run(nm, golden, tmp_path)
     path = str(tmp_path / "run.ckpt")
     fail_at = len(full_s.calls) * 2 // 3
     s1 = Failing(*sa, fail_at=fail_at)
-    with pytest.raises(nm.NmlmcError):
+    with pytest.raises(nm.NmlmcError, match="sampler lost") as e:
         nm.mlmc_run_cb(s1, targetTOL=kw["tol"], M0=kw["M0"], checkpoint=path, state=_state(s1))
+    assert isinstance(e.value.__cause__, RuntimeError)      # the sampler's own exception
     ck = nm.checkpoint.read_checkpoint(path)
     assert 0 < ck["itr_next"] < ck["total_itrs"] + 1 and ck["calls"] <= fail_at
     s2 = Synthetic(*sa)
@@ -137,9 +138,10 @@ def test_failing_state_hook_stops_the_run(nm, golden, tmp_path):
     def bad_save():
         raise RuntimeError("state unavailable")
 
-    with pytest.raises(nm.NmlmcError):
+    with pytest.raises(nm.NmlmcError, match="state unavailable") as e:
         nm.mlmc_run_cb(Synthetic(*sa), targetTOL=kw["tol"], M0=kw["M0"], checkpoint=str(tmp_path / "x.ckpt"),
                        state=(bad_save, lambda b: None))
+    assert e.value.status == nm.ERR_STATE and isinstance(e.value.__cause__, RuntimeError)
     assert not os.path.exists(str(tmp_path / "x.ckpt"))
 
 
