@@ -8,14 +8,16 @@ continuation MLMC to RMSE eps = 1e-4.  A step is one complete MLMC run (host dri
 sampler) to eps; synthetic inputs (the model problem has no data).
 
 Our arm: the batched FP32 sampler (OUTER streams, Kahan FP32 inner sums, FP64 moments), all levels
-of an MLMC round in one submission.  Reported next to it, on the same GPU and seed:
+of an MLMC round in one submission (one CUDA graph per round).  Reported next to it, on the same GPU and seed:
   * the all-FP64 run of the same sampler on the same streams (accuracy and speed),
   * the plain FP64 drop-in: the reference's stream semantics (a warp per virtual core, 2048
     cores like the reference's CUDA main), one synchronous launch per sample_level call.
 
-`value` is the device time of the run's kernels (CUDA events around every level call); `e2e` is
-the wall time of the whole run through the C ABI (host driver decisions, launches, the
-device->host copy of every level result).  Multi-GPU (torchrun): every rank samples its share of
+`value` is the device time of the run's levels (%globaltimer stamps written at the level
+boundaries inside each round's CUDA graph); `e2e` is the wall time of the whole run through the
+C ABI (host driver decisions, graph updates and launches, the device->host copy of every level
+result).  The phase kernel's roofline comes from a profiled repeat of the timed runs with CUDA
+events around every phase-kernel launch.  Multi-GPU (torchrun): every rank samples its share of
 each level call and the level results are all-reduced (16 doubles), so the estimate equals the
 single-GPU one and total work is fixed (strong scaling).
 
