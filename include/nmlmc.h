@@ -163,7 +163,8 @@ typedef struct nmlmc_level_result {
     double total_work;
     uint64_t M;
     uint64_t inner_stats[6];   /* inner samples, decisions, hit max, hit base, #randu, #randn */
-    double seconds;            /* device time of the call (CUDA events)                         */
+    double seconds;            /* device time of the level: CUDA events around a single call;
+                                  inside a round's graph, %globaltimer stamps at its boundaries */
 } nmlmc_level_result;
 
 typedef struct nmlmc_portfolio {
