@@ -531,7 +531,10 @@ def c3_case(args):
             "peak_source": "issue-slot peak 148 SM x 128 lanes x sampled SM clock",
             "timing": "CUDA events around each phase-kernel launch of one call per active level "
                       "(<= 8192 outer samples) after the timed runs",
-            "note": "latency-bound: dependent option-table gathers and the per-sample arithmetic chain"}
+            "note": "latency-bound: dependent option-table gathers and the per-sample arithmetic chain",
+            "traffic_note": "DRAM bytes per level-10 pilot launch of 8192 outer samples (ncu): 46-47 MB "
+                            "read, 1.0-1.2 MB written: the 40 MB option and alias tables once from "
+                            "DRAM, then L2-resident, so no HBM roofline applies"}
     a, b = runs["fp32_batched"], runs["fp64_dropin"]
     line = {"metric": f"time-to-eps (s) for MLMC P(L>K), large portfolio, eps={eps:g} absolute",
             "value": a["value"], "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 1,
