@@ -91,3 +91,19 @@ def test_plain_c_caller_builds_links_and_runs(nm, tmp_path):
     assert run.returncode == 0, run.stderr
     v, tol, m0 = run.stdout.split()
     assert int(v) == nm.lib().nmlmc_version()
+
+
+def test_null_arguments_are_errors_not_crashes(nm, tmp_path):
+    """Each native entry point given a NULL context or NULL required pointers returns a status
+    other than NMLMC_OK and does not crash (tests/abi/null_arguments.c)."""
+    exe = tmp_path / "null_arguments"
+    libdir = os.path.dirname(nm.LIB_PATH)
+    cc = subprocess.run(["gcc", "-std=c99", "-Wall", f"-I{os.path.join(ROOT, 'include')}",
+                         os.path.join(ROOT, "tests", "abi", "null_arguments.c"), "-o", str(exe),
+                         f"-L{libdir}", "-lnmlmc", f"-Wl,-rpath,{libdir}"],
+                        capture_output=True, text=True)
+    assert cc.returncode == 0, cc.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120, cwd=tmp_path)
+    assert run.returncode == 0, run.stdout + run.stderr
+    assert "ok-calls 0" in run.stdout
+    assert not (tmp_path / "x.ckpt").exists()
