@@ -107,3 +107,19 @@ def test_null_arguments_are_errors_not_crashes(nm, tmp_path):
     assert run.returncode == 0, run.stdout + run.stderr
     assert "ok-calls 0" in run.stdout
     assert not (tmp_path / "x.ckpt").exists()
+
+
+def test_reference_surface_out_of_order_is_recorded(nm, tmp_path):
+    """The reference-named entry points, called before init or with NULL arguments, record an
+    error (nmlmc_last_error) and return; the reference would exit() or crash there."""
+    exe = tmp_path / "reference_surface_order"
+    libdir = os.path.dirname(nm.LIB_PATH)
+    cc = subprocess.run(["gcc", "-std=c99", "-Wall", f"-I{os.path.join(ROOT, 'include')}",
+                         os.path.join(ROOT, "tests", "abi", "reference_surface_order.c"), "-o", str(exe),
+                         f"-L{libdir}", "-lnmlmc", f"-Wl,-rpath,{libdir}"],
+                        capture_output=True, text=True)
+    assert cc.returncode == 0, cc.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120, cwd=tmp_path)
+    assert run.returncode == 0, run.stdout + run.stderr
+    assert "ok-calls 0" in run.stdout
+    assert "failed" in run.stderr            # each error is also printed, as the reference prints
