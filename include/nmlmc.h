@@ -129,6 +129,16 @@ void portfolio_init(const portfolio_data* data, uint64_t seed);
 void portfolio_sample(uint32_t ell, uint64_t override_dyn_inner, uint64_t M, sample_output* out);
 void portfolio_cleanup(void);
 void portfolio_comp_params(portfolio_data* data);
+/* portfolio_gen_data / portfolio_free_data (portfolio_sampler.cpp:784-912): the reference demo
+ * main's portfolio, with the reference's values for the same arguments.  Q stocks, P >= 2Q
+ * options; options[m] gets floor(probs[m] * P) of them (m = BS, Exact, Unbiased; the three
+ * must add up to P), delta-hedged per stock, weights normalised to sum 1, prob = |w| (1 with
+ * uniform_prob), each method sorted by decreasing prob.  uniform_weights starts every weight at
+ * 1.  The arrays belong to the library until portfolio_free_data; invalid arguments return a
+ * zeroed portfolio_data and set nmlmc_last_error(). */
+portfolio_data portfolio_gen_data(uint32_t P, uint32_t Q, uint64_t seed, double* probs,
+                                  bool uniform_weights, bool uniform_prob);
+void portfolio_free_data(portfolio_data* data);
 
 /* norm_cdf_inv (common.cpp:53-86). */
 float norm_cdf_inv(float p);

@@ -1610,6 +1610,13 @@ static void ref_fail(int rc, const char* fn) {
 
 int nmlmc_last_error(void) { return g_last; }
 
+// Records the status of a reference-named call implemented in another translation unit
+// (portfolio_gen_data / portfolio_free_data in nmlmc_portfolio.cpp).  Not part of the ABI.
+__attribute__((visibility("hidden"))) void nmlmc_ref_status(int rc, const char* fn) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    ref_fail(rc, fn);
+}
+
 int nmlmc_default_set_precision(int32_t precision, int32_t streams) {
     if (precision < NMLMC_PREC_REF32 || precision > NMLMC_PREC_FP32) return NMLMC_ERR_ARG;
     if (streams != NMLMC_STREAMS_CORE && streams != NMLMC_STREAMS_OUTER) return NMLMC_ERR_ARG;

@@ -5,13 +5,22 @@
 // U[lo, hi], position ~ N(0, 1)).  Every random field is drawn from a counter-based Threefry2x64-20
 // stream — value(field f, index i) = Threefry(ctr = (i, f), key = (seed, 'PORTGEN')) — so a
 // portfolio is a pure function of (spec, seed), independent of platform, thread count and
-// generation order.  The reference's own generator (portfolio_gen_data, portfolio_sampler.cpp:
-// 784-904, mt19937 with a delta hedge and renormalised weights) builds a different, smaller
-// portfolio for its demo main and is not reproduced.
+// generation order.
+//
+// The reference's own demo generator, portfolio_gen_data / portfolio_free_data
+// (portfolio_sampler.cpp:784-912), is part of its extern "C" surface and is provided below with
+// the same outputs (same seeds, same libstdc++ random engines and distributions, same delta hedge,
+// normalisation and per-method sort), so the reference's portfolio main runs unchanged against
+// this library.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <random>
+#include <vector>
 
 #include "../../include/nmlmc.h"
+
+extern "C" void nmlmc_ref_status(int rc, const char* fn);   // nmlmc_api.cu
 
 namespace {
 
@@ -82,4 +91,152 @@ extern "C" int nmlmc_portfolio_generate(const nmlmc_portfolio_spec* sp, uint64_t
         w[i] = g.normal(F_WEIGHT, i);
     }
     return NMLMC_OK;
+}
+
+// ---- the reference's demo generator (portfolio_sampler.cpp:784-912) -------------------------
+//
+// Steps that decide the values, in the reference's order:
+//  * one std::mt19937 seeded with `seed`; every field is drawn from a fresh copy of that seeded
+//    engine (the reference hands the engine to std::bind by value, so each field restarts from
+//    the same state): S0 ~ U(90, 110), sigma ~ U(0.01, 0.4), mu ~ U(0.03, 0.3), type ~ U{0, 1},
+//    stock ~ U{0, Q-1}, maturity ~ U(1, 5), strike ~ U(80, 120), weight ~ N(0, 1), all real_t =
+//    float;
+//  * options i < Q and Q + i are a call and a put on stock i (so P >= 2Q);
+//  * options[m] takes the next floor(probs[m] * P) options (m = BS, Exact, Unbiased), which must
+//    add up to P;
+//  * start / delta_est from portfolio_comp_params; the calls' weights on each stock are scaled
+//    by -(sum of put delta * w) / (sum of call delta * w) (a delta hedge, sums in double), then
+//    every weight is divided by the sum of all weights;
+//  * prob = |w| / sqrt(W_est) (or 1 with uniform_prob), W_est = 1, and each method's options are
+//    sorted by decreasing prob with std::sort.
+// Two reference behaviours are not carried over: with uniform_weights the reference leaves every
+// weight at 0 (so the normalisation divides 0 by 0) where its caller documents weights of 1, and
+// the reference's W_est update of the Unbiased options changes a copy (so W_est stays 1, as here).
+extern "C" portfolio_data portfolio_gen_data(uint32_t P, uint32_t Q, uint64_t seed, double* probs,
+                                             bool uniform_weights, bool uniform_prob) {
+    portfolio_data d{};
+    if (!probs || Q == 0 || (uint64_t)P < 2ull * Q) {
+        nmlmc_ref_status(NMLMC_ERR_ARG, "portfolio_gen_data");
+        return d;
+    }
+    uint32_t count[3];
+    uint64_t total = 0;
+    for (int m = 0; m < 3; m++) {
+        if (!(probs[m] >= 0)) {
+            nmlmc_ref_status(NMLMC_ERR_ARG, "portfolio_gen_data");
+            return d;
+        }
+        count[m] = (uint32_t)(probs[m] * P);
+        total += count[m];
+    }
+    if (total != P) {                         // the reference asserts this
+        nmlmc_ref_status(NMLMC_ERR_ARG, "portfolio_gen_data");
+        return d;
+    }
+    d.r = 0.05f;
+    d.rho = 0.2f;
+    d.s1_rho2 = std::sqrt(1 - d.rho * d.rho);
+    d.max_loss = 0.7f;
+    d.tau = 0.02f;
+    d.dt_h0inv = 8;
+    d.dt_beta = 4;
+    d.dt_prob_expo = -1.5f;
+    d.phi_type = 0;                           // Indicator
+    d._phi_size = 1;
+    d.subsample = NMLMC_SUB_NONE;
+    d.use_delta_cv = true;
+    d.use_coarse_delta_cv = false;
+    d.use_antithetic_risk = true;
+    d.use_milstein = true;
+
+    const std::mt19937 engine(seed);
+    auto draw = [&engine](auto& out, auto dist) {
+        std::mt19937 g = engine;              // each field from the seeded state
+        for (auto& x : out) x = dist(g);
+    };
+    using uni = std::uniform_real_distribution<float>;
+    using unii = std::uniform_int_distribution<uint32_t>;
+    std::vector<float> S0(Q), sigma(Q), mu(Q), maturity(P, 1.f), strike(P), weight(P, 1.f);
+    std::vector<uint32_t> type(P), stock(P);
+    draw(S0, uni(90, 110));
+    draw(sigma, uni(0.01, 0.4));
+    draw(mu, uni(0.03, 0.3));
+    draw(type, unii(0, 1));
+    draw(stock, unii(0, Q - 1));
+    draw(maturity, uni(1, 5));
+    draw(strike, uni(80, 120));
+    if (!uniform_weights) draw(weight, std::normal_distribution<float>(0, 1));
+
+    option_params* ops = new option_params[P]();
+    stock_params* stocks = new stock_params[Q]();
+    for (uint32_t i = 0; i < Q; i++) {
+        type[i] = 0;
+        type[Q + i] = 1;
+        stock[i] = stock[Q + i] = i;
+        stocks[i].S0 = S0[i];
+        stocks[i].mu = mu[i];
+        stocks[i].sigma = sigma[i];
+    }
+    for (uint32_t i = 0; i < P; i++) {
+        ops[i].w = weight[i];
+        ops[i].strike = strike[i];
+        ops[i].type = type[i] ? -1 : 1;       // 1: put, 0: call
+        ops[i].maturity = maturity[i];
+        ops[i].stock_ind = stock[i];
+        ops[i].prob = -1;
+        ops[i].W_est = 1;
+    }
+    d.stocks.data = stocks;
+    d.stocks.size = Q;
+    uint32_t off = 0;
+    for (int m = 0; m < 3; m++) {
+        d.options[m].data = ops + off;
+        d.options[m].size = count[m];
+        off += count[m];
+    }
+    portfolio_comp_params(&d);
+
+    std::vector<double> call_dw(Q, 0.0), put_dw(Q, 0.0);
+    for (int m = 0; m < 3; m++)
+        for (size_t j = 0; j < d.options[m].size; j++) {
+            const option_params& op = d.options[m].data[j];
+            const double dw = op.delta_est * op.w;
+            (op.type > 0 ? call_dw : put_dw)[op.stock_ind] += dw;
+        }
+    double wsum = 0;
+    for (int m = 0; m < 3; m++)
+        for (size_t j = 0; j < d.options[m].size; j++) {
+            option_params& op = d.options[m].data[j];
+            if (op.type > 0) op.w *= -put_dw[op.stock_ind] / call_dw[op.stock_ind];
+            wsum += op.w;
+        }
+    for (int m = 0; m < 3; m++) {
+        option_params* b = d.options[m].data;
+        for (size_t j = 0; j < d.options[m].size; j++) {
+            b[j].w /= wsum;
+            b[j].prob = uniform_prob ? 1.f : std::abs(b[j].w) / std::sqrt(b[j].W_est);
+        }
+        std::sort(b, b + d.options[m].size,
+                  [](const option_params& x, const option_params& y) { return x.prob > y.prob; });
+    }
+    nmlmc_ref_status(NMLMC_OK, "portfolio_gen_data");
+    return d;
+}
+
+// Frees what portfolio_gen_data allocated (portfolio_sampler.cpp:906-912): the stock array and
+// the option array, which starts at options[0].
+extern "C" void portfolio_free_data(portfolio_data* d) {
+    if (!d) {
+        nmlmc_ref_status(NMLMC_ERR_ARG, "portfolio_free_data");
+        return;
+    }
+    delete[] d->stocks.data;
+    delete[] d->options[0].data;
+    d->stocks.data = nullptr;
+    d->stocks.size = 0;
+    for (int m = 0; m < 3; m++) {
+        d->options[m].data = nullptr;
+        d->options[m].size = 0;
+    }
+    nmlmc_ref_status(NMLMC_OK, "portfolio_free_data");
 }

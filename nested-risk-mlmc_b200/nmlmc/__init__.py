@@ -213,7 +213,8 @@ _lib = None
 EXPORTS = [
     "init_nestedmc_sampler", "cleanup_nestedmc_sampler", "model_update_data", "model_init",
     "model_sample", "portfolio_update_data", "portfolio_init", "portfolio_sample",
-    "portfolio_cleanup", "portfolio_comp_params", "norm_cdf_inv", "nmlmc_last_error",
+    "portfolio_cleanup", "portfolio_comp_params", "portfolio_gen_data", "portfolio_free_data",
+    "norm_cdf_inv", "nmlmc_last_error",
     "nmlmc_default_set_precision", "nmlmc_error_string", "nmlmc_version", "nmlmc_create",
     "nmlmc_destroy", "nmlmc_configure", "nmlmc_set_model", "nmlmc_set_portfolio",
     "nmlmc_reset_streams", "nmlmc_sample", "nmlmc_sample_levels", "nmlmc_set_trace",

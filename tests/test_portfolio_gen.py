@@ -1,0 +1,86 @@
+"""The reference demo main's portfolio generator (portfolio_gen_data / portfolio_free_data,
+portfolio_sampler.cpp:784-912) through libnmlmc.so: byte-identical to the compiled reference for
+the same arguments (host code, no device needed), and its argument checks."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+OPTION_FIELDS = ("strike", "maturity", "start", "w", "delta_est", "stock_ind", "type", "prob", "W_est")
+SCALARS = ("r", "rho", "s1_rho2", "max_loss", "tau", "dt_h0inv", "dt_beta", "dt_prob_expo",
+           "phi_type", "_phi_size", "subsample", "use_delta_cv", "use_coarse_delta_cv",
+           "use_antithetic_risk", "use_milstein")
+
+
+def _bind(nm, L):
+    L.portfolio_gen_data.restype = nm.PortfolioData
+    L.portfolio_gen_data.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64,
+                                     ctypes.POINTER(ctypes.c_double), ctypes.c_bool, ctypes.c_bool]
+    L.portfolio_free_data.restype = None
+    L.portfolio_free_data.argtypes = [ctypes.POINTER(nm.PortfolioData)]
+    return L
+
+
+def _dump(d):
+    """Scalars and every option / stock record as raw bytes (bit-exact comparison)."""
+    out = {k: getattr(d, k) for k in SCALARS}
+    for m in range(3):
+        n = d.options[m].size
+        out[f"options{m}"] = ctypes.string_at(d.options[m].data, n * ctypes.sizeof(d.options[m].data._type_)) if n else b""
+        out[f"n{m}"] = n
+    out["stocks"] = ctypes.string_at(d.stocks.data, d.stocks.size * 12)
+    return out
+
+
+CASES = [   # P, Q, seed, probs, uniform_weights, uniform_prob
+    (100, 10, 0, (1.0, 0.0, 0.0), False, False),
+    (1000, 20, 42, (0.3, 0.5, 0.2), False, False),     # the reference main's method fractions
+    (64, 32, 7, (0.5, 0.25, 0.25), False, True),
+    (500, 3, 2**40 + 5, (0.2, 0.2, 0.6), False, False),
+]
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+def test_generator_matches_the_reference(nm, case):
+    if not O.ref_available("f32"):
+        pytest.skip("oracle/_ref not built on this host")
+    P, Q, seed, probs, uw, up = CASES[case]
+    pr = (ctypes.c_double * 3)(*probs)
+    ours = _bind(nm, nm.lib())
+    ref = _bind(nm, ctypes.CDLL(os.path.join(O.REF_DIR, "libref_f32.so")))
+    a = ours.portfolio_gen_data(P, Q, seed, pr, uw, up)
+    assert nm.lib().nmlmc_last_error() == nm.OK
+    b = ref.portfolio_gen_data(P, Q, seed, pr, uw, up)
+    da, db = _dump(a), _dump(b)
+    for k in SCALARS:
+        assert da[k] == db[k], k
+    assert da["stocks"] == db["stocks"]
+    for m in range(3):
+        assert da[f"n{m}"] == db[f"n{m}"]
+        assert da[f"options{m}"] == db[f"options{m}"], f"method {m}"
+    w = np.array([a.options[m].data[j].w for m in range(3) for j in range(a.options[m].size)])
+    assert np.isfinite(w).all() and abs(w.sum() - 1) < 1e-4
+    ours.portfolio_free_data(ctypes.byref(a))
+    ref.portfolio_free_data(ctypes.byref(b))
+    assert not a.stocks.data and a.options[0].size == 0
+
+
+def test_generator_arguments(nm):
+    L = _bind(nm, nm.lib())
+    pr = (ctypes.c_double * 3)(0.5, 0.5, 0.0)
+    d = L.portfolio_gen_data(10, 6, 1, pr, False, False)        # P < 2Q
+    assert nm.lib().nmlmc_last_error() == nm.ERR_ARG and not d.stocks.data
+    d = L.portfolio_gen_data(10, 2, 1, (ctypes.c_double * 3)(0.3, 0.3, 0.3), False, False)   # 9 != 10
+    assert nm.lib().nmlmc_last_error() == nm.ERR_ARG and not d.stocks.data
+    d = L.portfolio_gen_data(10, 2, 1, None, False, False)
+    assert nm.lib().nmlmc_last_error() == nm.ERR_ARG
+    d = L.portfolio_gen_data(40, 4, 3, pr, True, False)          # weights start at 1
+    assert nm.lib().nmlmc_last_error() == nm.OK
+    w = np.array([d.options[m].data[j].w for m in range(3) for j in range(d.options[m].size)])
+    assert np.isfinite(w).all() and abs(w.sum() - 1) < 1e-5
+    L.portfolio_free_data(ctypes.byref(d))
+    L.portfolio_free_data(None)
+    assert nm.lib().nmlmc_last_error() == nm.ERR_ARG
