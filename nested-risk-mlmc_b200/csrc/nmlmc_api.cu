@@ -1602,6 +1602,9 @@ static nmlmc_ctx* g_ctx = nullptr;
 static int32_t g_default_prec = NMLMC_PREC_REF32, g_default_streams = NMLMC_STREAMS_CORE;
 static int g_last = NMLMC_OK;
 static std::mutex g_mu;
+// moments the caller's sample_output arrays hold (nested_sampler_params fine/diff_moments):
+// the reference copies exactly that many sums back (nested_sampler.hpp:571)
+static uint32_t g_fine_moments = 4, g_diff_moments = 4;
 
 static void ref_fail(int rc, const char* fn) {
     g_last = rc;
@@ -1634,6 +1637,8 @@ void init_nestedmc_sampler(uint32_t cores, const nested_sampler_params* params) 
         int rc = nmlmc_create(&g_ctx, 0);
         if (rc) return ref_fail(rc, "init_nestedmc_sampler");
     }
+    g_fine_moments = params->fine_moments;
+    g_diff_moments = params->diff_moments;
     nmlmc_config k{};
     k.cores = cores;
     k.N0 = params->N0;
@@ -1674,9 +1679,8 @@ void model_init(const model_data* d, uint64_t seed) {
 
 static void fill_sample_output(const nmlmc_level_result& r, sample_output* out) {
     out->M = r.M;
-    const uint32_t fm = 4, dm = 4;
-    if (out->fsums) for (uint32_t j = 0; j < fm; j++) out->fsums[j] = r.fsums[j];
-    if (out->diffsums) for (uint32_t j = 0; j < dm; j++) out->diffsums[j] = r.diffsums[j];
+    if (out->fsums) for (uint32_t j = 0; j < g_fine_moments; j++) out->fsums[j] = r.fsums[j];
+    if (out->diffsums) for (uint32_t j = 0; j < g_diff_moments; j++) out->diffsums[j] = r.diffsums[j];
     out->total_work = r.total_work;
     memcpy(out->inner_stats, r.inner_stats, sizeof(out->inner_stats));
 }

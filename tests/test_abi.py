@@ -123,3 +123,20 @@ def test_reference_surface_out_of_order_is_recorded(nm, tmp_path):
     assert run.returncode == 0, run.stdout + run.stderr
     assert "ok-calls 0" in run.stdout
     assert "failed" in run.stderr            # each error is also printed, as the reference prints
+
+
+def test_cpp_entry_points(nm, tmp_path):
+    """include/nmlmc.hpp: the driver's C++ interface (mlmc_real::run over a std::function level
+    sampler) takes the C driver's decisions and prints its table, a sampler exception leaves run()
+    unchanged, and sample<SAMPLER> before init is an error status (tests/abi/cpp_driver.cpp)."""
+    exe = tmp_path / "cpp_driver"
+    libdir = os.path.dirname(nm.LIB_PATH)
+    cc = subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror",
+                         f"-I{os.path.join(ROOT, 'include')}",
+                         os.path.join(ROOT, "tests", "abi", "cpp_driver.cpp"), "-o", str(exe),
+                         f"-L{libdir}", "-lnmlmc", f"-Wl,-rpath,{libdir}"],
+                        capture_output=True, text=True)
+    assert cc.returncode == 0, cc.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300, cwd=tmp_path)
+    assert run.returncode == 0, run.stdout[-2000:] + run.stderr[-2000:]
+    assert "ok-checks 0" in run.stdout
