@@ -1,7 +1,10 @@
 """Host logic of bench.py, without a GPU: the clock / throttle-reason parsing that decides whether
 a run's clocks are valid, the per-level extrapolation of the FP64 drop-in's time, and the report
-of the autotuner's per-level choices."""
+of the autotuner's per-level choices, and the reference arm's line."""
+import os
+
 import bench
+from conftest import ROOT
 
 
 def test_clock_samples_median_and_reasons():
@@ -49,3 +52,28 @@ def test_phase_choices_report():
         def phase_config(self, ell):
             return dict(variant=ell % 3, chunk=32, state=1 if ell < 2 else 0, probe_ms=1.0)
     assert bench.phase_choices(S(), 3) == {"0": [0, 32, True], "1": [1, 32, True], "2": [2, 32, False]}
+
+
+def test_reference_arm_line(tmp_path):
+    """`bench.py --impl reference` runs the reference's CPU level sampler (no GPU) and prints one
+    JSON line with the contract's keys; under torchrun only rank 0 prints."""
+    import json
+    import subprocess
+    import sys
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+           "--warmup", "3", "--ref-budget", "1"]
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=600, env=env)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for key in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+                "higher_is_better", "config", "cpu_baseline", "e2e"):
+        assert key in d, key
+    assert d["impl"] == "reference" and d["value"] > 0 and d["higher_is_better"] is False
+    assert d["cpu_baseline"]["kind"] in ("reference", "port") and d["cpu_baseline"]["cores"] >= 1
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
+    env1 = dict(env, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    out1 = subprocess.run(cmd, capture_output=True, text=True, timeout=600, env=env1)
+    assert out1.returncode == 0 and not out1.stdout.strip()
