@@ -222,7 +222,7 @@ class Sampler:
 
 
 # ------------------------------------------------------------------------------------------
-# The reference compiled here (oracle/_ref).  Present only where /root/reference was available
+# The reference compiled here (oracle/_ref).  Present only where the reference sources were available
 # at build time; callers skip when it is absent.
 def ref_available(variant: str = "f32") -> bool:
     return os.path.exists(os.path.join(REF_DIR, f"libref_{variant}.so"))

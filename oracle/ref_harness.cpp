@@ -9,7 +9,7 @@
 // What it adds on top of the reference:
 //   * ref_threefry / ref_stream_draws: raw Threefry2x64-20 blocks and random_state draws
 //     (Random123/threefry.h:190-286, par_omp.hpp:72-121).
-//   * baseline_model::sampler: the X = Y + Z model (Y ~ N(0,1), inner X = Y + Z, start = -K),
+//   * shift_model::sampler: the X = Y + Z model (Y ~ N(0,1), inner X = Y + Z, start = -K),
 //     plugged into the reference engine through the same SAMPLER concept as model::sampler
 //     (model_sampler.cpp:42-92).  The reference has no such model; the engine that drives it
 //     (nested_sampler.hpp:369-485, 646-694) is the reference's own.
@@ -59,7 +59,7 @@ public:
 
 // ---------------------------------------------------------------------------------------------
 // The X = Y + Z model of the nested-risk problem P(E[X|Y] > K).
-namespace baseline_model {
+namespace shift_model {
     struct data { real_t K; };
     static data g_data;
 
@@ -148,10 +148,10 @@ void ref_model_init(int kind, double tau, double max_loss, uint64_t seed, int tr
         if (traced_run) init_samplers<traced<model::sampler>>(seed, 0);
         else init_samplers<model::sampler>(seed, 0);
     } else {
-        baseline_model::g_data.K = (real_t)max_loss;
+        shift_model::g_data.K = (real_t)max_loss;
         PAR_SET_CONST(gc_phi_size, 1u);
-        if (traced_run) init_samplers<traced<baseline_model::sampler>>(seed, 0);
-        else init_samplers<baseline_model::sampler>(seed, 0);
+        if (traced_run) init_samplers<traced<shift_model::sampler>>(seed, 0);
+        else init_samplers<shift_model::sampler>(seed, 0);
     }
 }
 
@@ -160,8 +160,8 @@ static void run_sample(int which, uint32_t ell, uint64_t M, sample_output* out) 
     switch (which) {
     case 0: sample<model::sampler>(ell, 0, &out->M, out->fsums, out->diffsums, &out->total_work, out->inner_stats); break;
     case 1: sample<traced<model::sampler>>(ell, 0, &out->M, out->fsums, out->diffsums, &out->total_work, out->inner_stats); break;
-    case 2: sample<baseline_model::sampler>(ell, 0, &out->M, out->fsums, out->diffsums, &out->total_work, out->inner_stats); break;
-    case 3: sample<traced<baseline_model::sampler>>(ell, 0, &out->M, out->fsums, out->diffsums, &out->total_work, out->inner_stats); break;
+    case 2: sample<shift_model::sampler>(ell, 0, &out->M, out->fsums, out->diffsums, &out->total_work, out->inner_stats); break;
+    case 3: sample<traced<shift_model::sampler>>(ell, 0, &out->M, out->fsums, out->diffsums, &out->total_work, out->inner_stats); break;
     case 4: sample<portfolio::sampler>(ell, 0, &out->M, out->fsums, out->diffsums, &out->total_work, out->inner_stats); break;
     case 5: sample<traced<portfolio::sampler>>(ell, 0, &out->M, out->fsums, out->diffsums, &out->total_work, out->inner_stats); break;
     }
