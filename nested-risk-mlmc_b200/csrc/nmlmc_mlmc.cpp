@@ -315,6 +315,14 @@ int read_checkpoint(const char* path, Checkpoint& k) {
     }
     uint64_t ns = 0;
     if (!ok || !get(b, o, ns) || o + ns != b.size()) return NMLMC_ERR_ARG;
+    // a damaged file whose layout still parses: non-finite level sums or a bad TOL would turn
+    // into NaN sample counts
+    if (!std::isfinite(k.TOL) || !(k.TOL > 0)) return NMLMC_ERR_ARG;
+    for (const Level& l : k.levels) {
+        bool fin = std::isfinite(l.work) && l.work >= 0 && std::isfinite(l.time);
+        for (int j = 0; j < 4; j++) fin = fin && std::isfinite(l.f[j]) && std::isfinite(l.d[j]);
+        if (!fin) return NMLMC_ERR_ARG;
+    }
     k.sampler.assign(b.data() + o, ns);
     return NMLMC_OK;
 }

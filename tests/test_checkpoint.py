@@ -197,3 +197,55 @@ Total Time: 0
     r = nm.tables.parse_reports(text)[0]
     assert r["starting_level"] == 2 and r["Discarded Work"] == 10
     np.testing.assert_array_equal(nm.tables.column(r, "M"), [100, 50, 25])
+
+
+class Bounded(Synthetic):
+    """The synthetic sampler, refusing absurd sample counts (a damaged file must not turn into a
+    run that never ends)."""
+
+    def __call__(self, ell, M):
+        if M > 10**6:
+            raise RuntimeError("sample count out of range")
+        return super().__call__(ell, M)
+
+
+def test_damaged_checkpoints_are_errors_not_crashes(nm, golden, tmp_path):
+    """Every truncation of a checkpoint is rejected; a flipped bit gives an error or a normal
+    (bounded) run, never a crash, a hang or a NaN-sized request."""
+    import collections
+    kw, sa = _args(golden, 2)
+    path = str(tmp_path / "good.ckpt")
+    s = Synthetic(*sa)
+    nm.mlmc_run_cb(s, targetTOL=kw["tol"], M0=kw["M0"], checkpoint=path, state=_state(s), max_iterations=3)
+    good = open(path, "rb").read()
+    bad = str(tmp_path / "bad.ckpt")
+
+    def attempt(blob):
+        with open(bad, "wb") as f:
+            f.write(blob)
+        s2 = Bounded(*sa)
+        try:
+            nm.mlmc_run_cb(s2, targetTOL=kw["tol"], M0=kw["M0"], checkpoint=bad, resume=True,
+                           state=_state(s2), max_iterations=2)
+            return "ran"
+        except nm.NmlmcError:
+            return "error"
+
+    for n in range(0, len(good), max(1, len(good) // 97)):
+        assert attempt(good[:n]) == "error", n
+    assert attempt(good) == "ran"
+    rng = np.random.default_rng(5)
+    seen = collections.Counter()
+    for _ in range(300):
+        b = bytearray(good)
+        b[int(rng.integers(len(b)))] ^= 1 << int(rng.integers(8))
+        seen[attempt(bytes(b))] += 1
+    assert seen["error"] > 0 and seen["ran"] > 0, seen
+    # a level sum made non-finite (level 0's first fine sum: after the 120-byte header and the
+    # level's M) is rejected by the reader
+    import struct
+    b = bytearray(good)
+    b[128:136] = struct.pack("<d", float("nan"))
+    assert attempt(bytes(b)) == "error"
+    b[128:136] = struct.pack("<d", float("inf"))
+    assert attempt(bytes(b)) == "error"
