@@ -1,6 +1,9 @@
-"""The reference demo main's portfolio generator (portfolio_gen_data / portfolio_free_data,
-portfolio_sampler.cpp:784-912) through libnmlmc.so: byte-identical to the compiled reference for
-the same arguments (host code, no device needed), and its argument checks."""
+"""The portfolio generators of libnmlmc.so (host code, no device needed):
+
+* the reference demo main's (portfolio_gen_data / portfolio_free_data, portfolio_sampler.cpp:
+  784-912): byte-identical to the compiled reference for the same arguments, and its argument
+  checks;
+* the benchmark's (nmlmc_portfolio_generate): every field recomputed from the oracle's Threefry."""
 import ctypes
 import os
 
@@ -84,3 +87,36 @@ def test_generator_arguments(nm):
     L.portfolio_free_data(ctypes.byref(d))
     L.portfolio_free_data(None)
     assert nm.lib().nmlmc_last_error() == nm.ERR_ARG
+
+
+def test_benchmark_generator_against_the_oracle_threefry(nm):
+    """nmlmc_portfolio_generate (host code, no device): every field is the documented function of
+    Threefry2x64-20 blocks, recomputed here with the oracle's Threefry (itself pinned to Random123):
+    value(field f, index i) = Threefry(ctr = (i, f), key = (seed, 'PORTGEN'))."""
+    spec = dict(nm.PORTFOLIO_C2, Q=7, P=300)
+    seed = 11
+    pf = nm.generate_portfolio(spec, seed)
+    key = np.array([seed, 0x4E454754524F50], np.uint64)
+
+    def blocks(field, n):
+        ctr = np.stack([np.arange(n, dtype=np.uint64), np.full(n, field, np.uint64)], axis=1)
+        return O.threefry(ctr, np.tile(key, (n, 1)))
+
+    def u01(words):
+        return ((words >> np.uint64(11)).astype(np.float64) + 0.5) * 2.0 ** -53
+
+    Q, P = spec["Q"], spec["P"]
+    sig = spec["sigma_lo"] + (spec["sigma_hi"] - spec["sigma_lo"]) * u01(blocks(1, Q)[:, 0])
+    np.testing.assert_array_equal(pf["sigma"], sig)
+    stock = np.array([(int(v) * Q) >> 64 for v in blocks(2, P)[:, 0]], np.uint32)
+    np.testing.assert_array_equal(pf["stock_ind"], stock)
+    typ = np.where(u01(blocks(3, P)[:, 0]) < spec["call_fraction"], 1, -1)
+    np.testing.assert_array_equal(pf["type"], typ)
+    strike = spec["S0"] * (spec["strike_lo"] + (spec["strike_hi"] - spec["strike_lo"]) * u01(blocks(4, P)[:, 0]))
+    np.testing.assert_array_equal(pf["strike"], strike)
+    mat = spec["maturity_lo"] + (spec["maturity_hi"] - spec["maturity_lo"]) * u01(blocks(5, P)[:, 0])
+    np.testing.assert_array_equal(pf["maturity"], mat)
+    wb = blocks(6, P)
+    w = np.sqrt(-2.0 * np.log(u01(wb[:, 0]))) * np.cos(2.0 * np.pi * u01(wb[:, 1]))
+    np.testing.assert_allclose(pf["w"], w, rtol=1e-13, atol=1e-15)
+    np.testing.assert_array_equal(pf["S0"], np.full(Q, spec["S0"]))
