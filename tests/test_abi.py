@@ -5,6 +5,7 @@ import os
 import re
 import subprocess
 
+import numpy as np
 import pytest
 
 from conftest import ROOT
@@ -140,3 +141,14 @@ def test_cpp_entry_points(nm, tmp_path):
     run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300, cwd=tmp_path)
     assert run.returncode == 0, run.stdout[-2000:] + run.stderr[-2000:]
     assert "ok-checks 0" in run.stdout
+
+
+def test_norm_cdf_inv_export_matches_the_reference(nm, golden):
+    """The exported norm_cdf_inv (host code; common.cpp:53-86 in real_t = float) returns the
+    compiled reference's values bit for bit on the golden probabilities."""
+    _, A = golden
+    f = nm.lib().norm_cdf_inv
+    f.restype = ctypes.c_float
+    f.argtypes = [ctypes.c_float]
+    got = np.array([f(float(p)) for p in A["ncdfinv/p"]], dtype=np.float32)
+    np.testing.assert_array_equal(got.astype(np.float64), A["ncdfinv/f32"])
