@@ -86,3 +86,38 @@ def test_batched_driver_same_decisions(nm, golden):
     r2 = nm.mlmc_run_cb(det, targetTOL=tol, M0=int(M0), batched=True)
     np.testing.assert_array_equal(r1["level_M"], r2["level_M"])
     assert r1["Eg"] == r2["Eg"]
+
+
+# tol, M0, a, alpha, v, beta, w, gamma, seed: variance decay faster / slower than cost growth,
+# tiny and large M0, loose and tight tolerances, added levels and a starting level that moves up
+LIVE_DRIVER_GRID = [
+    (5e-2, 10, 1.0, 1.0, 0.5, 2.0, 1.0, 1.0, 11),
+    (2e-3, 1000, 0.4, 1.5, 0.2, 1.0, 1.0, 2.0, 12),
+    (5e-3, 20, 2.0, 0.5, 1.0, 1.5, 0.5, 1.0, 13),
+    (1e-3, 200, 0.2, 1.0, 0.01, 3.0, 2.0, 1.0, 14),
+    (8e-3, 64, 0.6, 2.0, 0.3, 2.0, 1.0, 3.0, 15),
+    (1e-2, 100, 0.5, 1.0, 0.3, 0.3, 1.0, 0.5, 17),     # slow variance decay: starting level 8
+    (5e-3, 100, 0.8, 1.2, 0.2, 0.5, 1.0, 0.8, 18),     # starting level 3
+]
+
+
+@pytest.mark.parametrize("case", range(len(LIVE_DRIVER_GRID)))
+def test_driver_matches_live_reference(nm, case):
+    """Where the reference is compiled here: its mlmc_t<double, 4>::run and this driver take the
+    same calls, sums, error split and print the same table over a grid of problems."""
+    import oracle as O
+    if not O.ref_available("f64"):
+        pytest.skip("oracle/_ref not built on this host")
+    tol, M0, a, alpha, v, beta, w, gamma, seed = LIVE_DRIVER_GRID[case]
+    ref = O.Reference("f64").mlmc_synthetic(tol, M0, a, alpha, v, beta, w, gamma, seed)
+    syn = Synthetic(a, alpha, v, beta, w, gamma, seed)
+    out = nm.mlmc_run_cb(syn, targetTOL=tol, M0=M0, verbose=False)
+    assert [c[0] for c in syn.calls] == ref["calls_ell"].tolist()
+    assert [c[1] for c in syn.calls] == ref["calls_M"].tolist()
+    lv = ref["levels"]
+    assert out["nlevels"] == len(lv)
+    np.testing.assert_array_equal(out["level_fsums"], lv[:, 0:4])
+    np.testing.assert_array_equal(out["level_diffsums"], lv[:, 4:8])
+    np.testing.assert_array_equal(out["level_M"].astype(float), lv[:, 9])
+    assert [out["starting_level"], out["bias_est"], out["stat_error"], out["TOL"]] == list(ref["misc"][:4])
+    assert out["table"] == ref["table"]
