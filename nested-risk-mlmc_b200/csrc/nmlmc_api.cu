@@ -8,6 +8,7 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <stdexcept>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -227,6 +228,18 @@ cudaError_t dev_malloc(T** p, size_t bytes) {
 int set_err(int e) {
     g_tls_error = e;
     return e;
+}
+
+// Host containers sized by the caller's input can throw; no exception may cross the C ABI.
+template <class F>
+int host_guard(F&& f) {
+    try {
+        return f();
+    } catch (const std::bad_alloc&) {
+        return set_err(NMLMC_ERR_NOMEM);
+    } catch (const std::length_error&) {
+        return set_err(NMLMC_ERR_ARG);
+    }
 }
 
 int cuda_status(cudaError_t e, const char* what) {
@@ -1161,13 +1174,13 @@ static int set_portfolio_impl(nmlmc_ctx* c, const nmlmc_portfolio* p, const nmlm
 }
 
 int nmlmc_set_portfolio(nmlmc_ctx* c, const nmlmc_portfolio* p, double* out_start, double* out_delta) {
-    return set_portfolio_impl(c, p, nullptr, out_start, out_delta);
+    return host_guard([&] { return set_portfolio_impl(c, p, nullptr, out_start, out_delta); });
 }
 
 int nmlmc_set_portfolio_methods(nmlmc_ctx* c, const nmlmc_portfolio* p, const nmlmc_path_methods* pm,
                                 double* out_start, double* out_delta) {
     if (!pm) return set_err(NMLMC_ERR_ARG);
-    return set_portfolio_impl(c, p, pm, out_start, out_delta);
+    return host_guard([&] { return set_portfolio_impl(c, p, pm, out_start, out_delta); });
 }
 
 // ---- path-simulated loss and its adjoint -------------------------------------------------------
@@ -1301,8 +1314,10 @@ int nmlmc_path_adjoint(nmlmc_ctx* c, const nmlmc_portfolio_batch* b, const nmlmc
     }
     if (b->stock_off[0] != 0 || b->option_off[0] != 0) return set_err(NMLMC_ERR_ARG);
     cudaSetDevice(c->device);
-    return a->precision == NMLMC_PREC_FP64 ? path_adjoint_t<double>(c, b, a, res, gwE, gwP, gsE, gsP, loss, seconds)
-                                           : path_adjoint_t<float>(c, b, a, res, gwE, gwP, gsE, gsP, loss, seconds);
+    return host_guard([&] {
+        return a->precision == NMLMC_PREC_FP64 ? path_adjoint_t<double>(c, b, a, res, gwE, gwP, gsE, gsP, loss, seconds)
+                                               : path_adjoint_t<float>(c, b, a, res, gwE, gwP, gsE, gsP, loss, seconds);
+    });
 }
 
 int nmlmc_set_trace(nmlmc_ctx* c, nmlmc_trace_rec* host_buf, uint64_t cap) {
@@ -1746,7 +1761,7 @@ static int portfolio_from_ref(const portfolio_data* d) {
 void portfolio_update_data(const portfolio_data* d) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (!g_ctx || !d) return ref_fail(!d ? NMLMC_ERR_ARG : NMLMC_ERR_STATE, "portfolio_update_data");
-    ref_fail(portfolio_from_ref(d), "portfolio_update_data");
+    ref_fail(host_guard([&] { return portfolio_from_ref(d); }), "portfolio_update_data");
 }
 
 void portfolio_init(const portfolio_data* d, uint64_t seed) {

@@ -26,7 +26,9 @@
 #include <iomanip>
 #include <iostream>
 #include <limits>
+#include <new>
 #include <sstream>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -513,6 +515,20 @@ int gpu_load_state(void* u, const void* buf, size_t size) {
 
 }  // namespace
 
+// No exception may cross the C ABI: a host allocation that fails inside the driver (levels,
+// report text, checkpoint buffers) becomes NMLMC_ERR_NOMEM.
+static int guarded_run(const nmlmc_mlmc_input& in, nmlmc_sample_level_fn level_fn,
+                       nmlmc_sample_levels_fn levels_fn, void* user, const nmlmc_checkpoint_io* io,
+                       nmlmc_mlmc_output* out, char* table, size_t table_cap) {
+    try {
+        return run(in, level_fn, levels_fn, user, io, out, table, table_cap);
+    } catch (const std::bad_alloc&) {
+        return NMLMC_ERR_NOMEM;
+    } catch (const std::length_error&) {
+        return NMLMC_ERR_ARG;
+    }
+}
+
 extern "C" {
 
 nmlmc_mlmc_input nmlmc_mlmc_default_input(void) {
@@ -534,14 +550,14 @@ int nmlmc_mlmc_run_cb(const nmlmc_mlmc_input* in, nmlmc_sample_level_fn level_fn
                       nmlmc_sample_levels_fn levels_fn, void* user, nmlmc_mlmc_output* out,
                       char* table, size_t table_cap) {
     if (!in || !level_fn || !(in->targetTOL > 0) || !(in->startTOL >= in->targetTOL)) return NMLMC_ERR_ARG;
-    return run(*in, level_fn, levels_fn, user, nullptr, out, table, table_cap);
+    return guarded_run(*in, level_fn, levels_fn, user, nullptr, out, table, table_cap);
 }
 
 int nmlmc_mlmc_run_cb_ckpt(const nmlmc_mlmc_input* in, nmlmc_sample_level_fn level_fn,
                            nmlmc_sample_levels_fn levels_fn, void* user, const nmlmc_checkpoint_io* io,
                            nmlmc_mlmc_output* out, char* table, size_t table_cap) {
     if (!in || !level_fn || !(in->targetTOL > 0) || !(in->startTOL >= in->targetTOL)) return NMLMC_ERR_ARG;
-    return run(*in, level_fn, levels_fn, user, io, out, table, table_cap);
+    return guarded_run(*in, level_fn, levels_fn, user, io, out, table, table_cap);
 }
 
 int nmlmc_mlmc_run(nmlmc_ctx* ctx, const nmlmc_mlmc_input* in, nmlmc_mlmc_output* out, char* table,

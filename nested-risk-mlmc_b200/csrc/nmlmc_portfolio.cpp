@@ -15,7 +15,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <memory>
+#include <new>
 #include <random>
+#include <stdexcept>
 #include <vector>
 
 #include "../../include/nmlmc.h"
@@ -112,8 +115,8 @@ extern "C" int nmlmc_portfolio_generate(const nmlmc_portfolio_spec* sp, uint64_t
 // Two reference behaviours are not carried over: with uniform_weights the reference leaves every
 // weight at 0 (so the normalisation divides 0 by 0) where its caller documents weights of 1, and
 // the reference's W_est update of the Unbiased options changes a copy (so W_est stays 1, as here).
-extern "C" portfolio_data portfolio_gen_data(uint32_t P, uint32_t Q, uint64_t seed, double* probs,
-                                             bool uniform_weights, bool uniform_prob) {
+static portfolio_data gen_data(uint32_t P, uint32_t Q, uint64_t seed, const double* probs,
+                               bool uniform_weights, bool uniform_prob) {
     portfolio_data d{};
     if (!probs || Q == 0 || (uint64_t)P < 2ull * Q) {
         nmlmc_ref_status(NMLMC_ERR_ARG, "portfolio_gen_data");
@@ -167,8 +170,10 @@ extern "C" portfolio_data portfolio_gen_data(uint32_t P, uint32_t Q, uint64_t se
     draw(strike, uni(80, 120));
     if (!uniform_weights) draw(weight, std::normal_distribution<float>(0, 1));
 
-    option_params* ops = new option_params[P]();
-    stock_params* stocks = new stock_params[Q]();
+    std::unique_ptr<option_params[]> ops_owner(new option_params[P]());
+    std::unique_ptr<stock_params[]> stocks_owner(new stock_params[Q]());
+    option_params* ops = ops_owner.get();
+    stock_params* stocks = stocks_owner.get();
     for (uint32_t i = 0; i < Q; i++) {
         type[i] = 0;
         type[Q + i] = 1;
@@ -219,8 +224,23 @@ extern "C" portfolio_data portfolio_gen_data(uint32_t P, uint32_t Q, uint64_t se
         std::sort(b, b + d.options[m].size,
                   [](const option_params& x, const option_params& y) { return x.prob > y.prob; });
     }
+    ops_owner.release();                     // now owned by d (portfolio_free_data)
+    stocks_owner.release();
     nmlmc_ref_status(NMLMC_OK, "portfolio_gen_data");
     return d;
+}
+
+// No exception may cross the C ABI: a failed host allocation returns the zeroed portfolio_data.
+extern "C" portfolio_data portfolio_gen_data(uint32_t P, uint32_t Q, uint64_t seed, double* probs,
+                                             bool uniform_weights, bool uniform_prob) {
+    try {
+        return gen_data(P, Q, seed, probs, uniform_weights, uniform_prob);
+    } catch (const std::bad_alloc&) {
+        nmlmc_ref_status(NMLMC_ERR_NOMEM, "portfolio_gen_data");
+    } catch (const std::length_error&) {
+        nmlmc_ref_status(NMLMC_ERR_ARG, "portfolio_gen_data");
+    }
+    return portfolio_data{};
 }
 
 // Frees what portfolio_gen_data allocated (portfolio_sampler.cpp:906-912): the stock array and
