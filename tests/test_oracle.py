@@ -303,3 +303,48 @@ def test_live_reference_portfolio_grid(variant, prec, case):
         np.testing.assert_array_equal(a["fsums"], b["fsums"])
         np.testing.assert_array_equal(a["diffsums"], b["diffsums"])
         np.testing.assert_array_equal(a["stats"], b["stats"])
+
+
+# path-simulated inner values: Q, P, generator seed, sub-sampling, delta CV, coarse CV,
+# antithetic risk, Milstein, h0 = 1/dt_h0inv, dt_beta, dt_prob_expo, cores, N0, beta, levels, M
+LIVE_METHODS_GRID = [
+    (2, 8, 41, O.SUB_NONE, False, False, True, True, 4, 2, -1.5, 2, 32, 2, (0, 1), 6),
+    (3, 12, 42, O.SUB_UNIFORM, True, True, False, False, 8, 4, -1.2, 3, 32, 4, (0, 2), 5),
+    (2, 10, 43, O.SUB_RANDOM, True, False, True, True, 16, 2, -2.0, 1, 16, 2, (1, 0, 1), 4),
+    (4, 9, 44, O.SUB_RANDOM, False, True, True, False, 8, 3, -1.5, 4, 32, 2, (2,), 8),
+]
+
+
+@pytest.mark.parametrize("variant,prec", [("f32_lzcnt", O.PREC_REF32), ("f64_lzcnt", O.PREC_FP64)])
+@pytest.mark.parametrize("case", range(len(LIVE_METHODS_GRID)))
+def test_live_reference_methods_grid(variant, prec, case):
+    """Where the reference is compiled here: mixed BS / Exact / Unbiased portfolios over the
+    path-simulation parameters (step sizes, level distribution, Milstein or Euler, antithetic
+    risk, coarse delta CV, sub-sampling modes): every event and level sum of the oracle equals
+    the reference's."""
+    if not O.ref_available(variant):
+        pytest.skip("oracle/_ref not built on this host")
+    (Q, P, g, sub, cv, ccv, arisk, mil, h0inv, dtb, expo, cores, N0, beta, ells, M) = LIVE_METHODS_GRID[case]
+    rng = np.random.default_rng(100 + case)
+    pf = O.synthetic_portfolio(Q, P, g, prob="w")
+    meth = rng.integers(0, 3, P).astype(np.int32)
+    meth[:3] = [0, 1, 2]                                    # every method present
+    kw = dict(rho=0.15, max_loss=0.25, subsample=sub, use_delta_cv=cv, use_coarse_delta_cv=ccv,
+              use_antithetic_risk=arisk, use_milstein=mil, dt_h0inv=h0inv, dt_beta=dtb,
+              dt_prob_expo=expo)
+    seed = 3000 + case
+    ref = O.Reference(variant)
+    ref.init(cores, N0, beta, 1.5, True)
+    ref.portfolio_init_methods(pf, meth, seed=seed, **kw)
+    s = O.Sampler(prec, O.STREAMS_CORE, cores, N0, beta, 1.5, True, False, seed)
+    s.set_portfolio_methods(pf, meth, **kw)
+    for ell in ells:
+        a = ref.sample(ell, M, events_cap=2_000_000)
+        b = s.sample(ell, M, events_cap=2_000_000)
+        assert a["events"][0] == b["events"][0], (case, ell)
+        np.testing.assert_array_equal(a["events"][1], b["events"][1])
+        np.testing.assert_array_equal(a["events"][2], b["events"][2])
+        np.testing.assert_array_equal(a["fsums"], b["fsums"])
+        np.testing.assert_array_equal(a["diffsums"], b["diffsums"])
+        np.testing.assert_array_equal(a["stats"], b["stats"])
+        assert a["work"] == b["work"]
