@@ -334,8 +334,9 @@ int nmlmc_portfolio_full_loss(nmlmc_ctx* ctx, uint32_t ell, uint64_t first, uint
                               double* host_loss);
 
 /* Sharding over ranks (OUTER layout): each nmlmc_sample(ell, M) call then evaluates only this
- * rank's static share [rank*M/world ...] of the call's M outer samples, with the stream indices
- * a single device would give them; the caller sums the ranks' level results (an all-reduce of
+ * rank's contiguous share of the call's M outer samples (ranks below M mod world take
+ * floor(M / world) + 1 of them, the others floor(M / world)), with the stream indices a single
+ * device would give them; the caller sums the ranks' level results (an all-reduce of
  * 16 doubles) and gets the single-device result.  world = 1 restores the default. */
 int nmlmc_set_shard(nmlmc_ctx* ctx, uint32_t rank, uint32_t world);
 /* CUDA-event timing of the phase kernel (the dominant kernel): 1 enables; the totals since
