@@ -1,7 +1,8 @@
 """Multi-GPU MLMC: one process per GPU, outer samples sharded, level results all-reduced.
 
-Every outer sample owns its random stream (OUTER layout), so rank r of W evaluates the static
-share [r*M/W ...] of each sample_level(ell, M) call (nmlmc_set_shard) and the 16-double level
+Every outer sample owns its random stream (OUTER layout), so rank r of W evaluates a contiguous
+share of each sample_level(ell, M) call (nmlmc_set_shard: floor(M/W) outer samples, one more on
+the first M mod W ranks) and the 16-double level
 results are summed over ranks with one all_reduce per call (NCCL on GPUs, gloo on CPU).  All ranks
 then hold the single-device result, run the same host driver and take the same decisions; no
 data-path collective exists.  The sampler is any object with set_shard(rank, world) and
