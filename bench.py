@@ -271,6 +271,84 @@ def small_case():
         print(f"level {ell} M {M}: {r['seconds'] * 1e3:.3f} ms, {r['stats'][0] / r['seconds']:.3e} inner/s")
 
 
+# The reference's own model main (model_sampler.cpp:120-147): reference model with tau = 0.02 and
+# max_loss = tau (Phi^-1(eta/2)^2 - 1), eta = 0.025 (the exact answer), N0 = 32, beta = 4,
+# r = 1.5, antithetic, TOL = 1e-3, M0 = 1024.
+REF_MAIN = dict(tau=0.02, eta=0.025, N0=32, beta=4, adaptive_r=1.5, tol=1e-3, M0=1024)
+
+
+def ref_main_max_loss(norm_cdf_inv) -> float:
+    """max_loss of the model main in real_t = float (model_sampler.cpp:144)."""
+    import numpy as np
+    x = np.float32(norm_cdf_inv(REF_MAIN["eta"] / 2))
+    return float(np.float32(REF_MAIN["tau"]) * (x * x - np.float32(1)))
+
+
+def ref_main_cpu(threads: int | None = None, tol: float | None = None) -> dict:
+    """The reference's CPU level sampler (oracle/_ref, OpenMP on `threads`) of the model main under
+    the host driver (whose decisions equal the reference's mlmc_t::run): wall seconds and result."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, PKG)
+    import oracle as O
+    import nmlmc as nm
+    threads = threads or os.cpu_count() or 1
+    variant = "f32_lzcnt" if O.ref_available("f32_lzcnt") else None
+    if variant is None:
+        return {"unavailable": "oracle/_ref not built"}
+    ml = ref_main_max_loss(O.Reference("f32").L.ref_norm_cdf_inv)
+    ref = O.Reference(variant)
+    ref.init(threads, REF_MAIN["N0"], REF_MAIN["beta"], REF_MAIN["adaptive_r"], True)
+    ref.model_init(0, REF_MAIN["tau"], ml, 0, traced=False)
+
+    def level(ell, M):
+        r = ref.sample(ell, M)
+        return dict(fsums=r["fsums"], diffsums=r["diffsums"], work=r["work"])
+
+    t = time.perf_counter()
+    out = nm.mlmc_run_cb(level, targetTOL=tol or REF_MAIN["tol"], M0=REF_MAIN["M0"], verbose=False)
+    return dict(seconds=time.perf_counter() - t, threads=threads, Eg=float(out["Eg"]),
+                levels=int(out["nlevels"]), total_work=float(out["total_work"]),
+                kind="reference", sample="the whole run (every level call of the reference's sampler)")
+
+
+def ref_main_case(args):
+    """The model main of the reference on the GPU (batched FP32 and the FP64 / REF32 drop-ins on
+    the reference's streams, 2048 virtual cores) beside the reference's CPU sampler, all under
+    the same host driver; each estimate against the exact eta."""
+    sys.path.insert(0, PKG)
+    import nmlmc as nm
+    ml = ref_main_max_loss(nm.norm_cdf_inv)
+    runs = {}
+    for name, prec, streams, batched in (("fp32_batched", nm.PREC_FP32, nm.STREAMS_OUTER, True),
+                                         ("fp64_dropin", nm.PREC_FP64, nm.STREAMS_CORE, False),
+                                         ("ref32_dropin", nm.PREC_REF32, nm.STREAMS_CORE, False)):
+        s = nm.Sampler(0, cores=2048, N0=REF_MAIN["N0"], beta=REF_MAIN["beta"],
+                       adaptive_r=REF_MAIN["adaptive_r"], precision=prec, streams=streams, seed=1)
+        s.set_model(nm.MODEL_REFERENCE, REF_MAIN["tau"], ml)
+        if prec == nm.PREC_FP32:
+            s.set_autotune(2)
+        s.mlmc_run(targetTOL=REF_MAIN["tol"], M0=REF_MAIN["M0"], batched=batched)     # warm-up
+        if prec == nm.PREC_FP32:
+            s.set_autotune(0)                  # the timed run keeps the warm-up's choices
+        s.configure(seed=0)
+        t = time.perf_counter()
+        out = s.mlmc_run(targetTOL=REF_MAIN["tol"], M0=REF_MAIN["M0"], batched=batched)
+        runs[name] = dict(value=float(out["level_time"].sum()), e2e=time.perf_counter() - t,
+                          Eg=float(out["Eg"]), abs_err_vs_eta=abs(float(out["Eg"]) - REF_MAIN["eta"]),
+                          levels=int(out["nlevels"]), total_work=float(out["total_work"]))
+    cpu = ref_main_cpu() if not args.no_cpu else {"skipped": True}
+    a = runs["fp32_batched"]
+    line = {"metric": "time-to-TOL (s), the reference's model main (TOL = 1e-3)", "value": a["value"],
+            "unit": "s", "n_gpus": 1, "higher_is_better": False, "dtype": "f32", "data": "synthetic",
+            "config": dict(workload="reference model main: tau 0.02, eta 0.025, N0 32, beta 4, r 1.5",
+                           **{k: v for k, v in REF_MAIN.items()}),
+            "e2e": {"value": a["e2e"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": None},
+            "runs": runs, "cpu_baseline": cpu, "vs_baseline": None}
+    if "seconds" in cpu:
+        line["speedup_vs_cpu_reference"] = {"e2e": cpu["seconds"] / a["e2e"]}
+    print(json.dumps(line))
+
+
 # Lane operations per inner time step of an antithetic Milstein pair on the FP32 path (one normal):
 #   Threefry2x64-20 block / 4 = 35, SFU Box-Muller pair / 2 = 11, the Milstein update of both
 #   paths (dW, dW^2 - h, correction, two growth factors, two products) = 9, loop and select = 3;
@@ -573,7 +651,7 @@ def main():
     ap.add_argument("--schedule-out", default=None,
                     help="write the run's outer samples per level (bench_schedule.json format) here")
     ap.add_argument("--case", default=None, choices=["small", "c3", "c3-level", "c3-table", "c3-sweep", "c4",
-                                                      "c4-small"],
+                                                      "c4-small", "ref-model"],
                     help="small: a few fixed level calls of the FP32 sampler (profiling case); "
                          "c4: the path-simulated loss with adjoint; c4-small: its profiling case")
     args = ap.parse_args()
@@ -591,6 +669,8 @@ def main():
         return c3_sweep_case()
     if args.case in ("c4", "c4-small"):
         return c4_case(args, small=args.case == "c4-small")
+    if args.case == "ref-model":
+        return ref_main_case(args)
 
     sys.path.insert(0, PKG)
     import nmlmc as nm

@@ -77,3 +77,18 @@ def test_reference_arm_line(tmp_path):
     env1 = dict(env, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
     out1 = subprocess.run(cmd, capture_output=True, text=True, timeout=600, env=env1)
     assert out1.returncode == 0 and not out1.stdout.strip()
+
+
+def test_reference_model_main_on_the_cpu(golden):
+    """The CPU leg of `--case ref-model`: the reference's sampler of its model main under the host
+    driver (a loose tolerance here); the model's exact answer is eta = 0.025, and the library's
+    max_loss of the main equals the compiled reference's."""
+    import nmlmc as nm
+    meta, _ = golden
+    assert bench.ref_main_max_loss(nm.norm_cdf_inv) == meta["model_max_loss_f32"]
+    r = bench.ref_main_cpu(threads=2, tol=1e-2)
+    if "unavailable" in r:
+        import pytest
+        pytest.skip(r["unavailable"])
+    assert r["threads"] == 2 and r["levels"] >= 2 and r["total_work"] > 0
+    assert abs(r["Eg"] - bench.REF_MAIN["eta"]) < 3e-2
