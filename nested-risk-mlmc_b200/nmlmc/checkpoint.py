@@ -15,8 +15,16 @@ MAGIC = b"NMLMCCK1"
 
 
 def read_checkpoint(path) -> dict:
+    """The checkpoint's fields; ValueError for anything that is not a complete checkpoint."""
     with open(path, "rb") as f:
         b = f.read()
+    try:
+        return _parse(b, path)
+    except struct.error as e:          # shorter than its own layout says
+        raise ValueError(f"{path}: truncated checkpoint ({e})") from None
+
+
+def _parse(b: bytes, path) -> dict:
     if b[:8] != MAGIC:
         raise ValueError(f"{path}: not an nmlmc checkpoint")
     version, fixed = struct.unpack_from("<II", b, 8)
@@ -33,6 +41,8 @@ def read_checkpoint(path) -> dict:
         raise ValueError(f"{path}: fixed part of {fixed} bytes, expected {o}")
     rec = np.dtype([("M", "<u8"), ("fsums", "<f8", 4), ("diffsums", "<f8", 4), ("work", "<f8"),
                     ("time", "<f8")])
+    if not 0 < nlev <= 64 or o + nlev * rec.itemsize > len(b):
+        raise ValueError(f"{path}: {nlev} levels do not fit the file")
     levels = np.frombuffer(b, rec, count=nlev, offset=o)
     o += nlev * rec.itemsize
     (ns,) = struct.unpack_from("<Q", b, o)

@@ -233,6 +233,8 @@ def test_damaged_checkpoints_are_errors_not_crashes(nm, golden, tmp_path):
 
     for n in range(0, len(good), max(1, len(good) // 97)):
         assert attempt(good[:n]) == "error", n
+        with pytest.raises(ValueError):           # the Python reader agrees
+            nm.checkpoint.read_checkpoint(bad)
     assert attempt(good) == "ran"
     rng = np.random.default_rng(5)
     seen = collections.Counter()
