@@ -43,7 +43,10 @@ def parse_reports(text: str) -> list:
         if not sep:
             raise ValueError(f"unrecognised line: {raw!r}")
         key = key.strip()
-        value = float(rest.split()[0])
+        parts = rest.split()
+        if not parts:
+            raise ValueError(f"no value: {raw!r}")
+        value = float(parts[0])
         if key == "TOL":
             cur = dict(columns=[], rows=[], starting_level=0)
             reports.append(cur)
