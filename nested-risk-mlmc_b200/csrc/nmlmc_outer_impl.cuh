@@ -155,6 +155,8 @@ __device__ __forceinline__ RT outer_normal_at(const TfKey& key, uint32_t tag, ui
 }
 
 // ---- portfolio inner value (BS path of portfolio::sampler) ----------------------------------
+// sample_inner_bs with option_diff_from_blackscholes and the delta CV (portfolio_sampler.cpp:
+// 453-468, 186-200, 202-210) in the reference's arithmetic (REF32 / FP64 tables).
 template <class RT>
 __device__ __forceinline__ RT pf_value(const OptionTable<RT>& ot, const RT* Rrow, uint32_t j) {
     uint32_t s = ot.stock_ind[j];
@@ -183,6 +185,8 @@ __device__ __forceinline__ uint32_t pf_index(const uint2* alias, uint32_t P, uin
     return coin < e.x ? j : e.y;
 }
 
+// The sub-sampled option index and its sampling probability (sample_inner_random_option_ind,
+// portfolio_sampler.cpp:346-370, on the OUTER layout's draws).
 template <class RT>
 __device__ __forceinline__ uint32_t pf_pick(const OptionTable<RT>& ot, uint64_t v, RT& prob) {
     const uint32_t j = pf_index(ot.subsample == SUB_UNIFORM ? nullptr : ot.alias, ot.P, v);
@@ -191,6 +195,8 @@ __device__ __forceinline__ uint32_t pf_pick(const OptionTable<RT>& ot, uint64_t 
 }
 
 // ---- one chunk: inner samples [s0, s0 + C) of phase `tag` of outer sample `item` ----------
+// The chunk's share of sample_inner's sums (nested_sampler.hpp:131-161; model::sampler::
+// sample_inner, model_sampler.cpp:66-79, or the portfolio's inner value above).
 // C (inner samples per chunk) is a compile-time constant so the independent Threefry blocks of a
 // chunk can be interleaved (two at a time) for instruction-level parallelism.
 template <class RT, int KIND, int PREC, uint32_t C, bool S2>
@@ -379,7 +385,8 @@ __device__ __forceinline__ uint32_t pilots_taken(uint32_t cnt, const CountParams
     return r + 1;
 }
 
-// Per-item completion of the final phase: phi_f, phi_c; their moments go into this thread's
+// Per-item completion of the final phase (sample_phi_antithetic, nested_sampler.hpp:171-216, and
+// add_moments, 87-100): phi_f, phi_c; their moments go into this thread's
 // moment slots mom[q * kTile] (q = 0..3 phi_f^k, 4..7 (phi_f - phi_c)^k; a zero phi adds
 // nothing and touches no slot), the counts of items that hit the maximum / stayed at the base
 // count, and the trace record.
@@ -425,6 +432,8 @@ __device__ __forceinline__ void final_item(const DevLevel<RT>& D, uint32_t item,
 
 // Block partial sums (OuterBuffers::block_sums layout): [0..3] phi_f moments, [4..7] difference
 // moments, [8] work, [9] inner samples, [10] hit the maximum count, [11] stayed at the base count.
+// The batched form of kernel_sample's per-outer-sample loop (nested_sampler.hpp:369-485): pilot
+// and final phases of many outer samples drained from device work queues.
 // MINB = CTAs per SM the register allocation must allow (1: up to 255 registers per thread,
 // 3: 80, 4: 64) — the register/occupancy variants the autotuner chooses between.  The variants
 // run the same arithmetic in the same order, so their results are identical.
@@ -668,6 +677,9 @@ __global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet S,
 }
 
 // ---- outer draws ---------------------------------------------------------------------------
+// sample_outer of the model (Y = randn_sync, model_sampler.cpp:57-59) or of the portfolio (the
+// stocks at tau and the delta-CV constant, portfolio_sampler.cpp:293-311, 606-614) per outer
+// sample, from the OUTER layout's phase-0 draws.
 template <class RT, int KIND, int PREC>
 __global__ void __launch_bounds__(kTile) k_outer(DevLevel<RT> D, uint32_t nb) {
     const OuterLevel<RT>& L = D.L;
