@@ -70,7 +70,7 @@ template cudaError_t outer_sample_level<double>(const OuterLevel<double>&, int, 
 
 // ---- full portfolio loss sweep ---------------------------------------------------------------
 // L(Y) over every option: init_inner_sampler without sub-sampling and sample_inner_all_options
-// (portfolio_sampler.cpp:312-324, 336-344), one thread per outer sample, for the K quantile.
+// (portfolio_sampler.cpp:312-324, 336-344), one warp per outer sample, for the K quantile.
 template <class RT, int PREC>
 __global__ void k_full_loss(DevLevel<RT> D, uint32_t nb, double* loss) {
     // one warp per outer sample: lanes stride the option table, double accumulation
