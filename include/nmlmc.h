@@ -219,12 +219,19 @@ typedef struct nmlmc_trace_rec {
 const char* nmlmc_error_string(int status);
 int nmlmc_version(void);
 
+/* A context replaces the reference's process-wide sampler state (g_p_nestedmc_data and the
+ * __constant__ parameters, common.cpp:15-31): create / destroy ~ init_nestedmc_sampler /
+ * cleanup_nestedmc_sampler, configure ~ nested_sampler_params (nested_sampler.hpp:14-34) plus
+ * the precision and stream layout. */
 int nmlmc_create(nmlmc_ctx** out, int device);
 int nmlmc_destroy(nmlmc_ctx* ctx);
 int nmlmc_configure(nmlmc_ctx* ctx, const nmlmc_config* cfg);
-/* kind NMLMC_MODEL_REFERENCE: model::sampler with tau, max_loss;
+/* model_init (model_sampler.cpp:99-104) with the model's data (model_sampler.cpp:21-39).
+ * kind NMLMC_MODEL_REFERENCE: model::sampler with tau, max_loss;
  * kind NMLMC_MODEL_SHIFT: Y ~ N(0,1), inner X = Y + Z, threshold K = max_loss. */
 int nmlmc_set_model(nmlmc_ctx* ctx, int32_t kind, double tau, double max_loss);
+/* portfolio_comp_params + portfolio_init (portfolio_sampler.cpp:618-756) from structure-of-arrays
+ * doubles; out_start / out_delta_est receive the options' start values and delta estimates. */
 int nmlmc_set_portfolio(nmlmc_ctx* ctx, const nmlmc_portfolio* pf, double* out_start,
                         double* out_delta_est);
 /* Path-simulated inner values (portfolio_sampler.cpp:74-87, 470-604; gbm_approx.hpp:18-57):
@@ -279,10 +286,10 @@ typedef struct nmlmc_adjoint_result {
 int nmlmc_path_adjoint(nmlmc_ctx* ctx, const nmlmc_portfolio_batch* batch, const nmlmc_adjoint_config* cfg,
                        nmlmc_adjoint_result* res, double* grad_w_EL, double* grad_w_P,
                        double* grad_sigma_EL, double* grad_sigma_P, double* loss, double* seconds);
-/* Restart every stream (CORE: random_state(seed, core) from counter 0; OUTER: outer indices
- * from 0). */
+/* Restart every stream, as init_samplers does (nested_sampler.hpp:618-643; CORE:
+ * random_state(seed, core) from counter 0; OUTER: outer indices from 0). */
 int nmlmc_reset_streams(nmlmc_ctx* ctx);
-/* One level: M outer samples at level ell. */
+/* One level: M outer samples at level ell (sample<SAMPLER>, nested_sampler.hpp:646-694). */
 int nmlmc_sample(nmlmc_ctx* ctx, uint32_t ell, uint64_t M, nmlmc_level_result* out);
 /* Several levels in one submission.  OUTER layout: the levels' launch sequences are captured
  * into one CUDA graph (kept and updated in place while the topology repeats), each level summing
