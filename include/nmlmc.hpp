@@ -1,4 +1,5 @@
-/* nmlmc.hpp — the reference's C++ entry points, over the C ABI of nmlmc.h (header-only).
+/* nmlmc.hpp — the reference's C++ entry points, over the C ABI of nmlmc.h (header-only, C++11 or
+ * later; the reference builds with C++14).
  *
  *  sample<SAMPLER>(ell, override_dyn_inner, &M, fsums, diffsums, &total_work, inner_stats)
  *      The level call of nested_sampler.hpp:646-694 for SAMPLER = model::sampler or

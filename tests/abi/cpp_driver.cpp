@@ -25,7 +25,7 @@ struct Synthetic {
         return z ^ (z >> 31);
     }
     static double normal(uint64_t& s) {
-        const double u1 = ((mix(s) >> 11) + 0.5) * 0x1p-53, u2 = ((mix(s) >> 11) + 0.5) * 0x1p-53;
+        const double u1 = std::ldexp((mix(s) >> 11) + 0.5, -53), u2 = std::ldexp((mix(s) >> 11) + 0.5, -53);
         return std::sqrt(-2 * std::log(u1)) * std::cos(6.283185307179586 * u2);
     }
     void level(uint32_t ell, uint64_t M, double* f, double* d, double& work) {

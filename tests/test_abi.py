@@ -132,7 +132,7 @@ def test_cpp_entry_points(nm, tmp_path):
     unchanged, and sample<SAMPLER> before init is an error status (tests/abi/cpp_driver.cpp)."""
     exe = tmp_path / "cpp_driver"
     libdir = os.path.dirname(nm.LIB_PATH)
-    cc = subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror",
+    cc = subprocess.run(["g++", "-std=c++14", "-Wall", "-Wextra", "-Werror",     # the reference's standard
                          f"-I{os.path.join(ROOT, 'include')}",
                          os.path.join(ROOT, "tests", "abi", "cpp_driver.cpp"), "-o", str(exe),
                          f"-L{libdir}", "-lnmlmc", f"-Wl,-rpath,{libdir}"],
