@@ -12,8 +12,6 @@ CUDA graph on GPUs) and one all_reduce of all its levels.
 """
 from __future__ import annotations
 
-import numpy as np
-
 from . import mlmc_run_cb
 
 
