@@ -9,6 +9,11 @@
  *      are recorded in nmlmc_last_error() and printed (the reference exit()s).  A SAMPLER type
  *      selects one of the library's kernels; the samplers' device code lives in the library.
  *
+ *  model:: / portfolio:: names of the reference (model::data with its constructor, PhiType,
+ *      ComputeMethod, OptionType, Subsampling, the entry points as model::model_init, ...) and
+ *      nmlmc::make_nested_sampler_params / nmlmc::level_output for the two C structs whose
+ *      reference constructors a C header cannot carry (nested_sampler_params, sample_output).
+ *
  *  nmlmc::mlmc_t<T, S>::run(mlmc_input_t&)
  *      The continuation-MLMC driver of mlmc.hpp:207-337 with its std::function level callback
  *      (mlmc_input_t::fn_sample_level_t, mlmc.hpp:224).  The loop is the library's C++ driver
@@ -21,6 +26,7 @@
 #ifndef NMLMC_HPP
 #define NMLMC_HPP
 
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <exception>
@@ -33,6 +39,23 @@
 #include "nmlmc.h"
 
 namespace model {
+enum class PhiType { Indicator = 0, Max = 1 };     /* model_sampler.cpp:16-19 (Indicator only here) */
+
+/* model::data (model_sampler.cpp:21-39): the same fields and layout as model_data. */
+struct data : ::model_data {
+    data() : ::model_data() {}
+    data(PhiType phi, float tau, float loss) : ::model_data() {
+        stau = std::sqrt(tau);
+        s1tau = std::sqrt(1 - tau);
+        max_loss = loss;
+        phi_type = static_cast<int32_t>(phi);
+    }
+    uint32_t phi_size() const { return 1; }
+};
+using ::model_update_data;
+using ::model_init;
+using ::model_sample;
+
 struct sampler {               /* model::sampler (model_sampler.cpp:42-92) */
     static void sample_level(uint32_t ell, uint64_t, sample_output* out) {
         model_sample(ell, out->M, out);
@@ -41,12 +64,64 @@ struct sampler {               /* model::sampler (model_sampler.cpp:42-92) */
 }  // namespace model
 
 namespace portfolio {
+enum class ComputeMethod { BS = 0, Exact = 1, Unbiased = 2 };        /* portfolio_sampler.cpp:17-22 */
+enum class OptionType { Call = 1, Put = -1 };                       /* :24-27 */
+enum class Subsampling { None = 0, Random = 1, Random_Uniform = -1 };  /* :36-40 */
+typedef ::portfolio_data data;
+typedef ::option_params option_params;
+typedef ::stock_params stock_params;
+using ::portfolio_update_data;
+using ::portfolio_init;
+using ::portfolio_sample;
+using ::portfolio_cleanup;
+using ::portfolio_comp_params;
+using ::portfolio_gen_data;
+using ::portfolio_free_data;
+
 struct sampler {               /* portfolio::sampler (portfolio_sampler.cpp:227-606) */
     static void sample_level(uint32_t ell, uint64_t override_dyn_inner, sample_output* out) {
         portfolio_sample(ell, override_dyn_inner, out->M, out);
     }
 };
 }  // namespace portfolio
+
+namespace nmlmc {
+/* nested_sampler_params(fine_moments, diff_moments, N0, beta, adaptive_r, antithetic), the
+ * reference's constructor argument order (nested_sampler.hpp:16-26). */
+inline nested_sampler_params make_nested_sampler_params(uint32_t fine_moments, uint32_t diff_moments,
+                                                        uint32_t N0, uint32_t beta, float adaptive_r,
+                                                        bool antithetic) {
+    nested_sampler_params p;
+    p.N0 = N0;
+    p.beta = beta;
+    p.antithetic = antithetic;
+    p.fine_moments = fine_moments;
+    p.diff_moments = diff_moments;
+    p.adaptive_r = adaptive_r;
+    return p;
+}
+
+/* A sample_output that owns its sums, as the reference's sample_output(fsize, dsize, phi_size)
+ * does (common.hpp:37-55); converts to the sample_output* the C entry points take. */
+class level_output {
+  public:
+    explicit level_output(uint32_t fsize, uint32_t dsize = 0, uint32_t phi_size = 1)
+        : f_(static_cast<size_t>(fsize) * phi_size, 0.0), d_(static_cast<size_t>(dsize) * phi_size, 0.0) {
+        std::memset(&o_, 0, sizeof o_);
+        o_.fsums = f_.empty() ? nullptr : f_.data();
+        o_.diffsums = d_.empty() ? nullptr : d_.data();
+    }
+    level_output(const level_output&) = delete;
+    level_output& operator=(const level_output&) = delete;
+    operator sample_output*() { return &o_; }
+    sample_output* operator->() { return &o_; }
+    const sample_output* operator->() const { return &o_; }
+
+  private:
+    std::vector<double> f_, d_;
+    sample_output o_;
+};
+}  // namespace nmlmc
 
 template <class SAMPLER>
 inline void sample(uint32_t ell, uint64_t override_dyn_inner, uint64_t* M, double* out_fsums,

@@ -3,7 +3,8 @@
 //  1. nmlmc::mlmc_real::run over a std::function level sampler takes exactly the decisions and
 //     prints exactly the table of the C driver (nmlmc_mlmc_run_cb) over the same sampler;
 //  2. an exception thrown by the level sampler leaves run() as that exception;
-//  3. sample<model::sampler> before model_init records an error instead of exiting.
+//  3. sample<model::sampler> before model_init records an error instead of exiting;
+//  4. the reference's model:: / portfolio:: names and constructors compile and behave.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -108,6 +109,29 @@ int main() {
     if (nmlmc_last_error() == NMLMC_OK) bad++;
     sample<portfolio::sampler>(2, 0, &M, f, d, &w, stats);
     if (nmlmc_last_error() == NMLMC_OK) bad++;
+    // 4. the reference's names: model::data and its constructor, model::model_sample on an owning
+    //    sample_output, the params constructor's argument order, portfolio::portfolio_gen_data
+    static_assert(sizeof(model::data) == sizeof(model_data), "model::data keeps model_data's layout");
+    const model::data md(model::PhiType::Indicator, 0.02f, 0.1f);
+    if (md.stau != std::sqrt(0.02f) || md.s1tau != std::sqrt(1 - 0.02f) || md.max_loss != 0.1f ||
+        md.phi_type != 0 || md.phi_size() != 1)
+        bad++;
+    nmlmc::level_output out(4, 4, 1);
+    model::model_sample(2, 10, out);                       // before model_init: an error status
+    if (nmlmc_last_error() == NMLMC_OK || out->fsums == nullptr || out->diffsums == nullptr) bad++;
+    const nested_sampler_params p = nmlmc::make_nested_sampler_params(4, 2, 32, 4, 1.5f, true);
+    if (p.fine_moments != 4 || p.diff_moments != 2 || p.N0 != 32 || p.beta != 4 || !p.antithetic ||
+        p.adaptive_r != 1.5f)
+        bad++;
+    double probs[3] = {0.5, 0.25, 0.25};
+    portfolio::data pd = portfolio::portfolio_gen_data(40, 4, 9, probs, false, false);
+    const int32_t t0 = pd.options[0].size ? pd.options[0].data[0].type : 0;
+    if (nmlmc_last_error() != NMLMC_OK || pd.options[0].size != 20 || pd.options[1].size != 10 ||
+        pd.stocks.size != 4 ||
+        (t0 != static_cast<int32_t>(portfolio::OptionType::Call) &&
+         t0 != static_cast<int32_t>(portfolio::OptionType::Put)))
+        bad++;
+    portfolio::portfolio_free_data(&pd);
     printf("ok-checks %d\n", bad);
     return bad != 0;
 }
