@@ -120,3 +120,32 @@ def test_benchmark_generator_against_the_oracle_threefry(nm):
     w = np.sqrt(-2.0 * np.log(u01(wb[:, 0]))) * np.cos(2.0 * np.pi * u01(wb[:, 1]))
     np.testing.assert_allclose(pf["w"], w, rtol=1e-13, atol=1e-15)
     np.testing.assert_array_equal(pf["S0"], np.full(Q, spec["S0"]))
+
+
+def test_comp_params_and_layout_helpers(nm):
+    """make_portfolio_data builds the reference's portfolio_data layout from SoA arrays (options
+    grouped by method, in order); the exported portfolio_comp_params fills start / delta_est like
+    the compiled reference's on the same struct; make_batch concatenates with offsets."""
+    pf = O.synthetic_portfolio(5, 60, 17, prob="w")
+    meth = np.array([0, 1, 2] * 20, np.int32)
+    d, keep = nm.make_portfolio_data(pf, rho=0.2, max_loss=0.3, method=meth)
+    assert [d.options[m].size for m in range(3)] == [20, 20, 20] and d.stocks.size == 5
+    for m in range(3):
+        for k, j in enumerate(np.flatnonzero(meth == m)):
+            assert d.options[m].data[k].strike == np.float32(pf["strike"][j])
+    L = nm.lib()
+    L.portfolio_comp_params.argtypes = [ctypes.POINTER(nm.PortfolioData)]
+    L.portfolio_comp_params(ctypes.byref(d))
+    ours = b"".join(ctypes.string_at(d.options[m].data, ctypes.sizeof(nm.OptionParams) * d.options[m].size) for m in range(3))
+    if O.ref_available("f32"):
+        e, keep2 = nm.make_portfolio_data(pf, rho=0.2, max_loss=0.3, method=meth)
+        R = ctypes.CDLL(os.path.join(O.REF_DIR, "libref_f32.so"))
+        R.portfolio_comp_params.argtypes = [ctypes.POINTER(nm.PortfolioData)]
+        R.portfolio_comp_params(ctypes.byref(e))
+        theirs = b"".join(ctypes.string_at(e.options[m].data, ctypes.sizeof(nm.OptionParams) * e.options[m].size) for m in range(3))
+        assert ours == theirs
+    starts = [d.options[m].data[k].start for m in range(3) for k in range(d.options[m].size)]
+    assert np.all(np.isfinite(starts)) and np.all(np.array(starts) >= 0)
+    b = nm.make_batch([pf, O.synthetic_portfolio(2, 7, 18)], [1.0, 2.0])
+    assert list(b["stock_off"]) == [0, 5, 7] and list(b["option_off"]) == [0, 60, 67]
+    assert len(b["strike"]) == 67 and list(b["K"]) == [1.0, 2.0]
