@@ -1,7 +1,7 @@
-"""The binding a maintainer would add (the ctypes stub printed in INTEGRATION.md) runs as written
-against the built library: its struct definitions and calls are valid.  Without a device the
-calls report errors through nmlmc_last_error instead of exiting, so the stub's final check is
-replaced by a print."""
+"""The code in INTEGRATION.md stays valid: the ctypes stub a maintainer would add runs as written
+against the built library (without a device its calls report errors through nmlmc_last_error
+instead of exiting, so its final check becomes a print), and the C snippets of the native API
+compile and link."""
 import os
 import re
 import subprocess
@@ -18,3 +18,25 @@ def test_integration_ctypes_stub_runs():
     out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=120)
     assert out.returncode == 0, out.stderr[-2000:]
     assert "status" in out.stdout
+
+
+def test_integration_c_snippets_compile_and_link(nm, tmp_path):
+    """The C snippets of INTEGRATION.md compile as C99 against include/nmlmc.h and link against
+    the library (not run: they need a device)."""
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    b0, b1, b2 = re.findall(r"```c\n(.*?)```", text, re.S)[:3]
+    src = ("#include <stdint.h>\n#include <stddef.h>\n#include \"nmlmc.h\"\nint main(void) {\n" + b0 +
+           "uint32_t ell = 3;\n" + b1 +
+           "{\nconst uint32_t so[3] = {0, 1, 2}, oo[3] = {0, 1, 2}, si[2] = {0, 0};\n"
+           "const int32_t ty[2] = {1, -1};\n"
+           "const double S0[2] = {100, 90}, mu[2] = {0.05, 0.05}, sg[2] = {0.2, 0.3}, K[2] = {100, 95},"
+           " T[2] = {1, 2}, w[2] = {1, -1}, Kloss[2] = {0, 0};\n"
+           "double dEL_dw[2], dP_dw[2], dEL_dsigma[2], dP_dsigma[2];\n" + b2 + "}\n"
+           "nmlmc_destroy(ctx);\nreturn 0;\n}\n")
+    c = tmp_path / "snippets.c"
+    c.write_text(src)
+    libdir = os.path.dirname(nm.LIB_PATH)
+    out = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-Wno-unused-variable",
+                          f"-I{os.path.join(ROOT, 'include')}", str(c), "-o", str(tmp_path / "snippets"),
+                          f"-L{libdir}", "-lnmlmc"], capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr[-3000:]
