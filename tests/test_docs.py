@@ -40,3 +40,21 @@ def test_integration_c_snippets_compile_and_link(nm, tmp_path):
                           f"-I{os.path.join(ROOT, 'include')}", str(c), "-o", str(tmp_path / "snippets"),
                           f"-L{libdir}", "-lnmlmc"], capture_output=True, text=True)
     assert out.returncode == 0, out.stderr[-3000:]
+
+
+def test_integration_cpp_snippet_compiles(nm, tmp_path):
+    """The C++ snippet of INTEGRATION.md compiles as C++14 against include/nmlmc.hpp and links."""
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    code = re.findall(r"```cpp\n(.*?)```", text, re.S)[0]
+    include, body = code.split("\n", 1)
+    assert include.startswith("#include")
+    src = ("#include <iostream>\n" + include + "\nint main() {\n"
+           "uint32_t ell = 2; uint64_t M = 10, inner_stats[6]; double fsums[4], diffsums[4], work;\n"
+           + body + "return 0;\n}\n")
+    c = tmp_path / "snippet.cpp"
+    c.write_text(src)
+    libdir = os.path.dirname(nm.LIB_PATH)
+    out = subprocess.run(["g++", "-std=c++14", "-Wall", "-Werror", "-Wno-unused-variable",
+                          "-Wno-unused-parameter", f"-I{os.path.join(ROOT, 'include')}", str(c), "-o",
+                          str(tmp_path / "snippet"), f"-L{libdir}", "-lnmlmc"], capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr[-3000:]
