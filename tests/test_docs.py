@@ -58,3 +58,14 @@ def test_integration_cpp_snippet_compiles(nm, tmp_path):
                           "-Wno-unused-parameter", f"-I{os.path.join(ROOT, 'include')}", str(c), "-o",
                           str(tmp_path / "snippet"), f"-L{libdir}", "-lnmlmc"], capture_output=True, text=True)
     assert out.returncode == 0, out.stderr[-3000:]
+
+
+def test_integration_python_snippets_parse():
+    """Every Python snippet of INTEGRATION.md is valid Python (the multi-GPU one needs torchrun
+    and GPUs to run)."""
+    import ast
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    blocks = re.findall(r"```python\n(.*?)```", text, re.S)
+    assert len(blocks) >= 2
+    for b in blocks:
+        ast.parse(b)
