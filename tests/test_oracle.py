@@ -348,3 +348,19 @@ def test_live_reference_methods_grid(variant, prec, case):
         np.testing.assert_array_equal(a["diffsums"], b["diffsums"])
         np.testing.assert_array_equal(a["stats"], b["stats"])
         assert a["work"] == b["work"]
+
+
+def test_alias_table_exact_masses_large_portfolio():
+    """The alias table at the large portfolio's size (P = 1e6, prob ~ |w|): integer masses per
+    option equal phat_j P 2^32 and sum exactly to P 2^32 (vectorised form of the check above)."""
+    P = 1_000_000
+    g = np.random.default_rng(7)
+    p = np.abs(g.standard_normal(P))
+    thr, al, ph = O.build_alias(p)
+    unit = np.uint64(1 << 32)
+    mass = thr.astype(np.uint64)
+    np.add.at(mass, al.astype(np.int64), unit - thr.astype(np.uint64))
+    assert int(mass.sum(dtype=np.uint64)) == P * (1 << 32)
+    W = np.rint(ph * (P * float(1 << 32))).astype(np.uint64)
+    np.testing.assert_array_equal(mass, W)
+    np.testing.assert_allclose(ph, p / p.sum(), rtol=0, atol=(P / 2 + 1) / (P * 2.0 ** 32) + 1e-16)
