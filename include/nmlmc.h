@@ -397,7 +397,8 @@ typedef struct nmlmc_mlmc_input {
     double Ca;                     /* 3    */
     uint64_t M0;                   /* 100  */
     int32_t verbose;               /* print the reference's "# Sampling" lines and tables */
-    uint32_t max_levels;           /* 0 = unbounded                                       */
+    uint32_t max_levels;           /* the run stops with NMLMC_ERR_ARG when it would need
+                                      more levels (0: NMLMC_MAX_LEVELS = 64)               */
     int32_t batched;               /* 1: one nmlmc_sample_levels submission per round      */
     uint32_t max_iterations;       /* stop after this many completed TOL iterations (0: run
                                       to targetTOL); with a checkpoint, resume later        */

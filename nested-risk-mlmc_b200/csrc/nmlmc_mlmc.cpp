@@ -433,7 +433,10 @@ int run(const nmlmc_mlmc_input& in, nmlmc_sample_level_fn level_fn, nmlmc_sample
             if (sq(out.stat_error) >= in.theta * sq(out.TOL)) continue;
             out.bias_est = default_bias_estimate(out);
             if (sq(out.bias_est) >= (1 - in.theta) * sq(out.TOL)) {
-                if (in.max_levels && out.levels.size() >= in.max_levels) return NMLMC_ERR_ARG;
+                // a bias that does not decay would add levels for good: the level arrays of the
+                // output and of checkpoints hold NMLMC_MAX_LEVELS
+                if ((in.max_levels && out.levels.size() >= in.max_levels) || out.levels.size() >= NMLMC_MAX_LEVELS)
+                    return NMLMC_ERR_ARG;
                 out.levels.resize(out.levels.size() + 1);
                 continue;
             }

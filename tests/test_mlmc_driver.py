@@ -121,3 +121,17 @@ def test_driver_matches_live_reference(nm, case):
     np.testing.assert_array_equal(out["level_M"].astype(float), lv[:, 9])
     assert [out["starting_level"], out["bias_est"], out["stat_error"], out["TOL"]] == list(ref["misc"][:4])
     assert out["table"] == ref["table"]
+
+
+def test_level_cap(nm):
+    """A bias that never decays (difference variance and mean constant over levels) would add
+    levels for good: the driver stops with NMLMC_ERR_ARG at max_levels, or at the 64 levels the
+    output and checkpoint arrays hold."""
+    syn = Synthetic(0.5, 1.0, 0.5, 0.0, 1.0, 1.0, 16)
+    with pytest.raises(nm.NmlmcError) as e:
+        nm.mlmc_run_cb(syn, targetTOL=2e-2, M0=50, verbose=False, max_levels=5)
+    assert e.value.status == nm.ERR_ARG and max(c[0] for c in syn.calls) == 4
+    syn = Synthetic(0.5, 1.0, 0.5, 0.0, 1.0, 1.0, 16)
+    with pytest.raises(nm.NmlmcError) as e:
+        nm.mlmc_run_cb(syn, targetTOL=2e-2, M0=50, verbose=False)
+    assert e.value.status == nm.ERR_ARG and max(c[0] for c in syn.calls) == 63
