@@ -425,6 +425,9 @@ typedef void (*nmlmc_sample_levels_fn)(void* user, uint32_t n, const uint32_t* e
                                        const uint64_t* Ms, nmlmc_level_result* outs);
 
 nmlmc_mlmc_input nmlmc_mlmc_default_input(void);
+/* The runs below return NMLMC_ERR_ARG before any sample call unless targetTOL and startTOL are
+ * finite with 0 < targetTOL <= startTOL, 0 < theta < 1, Ca > 0 and M0 >= 1 (other values ask for a
+ * loop that does not end or has no samples). */
 /* Runs the continuation MLMC with the GPU sampler of `ctx`.  `table` (may be NULL) receives the
  * final to_string() table of the reference's mlmc_output_t. */
 int nmlmc_mlmc_run(nmlmc_ctx* ctx, const nmlmc_mlmc_input* in, nmlmc_mlmc_output* out,

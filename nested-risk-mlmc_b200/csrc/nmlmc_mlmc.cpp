@@ -518,6 +518,15 @@ int gpu_load_state(void* u, const void* buf, size_t size) {
 
 }  // namespace
 
+// Inputs the loop can finish with: tolerances finite and positive, the error split theta strictly
+// inside (0, 1) (theta = 0 asks for a zero statistical error, theta = 1 for a zero bias: either
+// runs for good), Ca > 0 and at least one sample per new level.
+static bool valid_input(const nmlmc_mlmc_input& in) {
+    return std::isfinite(in.targetTOL) && in.targetTOL > 0 && std::isfinite(in.startTOL) &&
+           in.startTOL >= in.targetTOL && in.theta > 0 && in.theta < 1 && std::isfinite(in.Ca) &&
+           in.Ca > 0 && std::isfinite(in.starting_level_coeff) && in.M0 >= 1;
+}
+
 // No exception may cross the C ABI: a host allocation that fails inside the driver (levels,
 // report text, checkpoint buffers) becomes NMLMC_ERR_NOMEM.
 static int guarded_run(const nmlmc_mlmc_input& in, nmlmc_sample_level_fn level_fn,
@@ -552,14 +561,14 @@ nmlmc_mlmc_input nmlmc_mlmc_default_input(void) {
 int nmlmc_mlmc_run_cb(const nmlmc_mlmc_input* in, nmlmc_sample_level_fn level_fn,
                       nmlmc_sample_levels_fn levels_fn, void* user, nmlmc_mlmc_output* out,
                       char* table, size_t table_cap) {
-    if (!in || !level_fn || !(in->targetTOL > 0) || !(in->startTOL >= in->targetTOL)) return NMLMC_ERR_ARG;
+    if (!in || !level_fn || !valid_input(*in)) return NMLMC_ERR_ARG;
     return guarded_run(*in, level_fn, levels_fn, user, nullptr, out, table, table_cap);
 }
 
 int nmlmc_mlmc_run_cb_ckpt(const nmlmc_mlmc_input* in, nmlmc_sample_level_fn level_fn,
                            nmlmc_sample_levels_fn levels_fn, void* user, const nmlmc_checkpoint_io* io,
                            nmlmc_mlmc_output* out, char* table, size_t table_cap) {
-    if (!in || !level_fn || !(in->targetTOL > 0) || !(in->startTOL >= in->targetTOL)) return NMLMC_ERR_ARG;
+    if (!in || !level_fn || !valid_input(*in)) return NMLMC_ERR_ARG;
     return guarded_run(*in, level_fn, levels_fn, user, io, out, table, table_cap);
 }
 

@@ -135,3 +135,17 @@ def test_level_cap(nm):
     with pytest.raises(nm.NmlmcError) as e:
         nm.mlmc_run_cb(syn, targetTOL=2e-2, M0=50, verbose=False)
     assert e.value.status == nm.ERR_ARG and max(c[0] for c in syn.calls) == 63
+
+
+@pytest.mark.parametrize("bad", [dict(M0=0), dict(theta=0.0), dict(theta=1.0), dict(Ca=0.0),
+                                 dict(startTOL=float("inf")), dict(targetTOL=float("nan")),
+                                 dict(targetTOL=0.0), dict(startTOL=1e-4)])
+def test_driver_rejects_inputs_it_cannot_finish(nm, bad):
+    """theta = 0 or 1 asks for a zero statistical error or bias (the loop would never end), M0 = 0
+    samples nothing, non-finite tolerances break the TOL sequence: NMLMC_ERR_ARG before any call."""
+    syn = Synthetic(0.5, 1.0, 0.5, 1.5, 1.0, 1.0, 3)
+    kw = dict(targetTOL=1e-2, M0=50, verbose=False)
+    kw.update(bad)
+    with pytest.raises(nm.NmlmcError) as e:
+        nm.mlmc_run_cb(syn, **kw)
+    assert e.value.status == nm.ERR_ARG and syn.calls == []
