@@ -427,7 +427,9 @@ typedef void (*nmlmc_sample_levels_fn)(void* user, uint32_t n, const uint32_t* e
 nmlmc_mlmc_input nmlmc_mlmc_default_input(void);
 /* The runs below return NMLMC_ERR_ARG before any sample call unless targetTOL and startTOL are
  * finite with 0 < targetTOL <= startTOL, 0 < theta < 1, Ca > 0 and M0 >= 1 (other values ask for a
- * loop that does not end or has no samples). */
+ * loop that does not end or has no samples).  During a run, a level result with a non-finite sum
+ * or work (or M = 0) stops it with NMLMC_ERR_STATE; a level that would need 2^62 or more samples,
+ * or a level beyond max_levels, stops it with NMLMC_ERR_ARG. */
 /* Runs the continuation MLMC with the GPU sampler of `ctx`.  `table` (may be NULL) receives the
  * final to_string() table of the reference's mlmc_output_t. */
 int nmlmc_mlmc_run(nmlmc_ctx* ctx, const nmlmc_mlmc_input* in, nmlmc_mlmc_output* out,

@@ -203,6 +203,17 @@ uint32_t better_starting_level(const Output& out, double coeff) {      // mlmc.h
     return l0;
 }
 
+// A level's sample count from the optimal-allocation formula.  A variance that rounds below zero
+// makes the formula NaN (the reference then converts NaN to an integer, which C++ leaves
+// undefined): it counts as no further samples.  A count at or beyond 2^62 cannot be a run that
+// ends and is reported as kCountOverflow.
+constexpr uint64_t kCountOverflow = ~0ull;
+uint64_t to_count(double x) {
+    if (!(x > 0)) return 0;
+    const double c = std::ceil(x);
+    return c >= 0x1p62 ? kCountOverflow : static_cast<uint64_t>(c);
+}
+
 void optimal_Ml(double tol2, uint64_t M0, const Output& out, std::vector<uint64_t>& Ml) {  // 265-288
     uint32_t l = out.starting_level;
     Ml.resize(out.levels.size());
@@ -212,11 +223,16 @@ void optimal_Ml(double tol2, uint64_t M0, const Output& out, std::vector<uint64_
         lambda += out.levels[l].M == 0 ? 0 : std::sqrt(out.levels[l].Wl() * out.levels[l].dVl());
     lambda /= tol2;
     l = out.starting_level;
-    Ml[l] = (out.levels[l].M == 0) ? M0
-                                   : static_cast<uint64_t>(std::ceil(lambda * std::sqrt(out.levels[l].fVl() / out.levels[l].Wl())));
+    Ml[l] = (out.levels[l].M == 0) ? M0 : to_count(lambda * std::sqrt(out.levels[l].fVl() / out.levels[l].Wl()));
     for (l = out.starting_level + 1; l < out.levels.size(); l++)
-        Ml[l] = (out.levels[l].M == 0) ? M0
-                                       : static_cast<uint64_t>(std::ceil(lambda * std::sqrt(out.levels[l].dVl() / out.levels[l].Wl())));
+        Ml[l] = (out.levels[l].M == 0) ? M0 : to_count(lambda * std::sqrt(out.levels[l].dVl() / out.levels[l].Wl()));
+}
+
+// A sampler's level result the driver can use: finite sums and a finite, non-negative work.
+bool usable(const nmlmc_level_result& r) {
+    bool ok = std::isfinite(r.total_work) && r.total_work >= 0;
+    for (int j = 0; j < 4; j++) ok = ok && std::isfinite(r.fsums[j]) && std::isfinite(r.diffsums[j]);
+    return ok;
 }
 
 Level from_result(const nmlmc_level_result& r) {
@@ -396,6 +412,8 @@ int run(const nmlmc_mlmc_input& in, nmlmc_sample_level_fn level_fn, nmlmc_sample
         out.starting_level = better_starting_level(out, in.starting_level_coeff);
         while (true) {
             optimal_Ml(in.theta * sq(out.TOL) / in.Ca, in.M0, out, Ml);
+            for (uint64_t m : Ml)
+                if (m == kCountOverflow) return NMLMC_ERR_ARG;        // no run of this size ends
             std::vector<uint32_t> ells;
             std::vector<uint64_t> Ms;
             for (uint32_t l = 0; l < out.levels.size(); l++) {
@@ -412,7 +430,7 @@ int run(const nmlmc_mlmc_input& in, nmlmc_sample_level_fn level_fn, nmlmc_sample
                 levels_fn(user, (uint32_t)ells.size(), ells.data(), Ms.data(), rs.data());
                 calls += ells.size();
                 for (size_t i = 0; i < ells.size(); i++) {
-                    if (rs[i].M != Ms[i]) return NMLMC_ERR_STATE;
+                    if (rs[i].M != Ms[i] || !usable(rs[i])) return NMLMC_ERR_STATE;
                     out.levels[ells[i]] += from_result(rs[i]);
                 }
             } else {
@@ -424,7 +442,7 @@ int run(const nmlmc_mlmc_input& in, nmlmc_sample_level_fn level_fn, nmlmc_sample
                         memset(&r, 0, sizeof r);
                         level_fn(user, l, M, &r);
                         calls++;
-                        if (r.M == 0) return NMLMC_ERR_STATE;   // the sampler failed
+                        if (r.M == 0 || !usable(r)) return NMLMC_ERR_STATE;   // the sampler failed
                         out.levels[l] += from_result(r);
                     }
                 }

@@ -149,3 +149,33 @@ def test_driver_rejects_inputs_it_cannot_finish(nm, bad):
     with pytest.raises(nm.NmlmcError) as e:
         nm.mlmc_run_cb(syn, **kw)
     assert e.value.status == nm.ERR_ARG and syn.calls == []
+
+
+@pytest.mark.parametrize("key,level", [("diffsums", 1), ("fsums", 0), ("fsums", 2)])
+def test_non_finite_level_results_stop_the_run(nm, key, level):
+    """A sampler that returns a non-finite sum stops the run with NMLMC_ERR_STATE at that call,
+    instead of turning into NaN sample counts (an absurd next request) or a silent NaN estimate."""
+    syn = Synthetic(0.5, 1.0, 0.5, 1.5, 1.0, 1.0, 3)
+    calls = []
+
+    def bad(ell, M):
+        calls.append((ell, M))
+        assert M < 10**8, "absurd sample request"
+        r = syn(ell, M)
+        if ell == level:
+            r[key][1] = float("nan")
+        return r
+
+    with pytest.raises(nm.NmlmcError) as e:
+        nm.mlmc_run_cb(bad, targetTOL=1e-2, M0=50, verbose=False)
+    assert e.value.status == nm.ERR_STATE and e.value.__cause__ is None
+    assert calls[-1][0] == level
+
+
+def test_sample_count_beyond_range_is_an_error(nm):
+    """A tolerance no run can reach on this problem (over 2^62 samples on a level) is reported,
+    not converted into a wrapped integer request."""
+    syn = Synthetic(0.5, 1.0, 1e30, 1.5, 1.0, 1.0, 3)
+    with pytest.raises(nm.NmlmcError) as e:
+        nm.mlmc_run_cb(syn, targetTOL=1e-12, startTOL=1e-12, M0=50, verbose=False)
+    assert e.value.status == nm.ERR_ARG
