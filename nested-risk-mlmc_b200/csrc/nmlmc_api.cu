@@ -767,8 +767,9 @@ cudaError_t time_phase_config(nmlmc_ctx* c, uint32_t ell, uint64_t Mp, const Pha
 // Probe size, measured: starting from min(4096, M, batch) outer samples, the default
 // configuration is timed on growing probes (at most 8x per step, launch overheads make small
 // probes look cheap) until one takes kProbeMs of device time or the probe reaches the call's M or
-// one batch.  Shorter probes mis-ranked the variants of the large-portfolio levels.  The work per outer sample ranges from the base count to the maximum count of the level,
-// too wide to predict from the configuration.
+// one batch.  Shorter probes mis-ranked the variants of the large-portfolio levels.  The work per
+// outer sample ranges from the base count to the maximum count of the level, too wide to predict
+// from the configuration.
 template <class RT>
 cudaError_t probe_size(nmlmc_ctx* c, uint32_t ell, uint64_t M, uint64_t& Mp) {
     const uint64_t lim = M < c->ob.cap ? M : c->ob.cap;
