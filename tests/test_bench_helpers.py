@@ -92,3 +92,62 @@ def test_reference_model_main_on_the_cpu(golden):
         pytest.skip(r["unavailable"])
     assert r["threads"] == 2 and r["levels"] >= 2 and r["total_work"] > 0
     assert abs(r["Eg"] - bench.REF_MAIN["eta"]) < 3e-2
+
+
+class _FakeSampler:
+    """Stands in for nmlmc.Sampler in the bench's default path: fixed level results, so the
+    JSON line's assembly runs without a GPU."""
+
+    def __init__(self, device=0, **kw):
+        self.kw = kw
+
+    def set_model(self, *a):
+        pass
+
+    def set_autotune(self, mode):
+        pass
+
+    def configure(self, **kw):
+        pass
+
+    def set_profiling(self, on):
+        pass
+
+    def phase_kernel_time(self):
+        return 40, 0.1
+
+    def phase_config(self, ell):
+        return dict(variant=1, chunk=32, state=1, probe_ms=20.0)
+
+    def mlmc_run(self, targetTOL, M0, batched=False):
+        import numpy as np
+        n = 4
+        return dict(level_time=np.full(n, 0.03), total_work=2.0e9, calls=12, nlevels=n,
+                    level_M=np.array([1000, 500, 200, 100], np.uint64), Eg=0.1587)
+
+
+def test_default_line_with_a_fake_sampler(monkeypatch, capsys):
+    """bench.py's default run assembles a line with every key of the contract (value, e2e with
+    its byte counts, roofline, clocks, gpu_launches, config) from the sampler's results."""
+    import json
+    import sys
+    import types
+    fake = types.ModuleType("nmlmc")
+    fake.Sampler = _FakeSampler
+    fake.PREC_FP32, fake.PREC_FP64, fake.PREC_REF32 = 2, 1, 0
+    fake.STREAMS_OUTER, fake.STREAMS_CORE, fake.MODEL_SHIFT = 1, 0, 1
+    fake.kernel_launches = lambda: 0
+    monkeypatch.setitem(sys.modules, "nmlmc", fake)
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--steps", "2", "--warmup", "3", "--no-compare", "--no-cpu"])
+    for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK"):
+        monkeypatch.delenv(k, raising=False)
+    bench.main()
+    line = json.loads([l for l in capsys.readouterr().out.splitlines() if l.startswith("{")][-1])
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config", "e2e", "roofline", "clocks",
+                "gpu_launches"):
+        assert key in line, key
+    assert line["value"] == 0.12 and line["steps"] == 2 and line["warmup"] == 3
+    assert line["e2e"]["d2h_bytes_per_step"] == 12 * 144 and line["e2e"]["h2d_bytes_per_step"] == 0
+    assert line["config"]["workload"] and line["config"]["phase_config"]["0"] == [1, 32, True]
+    assert 0 < line["roofline"]["frac"] and line["roofline"]["unit"] == "Gop/s"
