@@ -356,7 +356,9 @@ int run(const nmlmc_mlmc_input& in, nmlmc_sample_level_fn level_fn, nmlmc_sample
     Output out;
     const double sqrt_2_inv = 1. / std::sqrt(2);
     uint32_t total_itrs = static_cast<uint32_t>(-(std::log2(in.targetTOL) - std::log2(in.startTOL)));
-    out.TOL = in.targetTOL * (1 << total_itrs);
+    // targetTOL 2^k as the reference's targetTOL * (1 << k), which is undefined from k = 31 on
+    // (startTOL / targetTOL >= 2^31); ldexp gives the same value below that and the right one above
+    out.TOL = std::ldexp(in.targetTOL, (int)total_itrs);
     total_itrs *= 2;
     out.levels.resize(1);
     std::vector<uint64_t> Ml(out.levels.size());

@@ -179,3 +179,12 @@ def test_sample_count_beyond_range_is_an_error(nm):
     with pytest.raises(nm.NmlmcError) as e:
         nm.mlmc_run_cb(syn, targetTOL=1e-12, startTOL=1e-12, M0=50, verbose=False)
     assert e.value.status == nm.ERR_ARG
+
+
+def test_tolerance_ratio_beyond_2_to_31(nm):
+    """startTOL / targetTOL >= 2^31: the TOL sequence still starts near startTOL (the reference's
+    targetTOL * (1 << k) is undefined from k = 31 on)."""
+    syn = Synthetic(0.5, 1.0, 0.5, 1.5, 1.0, 1.0, 3)
+    out = nm.mlmc_run_cb(syn, targetTOL=1e-11, startTOL=0.5, M0=50, verbose=False, max_iterations=1)
+    assert out["iterations_done"] == 1 and not out["complete"]
+    assert 0.5 / 2 ** 1.5 < out["TOL"] < 0.5
