@@ -69,3 +69,25 @@ def test_integration_python_snippets_parse():
     assert len(blocks) >= 2
     for b in blocks:
         ast.parse(b)
+
+
+def test_docs_cite_files_that_exist():
+    """Every repository file named in DESIGN.md, INTEGRATION.md and README.md (tests, profiles,
+    sources, headers) exists; names of the reference's own files are not checked."""
+    reference_files = {"common.cpp", "common.hpp", "mlmc.hpp", "model_sampler.cpp", "nested_sampler.hpp",
+                       "par_nvcc.hpp", "par_omp.hpp", "portfolio_sampler.cpp", "gbm_approx.hpp",
+                       "table_output.hpp", "threefry.h", "boxmuller.hpp", "uniform.hpp", "array.h",
+                       "mlmc_test.cpp", "parse_mlmc_output.py", "my_main.cpp"}
+    pkg = os.path.join(ROOT, "nested-risk-mlmc_b200")
+    roots = [ROOT, pkg, os.path.join(pkg, "csrc"), os.path.join(pkg, "nmlmc"), os.path.join(ROOT, "oracle"),
+             os.path.join(ROOT, "tests"), os.path.join(ROOT, "tests", "abi"), os.path.join(ROOT, "include")]
+    missing = []
+    for doc in ("DESIGN.md", "INTEGRATION.md", "README.md"):
+        text = open(os.path.join(ROOT, doc)).read()
+        for m in re.finditer(r"[\w./-]+\.(?:py|md|cu|cuh|cpp|c|h|hpp|inc|json)\b", text):
+            name = m.group(0).strip("./")
+            if os.path.basename(name) in reference_files or name.startswith("_body"):
+                continue
+            if not any(os.path.exists(os.path.join(r, name)) for r in roots):
+                missing.append((doc, name))
+    assert not missing, missing
