@@ -151,3 +151,13 @@ def test_default_line_with_a_fake_sampler(monkeypatch, capsys):
     assert line["e2e"]["d2h_bytes_per_step"] == 12 * 144 and line["e2e"]["h2d_bytes_per_step"] == 0
     assert line["config"]["workload"] and line["config"]["phase_config"]["0"] == [1, 32, True]
     assert 0 < line["roofline"]["frac"] and line["roofline"]["unit"] == "Gop/s"
+
+
+def test_cpu_baseline_falls_back_to_the_port(monkeypatch):
+    """Without oracle/_ref the CPU baseline times the C restatement (kind "port", one thread) on
+    the same bounded per-level samples."""
+    import oracle as O
+    monkeypatch.setattr(O, "ref_available", lambda variant="f32": False)
+    schedule = dict(levels=[0, 1], M=[4000, 1000])
+    v, kind, cores, desc = bench.cpu_reference_time(schedule, budget_s=0.2)
+    assert kind == "port" and cores == 1 and v > 0 and "C port" in desc
