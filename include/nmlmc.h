@@ -30,7 +30,9 @@ enum {
     NMLMC_OK = 0,
     NMLMC_ERR_ARG = 1,        /* invalid argument (also: unsupported configuration)       */
     NMLMC_ERR_CUDA = 2,       /* a CUDA runtime call failed                                */
-    NMLMC_ERR_STATE = 3,      /* call out of order (no model / portfolio set, no context) */
+    NMLMC_ERR_STATE = 3,      /* call out of order (no model / portfolio set, no context),
+                                 a level sampler that failed, or sampler-state / checkpoint
+                                 I/O that failed                                           */
     NMLMC_ERR_NOMEM = 4,      /* device or host allocation failed                          */
     NMLMC_ERR_TIMEOUT = 5,    /* a bounded device wait gave up                             */
     NMLMC_ERR_LIMIT = 6       /* a path-simulated inner sample drew a level whose step count

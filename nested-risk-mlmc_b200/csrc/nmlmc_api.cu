@@ -980,7 +980,7 @@ const char* nmlmc_error_string(int s) {
     case NMLMC_OK: return "ok";
     case NMLMC_ERR_ARG: return "invalid argument";
     case NMLMC_ERR_CUDA: return "CUDA error";
-    case NMLMC_ERR_STATE: return "call out of order";
+    case NMLMC_ERR_STATE: return "call out of order, failed level sampler or state / checkpoint I/O";
     case NMLMC_ERR_NOMEM: return "out of memory";
     case NMLMC_ERR_TIMEOUT: return "bounded device wait gave up";
     case NMLMC_ERR_LIMIT: return "a path-simulated inner sample exceeded NMLMC_MAX_PATH_STEPS";
