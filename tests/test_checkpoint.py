@@ -251,3 +251,13 @@ def test_damaged_checkpoints_are_errors_not_crashes(nm, golden, tmp_path):
     assert attempt(bytes(b)) == "error"
     b[128:136] = struct.pack("<d", float("inf"))
     assert attempt(bytes(b)) == "error"
+
+
+def test_unwritable_checkpoint_stops_the_run(nm, golden, tmp_path):
+    """A checkpoint that cannot be written (its directory is missing) stops the run with
+    NMLMC_ERR_STATE at the first save instead of running on unprotected."""
+    kw, sa = _args(golden)
+    s = Synthetic(*sa)
+    with pytest.raises(nm.NmlmcError) as e:
+        nm.mlmc_run_cb(s, targetTOL=kw["tol"], M0=kw["M0"], checkpoint=str(tmp_path / "missing" / "x.ckpt"))
+    assert e.value.status == nm.ERR_STATE and len(s.calls) > 0
