@@ -152,3 +152,20 @@ def test_norm_cdf_inv_export_matches_the_reference(nm, golden):
     f.argtypes = [ctypes.c_float]
     got = np.array([f(float(p)) for p in A["ncdfinv/p"]], dtype=np.float32)
     np.testing.assert_array_equal(got.astype(np.float64), A["ncdfinv/f32"])
+
+
+def test_python_constants_match_the_header(nm):
+    """The binding's status, precision, stream-layout, model and sub-sampling constants have the
+    values include/nmlmc.h gives them."""
+    src = open(os.path.join(ROOT, "include", "nmlmc.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    values = {m.group(1): int(m.group(2)) for m in re.finditer(r"\b(NMLMC_[A-Z0-9_]+)\s*=\s*(-?\d+)", src)}
+    pairs = {"NMLMC_OK": "OK", "NMLMC_ERR_ARG": "ERR_ARG", "NMLMC_ERR_CUDA": "ERR_CUDA",
+             "NMLMC_ERR_STATE": "ERR_STATE", "NMLMC_ERR_NOMEM": "ERR_NOMEM",
+             "NMLMC_ERR_TIMEOUT": "ERR_TIMEOUT", "NMLMC_ERR_LIMIT": "ERR_LIMIT",
+             "NMLMC_PREC_REF32": "PREC_REF32", "NMLMC_PREC_FP64": "PREC_FP64", "NMLMC_PREC_FP32": "PREC_FP32",
+             "NMLMC_STREAMS_CORE": "STREAMS_CORE", "NMLMC_STREAMS_OUTER": "STREAMS_OUTER",
+             "NMLMC_MODEL_REFERENCE": "MODEL_REFERENCE", "NMLMC_MODEL_SHIFT": "MODEL_SHIFT",
+             "NMLMC_SUB_NONE": "SUB_NONE", "NMLMC_SUB_RANDOM": "SUB_RANDOM", "NMLMC_SUB_UNIFORM": "SUB_UNIFORM"}
+    for c_name, py_name in pairs.items():
+        assert values[c_name] == getattr(nm, py_name), c_name
