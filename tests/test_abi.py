@@ -169,3 +169,38 @@ def test_python_constants_match_the_header(nm):
              "NMLMC_SUB_NONE": "SUB_NONE", "NMLMC_SUB_RANDOM": "SUB_RANDOM", "NMLMC_SUB_UNIFORM": "SUB_UNIFORM"}
     for c_name, py_name in pairs.items():
         assert values[c_name] == getattr(nm, py_name), c_name
+
+
+def test_ctypes_structs_match_the_c_header(nm, tmp_path):
+    """Every struct of the Python binding has the size and field offsets the C compiler gives the
+    header's struct of the same name (a mismatch would corrupt memory in the native calls)."""
+    structs = {"NestedSamplerParams": "nested_sampler_params", "SampleOutput": "sample_output",
+               "ModelData": "model_data", "OptionParams": "option_params", "StockParams": "stock_params",
+               "PortfolioData": "portfolio_data", "Config": "nmlmc_config", "LevelResult": "nmlmc_level_result",
+               "Portfolio": "nmlmc_portfolio", "PathMethods": "nmlmc_path_methods",
+               "PortfolioBatch": "nmlmc_portfolio_batch", "AdjointConfig": "nmlmc_adjoint_config",
+               "AdjointResult": "nmlmc_adjoint_result", "TraceRec": "nmlmc_trace_rec",
+               "MlmcInput": "nmlmc_mlmc_input", "MlmcOutput": "nmlmc_mlmc_output",
+               "PortfolioSpec": "nmlmc_portfolio_spec", "PhaseConfig": "nmlmc_phase_config",
+               "CheckpointIO": "nmlmc_checkpoint_io"}
+    lines, expect = [], {}
+    for py, c in structs.items():
+        cls = getattr(nm, py)
+        lines.append(f'printf("{c} sizeof %zu\\n", sizeof({c}));')
+        expect[(c, "sizeof")] = ctypes.sizeof(cls)
+        for f in cls._fields_:
+            lines.append(f'printf("{c} {f[0]} %zu\\n", offsetof({c}, {f[0]}));')
+            expect[(c, f[0])] = getattr(cls, f[0]).offset
+    src = tmp_path / "layout.c"
+    src.write_text("#include <stddef.h>\n#include <stdio.h>\n#include \"nmlmc.h\"\nint main(void) {\n" +
+                   "\n".join(lines) + "\nreturn 0;\n}\n")
+    exe = tmp_path / "layout"
+    cc = subprocess.run(["gcc", "-std=c99", f"-I{os.path.join(ROOT, 'include')}", str(src), "-o", str(exe)],
+                        capture_output=True, text=True)
+    assert cc.returncode == 0, cc.stderr[-3000:]
+    got = {}
+    for line in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        c, field, value = line.split()
+        got[(c, field)] = int(value)
+    mismatched = {k: (expect[k], got[k]) for k in expect if expect[k] != got[k]}
+    assert not mismatched, mismatched
