@@ -204,3 +204,24 @@ def test_ctypes_structs_match_the_c_header(nm, tmp_path):
         got[(c, field)] = int(value)
     mismatched = {k: (expect[k], got[k]) for k in expect if expect[k] != got[k]}
     assert not mismatched, mismatched
+
+
+def test_ctypes_argument_counts_match_the_header(nm):
+    """Each function the binding declares argument types for takes as many arguments as its C
+    prototype in include/nmlmc.h."""
+    src = open(os.path.join(ROOT, "include", "nmlmc.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    protos = {}
+    for m in re.finditer(r"^[A-Za-z_][\w \*]*?\b([A-Za-z_]\w*)\s*\(([^;{]*?)\)\s*;", src, flags=re.M):
+        if m.group(0).lstrip().startswith("typedef"):
+            continue
+        params = " ".join(m.group(2).split())
+        protos[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    lib = nm.lib()
+    checked = 0
+    for name, n in protos.items():
+        argtypes = getattr(lib, name).argtypes
+        if argtypes is not None:
+            assert len(argtypes) == n, (name, len(argtypes), n)
+            checked += 1
+    assert checked >= 20
