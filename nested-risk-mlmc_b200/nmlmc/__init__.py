@@ -300,6 +300,11 @@ def lib() -> ctypes.CDLL:
     L.portfolio_init.argtypes = [ctypes.POINTER(PortfolioData), ctypes.c_uint64]
     L.portfolio_sample.argtypes = [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(SampleOutput)]
     L.portfolio_comp_params.argtypes = [ctypes.POINTER(PortfolioData)]
+    L.portfolio_gen_data.restype = PortfolioData
+    L.portfolio_gen_data.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64,
+                                     ctypes.POINTER(ctypes.c_double), ctypes.c_bool, ctypes.c_bool]
+    L.portfolio_free_data.restype = None
+    L.portfolio_free_data.argtypes = [ctypes.POINTER(PortfolioData)]
     L.norm_cdf_inv.restype = ctypes.c_float
     L.norm_cdf_inv.argtypes = [ctypes.c_float]
     L.nmlmc_default_set_precision.argtypes = [ctypes.c_int32, ctypes.c_int32]
