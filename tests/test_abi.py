@@ -225,3 +225,22 @@ def test_ctypes_argument_counts_match_the_header(nm):
             assert len(argtypes) == n, (name, len(argtypes), n)
             checked += 1
     assert checked >= 20
+
+
+def test_ctypes_result_types_match_the_header(nm):
+    """Functions of the header that return something other than int or void have that result
+    type in the binding (a float or struct read as int would be garbage)."""
+    src = open(os.path.join(ROOT, "include", "nmlmc.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    want = {"uint64_t": ctypes.c_uint64, "const char*": ctypes.c_char_p, "float": ctypes.c_float,
+            "portfolio_data": nm.PortfolioData, "nmlmc_mlmc_input": nm.MlmcInput}
+    lib = nm.lib()
+    seen = 0
+    for m in re.finditer(r"^([A-Za-z_][\w \*]*?)\s*\b([A-Za-z_]\w*)\s*\(([^;{]*?)\)\s*;", src, flags=re.M):
+        ret = " ".join(m.group(1).split()).replace(" *", "*")
+        if ret.startswith("typedef") or ret in ("int", "void"):
+            continue
+        assert ret in want, (m.group(2), ret)
+        assert getattr(lib, m.group(2)).restype == want[ret], m.group(2)
+        seen += 1
+    assert seen >= 5
