@@ -1,30 +1,38 @@
-"""Benchmark: time-to-eps of the nested-MLMC estimate of P(E[X|Y] > K) on B200.
+"""Benchmark: time-to-eps of the nested-MLMC estimate of P(L > K) on B200.
 
-Workload (the adaptive model-problem configuration): Y ~ N(0,1), inner X = Y + Z, K = 1 (exact
-1 - Phi(1)); N0 = 32 inner samples at level 0, beta = 2, adaptive inner sampling with exponent
-r = 1.5 (the reference's default; the r = 2 rule keeps a 3-sigma stopping confidence at every
-level and its bias levels off above eps), antithetic coarse estimator, 4 moments,
-continuation MLMC to RMSE eps = 1e-4.  A step is one complete MLMC run (host driver + level
-sampler) to eps; synthetic inputs (the model problem has no data).
+Default workload (the large-portfolio configuration): d = 200 GBM stocks (S0 = 100, r = mu = 0.05,
+sigma ~ U[0.1, 0.4], tau = 1/52), P = 1e6 European options (seeded generator, seed 1: uniform
+stock, 50/50 call/put, strike ~ U[0.8, 1.2] S0, maturity ~ U[0.25, 2], position ~ N(0, 1)), loss
+L(Y) = sum_i w_i (V_i(0) - V_i(tau, S(tau))) with Black-Scholes values, K = the 99 % quantile of L
+over 1e5 full evaluations.  P(L > K) ~ 0.01 by continuation MLMC to RMSE eps = 1e-4 with the
+reference's default importance sub-sampling (prob ~ |w_i|), the delta control variate, adaptive
+inner sampling (N0 = 64, beta = 2, r = 1.5) and the antithetic estimator.  A step is one complete
+MLMC run (host driver + level sampler) to eps; synthetic inputs (seeded generator, no dataset).
 
-Our arm: the batched FP32 sampler (OUTER streams, Kahan FP32 inner sums, FP64 moments), all levels
-of an MLMC round in one submission (one CUDA graph per round).  Reported next to it, on the same GPU and seed:
-  * the all-FP64 run of the same sampler on the same streams (accuracy and speed),
-  * the plain FP64 drop-in: the reference's stream semantics (a warp per virtual core, 2048
-    cores like the reference's CUDA main), one synchronous launch per sample_level call.
+Our arm: the batched FP32 sampler (OUTER streams, SFU Black-Scholes, Kahan FP32 inner sums, FP64
+moments), all levels of an MLMC round in one submission (one CUDA graph per round).  `value` is the
+device time of the run's levels (%globaltimer stamps at the level boundaries inside each round's
+graph); `e2e` is the wall time of the same step through the C ABI from host buffers: the upload of
+the portfolio tables (set_portfolio: option records, alias table) and the whole run (host driver
+decisions, graph updates and launches, the device->host copy of every level result).  Reported
+beside it on the same GPU: the plain FP64 drop-in (the reference's stream layout, 2048 virtual
+cores, one synchronous call per level; timed per level on bounded samples and scaled by the level
+counts of the run, with a full measured run at eps = 1e-3 as its calibration), the per-level
+FP32 error against the all-FP64 sampler on the same streams, the phase kernel's roofline, the
+K-quantile sweep; and the reference's own CPU sampler (oracle/_ref, OpenMP on all host threads),
+timed the same way with a full measured CPU run at a looser eps as its calibration.
 
-`value` is the device time of the run's levels (%globaltimer stamps written at the level
-boundaries inside each round's CUDA graph); `e2e` is the wall time of the whole run through the
-C ABI (host driver decisions, graph updates and launches, the device->host copy of every level
-result).  The phase kernel's roofline comes from a profiled repeat of the timed runs with CUDA
-events around every phase-kernel launch.  Multi-GPU (torchrun): every rank samples its share of
-each level call and the level results are all-reduced (16 doubles), so the estimate equals the
-single-GPU one and total work is fixed (strong scaling).
+Multi-GPU (torchrun): every rank samples its share of each level call and the level results are
+all-reduced (16 doubles per level), so the estimate equals the single-GPU one and total work is
+fixed (strong scaling).
 
---impl reference times the reference's own CPU implementation (oracle/_ref: the reference
-sources compiled here, OpenMP on all host threads; the C restatement if absent) on bounded
-per-level samples and multiplies its per-outer-sample cost by the level sample counts the
-MLMC run needs at eps (bench_schedule.json).
+--case c1 is the adaptive model problem (Y ~ N(0,1), X = Y + Z, K = 1, exact 1 - Phi(1)) to
+eps = 1e-4; the other cases are profiling cases of single kernels.
+
+--impl reference times the reference's own CPU implementation (oracle/_ref: the reference sources
+compiled here, OpenMP on all host threads; the C restatement if absent) on bounded per-level
+samples and multiplies its per-outer-sample cost by the level sample counts the MLMC run needs at
+eps (bench_schedule.json, recorded from the GPU run).
 """
 from __future__ import annotations
 
@@ -45,12 +53,26 @@ SCHEDULE = os.path.join(ROOT, "bench_schedule.json")
 EPS = 1e-4
 METRIC = "time-to-ε (s) for MLMC P(loss>K) at ε=1e-4, batched FP32 vs plain FP64, 1 B200"
 ADAPTIVE_R = 1.5
-WORKLOAD = dict(workload="model problem X=Y+Z, K=1, adaptive inner sampling, levels to eps",
-                N0=32, beta=2, adaptive_r=ADAPTIVE_R, antithetic=True, moments=4, eps=EPS, M0=1024,
-                adaptive_rule_note=("r=1.5, the reference's default exponent; the r=2 rule (double "
-                                    "while |mean-K| < 3 sigma/sqrt(N)) keeps a fixed 3-sigma stopping "
-                                    "confidence at every level and its bias levels off at 3.7e-4 > eps"),
-                l2_flush="not needed: no input data; every inner draw is computed from a counter")
+# The large-portfolio configuration; the same dict is the `config` of both arms' lines.
+C3_CONFIG = dict(workload="large portfolio: d=200 GBM stocks, P=1e6 European options, P(L>K) with "
+                          "K the 99% loss quantile of 1e5 full evaluations",
+                 stocks=200, options=1_000_000, generator_seed=1, tau="1/52", r=0.05, rho=0.0,
+                 sub_sampling="importance, prob ~ |w_i|", delta_cv=True, N0=64, beta=2,
+                 adaptive_r=ADAPTIVE_R, antithetic=True, moments=4, eps=EPS, M0=1024,
+                 deviations=("r=1.5 (the reference's default exponent); the host driver adds levels "
+                             "until its bias test passes (to level 15, from starting level 11) where "
+                             "the configuration text names levels 0-10; the FP32 option table is one "
+                             "packed 32-byte record per option plus an 8-byte alias entry (40 MB) "
+                             "instead of the 21-byte structure of arrays; the loss carries no "
+                             "e^{-r tau} discount (the configuration's L(Y))"),
+                 l2_flush="not flushed: inputs (40 MB of option and alias tables) stay L2-resident "
+                          "by design; every inner draw is computed from a counter")
+C1_WORKLOAD = dict(workload="model problem X=Y+Z, K=1, adaptive inner sampling, levels to eps",
+                   N0=32, beta=2, adaptive_r=ADAPTIVE_R, antithetic=True, moments=4, eps=EPS, M0=1024,
+                   adaptive_rule_note=("r=1.5, the reference's default exponent; the r=2 rule (double "
+                                       "while |mean-K| < 3 sigma/sqrt(N)) keeps a fixed 3-sigma stopping "
+                                       "confidence at every level and its bias levels off at 3.7e-4 > eps"),
+                   l2_flush="not needed: no input data; every inner draw is computed from a counter")
 # Algorithmic lane operations per inner sample of the X = Y + Z model on the FP32 path:
 #   Threefry2x64-20 block = 140 INT32 ops (20 rounds x (64-bit add 2 + rotate 2 + xor 2) less
 #   two 32-bit rotations, 6 key injections x 4) shared by 4 normals -> 35;
@@ -145,24 +167,24 @@ def make_sampler(nm, device, precision, streams, seed, cores=2048):
 
 
 def phase_choices(s, nlevels):
-    """The autotuner's per-level phase-kernel configuration: [variant, chunk, tuned?]."""
+    """The per-level phase-kernel configuration: [variant, chunk, tuned or pinned?]."""
     out = {}
     for ell in range(nlevels):
         p = s.phase_config(ell)
-        out[str(ell)] = [p["variant"], p["chunk"], bool(p["state"] == 1)]
+        out[str(ell)] = [p["variant"], p["chunk"], bool(p["state"] in (1, 2))]
     return out
 
 
-def run_once(nm, s, batched, dist=None):
-    """One MLMC run to EPS. Returns (result dict, wall seconds)."""
+def run_once(nm, s, batched, dist=None, eps=EPS, M0=1024):
+    """One MLMC run to eps. Returns (result dict, wall seconds)."""
     if dist is None:
         t0 = time.perf_counter()
-        out = s.mlmc_run(targetTOL=EPS, M0=WORKLOAD["M0"], batched=batched)
+        out = s.mlmc_run(targetTOL=eps, M0=M0, batched=batched)
         return out, time.perf_counter() - t0
     from nmlmc.distributed import sharded_mlmc_run
     _, dev = dist
     t0 = time.perf_counter()
-    out = sharded_mlmc_run(s, device=dev, targetTOL=EPS, M0=WORKLOAD["M0"], batched=batched)
+    out = sharded_mlmc_run(s, device=dev, targetTOL=eps, M0=M0, batched=batched)
     return out, time.perf_counter() - t0
 
 
@@ -189,16 +211,36 @@ def per_level_error(nm, device, nlevels, M=1 << 16):
 
 
 # ---------------------------------------------------------------------------------------------
+def level_costs(sample, levels, Ms, budget_s, m0):
+    """Seconds per outer sample of `sample(ell, m)` at each level: calls of m0, 2 m0, ... outer
+    samples until a call takes a quarter of the level's share of the budget (or reaches M)."""
+    per_level = budget_s / max(1, len(levels))
+    cost, details = {}, []
+    for ell, M in zip(levels, Ms):
+        if M == 0:
+            continue
+        m = min(m0, M)
+        while True:
+            t0 = time.perf_counter()
+            sample(ell, m)
+            dt = time.perf_counter() - t0
+            if dt >= per_level / 4 or m >= M:
+                break
+            m = min(M, m * max(2, int(per_level / 4 / max(dt, 1e-4))))
+        cost[ell] = dt / m
+        details.append(f"l{ell}:{m}")
+    return cost, details
+
+
 def cpu_reference_time(schedule: dict, budget_s: float = 20.0, threads: int | None = None):
-    """The reference's CPU level sampler on bounded per-level samples; returns the time-to-eps
-    it implies for `schedule` (outer samples per level at eps) and a description."""
+    """The reference's CPU level sampler of the model problem on bounded per-level samples;
+    returns the time-to-eps it implies for `schedule` (outer samples per level at eps) and a
+    description."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import numpy as np
     import oracle as O
     threads = threads or os.cpu_count() or 1
     levels = [int(l) for l in schedule["levels"]]
     Ms = [int(m) for m in schedule["M"]]
-    per_level = budget_s / max(1, len(levels))
     if O.ref_available("f32_lzcnt"):
         kind = "reference"
         ref = O.Reference("f32_lzcnt")
@@ -212,48 +254,132 @@ def cpu_reference_time(schedule: dict, budget_s: float = 20.0, threads: int | No
         s.set_model(O.MODEL_SHIFT, 0.0, 1.0)
         sample = s.sample
         cores = 1
-    total = 0.0
-    details = []
-    for ell, M in zip(levels, Ms):
-        m = 64 * cores
-        while True:
-            t0 = time.perf_counter()
-            sample(ell, m)
-            dt = time.perf_counter() - t0
-            if dt >= per_level / 4 or m >= M:
-                break
-            m = min(M, m * max(2, int(per_level / 4 / max(dt, 1e-4))))
-        per_outer = dt / m
-        total += per_outer * M
-        details.append(f"l{ell}:{m}")
+    cost, details = level_costs(sample, levels, Ms, budget_s, 64 * cores)
+    total = sum(cost[l] * M for l, M in zip(levels, Ms) if M)
     desc = (f"reference level sampler ({'oracle/_ref, real_t=float' if kind == 'reference' else 'C port'}"
             f", {cores} threads) timed on bounded samples per level [{', '.join(details)} outer samples], "
             f"cost per outer sample x the level counts of the eps={EPS:g} run; extrapolated")
     return total, kind, cores, desc
 
 
+def c3_cpu_reference(pfw, K, threads=None):
+    """The reference's CPU level sampler of the large portfolio (oracle/_ref: the reference's
+    portfolio_sample with Subsampling::Random, prob ~ |w|, the delta control variate, N0 = 64,
+    beta = 2, r = 1.5, OpenMP on `threads`), or the C restatement on one thread when the
+    reference is not built.  Returns (sample(ell, M), kind, cores, reinit(seed))."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    threads = threads or os.cpu_count() or 1
+    if O.ref_available("f32_lzcnt"):
+        ref = O.Reference("f32_lzcnt")
+
+        def reinit(seed):
+            ref.init(threads, 64, 2, ADAPTIVE_R, True)
+            ref.portfolio_init(pfw, r=0.05, rho=0.0, max_loss=K, tau=1 / 52, subsample=O.SUB_RANDOM,
+                               use_delta_cv=True, seed=seed, traced=False)
+        reinit(0)
+        return ref.sample, "reference", threads, reinit
+    s = O.Sampler(O.PREC_REF32, O.STREAMS_CORE, 1, 64, 2, ADAPTIVE_R, True, False, 0)
+
+    def reinit_port(seed):
+        s.set_portfolio(pfw, r=0.05, rho=0.0, max_loss=K, tau=1 / 52, subsample=O.SUB_RANDOM,
+                        use_delta_cv=True, discount=False)
+    reinit_port(0)
+    return s.sample, "port", 1, reinit_port
+
+
+def c3_cpu_baseline(nm, pfw, K, schedule: dict, budget_s: float, calibrate_s: float = 0.0,
+                    threads=None) -> dict:
+    """The reference CPU sampler's time-to-eps for the large portfolio: its cost per outer sample
+    on every level (bounded samples) times the level counts of the GPU run at eps (`schedule`);
+    with `calibrate_s` > 0 also one complete CPU run of the host driver at the loosest eps in
+    (1e-2, 5e-3, 2.5e-3, ...) that is expected to finish within calibrate_s, measured, beside the
+    same extrapolation from that run's own level counts."""
+    sample, kind, cores, reinit = c3_cpu_reference(pfw, K, threads)
+    levels = [int(l) for l in schedule["levels"]]
+    Ms = [int(m) for m in schedule["M"]]
+    cost, details = level_costs(sample, levels, Ms, budget_s, cores)
+    total = sum(cost[l] * M for l, M in zip(levels, Ms) if M)
+    out = {"value": total, "unit": "s", "cores": cores, "kind": kind,
+           "sample": (f"reference level sampler ({'oracle/_ref, real_t=float' if kind == 'reference' else 'C port'}, "
+                      f"{cores} threads) timed on bounded samples per level [{', '.join(details)} outer samples], "
+                      f"cost per outer sample x the level counts of the GPU run at eps={schedule['eps']:g}; "
+                      f"extrapolated (the reference's loss keeps its e^(-r tau) discount: same cost)")}
+    if calibrate_s > 0:
+        def level(ell, M):
+            r = sample(ell, M)
+            return dict(fsums=r["fsums"], diffsums=r["diffsums"], work=r["work"])
+        eps_c, last = 1e-2, None
+        while True:
+            reinit(7)
+            t0 = time.perf_counter()
+            run = nm.mlmc_run_cb(level, targetTOL=eps_c, M0=1024)
+            wall = time.perf_counter() - t0
+            last = (eps_c, wall, run)
+            if wall * 4 > calibrate_s or eps_c < 1e-3:     # the next halving of eps costs ~4x
+                break
+            eps_c /= 2
+        eps_c, wall, run = last
+        lm = [int(x) for x in run["level_M"]]
+        miss = [l for l, M in enumerate(lm) if M and l not in cost]
+        if miss:
+            more, _ = level_costs(sample, miss, [lm[l] for l in miss], budget_s / 4, cores)
+            cost.update(more)
+        ext = sum(cost[l] * M for l, M in enumerate(lm) if M)
+        out["calibration"] = {"eps": eps_c, "measured_s": wall, "extrapolated_s": ext,
+                              "extrapolated_over_measured": ext / wall, "levels": len(lm),
+                              "level_M": lm, "Eg": float(run["Eg"]),
+                              "note": "one complete run of the host driver over the reference's CPU "
+                                      "sampler, and the per-level extrapolation from its level counts"}
+    return out
+
+
+def read_schedule(case: str) -> dict | None:
+    if not os.path.exists(SCHEDULE):
+        return None
+    with open(SCHEDULE) as f:
+        d = json.load(f)
+    return d.get(case)
+
+
 def reference_arm(args):
     world, rank, _ = ddp_env()
     if rank != 0:
         return
-    if not os.path.exists(SCHEDULE):
-        print(json.dumps({"impl": "reference", "unavailable": "bench_schedule.json missing"}))
+    case = "c1" if args.case == "c1" else "c3"
+    schedule = read_schedule(case)
+    if schedule is None:
+        print(json.dumps({"impl": "reference", "unavailable": f"bench_schedule.json has no {case} schedule"}))
         return
-    with open(SCHEDULE) as f:
-        schedule = json.load(f)
     times = []
-    kind = cores = desc = None
     t_all0 = time.perf_counter()
     per_step = max(5.0, args.ref_budget * 3 / max(1, args.steps))
-    for _ in range(args.steps):
-        v, kind, cores, desc = cpu_reference_time(schedule, budget_s=per_step)
-        times.append(v)
-    value = statistics.median(times)
+    if case == "c1":
+        kind = cores = desc = None
+        for _ in range(args.steps):
+            v, kind, cores, desc = cpu_reference_time(schedule, budget_s=per_step)
+            times.append(v)
+        value = statistics.median(times)
+        cpu = {"value": value, "unit": "s", "cores": cores, "kind": kind, "sample": desc}
+        config = C1_WORKLOAD
+    else:
+        sys.path.insert(0, PKG)
+        import nmlmc as nm
+        pfw = c3_portfolio(nm)
+        K = float(schedule["K"])
+        cpu = None
+        for k in range(args.steps):
+            c = c3_cpu_baseline(nm, pfw, K, schedule, budget_s=per_step,
+                                calibrate_s=(args.ref_budget if k == 0 else 0.0))
+            times.append(c["value"])
+            cpu = cpu or c
+        value = statistics.median(times)
+        cpu = dict(cpu, value=value)
+        config = C3_CONFIG
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3,
             "higher_is_better": False, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": WORKLOAD,
-            "cpu_baseline": {"value": value, "unit": "s", "cores": cores, "kind": kind, "sample": desc},
+            "data": "synthetic", "config": config, "cpu_baseline": cpu,
             "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "measure_wall_s": time.perf_counter() - t_all0}
     print(json.dumps(line))
@@ -454,6 +580,8 @@ def dropin_extrapolated(s, level_M, budget_s=60.0):
     total, detail = 0.0, []
     per_level = budget_s / max(1, len(level_M))
     for ell, M in enumerate(level_M):
+        if M == 0:
+            continue
         m = 2048
         while True:
             dt = s.sample(ell, m)["seconds"]
@@ -508,159 +636,254 @@ def c3_table_case():
             print(f"P {P} {name}: {r['seconds'] * 1e3:.3f} ms, {r['stats'][0] / r['seconds']:.3e} inner/s")
 
 
-def c3_case(args):
-    """Large portfolio: d = 200 stocks, P = 1e6 options (generator seed 1), K = the 99 % quantile
-    of the full loss over 1e5 outer samples; P(L > K) by continuation MLMC with the reference's
-    default importance sub-sampling (prob proportional to |w_i|, options sorted by |w_i|) and the
-    delta control variate, N0 = 64, beta = 2, adaptive r = 1.5.  The batched FP32 sampler (OUTER
-    streams, one CUDA graph per MLMC round) against the plain FP64 drop-in (reference stream
-    layout, 2048 virtual cores, one synchronous call per level) on the same GPU, both to the same
-    eps, and a direct estimate from 2e5 full evaluations as the accuracy check."""
-    import numpy as np
-    sys.path.insert(0, PKG)
-    import nmlmc as nm
-    eps = args.eps if args.eps else 1e-3
-    pfw = c3_portfolio(nm)
+def c3_sampler(nm, device, pfw, K, prec, streams, seed, cores=2048):
+    s = nm.Sampler(device, cores=cores, N0=64, beta=2, adaptive_r=ADAPTIVE_R, precision=prec,
+                   streams=streams, seed=seed)
+    s.set_portfolio(pfw, r=0.05, rho=0.0, max_loss=K, tau=nm.TAU_WEEK, subsample=nm.SUB_RANDOM,
+                    use_delta_cv=True, discount=False)
+    return s
 
-    def mk(prec, streams, K, seed, cores=0, sub=nm.SUB_RANDOM):
-        s = nm.Sampler(0, cores=cores or 2048, N0=64, beta=2, adaptive_r=1.5, precision=prec,
-                       streams=streams, seed=seed)
-        s.set_portfolio(pfw, r=0.05, rho=0.0, max_loss=K, tau=nm.TAU_WEEK, subsample=sub,
-                        use_delta_cv=True, discount=False)
-        return s
 
-    q = mk(nm.PREC_FP32, nm.STREAMS_OUTER, 0.0, seed=1)
-    K = nm.loss_quantile(q, 0.99, 100_000)
-    t = time.perf_counter()
-    Ld = q.full_loss(62, 0, 200_000)
-    t_sweep = time.perf_counter() - t
-    # the full-loss sweep streams the packed 32-byte records once per tile of 32 outer samples
-    P = len(pfw["w"])
-    sweep = {"outer_samples": len(Ld), "options": P, "seconds": t_sweep,
-             "option_evaluations_per_s": len(Ld) * P / t_sweep,
-             "table_bytes_per_s": P * 32 * -(-len(Ld) // 32) / t_sweep,
-             "note": "wall time of nmlmc_portfolio_full_loss (outer draws, sweep, 1.6 MB copy back); "
-                     "the 32 MB table is L2-resident, so the sweep streams it from L2"}
-    p_direct = float(np.mean(Ld > K))
-    sd = float(np.sqrt(p_direct * (1 - p_direct) / len(Ld)))
-    # warm-up of the FP32 sampler on another seed (module load, graph instantiation,
-    # allocations, the per-level phase-kernel autotuning): one MLMC run at the same tolerance,
-    # or at 3 eps for tight tolerances, where autotuning stays on for levels the warm-up missed
-    # (their bounded probes then run inside the timed run)
-    tight = eps < 5e-4
-    s32 = mk(nm.PREC_FP32, nm.STREAMS_OUTER, K, seed=4)
-    s32.set_autotune(2)
-    s32.mlmc_run(targetTOL=3 * eps if tight else eps, M0=1024, batched=True)
-    if not tight:
-        s32.set_autotune(0)
-    s32.configure(seed=5)
-    runs = {}
-    cs = ClockSampler(0)
-    cs.start()
-    for name, prec, streams, cores, batched in (("fp32_batched", nm.PREC_FP32, nm.STREAMS_OUTER, 0, True),
-                                                 ("fp64_dropin", nm.PREC_FP64, nm.STREAMS_CORE, 2048, False)):
-        s = s32 if prec == nm.PREC_FP32 else mk(prec, streams, K, seed=5, cores=cores)
-        if tight and prec == nm.PREC_FP64:
-            runs[name] = dropin_extrapolated(s, runs["fp32_batched"]["level_M"], budget_s=60.0)
+def c3_upload_bytes(P: int, Q: int) -> int:
+    """Host->device bytes of set_portfolio on the FP32 path: per option seven float arrays of the
+    reference-arithmetic table (strike, maturity, V0, w, prob, W_est, CDF), the stock index (4 B),
+    the type (1 B), the alias entry (8 B), its sampling probability (4 B) and two packed 32-byte
+    records (full-loss and sampler); per stock S0, mu, sigma and the delta coefficient (4 x 4 B)."""
+    return P * (7 * 4 + 4 + 1 + 8 + 4 + 2 * 32) + Q * 16
+
+
+def c3_fp32_vs_fp64(nm, device, pfw, K, level_M, starting_level, m_max=4096):
+    """Each active level's FP32 estimate against the all-FP64 batched sampler on the same OUTER
+    streams (at most m_max outer samples per level): level means, phi flips, count mismatches."""
+    out = []
+    for ell, M in enumerate(level_M):
+        if ell < starting_level or M == 0:
             continue
-        t = time.perf_counter()
-        out = s.mlmc_run(targetTOL=eps, M0=1024, batched=batched)
-        wall = time.perf_counter() - t
-        runs[name] = dict(value=float(out["level_time"].sum()), e2e=wall, Eg=out["Eg"],
-                          levels=int(out["nlevels"]), starting_level=int(out["starting_level"]),
-                          level_M=[int(x) for x in out["level_M"]],
-                          inner_samples=float(out["total_work"]), calls=int(out["calls"]))
-        if prec == nm.PREC_FP32:
-            runs[name]["phase_config"] = phase_choices(s, int(out["nlevels"]))
-    clk = cs.stop()
-    # each active level's FP32 estimate against the all-FP64 batched sampler on the same OUTER
-    # streams (at most 4096 outer samples per level)
-    per_level = []
-    for ell, M in enumerate(runs["fp32_batched"]["level_M"]):
-        if ell < runs["fp32_batched"]["starting_level"] or M == 0:
-            continue
-        m = min(M, 4096)
-        x, y = mk(nm.PREC_FP32, nm.STREAMS_OUTER, K, seed=17), mk(nm.PREC_FP64, nm.STREAMS_OUTER, K, seed=17)
+        m = min(int(M), m_max)
+        x = c3_sampler(nm, device, pfw, K, nm.PREC_FP32, nm.STREAMS_OUTER, seed=17)
+        y = c3_sampler(nm, device, pfw, K, nm.PREC_FP64, nm.STREAMS_OUTER, seed=17)
         x.set_autotune(0)
         rx, ry = x.sample(ell, m, trace=True), y.sample(ell, m, trace=True)
         tx, ty = rx["trace"], ry["trace"]
         flip = (tx["phi_f"] != ty["phi_f"]) | (tx["phi_c"] != ty["phi_c"])
-        per_level.append({"level": ell, "M": m,
-                          "fEl_fp32_minus_fp64": (rx["fsums"][0] - ry["fsums"][0]) / m,
-                          "dEl_fp32_minus_fp64": (rx["diffsums"][0] - ry["diffsums"][0]) / m,
-                          "phi_flips": int(flip.sum()),
-                          "count_mismatches": int(((tx["count_f"] != ty["count_f"]) | (tx["count_c"] != ty["count_c"])).sum())})
-    # phase-kernel roofline: CUDA events around every phase-kernel launch while the FP32 sampler
-    # repeats one call per active level of its run (at most 8192 outer samples each)
-    a = runs["fp32_batched"]
-    s32.set_profiling(True)
-    inner = 0.0
-    for ell, M in enumerate(a["level_M"]):
-        if ell >= a["starting_level"] and M > 0:
-            inner += float(s32.sample(ell, min(M, 8192))["stats"][0])
-    n_phase, t_phase = s32.phase_kernel_time()
-    s32.set_profiling(False)
+        out.append({"level": ell, "M": m,
+                    "fEl_fp32_minus_fp64": (rx["fsums"][0] - ry["fsums"][0]) / m,
+                    "dEl_fp32_minus_fp64": (rx["diffsums"][0] - ry["diffsums"][0]) / m,
+                    "phi_flips": int(flip.sum()),
+                    "count_mismatches": int(((tx["count_f"] != ty["count_f"]) | (tx["count_c"] != ty["count_c"])).sum())})
+        x.close()
+        y.close()
+    return out
+
+
+def c3_main(args):
+    """The large-portfolio line (the default): W warm-up runs and K timed runs of the batched FP32
+    sampler to eps, each step uploading the portfolio tables from host buffers (set_portfolio)
+    and running the host driver; then the comparators (FP64 drop-in on the same GPU, all-FP64 on
+    the same streams per level, the reference CPU sampler), the phase kernel's roofline and the
+    K-quantile sweep."""
+    import numpy as np
+    sys.path.insert(0, PKG)
+    import nmlmc as nm
+    eps = args.eps if args.eps else EPS
+    world, rank, local = ddp_env()
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as td
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        td.init_process_group("nccl", timeout=timedelta(seconds=300))
+        dist = (td, torch.device("cuda", local))
+
+    def barrier():
+        if dist:
+            dist[0].barrier()
+
+    pfw = c3_portfolio(nm)
+    P, Q = len(pfw["w"]), len(pfw["S0"])
+    # K: the 99 % quantile of the full loss over 1e5 outer samples (FP32 sweep of the packed table)
+    q = c3_sampler(nm, local, pfw, 0.0, nm.PREC_FP32, nm.STREAMS_OUTER, seed=1)
+    K = nm.loss_quantile(q, 0.99, 100_000)
+    t = time.perf_counter()
+    Ld = q.full_loss(62, 0, 200_000)
+    t_sweep = time.perf_counter() - t
+    q.close()
+    p_direct = float(np.mean(Ld > K))
+    sd = float(np.sqrt(p_direct * (1 - p_direct) / len(Ld)))
+    sweep = {"outer_samples": len(Ld), "options": P, "seconds": t_sweep,
+             "option_evaluations_per_s": len(Ld) * P / t_sweep,
+             "note": "wall time of nmlmc_portfolio_full_loss (outer draws, sweep of the packed records "
+                     "32 outer samples per pass, 1.6 MB copy back); the 32 MB table is L2-resident"}
+
+    s = c3_sampler(nm, local, pfw, K, nm.PREC_FP32, nm.STREAMS_OUTER, seed=1000)
+    s.set_autotune(2)           # the warm-up runs tune every level: variant and chunk length
+    for w in range(args.warmup):
+        s.configure(seed=1000 + w)
+        run_once(nm, s, batched=True, dist=dist, eps=eps)
+    # keep the tuned choices fixed for the timed runs (set_portfolio would otherwise drop them)
+    nlev_seen = 0
+    for ell in range(64):
+        pc = s.phase_config(ell)
+        if pc["state"] == 1:
+            s.set_phase_config(ell, pc["variant"], pc["chunk"])
+            nlev_seen = ell + 1
+    s.set_autotune(0)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = nm.kernel_launches()
+    barrier()
+    dev_times, walls, outs = [], [], []
+    t_region = time.perf_counter()
+    for k in range(args.steps):
+        s.configure(seed=k)
+        t0 = time.perf_counter()
+        s.set_portfolio(pfw, r=0.05, rho=0.0, max_loss=K, tau=nm.TAU_WEEK, subsample=nm.SUB_RANDOM,
+                        use_delta_cv=True, discount=False)
+        out, _ = run_once(nm, s, batched=True, dist=dist, eps=eps)
+        walls.append(time.perf_counter() - t0)
+        outs.append(out)
+        dev_times.append(float(out["level_time"].sum()))
+    barrier()
+    region = time.perf_counter() - t_region
+    launches = nm.kernel_launches() - launches0
+    clk = clocks.stop()
+
+    dev_t = sum(dev_times) / len(dev_times)
+    wall_t = sum(walls) / len(walls)
+    if dist:
+        import torch
+        tt = torch.tensor([dev_t, wall_t], dtype=torch.float64, device=dist[1])
+        dist[0].all_reduce(tt, op=dist[0].ReduceOp.MAX)
+        dev_t, wall_t = float(tt[0]), float(tt[1])
+    a = outs[0]
+    level_M = [int(x) for x in a["level_M"]]
+    sl = int(a["starting_level"])
+    calls = sum(int(o["calls"]) for o in outs) / len(outs)
+    inner = sum(float(o["total_work"]) for o in outs)
+    if rank != 0:
+        if dist:
+            dist[0].destroy_process_group()
+        return
+
+    schedule = dict(eps=eps, K=K, levels=list(range(len(level_M))), M=level_M, starting_level=sl,
+                    note="outer samples per level of the eps run (seed 0) of the batched sampler")
+    if args.schedule_out:
+        os.makedirs(os.path.dirname(os.path.abspath(args.schedule_out)), exist_ok=True)
+        with open(args.schedule_out, "w") as f:
+            json.dump({"c3": schedule}, f)
+
+    # phase-kernel roofline: CUDA events around every phase-kernel launch while the sampler repeats
+    # one call per active level of the run (at most 2^18 outer samples each; profiling submits the
+    # levels one call at a time, outside the timed region)
+    s.set_profiling(True)
+    prof_inner = 0.0
+    for ell, M in enumerate(level_M):
+        if ell >= sl and M > 0:
+            prof_inner += float(s.sample(ell, min(M, 1 << 18))["stats"][0])
+    n_phase, t_phase = s.phase_kernel_time()
+    s.set_profiling(False)
     sm_mhz = clk.get("sm_mhz") or 1965.0
     peak = 148 * 128 * sm_mhz * 1e6 / 1e12
-    ach = inner * C3_OPS_PER_INNER / t_phase / 1e12
+    ach = prof_inner * C3_OPS_PER_INNER / t_phase / 1e12
     roof = {"bound": "alu", "achieved": ach, "peak": peak, "unit": "Tops/s", "frac": ach / peak,
             "traffic": None, "kernel": "k_phase (FP32, portfolio)", "launches": n_phase,
-            "kernel_seconds": t_phase, "inner_samples": inner, "ops_per_inner_sample": C3_OPS_PER_INNER,
-            "peak_source": "issue-slot peak 148 SM x 128 lanes x sampled SM clock",
+            "kernel_seconds": t_phase, "inner_samples": prof_inner, "ops_per_inner_sample": C3_OPS_PER_INNER,
+            "peak_source": "issue-slot peak 148 SM x 4 SMSP x 32 lanes x sampled SM clock (the measured-"
+                           "peaks file holds only HBM copy and bf16 GEMM figures)",
             "timing": "CUDA events around each phase-kernel launch of one call per active level "
-                      "(<= 8192 outer samples) after the timed runs",
-            "note": "latency-bound: dependent option-table gathers and the per-sample arithmetic chain",
-            "traffic_note": "DRAM bytes per level-10 pilot launch of 8192 outer samples (ncu): 46-47 MB "
-                            "read, 1.0-1.2 MB written: the 40 MB option and alias tables once from "
-                            "DRAM, then L2-resident, so no HBM roofline applies"}
-    a, b = runs["fp32_batched"], runs["fp64_dropin"]
-    line = {"metric": f"time-to-eps (s) for MLMC P(L>K), large portfolio, eps={eps:g} absolute",
-            "value": a["value"], "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 1,
-            "ms_per_step": a["value"] * 1e3, "higher_is_better": False, "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic (seeded generator)",
-            "config": {"workload": "large portfolio d=200, P=1e6, K = 99% loss quantile",
-                       "sub_sampling": "random, prob ~ |w|, delta CV", "N0": 64, "beta": 2,
-                       "adaptive_r": 1.5, "eps": eps, "K": K,
-                       "eps_note": ("below 5e-4 the FP64 drop-in is timed per level on bounded samples and "
-                                    "scaled by the FP32 run's level counts (extrapolated)")},
-            "e2e": {"value": a["e2e"], "unit": "s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": a["calls"] * (16 * 8 + 2 * 8),
-                    "h2d_note": "the portfolio's option records and alias table are uploaded by "
-                                "set_portfolio before the timed run and stay resident; each round's "
-                                "level counts travel as kernel arguments",
+                      "(<= 2^18 outer samples) after the timed runs",
+            "traffic_note": "the 40 MB option and alias tables are L2-resident; DRAM traffic per launch "
+                            "is the R_tau rows and per-outer-sample counts (profiles/), so no HBM "
+                            "roofline applies"}
+    line = {"metric": METRIC, "value": dev_t, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_t * 1e3, "higher_is_better": False,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
+            "config": dict(C3_CONFIG, eps=eps),
+            "e2e": {"value": wall_t, "unit": "s", "h2d_bytes_per_step": c3_upload_bytes(P, Q),
+                    "d2h_bytes_per_step": int(calls * (16 * 8 + 2 * 8)),
+                    "h2d_note": "set_portfolio from host buffers every step: the reference-arithmetic "
+                                "option arrays, the alias table and the two packed FP32 record tables "
+                                "(host-side table construction included); each round's level counts "
+                                "travel as kernel arguments",
                     "d2h_note": "per sampled level: 16 FP64 sums and two device clock stamps"},
-            "runs": runs, "p_direct": p_direct, "p_direct_sd": sd,
-            "speedup_vs_fp64_dropin": {"value": b["value"] / a["value"],
-                                       "e2e": (b["e2e"] / a["e2e"]) if b.get("e2e") else None},
-            "roofline": roof, "full_loss_sweep": sweep, "fp32_vs_fp64_per_level": per_level,
-            "clocks": clk}
+            "roofline": roof, "clocks": clk, "gpu_launches": int(launches),
+            "parallelism": f"outer-sample shards x{world}",
+            "phase_config": phase_choices(s, max(nlev_seen, len(level_M))),
+            "inner_samples_per_step": inner / len(outs), "inner_samples_per_s": inner / sum(dev_times),
+            "Eg": float(a["Eg"]), "p_direct": p_direct, "p_direct_sd": sd, "K": K,
+            "levels": len(level_M), "starting_level": sl, "level_M": level_M,
+            "timed_region_s": region, "full_loss_sweep": sweep}
+    s.close()
+
+    if world == 1 and not args.no_compare:
+        # plain FP64 drop-in on the same GPU: per-level cost on bounded samples x the level counts
+        # of the FP32 run; calibrated by one complete measured run at eps = 1e-3
+        d = c3_sampler(nm, local, pfw, K, nm.PREC_FP64, nm.STREAMS_CORE, seed=5, cores=2048)
+        drop = dropin_extrapolated(d, level_M, budget_s=60.0) if eps < 5e-4 else None
+        d.close()
+        cal_eps = 1e-3
+        f = c3_sampler(nm, local, pfw, K, nm.PREC_FP32, nm.STREAMS_OUTER, seed=6)
+        f.set_autotune(1)
+        of, _ = run_once(nm, f, batched=True, eps=cal_eps)
+        f.close()
+        d = c3_sampler(nm, local, pfw, K, nm.PREC_FP64, nm.STREAMS_CORE, seed=6, cores=2048)
+        od, wd = run_once(nm, d, batched=False, eps=cal_eps)
+        d.close()
+        d = c3_sampler(nm, local, pfw, K, nm.PREC_FP64, nm.STREAMS_CORE, seed=6, cores=2048)
+        ext = dropin_extrapolated(d, [int(x) for x in of["level_M"]], budget_s=20.0)
+        d.close()
+        cal = {"eps": cal_eps, "measured_s": float(od["level_time"].sum()), "measured_e2e_s": wd,
+               "extrapolated_s": ext["value"], "Eg": float(od["Eg"]),
+               "extrapolated_over_measured": ext["value"] / float(od["level_time"].sum()),
+               "fp32_batched_s": float(of["level_time"].sum()),
+               "note": "the drop-in's own complete run at this eps, and the per-level extrapolation "
+                       "from the FP32 run's level counts at the same eps"}
+        if drop is None:
+            drop = {"value": float(od["level_time"].sum()), "e2e": wd, "extrapolated": False}
+        drop["calibration"] = cal
+        drop["streams"] = "reference (CORE) layout, 2048 virtual cores, one synchronous call per level"
+        line["fp64_dropin"] = drop
+        line["speedup_vs_fp64_dropin"] = {"value": drop["value"] / dev_t,
+                                          "note": "extrapolated drop-in time over the measured FP32 time"
+                                                  if drop.get("extrapolated") else "measured"}
+        line["fp32_vs_fp64_per_level"] = c3_fp32_vs_fp64(nm, local, pfw, K, level_M, sl)
+    if world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = c3_cpu_baseline(nm, pfw, K, schedule, budget_s=args.ref_budget,
+                                               calibrate_s=args.ref_budget)
     print(json.dumps(line))
+    if dist:
+        dist[0].destroy_process_group()
 
 
 # ---------------------------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--ref-budget", type=float, default=20.0, help="CPU seconds of reference sampling")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison runs")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--eps", type=float, default=None, help="--case c3: target RMSE (default 1e-3)")
+    ap.add_argument("--eps", type=float, default=None, help="target RMSE of the large-portfolio line (default 1e-4)")
     ap.add_argument("--schedule-out", default=None,
                     help="write the run's outer samples per level (bench_schedule.json format) here")
-    ap.add_argument("--case", default=None, choices=["small", "c3", "c3-level", "c3-table", "c3-sweep", "c4",
+    ap.add_argument("--case", default=None, choices=["c1", "small", "c3-level", "c3-table", "c3-sweep", "c4",
                                                       "c4-small", "ref-model"],
-                    help="small: a few fixed level calls of the FP32 sampler (profiling case); "
-                         "c4: the path-simulated loss with adjoint; c4-small: its profiling case")
+                    help="default: the large portfolio to eps; c1: the adaptive model problem to eps; "
+                         "small, c3-level, c3-table, c3-sweep, c4-small: profiling cases; c4: the "
+                         "path-simulated loss with adjoint; ref-model: the reference's model main")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.case is None:
+        return c3_main(args)
+    if args.case == "c1":
+        return c1_main(args)
     if args.case == "small":
         return small_case()
-    if args.case == "c3":
-        return c3_case(args)
     if args.case == "c3-level":
         return c3_level_case()
     if args.case == "c3-table":
@@ -672,6 +895,11 @@ def main():
     if args.case == "ref-model":
         return ref_main_case(args)
 
+
+def c1_main(args):
+    """The adaptive model problem to eps = 1e-4 (X = Y + Z, K = 1): W warm-up and K timed runs of
+    the batched FP32 sampler, the all-FP64 run and the FP64 drop-in on the same GPU, the per-level
+    FP32 error, the phase kernel's roofline and the reference CPU sampler."""
     sys.path.insert(0, PKG)
     import nmlmc as nm
     world, rank, local = ddp_env()
@@ -747,7 +975,7 @@ def main():
     if args.schedule_out:          # the level counts of this run (the reference arm's schedule)
         os.makedirs(os.path.dirname(os.path.abspath(args.schedule_out)), exist_ok=True)
         with open(args.schedule_out, "w") as f:
-            json.dump(schedule, f)
+            json.dump({"c1": schedule}, f)
 
     # roofline of the phase kernel (the dominant kernel): lane-ops per inner sample x inner
     # samples / its CUDA-event time; peak = issue slots at the sampled SM clock
@@ -768,8 +996,8 @@ def main():
     line = {"metric": METRIC, "value": dev_t, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_t * 1e3, "higher_is_better": False,
             "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": dict(WORKLOAD, parallelism=f"outer-sample shards x{world}",
-                           phase_config=phase_choices(s, int(ref["nlevels"]))),
+            "config": C1_WORKLOAD, "parallelism": f"outer-sample shards x{world}",
+            "phase_config": phase_choices(s, int(ref["nlevels"])),
             "e2e": {"value": wall_t, "unit": "s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": int(calls / len(outs) * (16 * 8 + 2 * 8)),
                     "h2d_note": "no input arrays: tau, K and each round's level counts travel as kernel "

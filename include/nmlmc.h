@@ -145,8 +145,8 @@ void portfolio_free_data(portfolio_data* data);
 /* norm_cdf_inv (common.cpp:53-86). */
 float norm_cdf_inv(float p);
 
-/* Status of the last reference-surface call, and the precision used by it (the reference
- * surface computes at NMLMC_PREC_REF32 unless nmlmc_default_set_precision changes it). */
+/* Status of the last reference-surface call (or allocation-free level call), and the precision
+ * used by the reference surface (NMLMC_PREC_REF32 unless nmlmc_default_set_precision changes it). */
 int nmlmc_last_error(void);
 int nmlmc_default_set_precision(int32_t precision, int32_t streams);
 
@@ -377,8 +377,11 @@ int nmlmc_norm_cdf_fast(const float* x, float* out, uint64_t n);
  * NMLMC_NOALLOC_SCRATCH_BYTES that every process loading this library reserves on each GPU it
  * uses until exit, which limits a call to M <= NMLMC_NOALLOC_MAX_OUTER (larger M is rejected
  * with NMLMC_ERR_ARG).  The first call on a device looks the array's device address up
- * (cudaGetSymbolAddress), so make that first call before any stream capture.  Calls share the
- * array — each clears what it accumulates into, but calls that overlap on the GPU race.
+ * (cudaGetSymbolAddress), so make that first call before any stream capture; that address is
+ * kept for the life of the process, so a device reset (cudaDeviceReset, or a destroyed primary
+ * context) after the first call is not supported.  Calls share the array — each clears what it
+ * accumulates into, but calls that overlap on the GPU race.  Failures return a status and set
+ * nmlmc_last_error(), with the input checks of nmlmc_set_model and nmlmc_sample.
  * d_out (device memory, 16 doubles) receives: sums of phi_f^k (k = 1..4), sums of
  * (phi_f - phi_c)^k, work, inner samples, outer samples that hit the maximum count, outer
  * samples that stayed at the base count, and 4 zeros.  The copy into d_out is ordered on

@@ -122,6 +122,7 @@ struct DevPortfolio {
     int8_t* type = nullptr;
     FastOption* fast = nullptr;       // packed records of the FP32 path
     FastOption* fast_s = nullptr;     // the same, scaled by 1 / sampling probability
+    FastColumn* fast_col = nullptr;   // sampler records fused with the alias table
     uint2* alias = nullptr;           // alias table (OUTER, Subsampling::Random)
     RT* phat = nullptr;
     OptionTable<RT> table{};
@@ -264,7 +265,7 @@ template <class RT>
 void free_dev_portfolio(DevPortfolio<RT>& d) {
     dfree(d.strike); dfree(d.maturity); dfree(d.start); dfree(d.w); dfree(d.prob); dfree(d.W_est);
     dfree(d.cdf); dfree(d.S0); dfree(d.mu); dfree(d.sigma); dfree(d.delta_coalesce);
-    dfree(d.stock_ind); dfree(d.type); dfree(d.fast); dfree(d.fast_s); dfree(d.alias); dfree(d.phat);
+    dfree(d.stock_ind); dfree(d.type); dfree(d.fast); dfree(d.fast_s); dfree(d.fast_col); dfree(d.alias); dfree(d.phat);
     d.table = OptionTable<RT>{};
 }
 
@@ -387,13 +388,14 @@ int build_dev_portfolio(nmlmc_ctx* c, DevPortfolio<RT>& d) {
     t.use_milstein = h.use_milstein;
     t.fast = nullptr;
     t.fast_s = nullptr;
+    t.fast_col = nullptr;
     t.alias = nullptr;
     t.phat = nullptr;
     std::vector<double> phat;
+    std::vector<uint2> tab;
     if (h.subsample == SUB_RANDOM && !h.mixed()) {
         std::vector<double> pr(P);
         for (uint32_t j = 0; j < P; j++) pr[j] = (double)prob[j];
-        std::vector<uint2> tab;
         build_alias(P, pr, tab, phat);
         std::vector<RT> ph(P);
         for (uint32_t j = 0; j < P; j++) ph[j] = (RT)phat[j];
@@ -407,42 +409,49 @@ int build_dev_portfolio(nmlmc_ctx* c, DevPortfolio<RT>& d) {
         bool unit = true;
         for (uint32_t j = 0; j < P; j++) unit = unit && h.W_est[j] == 1.0;
         if (unit && !h.mixed()) {
-            std::vector<FastOption> fo(P);
-            const double disc = h.discount ? exp(-h.r * h.tau) : 1.0;
-            for (uint32_t j = 0; j < P; j++) {
+            // Record of option j with its weights scaled by sc and, with cv_on, the delta control
+            // variate: cv = sc w Delta_BS(S0, T) and its constant -cv S0 folded into wV0.
+            auto record = [&](uint32_t j, double sc, bool cv_on) {
                 const uint32_t s = h.stock_ind[j];
                 const double sg = h.sigma[s], K = h.strike[j], T = h.maturity[j], Tr = T - h.tau;
                 const double m = h.type[j] > 0 ? 1.0 : -1.0;
                 const double sd = sg * sqrt(Tr);
                 const double V0 = h_calc_bs<double>(h.type[j], h.S0[s], K, h.r, T, sg);
-                FastOption& o = fo[j];
+                const double disc = h.discount ? exp(-h.r * h.tau) : 1.0;
+                const double cv = cv_on ? sc * h.w[j] * h_calc_delta<double>(h.type[j], h.S0[s], K, h.r, T, sg) : 0.0;
+                FastOption o;
                 o.c1 = (float)(-log(K) + (h.r + 0.5 * sg * sg) * Tr);
-                o.inv_s = (float)(1.0 / sd);
-                o.s = (float)sd;
-                o.wR = (float)(-h.w[j] * disc * m);
-                o.wK = (float)(h.w[j] * disc * m * K * exp(-h.r * Tr));
-                o.wV0 = (float)(h.w[j] * V0);
-                o.cv = h.use_delta_cv ? (float)(h.w[j] * h_calc_delta<double>(h.type[j], h.S0[s], K, h.r, T, sg)) : 0.f;
-                o.asset_type = s | (h.type[j] > 0 ? 0u : 0x80000000u);
-            }
+                o.inv_s = (float)(m / sd);
+                o.s = (float)(m * sd);
+                o.wR = (float)(-sc * h.w[j] * disc * m);
+                o.wK = (float)(sc * h.w[j] * disc * m * K * exp(-h.r * Tr));
+                o.wV0 = (float)(sc * h.w[j] * V0 - cv * h.S0[s]);
+                o.cv = (float)cv;
+                o.stock = s;
+                return o;
+            };
+            // full-loss records: the loss L(Y) itself, no control variate
+            std::vector<FastOption> fo(P);
+            for (uint32_t j = 0; j < P; j++) fo[j] = record(j, 1.0, false);
             if ((rc = upload(d.fast, fo))) return rc;
             t.fast = d.fast;
             if (h.subsample != SUB_NONE) {
                 // sampler records: the inner value X = loss_j / phat_j folded into the weights
                 for (uint32_t j = 0; j < P; j++) {
                     const double sc = h.subsample == SUB_UNIFORM ? (double)P : (phat[j] > 0 ? 1.0 / phat[j] : 0.0);
-                    const uint32_t s = h.stock_ind[j];
-                    const double sg = h.sigma[s], K = h.strike[j], T = h.maturity[j], Tr = T - h.tau;
-                    const double m = h.type[j] > 0 ? 1.0 : -1.0;
-                    const double V0 = h_calc_bs<double>(h.type[j], h.S0[s], K, h.r, T, sg);
-                    const double disc = h.discount ? exp(-h.r * h.tau) : 1.0;
-                    fo[j].wR = (float)(-sc * h.w[j] * disc * m);
-                    fo[j].wK = (float)(sc * h.w[j] * disc * m * K * exp(-h.r * Tr));
-                    fo[j].wV0 = (float)(sc * h.w[j] * V0);
-                    fo[j].cv = h.use_delta_cv ? (float)(sc * h.w[j] * h_calc_delta<double>(h.type[j], h.S0[s], K, h.r, T, sg)) : 0.f;
+                    fo[j] = record(j, sc, h.use_delta_cv != 0);
                 }
                 if ((rc = upload(d.fast_s, fo))) return rc;
                 t.fast_s = d.fast_s;
+                if (h.subsample == SUB_RANDOM && Q <= kColumnMaxStocks && P < kColumnMaxOptions) {
+                    std::vector<FastColumn> col(P);
+                    for (uint32_t j = 0; j < P; j++) {
+                        const FastOption& o = fo[j];
+                        col[j] = FastColumn{o.c1, o.inv_s, o.wR, o.wK, o.wV0, o.cv, tab[j].x, (tab[j].y << 8) | o.stock};
+                    }
+                    if ((rc = upload(d.fast_col, col))) return rc;
+                    t.fast_col = d.fast_col;
+                }
             }
         }
     }
@@ -1628,6 +1637,17 @@ static void ref_fail(int rc, const char* fn) {
 }
 
 int nmlmc_last_error(void) { return g_last; }
+
+}  // extern "C"
+
+// The status that nmlmc_last_error() reports, for entry points outside this file.
+int nmlmc::set_last_error(int e) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_last = e;
+    return set_err(e);
+}
+
+extern "C" {
 
 // Records the status of a reference-named call implemented in another translation unit
 // (portfolio_gen_data / portfolio_free_data in nmlmc_portfolio.cpp).  Not part of the ABI.

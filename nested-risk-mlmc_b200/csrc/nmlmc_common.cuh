@@ -27,7 +27,9 @@ struct CountParams {
     double tmp;          // real_t value widened
 };
 
-enum Kind : int { KIND_REF_MODEL = 0, KIND_SHIFT_MODEL = 1, KIND_PORTFOLIO = 2 };
+// Sampler kinds: the reference's model, the X = Y + Z model, the portfolio, and a caller-written
+// SAMPLER class (include/nmlmc_sampler.cuh).
+enum Kind : int { KIND_REF_MODEL = 0, KIND_SHIFT_MODEL = 1, KIND_PORTFOLIO = 2, KIND_USER = 3 };
 enum Sub : int { SUB_NONE = 0, SUB_RANDOM = 1, SUB_UNIFORM = -1 };
 
 enum Method : int { METHOD_BS = 0, METHOD_EXACT = 1, METHOD_UNBIASED = 2 };
@@ -58,6 +60,8 @@ struct OptionTable {
     const struct FastOption* fast;   // FP32 path: packed records (nmlmc_bs.cuh), else nullptr
     const struct FastOption* fast_s; // the same records scaled by 1 / (sampling probability)
     const uint2* alias;              // OUTER Subsampling::Random: alias table {threshold, alias}
+    const struct FastColumn* fast_col; // FP32 path, Subsampling::Random: records fused with the
+                                       // alias table (nmlmc_bs.cuh), or nullptr
     const RT* phat;                  // sampling probability of each option under the alias table
     uint32_t P, Q;
     RT r, rho, s1_rho2, max_loss, tau, stau, prob_norm, compute_prob0, inv_count_prob;

@@ -58,7 +58,8 @@ struct OuterBuffers {
     uint64_t cap;
     uint32_t Q;
     void* Yv;                // RT[cap]       model Y / portfolio constant
-    void* Rt;                // RT[cap * Q]   portfolio R_tau rows
+    void* Rt;                // cap * Q slots of 8 bytes: portfolio R_tau rows (RT R, or the
+                             // float pair (R, ln R) on the FP32 path)
     uint32_t* cnt_f;         // final fine count / chunk size (0 = undecided)
     uint32_t* cnt_c;
     uint32_t* lists;         // 4 * cap: fine/coarse round lists, ping-pong
@@ -67,10 +68,18 @@ struct OuterBuffers {
     double* block_sums;      // per-CTA partial moments [grid][16]
     double* level_acc;       // accumulated level result [16]
     int grid;
+    // KIND_USER only (caller-written SAMPLER classes): the SAMPLER object of every outer sample
+    // (its outer state, state_bytes each) and its workspace (ws_bytes each)
+    void* user_state;
+    void* user_ws;
+    uint32_t state_bytes, ws_bytes;
     // optional CUDA-event timing of the phase kernel: called around each k_phase launch
     void (*prof_mark)(void* user, int end, cudaStream_t stream);
     void* prof_user;
 };
+
+// Records a failed status for nmlmc_last_error() (this thread) and returns it.
+int set_last_error(int e);
 
 // Kernel launches issued by the library (incremented at every launch site).
 void count_launch(uint64_t n = 1);

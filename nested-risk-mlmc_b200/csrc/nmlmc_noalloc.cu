@@ -11,6 +11,11 @@
 // until the process exits (NMLMC_NOALLOC_SCRATCH_BYTES, 3 MiB).  All calls share it: a call
 // clears the counters and partial sums it relies on before use, and two calls whose work
 // overlaps on the GPU (different streams, or different host threads on one device) race on it.
+// The first call on a device looks up the array's device address and keeps it for the life of
+// the process: a device reset (cudaDeviceReset) or a destroyed primary context after that first
+// call is not supported.  Failures are reported like every other entry point's, through the
+// return value and nmlmc_last_error().
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -103,24 +108,30 @@ extern "C" int nmlmc_sample_level_noalloc(int32_t kind, double tau, double max_l
                                           int32_t precision, uint64_t seed, uint32_t ell,
                                           uint64_t first_index, uint64_t M, double* d_out,
                                           void* stream) {
-    if (kind != NMLMC_MODEL_REFERENCE && kind != NMLMC_MODEL_SHIFT) return NMLMC_ERR_ARG;
-    if (precision != NMLMC_PREC_FP32 && precision != NMLMC_PREC_FP64) return NMLMC_ERR_ARG;
+    if (kind != NMLMC_MODEL_REFERENCE && kind != NMLMC_MODEL_SHIFT) return set_last_error(NMLMC_ERR_ARG);
+    if (precision != NMLMC_PREC_FP32 && precision != NMLMC_PREC_FP64) return set_last_error(NMLMC_ERR_ARG);
+    // the model checks of nmlmc_set_model: finite inputs, and the reference model's sqrt(tau),
+    // sqrt(1 - tau) (model_sampler.cpp:21-39) need 0 <= tau <= 1
+    if (!std::isfinite(tau) || !std::isfinite(max_loss) || !std::isfinite(adaptive_r)) return set_last_error(NMLMC_ERR_ARG);
+    if (kind == NMLMC_MODEL_REFERENCE && !(tau >= 0 && tau <= 1)) return set_last_error(NMLMC_ERR_ARG);
     if (M > kMaxOuter) {
         fprintf(stderr, "nmlmc_sample_level_noalloc: M = %llu exceeds the scratch limit of %llu outer samples\n",
                 (unsigned long long)M, (unsigned long long)kMaxOuter);
-        return NMLMC_ERR_ARG;
+        return set_last_error(NMLMC_ERR_ARG);
     }
-    if (!d_out || N0 == 0 || beta < 2 || (beta & (beta - 1)) || ell >= NMLMC_MAX_LEVELS) return NMLMC_ERR_ARG;
+    if (!d_out || N0 == 0 || beta < 2 || (beta & (beta - 1)) || ell >= NMLMC_MAX_LEVELS) return set_last_error(NMLMC_ERR_ARG);
     const uint32_t chunk = N0 >= 32 ? 32 : N0;
-    if ((N0 % chunk) != 0 || (chunk & (chunk - 1)) != 0 || chunk < 4) return NMLMC_ERR_ARG;
-    if ((double)N0 * (double)upow(beta, ell) > 4.0e9) return NMLMC_ERR_ARG;
+    if ((N0 % chunk) != 0 || (chunk & (chunk - 1)) != 0 || chunk < 4) return set_last_error(NMLMC_ERR_ARG);
+    // the level's largest inner count N0 beta^ell, in double like nmlmc_sample (an integer power
+    // would wrap around for large beta and ell), checked before any count is formed
+    if ((double)N0 * pow((double)beta, (double)ell) > 4.0e9) return set_last_error(NMLMC_ERR_ARG);
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return NMLMC_ERR_CUDA;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return set_last_error(NMLMC_ERR_CUDA);
     DeviceScratch* ds = nullptr;
     int rc = setup_device(dev, ds);
-    if (rc) return rc;
+    if (rc) return set_last_error(rc);
     OuterBuffers B;
-    if (!carve(ds->base, ds->grid, B)) return NMLMC_ERR_NOMEM;
+    if (!carve(ds->base, ds->grid, B)) return set_last_error(NMLMC_ERR_NOMEM);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
 
     // get_samples_count parameters of the fine and coarse levels (nested_sampler.hpp:225-239)
@@ -172,7 +183,7 @@ extern "C" int nmlmc_sample_level_noalloc(int32_t kind, double tau, double max_l
         e = cudaMemcpyAsync(d_out, B.level_acc, 16 * sizeof(double), cudaMemcpyDeviceToDevice, st);
     if (e != cudaSuccess) {
         fprintf(stderr, "nmlmc_sample_level_noalloc: %s\n", cudaGetErrorString(e));
-        return NMLMC_ERR_CUDA;
+        return set_last_error(NMLMC_ERR_CUDA);
     }
-    return NMLMC_OK;
+    return set_last_error(NMLMC_OK);
 }

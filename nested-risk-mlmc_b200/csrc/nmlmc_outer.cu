@@ -78,11 +78,12 @@ __global__ void k_full_loss(DevLevel<RT> D, uint32_t nb, double* loss) {
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     const OptionTable<RT>& ot = D.L.ot;
     for (uint32_t i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < nb; i += warps) {
-        const RT* Rrow = reinterpret_cast<const RT*>(D.B.Rt) + (size_t)i * ot.Q;
+        constexpr uint32_t RS = RStride<PREC>::v;
+        const RT* Rrow = reinterpret_cast<const RT*>(D.B.Rt) + (size_t)i * ot.Q * RS;
         double s = 0;
         for (uint32_t j = lane; j < ot.P; j += 32) {
             uint32_t st = ot.stock_ind[j];
-            RT bs = calc_bs_ref<RT>(ot.type[j], Rrow[st], ot.strike[j], ot.r, xsub(ot.maturity[j], ot.tau), ot.sigma[st]);
+            RT bs = calc_bs_ref<RT>(ot.type[j], Rrow[st * RS], ot.strike[j], ot.r, xsub(ot.maturity[j], ot.tau), ot.sigma[st]);
             RT finish = ot.discount ? xmul(xexp(xmul(-ot.r, ot.tau)), bs) : bs;
             s += (double)xmul(ot.w[j], xsub(ot.start[j], finish));
         }
@@ -105,29 +106,26 @@ __global__ void __launch_bounds__(kTile) k_full_loss_fast(DevLevel<float> D, uin
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     float* sR = sm_rows;
     float* slnR = sm_rows + (size_t)kLossTile * Q;
-    const float* Rt = reinterpret_cast<const float*>(D.B.Rt);
+    const float2* Rt = reinterpret_cast<const float2*>(D.B.Rt);     // (R, ln R) per stock
     const uint32_t ntiles = (nb + kLossTile - 1) / kLossTile;
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const uint32_t o0 = tile * kLossTile;
         const uint32_t n_here = (nb - o0) < (uint32_t)kLossTile ? (nb - o0) : (uint32_t)kLossTile;
         for (uint32_t k = t; k < (uint32_t)kLossTile * Q; k += blockDim.x) {
             const uint32_t o = k / Q;
-            const float R = o < n_here ? Rt[(size_t)(o0 + o) * Q + (k - o * Q)] : 1.0f;
-            sR[k] = R;
-            slnR[k] = __logf(R);
+            const float2 R = o < n_here ? Rt[(size_t)(o0 + o) * Q + (k - o * Q)] : make_float2(1.0f, 0.0f);
+            sR[k] = R.x;
+            slnR[k] = R.y;
         }
         __syncthreads();
         float acc[kLossTile];
 #pragma unroll
         for (int o = 0; o < kLossTile; o++) acc[o] = 0.f;
         for (uint32_t j = t; j < P; j += blockDim.x) {
-            const FastOption op = ot.fast[j];
-            const uint32_t st = op.asset_type & 0x7fffffffu;
+            const FastOption op = ot.fast[j];     // full-loss records: no control variate
+            const uint32_t st = op.stock;
 #pragma unroll
-            for (int o = 0; o < kLossTile; o++) {
-                const float R = sR[o * Q + st];
-                acc[o] += option_loss_fast(op, R, slnR[o * Q + st], R);   // no control variate
-            }
+            for (int o = 0; o < kLossTile; o++) acc[o] += option_loss_fast(op, sR[o * Q + st], slnR[o * Q + st]);
         }
 #pragma unroll
         for (int o = 0; o < kLossTile; o++) {

@@ -157,17 +157,23 @@ __device__ __forceinline__ RT outer_normal_at(const TfKey& key, uint32_t tag, ui
 // ---- portfolio inner value (BS path of portfolio::sampler) ----------------------------------
 // sample_inner_bs with option_diff_from_blackscholes and the delta CV (portfolio_sampler.cpp:
 // 453-468, 186-200, 202-210) in the reference's arithmetic (REF32 / FP64 tables).
-template <class RT>
+// R_tau rows of the batched path: per outer sample and stock, R alone (the reference-arithmetic
+// precisions) or the pair (R, ln R) on the FP32 path, whose Black-Scholes needs ln R and takes it
+// from the row instead of a logarithm per inner sample.
+template <int PREC> struct RStride { static constexpr uint32_t v = PREC == PREC_FP32 ? 2 : 1; };
+
+template <class RT, uint32_t RS>
 __device__ __forceinline__ RT pf_value(const OptionTable<RT>& ot, const RT* Rrow, uint32_t j) {
     uint32_t s = ot.stock_ind[j];
     int type = ot.type[j];
     RT sigma = ot.sigma[s];
-    RT bs = calc_bs_ref<RT>(type, Rrow[s], ot.strike[j], ot.r, xsub(ot.maturity[j], ot.tau), sigma);
+    const RT R = Rrow[s * RS];
+    RT bs = calc_bs_ref<RT>(type, R, ot.strike[j], ot.r, xsub(ot.maturity[j], ot.tau), sigma);
     RT finish = ot.discount ? xmul(xexp(xmul(-ot.r, ot.tau)), bs) : bs;
     RT val = xmul(ot.w[j], xsub(ot.start[j], finish));
     if (ot.use_delta_cv) {
         RT derv = xmul(ot.w[j], calc_delta_ref<RT>(type, ot.S0[s], ot.strike[j], ot.r, ot.maturity[j], sigma));
-        val = xadd(val, xmul(xsub(Rrow[s], ot.S0[s]), derv));
+        val = xadd(val, xmul(xsub(R, ot.S0[s]), derv));
     }
     return val;
 }
@@ -194,18 +200,161 @@ __device__ __forceinline__ uint32_t pf_pick(const OptionTable<RT>& ot, uint64_t 
     return j;
 }
 
+// Table gathers of the FP32 portfolio path.  Every inner sample reads a random entry of the
+// option tables (alias entry, record or alias column; L2-resident, 8 to 32 bytes each), so a warp
+// load touches ~32 cache lines and the L1's tag stage, about one line per clock per SM, is the
+// path's throughput limit.  The gathers are single requests per lane (a record or column in one
+// 256-bit load, ld.global.v8 on sm_100) that bypass L1 allocation (L1::no_allocate).
+__device__ __forceinline__ uint2 load_alias(const uint2* p) {
+    uint2 e;
+    asm("ld.global.nc.L1::no_allocate.v2.u32 {%0,%1}, [%2];" : "=r"(e.x), "=r"(e.y) : "l"(p));
+    return e;
+}
+__device__ __forceinline__ FastOption load_record(const FastOption* p) {
+    FastOption o;
+    float st;
+    asm("ld.global.nc.L1::no_allocate.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=f"(o.c1), "=f"(o.inv_s), "=f"(o.s), "=f"(o.wR), "=f"(o.wK), "=f"(o.wV0), "=f"(o.cv), "=f"(st)
+        : "l"(p));
+    o.stock = __float_as_uint(st);
+    return o;
+}
+__device__ __forceinline__ FastColumn load_column(const FastColumn* p) {
+    FastColumn c;
+    float thr, link;
+    asm("ld.global.nc.L1::no_allocate.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=f"(c.c1), "=f"(c.inv_s), "=f"(c.wR), "=f"(c.wK), "=f"(c.wV0), "=f"(c.cv), "=f"(thr), "=f"(link)
+        : "l"(p));
+    c.thr = __float_as_uint(thr);
+    c.link = __float_as_uint(link);
+    return c;
+}
+
+// How the FP32 portfolio path draws an option: uniformly (records), from the alias table
+// (alias entry, then record) or from the alias columns (column, and the alias column when the coin
+// says so).
+enum PfMode : int { PF_UNIFORM = 0, PF_ALIAS = 1, PF_COLUMN = 2 };
+
+// Loss of the option drawn by the 64-bit value v: column j = floor(v P / 2^64), alias coin
+// (v P mod 2^64) >> 32, the option kept when coin < threshold and its alias otherwise (the same
+// option in every mode); Rrow holds (R, ln R) per stock of this outer sample.
+template <int MODE>
+__device__ __forceinline__ float pf_sample_loss(uint64_t v, const OptionTable<float>& ot, const float2* Rrow) {
+    const uint32_t j = (uint32_t)__umul64hi(v, (uint64_t)ot.P);
+    if (MODE == PF_COLUMN) {
+        const uint32_t coin = (uint32_t)((v * (uint64_t)ot.P) >> 32);
+        FastColumn c = load_column(ot.fast_col + j);
+        if (coin >= c.thr) c = load_column(ot.fast_col + (c.link >> 8));
+        const float2 r = Rrow[c.link & 0xffu];
+        return column_loss_fast(c, r.x, r.y);
+    }
+    uint32_t i = j;
+    if (MODE == PF_ALIAS) {
+        const uint32_t coin = (uint32_t)((v * (uint64_t)ot.P) >> 32);
+        const uint2 e = load_alias(ot.alias + j);
+        i = coin < e.x ? j : e.y;
+    }
+    const FastOption o = load_record(ot.fast_s + i);
+    const float2 r = Rrow[o.stock];
+    return option_loss_fast(o, r.x, r.y);
+}
+
+// C inner samples of the FP32 portfolio path from Threefry blocks b0, b0 + 1, ... (two samples per
+// block, one 64-bit value each).  Pilots (S2) accumulate the losses shifted by `shift`.
+template <int PREC, uint32_t C, bool S2, int MODE>
+__device__ __forceinline__ void pf_chunk_fast(const TfKey& key, uint32_t tag, uint64_t b0,
+                                              const OptionTable<float>& ot, const float2* Rrow, float shift,
+                                              Acc<PREC>& a1, Acc<PREC>& a2) {
+#pragma unroll 2
+    for (uint32_t b = 0; b < C / 2; b++) {
+        uint64_t v[2];
+        threefry2x64(b0 + b, tag, key, v[0], v[1]);
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            float x = pf_sample_loss<MODE>(v[q], ot, Rrow);
+            if (S2) x += shift;
+            a1.add(x);
+            if (S2) a2.add(x * x);
+        }
+    }
+}
+
+// R_tau rows staged in shared memory: segments whose tiles hold at most kRowItems outer samples
+// (every segment with 32 or more chunks per outer sample, where nearly all inner samples of a
+// level are) read R and ln R from shared memory, which takes the per-sample row lookups off the L1
+// tag stage.  kMaxStagedStocks bounds the dynamic shared memory (kRowItems x Q float2 = 16 KB).
+constexpr uint32_t kRowItems = 8;
+constexpr uint32_t kMaxStagedStocks = 256;
+constexpr size_t kRowSmemBytes = (size_t)kRowItems * kMaxStagedStocks * sizeof(float2);
+
+// Copies the rows of the outer samples lin0 .. lin0 + n - 1 of a segment into dst (n rows of Q).
+__device__ __forceinline__ void stage_rows(const float2* Rt, uint32_t Q, const uint32_t* list, uint64_t lin0,
+                                           uint32_t n, uint32_t n_items, float2* dst) {
+    for (uint32_t k = threadIdx.x; k < n * Q; k += blockDim.x) {
+        const uint32_t r = k / Q, q = k - r * Q;
+        const uint64_t lin = lin0 + r;
+        if (lin < n_items) {
+            const uint32_t item = list ? list[lin] : (uint32_t)lin;
+            dst[k] = Rt[(size_t)item * Q + q];
+        }
+    }
+}
+
+// ---- sampler kinds -------------------------------------------------------------------------
+// KIND_USER runs a caller-written SAMPLER class (the reference's SAMPLER concept, nested_sampler.hpp:
+// 36-85 and model_sampler.cpp:42-92, on the OUTER streams; include/nmlmc_sampler.cuh): its
+// sample_outer, init_inner_sampler, sample_inner and add_phi replace the built-in kinds' code, and
+// the batched machinery below is the same.  S is that class (NoSampler for the built-in kinds).
+struct NoSampler {};
+
+// The phi contribution coeff * phi(mean) of one inner mean (add_phi): the Indicator phi of the
+// built-in kinds (model_sampler.cpp:77-86), or the SAMPLER's own add_phi.
+template <int KIND, class S, class RT>
+__device__ __forceinline__ float phi_of(RT mean, float coeff) {
+    if constexpr (KIND == KIND_USER) {
+        RT p = 0;
+        S::add_phi(mean, (RT)coeff, &p);
+        return (float)p;
+    } else {
+        return mean >= (RT)0 ? coeff : 0.f;
+    }
+}
+
+// SAMPLER objects of KIND_USER: the one of outer sample `item` (its outer state, stored by
+// k_outer) and its workspace (OuterBuffers::user_ws, ws_bytes per outer sample).
+template <class S>
+__device__ __forceinline__ const S* user_state(const OuterBuffers& B, uint32_t item) {
+    return reinterpret_cast<const S*>(static_cast<const unsigned char*>(B.user_state) + (size_t)item * B.state_bytes);
+}
+__device__ __forceinline__ void* user_ws(const OuterBuffers& B, uint32_t item) {
+    return B.ws_bytes ? static_cast<unsigned char*>(B.user_ws) + (size_t)item * B.ws_bytes : nullptr;
+}
+
 // ---- one chunk: inner samples [s0, s0 + C) of phase `tag` of outer sample `item` ----------
 // The chunk's share of sample_inner's sums (nested_sampler.hpp:131-161; model::sampler::
 // sample_inner, model_sampler.cpp:66-79, or the portfolio's inner value above).
 // C (inner samples per chunk) is a compile-time constant so the independent Threefry blocks of a
 // chunk can be interleaved (two at a time) for instruction-level parallelism.
-template <class RT, int KIND, int PREC, uint32_t C, bool S2>
+template <class RT, int KIND, int PREC, uint32_t C, bool S2, class S>
 __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t item, uint32_t tag,
-                                             uint64_t s0, Acc<PREC>& a1, Acc<PREC>& a2, double& work) {
+                                             uint64_t s0, uint64_t count, float shift, const float2* srow,
+                                             Acc<PREC>& a1, Acc<PREC>& a2, double& work) {
     const OuterLevel<RT>& L = D.L;
     const TfKey key = tf_key(L.seed, outer_stream_id(L.ell, L.first_index + item));
     const RT* Yv = reinterpret_cast<const RT*>(D.B.Yv);
-    if (KIND == KIND_SHIFT_MODEL) {              // X = Y + Z: one normal per inner sample
+    if constexpr (KIND == KIND_USER) {           // the caller's SAMPLER (sample_inner)
+        S smp(user_ws(D.B, item));
+        smp.copy_outer(*user_state<S>(D.B, item));
+        double w = 0;
+        for (uint32_t q = 0; q < C; q++) {
+            smp.template nm_begin_inner_of<S>(key, tag, s0 + q);
+            RT d = smp.sample_inner(s0 + q, count, w);
+            if (PREC == PREC_FP32 && S2) d = (RT)((float)d + shift);
+            a1.add(d);
+            if (S2) a2.add(d * d);
+        }
+        work += w;
+    } else if (KIND == KIND_SHIFT_MODEL) {       // X = Y + Z: one normal per inner sample
         const RT Y = Yv[item];
 #pragma unroll 2
         for (uint32_t b = 0; b < C / 4; b++) {
@@ -217,6 +366,7 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 RT d = (PREC == PREC_FP32) ? (RT)(Y + z[q]) : xadd(Y, z[q]);
+                if (PREC == PREC_FP32 && S2) d = (RT)((float)d + shift);
                 a1.add(d);
                 if (S2) a2.add((PREC == PREC_FP32) ? (RT)(d * d) : xmul(d, d));
             }
@@ -237,6 +387,7 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
                 RT a = xadd(xmul(st, Y), xmul(s1t, X[q]));
                 RT c = xadd(xmul(st, Y2[q]), xmul(s1t, X[q]));
                 RT d = xsub(xmul(a, a), xmul(c, c));
+                if (PREC == PREC_FP32 && S2) d = (RT)((float)d + shift);
                 a1.add(d);
                 if (S2) a2.add(xmul(d, d));
             }
@@ -244,30 +395,28 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
         work += (double)C;
     } else if (PREC == PREC_FP32 && L.ot.fast_s) {
         // portfolio, FP32: packed records scaled by 1 / (sampling probability), the SFU
-        // Black-Scholes (nmlmc_bs.cuh); X = loss_j / phat_j
-        const OptionTable<RT>& ot = L.ot;
-        const float* Rrow = reinterpret_cast<const float*>(D.B.Rt) + (size_t)item * ot.Q;
-        const uint2* alias = ot.subsample == SUB_UNIFORM ? nullptr : ot.alias;
-#pragma unroll 2
-        for (uint32_t b = 0; b < C / 2; b++) {
-            uint64_t v[2];
-            threefry2x64((s0 >> 1) + b, tag, key, v[0], v[1]);
-#pragma unroll
-            for (int q = 0; q < 2; q++) {
-                const uint32_t j = pf_index(alias, ot.P, v[q]);
-                const FastOption o = ot.fast_s[j];
-                const uint32_t st = o.asset_type & 0x7fffffffu;
-                const float R = Rrow[st];
-                const float S0 = o.cv != 0.f ? (float)ot.S0[st] : 0.f;
-                const float d = option_loss_fast(o, R, __logf(R), S0);
-                a1.add((RT)d);
-                if (S2) a2.add((RT)(d * d));
+        // Black-Scholes (nmlmc_bs.cuh); X = loss_j / phat_j.  srow: the outer sample's R_tau row
+        // staged in shared memory, else read from the batch buffer.
+        if constexpr (sizeof(RT) == 4) {
+            const OptionTable<float>& ot = L.ot;
+            const float2* grow = reinterpret_cast<const float2*>(D.B.Rt) + (size_t)item * ot.Q;
+            const uint64_t b0 = s0 >> 1;
+            if (ot.fast_col) {
+                if (srow) pf_chunk_fast<PREC, C, S2, PF_COLUMN>(key, tag, b0, ot, srow, shift, a1, a2);
+                else pf_chunk_fast<PREC, C, S2, PF_COLUMN>(key, tag, b0, ot, grow, shift, a1, a2);
+            } else if (ot.subsample == SUB_UNIFORM) {
+                if (srow) pf_chunk_fast<PREC, C, S2, PF_UNIFORM>(key, tag, b0, ot, srow, shift, a1, a2);
+                else pf_chunk_fast<PREC, C, S2, PF_UNIFORM>(key, tag, b0, ot, grow, shift, a1, a2);
+            } else {
+                if (srow) pf_chunk_fast<PREC, C, S2, PF_ALIAS>(key, tag, b0, ot, srow, shift, a1, a2);
+                else pf_chunk_fast<PREC, C, S2, PF_ALIAS>(key, tag, b0, ot, grow, shift, a1, a2);
             }
         }
         work += (double)C;
     } else {                                     // portfolio: one 64-bit value per inner sample
         const OptionTable<RT>& ot = L.ot;
-        const RT* Rrow = reinterpret_cast<const RT*>(D.B.Rt) + (size_t)item * ot.Q;
+        constexpr uint32_t RS = RStride<PREC>::v;
+        const RT* Rrow = reinterpret_cast<const RT*>(D.B.Rt) + (size_t)item * ot.Q * RS;
 #pragma unroll 2
         for (uint32_t b = 0; b < C / 2; b++) {
             uint64_t v[2];
@@ -276,7 +425,7 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
             for (int q = 0; q < 2; q++) {
                 RT prob;
                 uint32_t j = pf_pick<RT>(ot, v[q], prob);
-                RT d = xdiv(pf_value<RT>(ot, Rrow, j), prob);
+                RT d = xdiv(pf_value<RT, RS>(ot, Rrow, j), prob);
                 work += (double)ot.W_est[j];
                 a1.add(d);
                 if (S2) a2.add(xmul(d, d));
@@ -285,27 +434,32 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
     }
 }
 
-template <class RT, int KIND, int PREC, bool S2>
+template <class RT, int KIND, int PREC, bool S2, class S>
 __device__ __forceinline__ void eval_chunk_s(const DevLevel<RT>& D, uint32_t item, uint32_t tag,
-                                             uint64_t s0, uint32_t C, Acc<PREC>& a1, Acc<PREC>& a2,
-                                             double& work) {
+                                             uint64_t s0, uint64_t count, uint32_t C, float shift,
+                                             const float2* srow, Acc<PREC>& a1, Acc<PREC>& a2, double& work) {
     switch (C) {
-    case 64: eval_chunk_c<RT, KIND, PREC, 64, S2>(D, item, tag, s0, a1, a2, work); break;
-    case 32: eval_chunk_c<RT, KIND, PREC, 32, S2>(D, item, tag, s0, a1, a2, work); break;
-    case 16: eval_chunk_c<RT, KIND, PREC, 16, S2>(D, item, tag, s0, a1, a2, work); break;
-    case 8: eval_chunk_c<RT, KIND, PREC, 8, S2>(D, item, tag, s0, a1, a2, work); break;
-    default: eval_chunk_c<RT, KIND, PREC, 4, S2>(D, item, tag, s0, a1, a2, work); break;
+    case 64: eval_chunk_c<RT, KIND, PREC, 64, S2, S>(D, item, tag, s0, count, shift, srow, a1, a2, work); break;
+    case 32: eval_chunk_c<RT, KIND, PREC, 32, S2, S>(D, item, tag, s0, count, shift, srow, a1, a2, work); break;
+    case 16: eval_chunk_c<RT, KIND, PREC, 16, S2, S>(D, item, tag, s0, count, shift, srow, a1, a2, work); break;
+    case 8: eval_chunk_c<RT, KIND, PREC, 8, S2, S>(D, item, tag, s0, count, shift, srow, a1, a2, work); break;
+    default: eval_chunk_c<RT, KIND, PREC, 4, S2, S>(D, item, tag, s0, count, shift, srow, a1, a2, work); break;
     }
 }
 
 // want_s2 (pilots: the sum of squares for the variance) is resolved once per chunk, so the
-// inner loop carries no per-sample test.
-template <class RT, int KIND, int PREC>
+// inner loop carries no per-sample test.  `count`: the segment's inner count per outer sample (the
+// SAMPLER's sample_inner argument).  On the FP32 path a pilot accumulates the inner values
+// shifted by the outer sample's start value (d + start, whose mean is the distance from the
+// threshold that the adaptive rule compares with the spread), so the one-pass variance
+// s2 - s1^2 / n does not cancel where the decision is close; the final phase accumulates d.
+// `srow`: the outer sample's R_tau row in shared memory, or nullptr (FP32 portfolio path).
+template <class RT, int KIND, int PREC, class S>
 __device__ __forceinline__ void eval_chunk(const DevLevel<RT>& D, uint32_t item, uint32_t tag,
-                                           uint64_t s0, uint32_t C, bool want_s2, Acc<PREC>& a1,
-                                           Acc<PREC>& a2, double& work) {
-    if (want_s2) eval_chunk_s<RT, KIND, PREC, true>(D, item, tag, s0, C, a1, a2, work);
-    else eval_chunk_s<RT, KIND, PREC, false>(D, item, tag, s0, C, a1, a2, work);
+                                           uint64_t s0, uint64_t count, uint32_t C, bool want_s2, RT start,
+                                           const float2* srow, Acc<PREC>& a1, Acc<PREC>& a2, double& work) {
+    if (want_s2) eval_chunk_s<RT, KIND, PREC, true, S>(D, item, tag, s0, count, C, (float)start, srow, a1, a2, work);
+    else eval_chunk_s<RT, KIND, PREC, false, S>(D, item, tag, s0, count, C, 0.f, srow, a1, a2, work);
 }
 
 // ---- segments of uniform chunk count ------------------------------------------------------
@@ -338,10 +492,10 @@ __device__ __forceinline__ bool pilot_decide(const DevLevel<RT>& D, const Seg& g
     const uint64_t cur = g.count;
     RT delta2;
     if (PREC == PREC_FP32) {
+        // the sums are of d + start (eval_chunk): their mean is the distance start + mean(d)
         float s1 = (float)a1.value(), s2 = (float)a2.value(), n = (float)cur;
-        float mean_d = div_count(s1, cur);
-        float var = __fdiv_rn(__fsub_rn(s2, __fmul_rn(s1, mean_d)), n - 1.0f);
-        float dist = __fadd_rn((float)start, mean_d);
+        float dist = div_count(s1, cur);
+        float var = __fdiv_rn(__fsub_rn(s2, __fmul_rn(s1, dist)), n - 1.0f);
         delta2 = (RT)__fdiv_rn(__fmul_rn(dist, dist), var);
     } else {
         double s1 = (double)a1.value(), s2 = (double)a2.value();
@@ -390,11 +544,11 @@ __device__ __forceinline__ uint32_t pilots_taken(uint32_t cnt, const CountParams
 // moment slots mom[q * kTile] (q = 0..3 phi_f^k, 4..7 (phi_f - phi_c)^k; a zero phi adds
 // nothing and touches no slot), the counts of items that hit the maximum / stayed at the base
 // count, and the trace record.
-template <class RT>
+template <class RT, int KIND, class S>
 __device__ __forceinline__ void final_item(const DevLevel<RT>& D, uint32_t item, RT mean_big, RT phi_small,
                                            bool fine_big, double* mom, uint32_t& n_max, uint32_t& n_base,
                                            TraceRec* trace) {
-    RT phi_big = (mean_big >= (RT)0) ? (RT)1 : (RT)0;
+    RT phi_big = (RT)phi_of<KIND, S, RT>(mean_big, 1.f);
     RT f_phi, c_phi;
     if (D.L.fine_only) { f_phi = phi_big; c_phi = 0; }
     else if (fine_big) { f_phi = phi_big; c_phi = phi_small; }
@@ -437,15 +591,21 @@ __device__ __forceinline__ void final_item(const DevLevel<RT>& D, uint32_t item,
 // MINB = CTAs per SM the register allocation must allow (1: up to 255 registers per thread,
 // 3: 80, 4: 64) — the register/occupancy variants the autotuner chooses between.  The variants
 // run the same arithmetic in the same order, so their results are identical.
-template <class RT, int KIND, int PREC, int MINB>
-__global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet S, TraceRec* trace) {
+template <class RT, int KIND, int PREC, int MINB, class S = NoSampler>
+__global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet SS, TraceRec* trace) {
     __shared__ Acc<PREC> sm_a1[kWarps];
     __shared__ Acc<PREC> sm_a2[kWarps];
     __shared__ float sm_ind[kWarps];
     __shared__ double sm_mom[8 * kTile];        // per-thread moment slots [q][thread]
     __shared__ double sm_acc[kWarps][16];
     __shared__ uint32_t sm_ticket;
+    extern __shared__ float2 k_phase_rows[];             // staged R_tau rows (FP32 portfolio path)
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    // R_tau rows of the FP32 portfolio path can be staged (kRowItems rows of Q stocks)
+    const uint32_t Qs = D.L.ot.Q;
+    const float2* Rt2 = reinterpret_cast<const float2*>(D.B.Rt);
+    const bool can_stage = KIND == KIND_PORTFOLIO && PREC == PREC_FP32 && D.L.ot.fast_s != nullptr &&
+                           Qs <= kMaxStagedStocks;
     const uint32_t C = D.L.chunk;
     uint32_t* counters = D.B.counters;
     double wsum = 0;                                     // work of this thread's chunks
@@ -457,8 +617,8 @@ __global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet S,
     __syncthreads();
     const RT* Yv = reinterpret_cast<const RT*>(D.B.Yv);
 
-    for (int si = 0; si < S.n; si++) {
-        const Seg g = S.s[si];
+    for (int si = 0; si < SS.n; si++) {
+        const Seg g = SS.s[si];
         const uint32_t* list = g.list;
         uint32_t n_items = g.list ? counters[g.n_slot] : g.n_host;
         if (g.mode == 2 && g.list) {
@@ -483,11 +643,17 @@ __global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet S,
             // ---- a tile holds kTile / nch whole items ----
             const uint32_t per_tile = kTile / nch;
             const uint64_t tiles = ((uint64_t)n_items + per_tile - 1) / per_tile;
+            const bool stage = can_stage && per_tile <= kRowItems;
             for (;;) {
                 __syncthreads();                         // every thread has read the ticket
                 if (ticket >= tiles) break;
                 uint32_t next = 0;
                 if (t == 0) next = atomicAdd(queue, 1u);
+                if (stage) {                             // the tile's rows (the previous tile is done)
+                    stage_rows(Rt2, Qs, list, ticket * per_tile, per_tile, n_items, k_phase_rows);
+                    __syncthreads();
+                }
+                const float2* srow = stage ? k_phase_rows + (size_t)(t >> g.nch_log2) * Qs : nullptr;
                 const uint64_t lin = ticket * per_tile + (t >> g.nch_log2);
                 const uint32_t j = t & (nch - 1);
                 const bool valid = lin < n_items;
@@ -501,21 +667,21 @@ __global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet S,
                     fine_big = cf > cc;
                     gs = (uint32_t)(csmall / C);
                 }
-                const RT start = valid ? (D.L.ot.P ? Yv[item] : -D.L.mp.max_loss) : (RT)0;
+                const RT start = valid ? ((KIND == KIND_USER || D.L.ot.P) ? Yv[item] : -D.L.mp.max_loss) : (RT)0;
                 Acc<PREC> a1, a2;
                 a1.zero();
                 a2.zero();
-                if (valid) eval_chunk<RT, KIND, PREC>(D, item, g.tag, (uint64_t)j * C, C, pilot, a1, a2, wsum);
+                if (valid) eval_chunk<RT, KIND, PREC, S>(D, item, g.tag, (uint64_t)j * C, g.count, C, pilot, start, srow, a1, a2, wsum);
                 const float coeff = (float)gs / (float)nch;     // 1 / groups (a power of two)
                 float ind = 0.f;
-                if (!pilot && gs == 1) ind = inner_mean<RT, PREC>(start, a1, csmall) >= (RT)0 ? coeff : 0.f;
+                if (!pilot && gs == 1) ind = phi_of<KIND, S, RT>(inner_mean<RT, PREC>(start, a1, csmall), coeff);
                 const uint32_t wl = nch < 32 ? nch : 32;
                 for (uint32_t m = 1; m < wl; m <<= 1) {
                     a1.merge(a1.shfl_xor(m));
                     if (pilot) a2.merge(a2.shfl_xor(m));
                     else {
                         ind += __shfl_xor_sync(0xffffffffu, ind, m);
-                        if (2 * m == gs) ind = inner_mean<RT, PREC>(start, a1, csmall) >= (RT)0 ? coeff : 0.f;
+                        if (2 * m == gs) ind = phi_of<KIND, S, RT>(inner_mean<RT, PREC>(start, a1, csmall), coeff);
                     }
                 }
                 const bool leader = (j == 0) && valid;
@@ -534,7 +700,7 @@ __global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet S,
                                 Acc<PREC> gsum;
                                 gsum.zero();
                                 for (uint32_t q = 0; q < gw; q++) gsum.merge(sm_a1[warp + gq * gw + q]);
-                                ti += inner_mean<RT, PREC>(start, gsum, csmall) >= (RT)0 ? coeff : 0.f;
+                                ti += phi_of<KIND, S, RT>(inner_mean<RT, PREC>(start, gsum, csmall), coeff);
                                 t1.merge(gsum);
                             }
                         } else {
@@ -554,7 +720,7 @@ __global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet S,
                     const bool surv = leader && pilot_decide<RT, PREC>(D, g, item, start, a1, a2);
                     warp_append(surv, item, counters + g.next_slot, g.next_list, lane);
                 } else if (leader) {
-                    final_item<RT>(D, item, inner_mean<RT, PREC>(start, a1, g.count), (RT)ind, fine_big, mom,
+                    final_item<RT, KIND, S>(D, item, inner_mean<RT, PREC>(start, a1, g.count), (RT)ind, fine_big, mom,
                                    n_max, n_base, trace);
                 }
                 if (t == 0) sm_ticket = next;
@@ -570,6 +736,11 @@ __global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet S,
                 uint32_t next = 0;
                 if (t == 0) next = atomicAdd(queue, 1u);
                 const uint32_t item = list ? list[ticket] : (uint32_t)ticket;
+                if (can_stage) {                         // this item's row (the previous item is done)
+                    stage_rows(Rt2, Qs, nullptr, item, 1, item + 1, k_phase_rows);
+                    __syncthreads();
+                }
+                const float2* srow = can_stage ? k_phase_rows : nullptr;
                 uint32_t gs = nch;
                 uint64_t csmall = g.count;
                 bool fine_big = true;
@@ -579,7 +750,7 @@ __global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet S,
                     fine_big = cf > cc;
                     gs = (uint32_t)(csmall / C);
                 }
-                const RT start = D.L.ot.P ? Yv[item] : -D.L.mp.max_loss;
+                const RT start = (KIND == KIND_USER || D.L.ot.P) ? Yv[item] : -D.L.mp.max_loss;
                 const float coeff = (float)gs / (float)nch;
                 Acc<PREC> tot1, tot2, gacc;
                 tot1.zero();
@@ -591,15 +762,15 @@ __global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet S,
                     Acc<PREC> a1, a2;
                     a1.zero();
                     a2.zero();
-                    eval_chunk<RT, KIND, PREC>(D, item, g.tag, (uint64_t)j * C, C, pilot, a1, a2, wsum);
+                    eval_chunk<RT, KIND, PREC, S>(D, item, g.tag, (uint64_t)j * C, g.count, C, pilot, start, srow, a1, a2, wsum);
                     float ind = 0.f;
-                    if (!pilot && gs == 1) ind = inner_mean<RT, PREC>(start, a1, csmall) >= (RT)0 ? coeff : 0.f;
+                    if (!pilot && gs == 1) ind = phi_of<KIND, S, RT>(inner_mean<RT, PREC>(start, a1, csmall), coeff);
                     for (uint32_t m = 1; m < 32; m <<= 1) {
                         a1.merge(a1.shfl_xor(m));
                         if (pilot) a2.merge(a2.shfl_xor(m));
                         else {
                             ind += __shfl_xor_sync(0xffffffffu, ind, m);
-                            if (2 * m == gs) ind = inner_mean<RT, PREC>(start, a1, csmall) >= (RT)0 ? coeff : 0.f;
+                            if (2 * m == gs) ind = phi_of<KIND, S, RT>(inner_mean<RT, PREC>(start, a1, csmall), coeff);
                         }
                     }
                     if (lane == 0) { sm_a1[warp] = a1; sm_a2[warp] = a2; sm_ind[warp] = ind; }
@@ -611,7 +782,7 @@ __global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet S,
                                 Acc<PREC> gsum;
                                 gsum.zero();
                                 for (uint32_t q = 0; q < gw; q++) gsum.merge(sm_a1[gq * gw + q]);
-                                tind += inner_mean<RT, PREC>(start, gsum, csmall) >= (RT)0 ? coeff : 0.f;
+                                tind += phi_of<KIND, S, RT>(inner_mean<RT, PREC>(start, gsum, csmall), coeff);
                                 tot1.merge(gsum);
                             }
                         } else {
@@ -626,7 +797,7 @@ __global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet S,
                             if (!pilot && gs >= (uint32_t)kTile) {
                                 gacc.merge(t1);
                                 if ((((uint64_t)tl + 1) * kTile) % gs == 0) {
-                                    tind += inner_mean<RT, PREC>(start, gacc, csmall) >= (RT)0 ? coeff : 0.f;
+                                    tind += phi_of<KIND, S, RT>(inner_mean<RT, PREC>(start, gacc, csmall), coeff);
                                     gacc.zero();
                                 }
                             }
@@ -639,7 +810,7 @@ __global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet S,
                         if (pilot_decide<RT, PREC>(D, g, item, start, tot1, tot2))
                             g.next_list[atomicAdd(&counters[g.next_slot], 1u)] = item;
                     } else {
-                        final_item<RT>(D, item, inner_mean<RT, PREC>(start, tot1, g.count), (RT)tind, fine_big, mom,
+                        final_item<RT, KIND, S>(D, item, inner_mean<RT, PREC>(start, tot1, g.count), (RT)tind, fine_big, mom,
                                        n_max, n_base, trace);
                     }
                     sm_ticket = next;
@@ -680,7 +851,7 @@ __global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet S,
 // sample_outer of the model (Y = randn_sync, model_sampler.cpp:57-59) or of the portfolio (the
 // stocks at tau and the delta-CV constant, portfolio_sampler.cpp:293-311, 606-614) per outer
 // sample, from the OUTER layout's phase-0 draws.
-template <class RT, int KIND, int PREC>
+template <class RT, int KIND, int PREC, class S = NoSampler>
 __global__ void __launch_bounds__(kTile) k_outer(DevLevel<RT> D, uint32_t nb) {
     const OuterLevel<RT>& L = D.L;
     RT* Yv = reinterpret_cast<RT*>(D.B.Yv);
@@ -688,12 +859,24 @@ __global__ void __launch_bounds__(kTile) k_outer(DevLevel<RT> D, uint32_t nb) {
         const TfKey key = tf_key(L.seed, outer_stream_id(L.ell, L.first_index + i));
         D.B.cnt_f[i] = L.adaptive_f ? 0u : (uint32_t)L.cf.max_count;
         D.B.cnt_c[i] = L.adaptive_c ? 0u : (uint32_t)L.cc.max_count;
-        if (KIND != KIND_PORTFOLIO) {
+        if constexpr (KIND == KIND_USER) {
+            // the caller's SAMPLER: sample_outer from the outer stream, then the start value of its
+            // inner estimates (init_inner_sampler, called once per outer sample: the batched path
+            // needs a start that does not depend on the count); the object keeps the outer state
+            S smp(user_ws(D.B, i));
+            smp.nm_begin_outer(key);
+            double w = 0;
+            smp.sample_outer(L.ell, w);
+            uint64_t cnt = L.cf.base_count;
+            Yv[i] = smp.init_inner_sampler(cnt, w);
+            *const_cast<S*>(user_state<S>(D.B, i)) = smp;
+        } else if (KIND != KIND_PORTFOLIO) {
             Yv[i] = outer_normal_at<PREC, RT>(key, PH_OUTER, 0);
         } else {
             // portfolio_sampler.cpp:293-311 on the OUTER layout: normal 0 systemic, 1 + s per stock
             const OptionTable<RT>& ot = L.ot;
-            RT* Rrow = reinterpret_cast<RT*>(D.B.Rt) + (size_t)i * ot.Q;
+            constexpr uint32_t RS = RStride<PREC>::v;
+            RT* Rrow = reinterpret_cast<RT*>(D.B.Rt) + (size_t)i * ot.Q * RS;
             RT dW_sys = 0, cv = (RT)0;
             const uint32_t nnorm = ot.Q == 1 ? 1 : ot.Q + 1;
             for (uint32_t b = 0; 4 * b < nnorm; b++) {          // four normals per block
@@ -709,13 +892,15 @@ __global__ void __launch_bounds__(kTile) k_outer(DevLevel<RT> D, uint32_t nb) {
                     const uint32_t s = ot.Q == 1 ? 0 : k - 1;
                     RT W = ot.Q == 1 ? dW_sys : xadd(xmul(ot.rho, dW_sys), xmul(ot.s1_rho2, xmul(ot.stau, z[q])));
                     RT R;
-                    if (PREC == PREC_FP32) {     // GBM at tau in float (expf), the fast path's R
-                        const float sg = (float)ot.sigma[s];
-                        R = (RT)((float)ot.S0[s] * expf(sg * (float)W + ((float)ot.mu[s] - 0.5f * sg * sg) * (float)ot.tau));
+                    if (PREC == PREC_FP32) {     // GBM at tau in float (expf) and its logarithm
+                        const float sg = (float)ot.sigma[s], S0 = (float)ot.S0[s];
+                        const float e = sg * (float)W + ((float)ot.mu[s] - 0.5f * sg * sg) * (float)ot.tau;
+                        R = (RT)(S0 * expf(e));
+                        Rrow[s * RS + 1] = (RT)(logf(S0) + e);
                     } else {
                         R = simulate_stock_ref<RT>(ot.S0[s], ot.mu[s], ot.sigma[s], ot.tau, W);
                     }
-                    Rrow[s] = R;
+                    Rrow[s * RS] = R;
                     if (ot.use_delta_cv) cv = xadd(cv, xmul(xsub(R, ot.S0[s]), ot.delta_coalesce[s]));
                 }
             }
@@ -779,14 +964,22 @@ static __global__ void __launch_bounds__(256) k_reduce_blocks(const double* bloc
 
 // Persistent grid of the phase kernel: the CTAs that are resident at once (occupancy x SMs),
 // at most the grid the partial-sum buffer was sized for.
-template <class RT, int KIND, int PREC, int MINB>
+// Dynamic shared memory of a phase-kernel instantiation: the staged R_tau rows of the FP32
+// portfolio path (set as the kernel's maximum once, before the occupancy query and the first
+// launch).
+template <int KIND, int PREC>
+constexpr size_t phase_dyn_smem() { return (KIND == KIND_PORTFOLIO && PREC == PREC_FP32) ? kRowSmemBytes : 0; }
+
+template <class RT, int KIND, int PREC, int MINB, class S = NoSampler>
 static int phase_grid(int cap) {
     static int g = 0;
     if (g == 0) {
         int dev = 0, sms = 148, per_sm = 0;
+        constexpr size_t dyn = phase_dyn_smem<KIND, PREC>();
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_phase<RT, KIND, PREC, MINB>, kTile, 0) != cudaSuccess ||
+        if (dyn) cudaFuncSetAttribute(k_phase<RT, KIND, PREC, MINB, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_phase<RT, KIND, PREC, MINB, S>, kTile, dyn) != cudaSuccess ||
             per_sm < 1)
             per_sm = 1;
         g = per_sm * sms;
@@ -794,24 +987,25 @@ static int phase_grid(int cap) {
     return g < cap ? g : cap;
 }
 
-template <class RT, int KIND, int PREC, int MINB>
-static void launch_phase_v(const DevLevel<RT>& D, const SegSet& S, TraceRec* trace, cudaStream_t stream) {
+template <class RT, int KIND, int PREC, int MINB, class S = NoSampler>
+static void launch_phase_v(const DevLevel<RT>& D, const SegSet& SS, TraceRec* trace, cudaStream_t stream) {
     cudaMemsetAsync(D.B.counters + CNT_QUEUE, 0, kMaxSegs * sizeof(uint32_t), stream);
     if (D.B.prof_mark) D.B.prof_mark(D.B.prof_user, 0, stream);
-    k_phase<RT, KIND, PREC, MINB><<<phase_grid<RT, KIND, PREC, MINB>(D.B.grid), kTile, 0, stream>>>(D, S, trace);
+    const int grid = phase_grid<RT, KIND, PREC, MINB, S>(D.B.grid);
+    k_phase<RT, KIND, PREC, MINB, S><<<grid, kTile, phase_dyn_smem<KIND, PREC>(), stream>>>(D, SS, trace);
     if (D.B.prof_mark) D.B.prof_mark(D.B.prof_user, 1, stream);
     count_launch();
 }
 
 // The FP32 path has three register/occupancy variants (OuterLevel::variant 0, 1, 2 -> 1, 3, 4
 // resident CTAs per SM guaranteed); the parity precisions run variant 0.
-template <class RT, int KIND, int PREC>
-static void launch_phase(const DevLevel<RT>& D, const SegSet& S, TraceRec* trace, cudaStream_t stream) {
-    if constexpr (PREC == PREC_FP32) {
-        if (D.L.variant == 1) return launch_phase_v<RT, KIND, PREC, 3>(D, S, trace, stream);
-        if (D.L.variant == 2) return launch_phase_v<RT, KIND, PREC, 4>(D, S, trace, stream);
+template <class RT, int KIND, int PREC, class S = NoSampler>
+static void launch_phase(const DevLevel<RT>& D, const SegSet& SS, TraceRec* trace, cudaStream_t stream) {
+    if constexpr (PREC == PREC_FP32 && KIND != KIND_USER) {
+        if (D.L.variant == 1) return launch_phase_v<RT, KIND, PREC, 3>(D, SS, trace, stream);
+        if (D.L.variant == 2) return launch_phase_v<RT, KIND, PREC, 4>(D, SS, trace, stream);
     }
-    launch_phase_v<RT, KIND, PREC, 1>(D, S, trace, stream);
+    launch_phase_v<RT, KIND, PREC, 1, S>(D, SS, trace, stream);
 }
 
 static inline uint32_t ilog2_u64(uint64_t v) {
@@ -820,7 +1014,7 @@ static inline uint32_t ilog2_u64(uint64_t v) {
     return r;
 }
 
-template <class RT, int KIND, int PREC>
+template <class RT, int KIND, int PREC, class S = NoSampler>
 static cudaError_t run_batch(DevLevel<RT>& D, uint32_t nb, TraceRec* trace, cudaStream_t stream) {
     const OuterLevel<RT>& L = D.L;
     OuterBuffers& B = D.B;
@@ -830,7 +1024,7 @@ static cudaError_t run_batch(DevLevel<RT>& D, uint32_t nb, TraceRec* trace, cuda
     int og = (int)((nb + kTile - 1) / kTile);
     if (og > grid) og = grid;
     if (og < 1) og = 1;
-    k_outer<RT, KIND, PREC><<<og, kTile, 0, stream>>>(D, nb);
+    k_outer<RT, KIND, PREC, S><<<og, kTile, 0, stream>>>(D, nb);
     count_launch();
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
 
@@ -846,13 +1040,13 @@ static cudaError_t run_batch(DevLevel<RT>& D, uint32_t nb, TraceRec* trace, cuda
             e = cudaMemsetAsync(B.counters + CNT_LIST + nxt, 0, sizeof(uint32_t), stream);
             if (e == cudaSuccess) e = cudaMemsetAsync(B.counters + CNT_LIST + 2 + nxt, 0, sizeof(uint32_t), stream);
             if (e != cudaSuccess) return e;
-            SegSet S;
-            S.n = 0;
+            SegSet SS;
+            SS.n = 0;
             for (int which = 0; which < 2; which++) {
                 const bool fine = which == 0;
                 if (fine ? (r >= rounds_f) : (r >= rounds_c)) continue;
                 const CountParams& cp = fine ? L.cf : L.cc;
-                Seg& g = S.s[S.n++];
+                Seg& g = SS.s[SS.n++];
                 g.list = (r == 0) ? nullptr : (fine ? listF[cur] : listC[cur]);
                 g.n_slot = CNT_LIST + (fine ? 0 : 2) + cur;
                 g.n_host = nb;
@@ -864,8 +1058,8 @@ static cudaError_t run_batch(DevLevel<RT>& D, uint32_t nb, TraceRec* trace, cuda
                 g.next_slot = CNT_LIST + (fine ? 0 : 2) + nxt;
                 g.next_list = fine ? listF[nxt] : listC[nxt];
             }
-            if (S.n == 0) continue;
-            launch_phase<RT, KIND, PREC>(D, S, nullptr, stream);
+            if (SS.n == 0) continue;
+            launch_phase<RT, KIND, PREC, S>(D, SS, nullptr, stream);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         e = cudaMemsetAsync(B.counters + CNT_CLASS, 0, 128 * sizeof(uint32_t), stream);
@@ -876,10 +1070,10 @@ static cudaError_t run_batch(DevLevel<RT>& D, uint32_t nb, TraceRec* trace, cuda
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         const uint64_t maxc = L.cf.max_count > L.cc.max_count ? L.cf.max_count : L.cc.max_count;
         const uint32_t kmax = ilog2_u64(maxc / C);
-        SegSet S;
-        S.n = 0;
-        for (uint32_t k = 0; k <= kmax && S.n < kMaxSegs; k++) {
-            Seg& g = S.s[S.n++];
+        SegSet SS;
+        SS.n = 0;
+        for (uint32_t k = 0; k <= kmax && SS.n < kMaxSegs; k++) {
+            Seg& g = SS.s[SS.n++];
             g.list = B.class_items;
             g.n_slot = CNT_CLASS + k;
             g.n_host = 0;
@@ -891,13 +1085,13 @@ static cudaError_t run_batch(DevLevel<RT>& D, uint32_t nb, TraceRec* trace, cuda
             g.next_slot = 0;
             g.next_list = nullptr;
         }
-        launch_phase<RT, KIND, PREC>(D, S, trace, stream);
+        launch_phase<RT, KIND, PREC, S>(D, SS, trace, stream);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     } else {
         const uint64_t cbig = (L.fine_only || L.cf.max_count >= L.cc.max_count) ? L.cf.max_count : L.cc.max_count;
-        SegSet S;
-        S.n = 1;
-        Seg& g = S.s[0];
+        SegSet SS;
+        SS.n = 1;
+        Seg& g = SS.s[0];
         g.list = nullptr;
         g.n_slot = 0;
         g.n_host = nb;
@@ -908,13 +1102,13 @@ static cudaError_t run_batch(DevLevel<RT>& D, uint32_t nb, TraceRec* trace, cuda
         g.class_k = 0;
         g.next_slot = 0;
         g.next_list = nullptr;
-        launch_phase<RT, KIND, PREC>(D, S, trace, stream);
+        launch_phase<RT, KIND, PREC, S>(D, SS, trace, stream);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     return cudaSuccess;
 }
 
-template <class RT, int KIND, int PREC>
+template <class RT, int KIND, int PREC, class S = NoSampler>
 cudaError_t sample_level_t(const OuterLevel<RT>& L, OuterBuffers& B, TraceRec* trace,
                                   cudaStream_t stream) {
     DevLevel<RT> D;
@@ -923,7 +1117,7 @@ cudaError_t sample_level_t(const OuterLevel<RT>& L, OuterBuffers& B, TraceRec* t
     for (uint64_t done = 0; done < L.M;) {
         const uint64_t nb = (L.M - done) < B.cap ? (L.M - done) : B.cap;
         D.L.first_index = L.first_index + done;
-        cudaError_t e = run_batch<RT, KIND, PREC>(D, (uint32_t)nb, trace ? trace + done : nullptr, stream);
+        cudaError_t e = run_batch<RT, KIND, PREC, S>(D, (uint32_t)nb, trace ? trace + done : nullptr, stream);
         if (e != cudaSuccess) return e;
         done += nb;
     }

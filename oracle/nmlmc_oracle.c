@@ -144,12 +144,16 @@ struct o_ctx {
     /* OUTER layout: next outer index per level, shard */
     uint64_t next_outer[64];
     uint32_t shard_rank, shard_world;
+    /* optional per-outer-sample record of the adaptive decisions' distance from their threshold */
+    double *margins;
 };
 
 void o_set_shard(o_ctx *c, uint32_t rank, uint32_t world) {
     c->shard_rank = rank;
     c->shard_world = world ? world : 1;
 }
+
+void o_set_margins(o_ctx *c, double *buf) { c->margins = buf; }
 
 o_ctx *o_create(int prec, int streams, uint32_t cores, uint32_t N0, uint32_t beta,
                 double adaptive_r, int antithetic, int adaptive_incl_r2, uint64_t seed) {

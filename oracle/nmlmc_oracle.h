@@ -59,6 +59,11 @@ void o_destroy(o_ctx *);
 /* OUTER layout sharding: each o_sample(ell, M) evaluates the rank's static share of the M outer
  * samples with their single-device stream indices (the semantics of nmlmc_set_shard). */
 void o_set_shard(o_ctx *, uint32_t rank, uint32_t world);
+/* With buf set, every o_sample call writes buf[m] for its outer sample m: the smallest
+ * |ln(new_count / cur)| over that sample's adaptive decisions (get_samples_count's test
+ * new_count <= cur, nested_sampler.hpp:262-266), +inf if it took none.  Test instrumentation:
+ * how far an FP64 decision was from flipping. */
+void o_set_margins(o_ctx *, double *buf);
 void o_set_model(o_ctx *, int kind, double tau, double max_loss);
 /* Portfolio of BS options (ComputeMethod::BS only).  start/delta_est are computed as
  * portfolio_comp_params does (portfolio_sampler.cpp:687-700) and returned. */

@@ -190,7 +190,9 @@ class Sampler:
         if rc != 0:
             raise ValueError("invalid portfolio (stock index, or prob not positive/non-increasing)")
 
-    def sample(self, ell: int, M: int, trace: bool = False, events_cap: int = 0):
+    def sample(self, ell: int, M: int, trace: bool = False, events_cap: int = 0, margins: bool = False):
+        """One sample(ell, M) call; with `margins`, out["margins"][m] is the smallest
+        |ln(new_count / cur)| of outer sample m's adaptive decisions (o_set_margins)."""
         f = np.zeros(4)
         dd = np.zeros(4)
         w = np.zeros(1)
@@ -204,12 +206,22 @@ class Sampler:
             aux = np.zeros(events_cap)
             bufs = (kinds, vals, aux)
             ev = Events(ctypes.cast(kinds, ctypes.c_char_p), _p(vals, _dp), _p(aux, _dp), events_cap, 0)
-        rc = self.L.o_sample(self.h, ell, M, _p(f, _dp), _p(dd, _dp), _p(w, _dp), _p(st, _u64p),
-                             tr.ctypes.data if tr is not None else None,
-                             ctypes.addressof(ev) if ev is not None else None)
+        mg = None
+        if margins:
+            mg = np.full(M, np.inf)
+            _margins_bind().o_set_margins(self.h, _p(mg, _dp))
+        try:
+            rc = self.L.o_sample(self.h, ell, M, _p(f, _dp), _p(dd, _dp), _p(w, _dp), _p(st, _u64p),
+                                 tr.ctypes.data if tr is not None else None,
+                                 ctypes.addressof(ev) if ev is not None else None)
+        finally:
+            if margins:
+                _margins_bind().o_set_margins(self.h, None)
         if rc != 0:
             raise RuntimeError("event buffer too small")
         out = dict(fsums=f, diffsums=dd, work=float(w[0]), stats=st, trace=tr)
+        if margins:
+            out["margins"] = mg
         if ev is not None:
             n = ev.n
             out["events"] = (bufs[0].raw[:n].decode(), bufs[1][:n].copy(), bufs[2][:n].copy())
@@ -414,6 +426,14 @@ def _shard_bind():
     if not getattr(L, "_shard_bound", False):
         L.o_set_shard.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32]
         L._shard_bound = True
+    return L
+
+
+def _margins_bind():
+    L = lib()
+    if not getattr(L, "_margins_bound", False):
+        L.o_set_margins.argtypes = [ctypes.c_void_p, _dp]
+        L._margins_bound = True
     return L
 
 

@@ -244,3 +244,28 @@ def test_ctypes_result_types_match_the_header(nm):
         assert getattr(lib, m.group(2)).restype == want[ret], m.group(2)
         seen += 1
     assert seen >= 5
+
+
+@pytest.mark.parametrize("case", ["beta_overflow", "tau_nan", "max_loss_inf", "tau_above_one", "tau_below_zero"])
+def test_noalloc_argument_checks(nm, case):
+    """nmlmc_sample_level_noalloc rejects, before any device work, what nmlmc_set_model and
+    nmlmc_sample reject: a level whose inner count N0 beta^ell overflows (beta = 65536, ell = 4:
+    2^64 wraps to 0 as an integer power), non-finite tau or max_loss, and tau outside [0, 1] for
+    the reference model; the status is also what nmlmc_last_error() reports afterwards."""
+    lib = nm.lib()
+    kind, tau, max_loss, beta, ell = nm.MODEL_SHIFT, 0.0, 1.0, 2, 3
+    if case == "beta_overflow":
+        beta, ell = 65536, 4
+    elif case == "tau_nan":
+        tau = float("nan")
+    elif case == "max_loss_inf":
+        max_loss = float("inf")
+    elif case == "tau_above_one":
+        kind, tau = nm.MODEL_REFERENCE, 1.5
+    else:
+        kind, tau = nm.MODEL_REFERENCE, -0.25
+    # d_out is never dereferenced: every case is rejected before the device is touched
+    rc = lib.nmlmc_sample_level_noalloc(kind, tau, max_loss, 32, beta, 1.5, 0, nm.PREC_FP32, 1, ell, 0, 1000,
+                                        ctypes.c_void_p(256), None)
+    assert rc == nm.ERR_ARG
+    assert lib.nmlmc_last_error() == nm.ERR_ARG

@@ -1,6 +1,7 @@
 """Host logic of bench.py, without a GPU: the clock / throttle-reason parsing that decides whether
-a run's clocks are valid, the per-level extrapolation of the FP64 drop-in's time, and the report
-of the autotuner's per-level choices, and the reference arm's line."""
+a run's clocks are valid, the per-level extrapolation of the FP64 drop-in's time, the report of the
+autotuner's per-level choices, the reference arm's lines (model problem and large portfolio) and
+the assembly of both workloads' lines from fake samplers."""
 import os
 
 import bench
@@ -60,8 +61,8 @@ def test_reference_arm_line(tmp_path):
     import json
     import subprocess
     import sys
-    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
-           "--warmup", "3", "--ref-budget", "1"]
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--case", "c1",
+           "--steps", "1", "--warmup", "3", "--ref-budget", "1"]
     env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
     out = subprocess.run(cmd, capture_output=True, text=True, timeout=600, env=env)
     assert out.returncode == 0, out.stderr[-2000:]
@@ -138,7 +139,8 @@ def test_default_line_with_a_fake_sampler(monkeypatch, capsys):
     fake.STREAMS_OUTER, fake.STREAMS_CORE, fake.MODEL_SHIFT = 1, 0, 1
     fake.kernel_launches = lambda: 0
     monkeypatch.setitem(sys.modules, "nmlmc", fake)
-    monkeypatch.setattr(sys, "argv", ["bench.py", "--steps", "2", "--warmup", "3", "--no-compare", "--no-cpu"])
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--case", "c1", "--steps", "2", "--warmup", "3", "--no-compare",
+                                      "--no-cpu"])
     for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK"):
         monkeypatch.delenv(k, raising=False)
     bench.main()
@@ -149,7 +151,7 @@ def test_default_line_with_a_fake_sampler(monkeypatch, capsys):
         assert key in line, key
     assert line["value"] == 0.12 and line["steps"] == 2 and line["warmup"] == 3
     assert line["e2e"]["d2h_bytes_per_step"] == 12 * 144 and line["e2e"]["h2d_bytes_per_step"] == 0
-    assert line["config"]["workload"] and line["config"]["phase_config"]["0"] == [1, 32, True]
+    assert line["config"]["workload"] and line["phase_config"]["0"] == [1, 32, True]
     assert 0 < line["roofline"]["frac"] and line["roofline"]["unit"] == "Gop/s"
 
 
@@ -161,3 +163,85 @@ def test_cpu_baseline_falls_back_to_the_port(monkeypatch):
     schedule = dict(levels=[0, 1], M=[4000, 1000])
     v, kind, cores, desc = bench.cpu_reference_time(schedule, budget_s=0.2)
     assert kind == "port" and cores == 1 and v > 0 and "C port" in desc
+
+
+class _FakePortfolioSampler(_FakeSampler):
+    """Stands in for nmlmc.Sampler on the large-portfolio line: a table set-up, a loss sweep and
+    fixed MLMC results (levels 0-3, starting level 2)."""
+
+    def set_portfolio(self, *a, **kw):
+        pass
+
+    def full_loss(self, ell, first, n):
+        import numpy as np
+        return np.linspace(0.0, 1.0, n)
+
+    def set_phase_config(self, ell, variant=None, chunk=None):
+        pass
+
+    def sample(self, ell, M, trace=False):
+        import numpy as np
+        return dict(stats=np.array([64.0 * M, 0, 0, 0]), seconds=1e-3, fsums=np.zeros(4), diffsums=np.zeros(4))
+
+    def close(self):
+        pass
+
+    def mlmc_run(self, targetTOL, M0, batched=False):
+        d = super().mlmc_run(targetTOL, M0, batched)
+        return dict(d, starting_level=2)
+
+
+def test_large_portfolio_line_with_a_fake_sampler(monkeypatch, capsys):
+    """The default line (large portfolio): the contract's keys, the table upload counted as host->
+    device bytes of every step, the configuration dict shared with the reference arm."""
+    import json
+    import sys
+    import types
+    import numpy as np
+    fake = types.ModuleType("nmlmc")
+    fake.Sampler = _FakePortfolioSampler
+    fake.PREC_FP32, fake.PREC_FP64, fake.PREC_REF32 = 2, 1, 0
+    fake.STREAMS_OUTER, fake.STREAMS_CORE, fake.SUB_RANDOM, fake.TAU_WEEK = 1, 0, 1, 1 / 52
+    fake.PORTFOLIO_C3 = dict(Q=3, P=10)
+    fake.kernel_launches = lambda: 0
+    fake.generate_portfolio = lambda spec, seed: dict(S0=np.full(3, 100.0), mu=np.full(3, 0.05),
+                                                      sigma=np.full(3, 0.2), strike=np.full(10, 100.0),
+                                                      maturity=np.ones(10), w=np.arange(10.0) - 4.5,
+                                                      stock_ind=np.zeros(10, np.uint32),
+                                                      type=np.ones(10, np.int32), prob=np.ones(10))
+    fake.loss_quantile = lambda s, q, n: 0.99
+    monkeypatch.setitem(sys.modules, "nmlmc", fake)
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--steps", "2", "--warmup", "3", "--no-compare", "--no-cpu"])
+    for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK"):
+        monkeypatch.delenv(k, raising=False)
+    bench.main()
+    line = json.loads([l for l in capsys.readouterr().out.splitlines() if l.startswith("{")][-1])
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config", "e2e", "roofline", "clocks",
+                "gpu_launches"):
+        assert key in line, key
+    assert line["metric"] == bench.METRIC and line["value"] == 0.12 and line["steps"] == 2
+    assert line["config"] == bench.C3_CONFIG
+    assert line["e2e"]["h2d_bytes_per_step"] == bench.c3_upload_bytes(10, 3)
+    assert line["e2e"]["d2h_bytes_per_step"] == 12 * 144
+    assert line["starting_level"] == 2 and line["roofline"]["frac"] > 0
+
+
+def test_large_portfolio_reference_arm_line():
+    """`bench.py --impl reference` (default: the large portfolio) times the reference's CPU
+    sampler on the schedule recorded from the GPU run (with its K) and calibrates the
+    extrapolation with one complete CPU run; its config is the GPU line's."""
+    import json
+    import subprocess
+    import sys
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+           "--warmup", "3", "--ref-budget", "2"]
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=900, env=env)
+    assert out.returncode == 0, out.stderr[-2000:]
+    d = json.loads([l for l in out.stdout.splitlines() if l.startswith("{")][-1])
+    assert d["impl"] == "reference" and d["config"] == bench.C3_CONFIG and d["value"] > 0
+    c = d["cpu_baseline"]
+    assert c["kind"] in ("reference", "port") and c["value"] == d["value"]
+    cal = c["calibration"]
+    assert cal["measured_s"] > 0 and cal["extrapolated_s"] > 0 and cal["eps"] <= 1e-2

@@ -3,13 +3,19 @@ fixtures of the unmodified reference.
 
 Tolerances (stated here, used below):
   * Threefry2x64-20 blocks: bit-exact.
-  * CORE layout (the reference's streams), REF32 and FP64: per-outer-sample inner counts equal;
-    phi equal except where |inner mean| < 1e-5 (REF32) / 1e-12 (FP64) — the GPU's libm and sum
-    order differ from glibc's by a few ulp; level sums / inner_stats equal when no such flip.
-  * OUTER layout FP64 / REF32 vs the oracle on the same streams: same rule.
-  * OUTER layout FP32 (SFU Box-Muller, Kahan FP32 sums) vs FP64 on the same streams: a phi may
+  * CORE layout (the reference's streams), REF32 and FP64: per-outer-sample inner counts equal
+    except where the oracle's adaptive decision (new_count <= cur, get_samples_count) was within
+    MARGIN_REF32 = 1e-5 / MARGIN_FP64 = 1e-10 of its threshold in |ln(new_count / cur)|; phi equal
+    except where |inner mean| < 1e-5 (REF32) / 1e-12 (FP64) — the GPU's libm and sum order differ
+    from glibc's by a few ulp.
+  * OUTER layout FP64 / REF32 vs the oracle on the same streams: same rules.
+  * OUTER layout FP32 (SFU Box-Muller, Kahan sums) vs FP64 on the same streams: a phi may
     flip only where |inner mean| < FLIP_FP32 = 2e-5 (model) and an adaptive count may differ only
-    where the FP64 decision is within 1e-4 of its threshold; at most 0.5% of outer samples.
+    where the FP64 decision is within MARGIN_FP32 = 1e-4 of its threshold; at most 0.5% of outer
+    samples.
+  * Level sums: the GPU's and the oracle's moment sums differ by at most what their differing
+    outer samples explain (sum over those samples of |phi_gpu^k - phi_oracle^k|, plus 1e-12 per
+    outer sample for the order of the double sums); equal traces give equal sums.
 """
 import math
 
@@ -23,6 +29,9 @@ pytestmark = pytest.mark.gpu
 FLIP_REF32 = 1e-5
 FLIP_FP64 = 1e-12
 FLIP_FP32 = 2e-5
+MARGIN_REF32 = 1e-5
+MARGIN_FP64 = 1e-10
+MARGIN_FP32 = 1e-4
 
 
 def nm_prec(o_prec):
@@ -30,9 +39,13 @@ def nm_prec(o_prec):
     return nmlmc.PREC_REF32 if o_prec == O.PREC_REF32 else nmlmc.PREC_FP64
 
 
-def compare_traces(gpu, ora, bound, per_core=False, max_frac=0.0):
-    """Counts equal and phi equal except explained flips.  In the CORE layout a count difference
-    shifts that core's later draws, so comparison of a core stops at its first difference."""
+def compare_traces(gpu, ora, bound, per_core=False, max_frac=0.0, margins=None, margin_bound=0.0):
+    """Counts equal and phi equal except explained differences: a count may differ only where the
+    oracle's adaptive decision was within margin_bound of its threshold (`margins`: the oracle's
+    per-outer-sample decision margins; without them a count difference is an error), a phi only
+    where its inner mean was within `bound` of the threshold.  In the CORE layout a count
+    difference shifts that core's later draws, so comparison of a core stops at its first
+    difference."""
     assert len(gpu) == len(ora)
     bad = 0
     stopped = set()
@@ -42,6 +55,8 @@ def compare_traces(gpu, ora, bound, per_core=False, max_frac=0.0):
         if per_core and core in stopped:
             continue
         if g["count_f"] != o["count_f"] or g["count_c"] != o["count_c"]:
+            assert margins is not None and margins[m] < margin_bound, \
+                (m, g, o, None if margins is None else margins[m])
             bad += 1
             if per_core:
                 stopped.add(core)
@@ -53,6 +68,31 @@ def compare_traces(gpu, ora, bound, per_core=False, max_frac=0.0):
             bad += 1
     assert bad <= max_frac * len(gpu) + (2 if max_frac == 0 else 0), bad
     return bad
+
+
+def assert_sums_explained(gres, ores, f32=False):
+    """The GPU's level sums against the oracle's: differences bounded by the outer samples whose
+    phi differ (sum of |phi_gpu^k - phi_oracle^k| over them, the powers taken in the sampler's
+    real type), plus 1e-12 per outer sample for the order of the double sums."""
+    gt, ot = gres["trace"], ores["trace"]
+    rt = np.float32 if f32 else np.float64
+    M = len(gt)
+
+    def powers(x):
+        x = x.astype(rt)
+        p, out = np.ones_like(x), []
+        for _ in range(4):
+            p = (p * x).astype(rt)
+            out.append(p.astype(np.float64))
+        return out
+
+    for key, gv, ov in (("fsums", gt["phi_f"], ot["phi_f"]),
+                        ("diffsums", gt["phi_f"] - gt["phi_c"], ot["phi_f"] - ot["phi_c"])):
+        pg, po = powers(gv), powers(ov)
+        for k in range(4):
+            B = float(np.sum(np.abs(pg[k] - po[k])))
+            d = abs(float(gres[key][k]) - float(ores[key][k]))
+            assert d <= B + 1e-12 * M, (key, k, d, B)
 
 
 def make_pair(case, o_prec, streams_o, streams_n, cores=None, seed=None):
@@ -126,10 +166,13 @@ def test_core_layout_matches_reference(nm, golden, prec_name, o_prec):
     for case in meta["engine"]:
         res = case["results"][prec_name]
         s_o, s_g = make_pair(case, o_prec, O.STREAMS_CORE, nm.STREAMS_CORE)
+        margin = MARGIN_REF32 if o_prec == O.PREC_REF32 else MARGIN_FP64
         for call in res["calls"]:
-            go = s_o.sample(call["ell"], call["M"], trace=True)
+            go = s_o.sample(call["ell"], call["M"], trace=True, margins=True)
             gg = s_g.sample(call["ell"], call["M"], trace=True)
-            bad = compare_traces(gg["trace"], go["trace"], bound, per_core=True)
+            bad = compare_traces(gg["trace"], go["trace"], bound, per_core=True, margins=go["margins"],
+                                 margin_bound=margin)
+            assert_sums_explained(gg, go, f32=o_prec == O.PREC_REF32)
             if bad == 0:
                 np.testing.assert_array_equal(gg["fsums"], call["fsums"], err_msg=case["name"])
                 np.testing.assert_array_equal(gg["diffsums"], call["diffsums"], err_msg=case["name"])
@@ -237,10 +280,13 @@ OUTER_CASES = [
 def test_outer_layout_matches_oracle(nm, case, o_prec):
     bound = FLIP_REF32 if o_prec == O.PREC_REF32 else FLIP_FP64
     s_o, s_g = make_pair(case, o_prec, O.STREAMS_OUTER, nm.STREAMS_OUTER)
+    margin = MARGIN_REF32 if o_prec == O.PREC_REF32 else MARGIN_FP64
     for ell, M in case["calls"]:
-        go = s_o.sample(ell, M, trace=True)
+        go = s_o.sample(ell, M, trace=True, margins=True)
         gg = s_g.sample(ell, M, trace=True)
-        bad = compare_traces(gg["trace"], go["trace"], bound, max_frac=0.001)
+        bad = compare_traces(gg["trace"], go["trace"], bound, max_frac=0.001, margins=go["margins"],
+                             margin_bound=margin)
+        assert_sums_explained(gg, go, f32=o_prec == O.PREC_REF32)
         if bad == 0:
             np.testing.assert_array_equal(gg["fsums"], go["fsums"])
             np.testing.assert_array_equal(gg["diffsums"], go["diffsums"])
@@ -262,9 +308,11 @@ def test_fp32_against_fp64_same_streams(nm, case):
                           use_delta_cv=case["cv"])
     scale = 1.0 if case["kind"] == "model" else 1e3
     for ell, M in case["calls"]:
-        go = s_o.sample(ell, M, trace=True)
+        go = s_o.sample(ell, M, trace=True, margins=True)
         gg = s32.sample(ell, M, trace=True)
-        compare_traces(gg["trace"], go["trace"], FLIP_FP32 * scale, max_frac=0.005)
+        compare_traces(gg["trace"], go["trace"], FLIP_FP32 * scale, max_frac=0.005, margins=go["margins"],
+                       margin_bound=MARGIN_FP32)
+        assert_sums_explained(gg, go, f32=True)
 
 
 def test_edge_cases(nm):

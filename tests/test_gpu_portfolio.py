@@ -6,7 +6,9 @@ Tolerances (stated here, used below):
   * full-portfolio loss, FP32 vs FP64 on the same outer draws: |dL| <= 2e-6 * sum_i |w_i| (S0 + K_i)
     (per-option bound 1e-6 relative on each term of the regrouped BS value, nmlmc_bs.cuh);
   * FP32 vs FP64 level traces on the same streams: a phi may differ only where |inner mean| <
-    2e-6 * P * mean_i |w_i| (S0 + K_i); at most 0.5 % of outer samples;
+    2e-6 * P * mean_i |w_i| (S0 + K_i), an adaptive count only where the FP64 decision was within
+    1e-4 of its threshold (|ln(new_count / cur)|, the oracle's margins); at most 0.5 % of outer
+    samples; level sums differ only by what the differing outer samples explain;
   * the MLMC estimate of P(L > K) within 3 eps + 4 sigma of an independent full-evaluation
     Monte Carlo estimate over 2e5 outer samples.
 """
@@ -14,7 +16,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from test_gpu_parity import compare_traces
+from test_gpu_parity import MARGIN_FP32, MARGIN_FP64, assert_sums_explained, compare_traces
 
 pytestmark = pytest.mark.gpu
 
@@ -79,14 +81,24 @@ def test_fp32_loss_sweep_against_fp64(nm):
 
 @pytest.mark.parametrize("cv", [False, True])
 def test_fp32_level_traces_against_fp64(nm, cv):
+    """FP32 against FP64 on the same streams; a count may differ only where the FP64 decision
+    (the oracle's, on the same streams) was within MARGIN_FP32 of its threshold, and the level
+    sums differ only by what the differing outer samples explain."""
     pf = nm.generate_portfolio(small_spec(nm, Q=8, P=500), 4)
     s64 = sampler(nm, nm.PREC_FP64, pf, adaptive_r=1.5, K=30.0, cv=cv)
     s32 = sampler(nm, nm.PREC_FP32, pf, adaptive_r=1.5, K=30.0, cv=cv)
+    o = O.Sampler(O.PREC_FP64, O.STREAMS_OUTER, 1, 64, 2, 1.5, True, False, 0)
+    o.set_portfolio(pf, r=0.05, rho=0.0, max_loss=30.0, tau=nm.TAU_WEEK, subsample=O.SUB_UNIFORM,
+                    use_delta_cv=cv, discount=False)
     scale = 500 * np.mean(np.abs(pf["w"]) * (100.0 + pf["strike"]))
     for ell, M in ((0, 4000), (2, 2000), (5, 500)):
         g64 = s64.sample(ell, M, trace=True)
         g32 = s32.sample(ell, M, trace=True)
-        compare_traces(g32["trace"], g64["trace"], 2e-6 * scale, max_frac=0.005)
+        go = o.sample(ell, M, trace=True, margins=True)
+        compare_traces(g64["trace"], go["trace"], 1e-9 * scale, margins=go["margins"], margin_bound=MARGIN_FP64)
+        compare_traces(g32["trace"], g64["trace"], 2e-6 * scale, max_frac=0.005, margins=go["margins"],
+                       margin_bound=MARGIN_FP32)
+        assert_sums_explained(g32, g64, f32=True)
 
 
 def test_c2_end_to_end(nm):
@@ -106,3 +118,22 @@ def test_c2_end_to_end(nm):
     out = s.mlmc_run(targetTOL=eps, M0=1024, batched=True)
     assert abs(out["Eg"] - p_direct) < 3 * eps + 4 * sd, (out["Eg"], p_direct, sd)
     assert 0.007 < p_direct < 0.013
+
+
+def test_c3_end_to_end_at_its_eps(nm):
+    """The large portfolio (d = 200, P = 1e6, importance sub-sampling prob ~ |w| with the delta
+    control variate, adaptive r = 1.5) at the configuration's eps = 1e-4: the batched FP32 MLMC
+    estimate of P(L > K) within 3 eps + 4 sigma of a direct estimate from 2e6 full evaluations of
+    the loss (sigma ~ 7e-5), and P(L > K) near 0.01 by construction of K."""
+    import bench
+    pfw = bench.c3_portfolio(nm)
+    q = bench.c3_sampler(nm, 0, pfw, 0.0, nm.PREC_FP32, nm.STREAMS_OUTER, seed=1)
+    K = nm.loss_quantile(q, 0.99, 100_000)
+    Ld = np.concatenate([q.full_loss(61, k * 500_000, 500_000) for k in range(4)])
+    p_direct = float(np.mean(Ld > K))
+    sd = float(np.sqrt(p_direct * (1 - p_direct) / len(Ld)))
+    s = bench.c3_sampler(nm, 0, pfw, K, nm.PREC_FP32, nm.STREAMS_OUTER, seed=21)
+    eps = 1e-4
+    out = s.mlmc_run(targetTOL=eps, M0=1024, batched=True)
+    assert abs(out["Eg"] - p_direct) < 3 * eps + 4 * sd, (out["Eg"], p_direct, sd)
+    assert 0.008 < p_direct < 0.012
