@@ -561,14 +561,15 @@ def c3_portfolio(nm):
 
 def c3_level_case():
     """Profiling case of the large-portfolio phase kernel: two level-10 calls of 8192 outer
-    samples (9 adaptive pilot phases and the final phase each) with K = 4726.3 (the 99 % loss
-    quantile of the bench's c3 case)."""
+    samples (9 adaptive pilot phases and the final phase each), then two level-11 calls of 2^18
+    outer samples (the level that carries most of the eps = 1e-4 run), with K = 4726.3 (the 99 %
+    loss quantile of the large-portfolio configuration)."""
     sys.path.insert(0, PKG)
     import nmlmc as nm
     s = nm.Sampler(0, N0=64, beta=2, adaptive_r=1.5, precision=nm.PREC_FP32, streams=nm.STREAMS_OUTER, seed=5)
     s.set_portfolio(c3_portfolio(nm), r=0.05, rho=0.0, max_loss=4726.308348894119, tau=nm.TAU_WEEK,
                     subsample=nm.SUB_RANDOM, use_delta_cv=True, discount=False)
-    for ell, M in ((10, 8192), (10, 8192)):
+    for ell, M in ((10, 8192), (10, 8192), (11, 1 << 18), (11, 1 << 18)):
         r = s.sample(ell, M)
         print(f"level {ell} M {M}: {r['seconds'] * 1e3:.3f} ms, {r['stats'][0] / r['seconds']:.3e} inner/s")
 
@@ -634,6 +635,72 @@ def c3_table_case():
             for _ in range(3):
                 r = s.sample(6, 1 << 14)
             print(f"P {P} {name}: {r['seconds'] * 1e3:.3f} ms, {r['stats'][0] / r['seconds']:.3e} inner/s")
+
+
+# Path-simulated large portfolio: d = 50 stocks, P = 1e5 options (the large portfolio's generator,
+# seed 1), every option valued by coupled fine / coarse Milstein paths from tau to maturity with
+# the reference's Unbiased method (sample_inner_unbiased / sample_inner_approx,
+# portfolio_sampler.cpp:521-604): h0 = 1, time steps doubling per path level (dt_beta = 2), level
+# L drawn with P(L) ~ 2^(-1.5 L), so 2^L Milstein steps (L = 0..8 covers 99.9999 % of the draws).
+C4_MLMC = dict(workload="path-simulated portfolio: d=50 GBM stocks, P=1e5 options, Milstein paths (Unbiased "
+                        "method, 2^L steps), P(L>K) with K the 99% Black-Scholes loss quantile",
+               stocks=50, options=100_000, generator_seed=1, sub_sampling="importance, prob ~ |w_i|",
+               delta_cv=True, N0=64, beta=2, adaptive_r=ADAPTIVE_R, dt_h0inv=1, dt_beta=2, dt_prob_expo=-1.5,
+               milstein=True, antithetic_risk=True, eps=1e-3)
+
+
+def c4_mlmc_case(args):
+    """Time-to-eps of the path-simulated portfolio: the batched FP32 sampler (OUTER streams, each
+    path-simulated inner sample on its own counter namespaces) against the FP64 drop-in on the
+    reference's stream layout (2048 virtual cores), both measured to the same eps."""
+    import numpy as np
+    sys.path.insert(0, PKG)
+    import nmlmc as nm
+    eps = args.eps if args.eps else C4_MLMC["eps"]
+    pf = nm.generate_portfolio(dict(nm.PORTFOLIO_C3, Q=C4_MLMC["stocks"], P=C4_MLMC["options"]), 1)
+    order = np.argsort(-np.abs(pf["w"]), kind="stable")
+    for k in ("strike", "maturity", "w", "stock_ind", "type"):
+        pf[k] = pf[k][order]
+    pf = dict(pf, prob=np.abs(pf["w"]))
+    methods = dict(method=np.full(len(pf["w"]), nm.METHOD_UNBIASED, np.int32), dt_h0inv=1, dt_beta=2,
+                   dt_prob_expo=-1.5, use_milstein=True, use_antithetic_risk=True)
+
+    def mk(prec, streams, K, seed, methods_on=True):
+        s = nm.Sampler(0, cores=2048, N0=64, beta=2, adaptive_r=ADAPTIVE_R, precision=prec, streams=streams,
+                       seed=seed)
+        s.set_portfolio(pf, r=0.05, rho=0.0, max_loss=K, tau=nm.TAU_WEEK, subsample=nm.SUB_RANDOM,
+                        use_delta_cv=True, discount=True, methods=methods if methods_on else None)
+        return s
+
+    q = mk(nm.PREC_FP32, nm.STREAMS_OUTER, 0.0, 1, methods_on=False)
+    K = nm.loss_quantile(q, 0.99, 100_000)
+    q.close()
+    runs = {}
+    clk = None
+    for name, prec, streams, batched in (("fp32_batched", nm.PREC_FP32, nm.STREAMS_OUTER, True),
+                                         ("fp64_dropin", nm.PREC_FP64, nm.STREAMS_CORE, False)):
+        s = mk(prec, streams, K, 3)
+        s.mlmc_run(targetTOL=3 * eps, M0=1024, batched=batched)      # warm-up at a looser eps
+        s.configure(seed=5)
+        cs = ClockSampler(0)
+        cs.start()
+        t = time.perf_counter()
+        out = s.mlmc_run(targetTOL=eps, M0=1024, batched=batched)
+        wall = time.perf_counter() - t
+        c = cs.stop()
+        clk = clk or c
+        runs[name] = dict(value=float(out["level_time"].sum()), e2e=wall, Eg=float(out["Eg"]),
+                          levels=int(out["nlevels"]), starting_level=int(out["starting_level"]),
+                          level_M=[int(x) for x in out["level_M"]], work=float(out["total_work"]))
+        s.close()
+    a, b = runs["fp32_batched"], runs["fp64_dropin"]
+    line = {"metric": f"time-to-eps (s) for MLMC P(L>K), path-simulated portfolio, eps={eps:g} absolute",
+            "value": a["value"], "unit": "s", "n_gpus": 1, "higher_is_better": False, "dtype": "f32 paths, f64 states",
+            "data": "synthetic (seeded generator)", "config": dict(C4_MLMC, eps=eps, K=K),
+            "e2e": {"value": a["e2e"], "unit": "s"}, "runs": runs,
+            "speedup_vs_fp64_dropin": {"value": b["value"] / a["value"], "e2e": b["e2e"] / a["e2e"]},
+            "clocks": clk, "vs_baseline": None}
+    print(json.dumps(line))
 
 
 def c3_sampler(nm, device, pfw, K, prec, streams, seed, cores=2048):
@@ -871,10 +938,11 @@ def main():
     ap.add_argument("--schedule-out", default=None,
                     help="write the run's outer samples per level (bench_schedule.json format) here")
     ap.add_argument("--case", default=None, choices=["c1", "small", "c3-level", "c3-table", "c3-sweep", "c4",
-                                                      "c4-small", "ref-model"],
+                                                      "c4-small", "c4-mlmc", "ref-model"],
                     help="default: the large portfolio to eps; c1: the adaptive model problem to eps; "
                          "small, c3-level, c3-table, c3-sweep, c4-small: profiling cases; c4: the "
-                         "path-simulated loss with adjoint; ref-model: the reference's model main")
+                         "path-simulated loss with adjoint; c4-mlmc: MLMC of the path-simulated "
+                         "portfolio to eps; ref-model: the reference's model main")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -890,6 +958,8 @@ def main():
         return c3_table_case()
     if args.case == "c3-sweep":
         return c3_sweep_case()
+    if args.case == "c4-mlmc":
+        return c4_mlmc_case(args)
     if args.case in ("c4", "c4-small"):
         return c4_case(args, small=args.case == "c4-small")
     if args.case == "ref-model":

@@ -9,7 +9,7 @@
 // code as the built-in kinds; csrc/nmlmc_outer_impl.cuh) for the caller's own sm_100a build:
 //
 //   nvcc -gencode arch=compute_100a,code=sm_100a -std=c++17 --expt-relaxed-constexpr
-//        -I include -I nested-risk-mlmc_b200/csrc  my_sampler.cu ...
+//        -I include -I nested-risk-mlmc_b200/csrc  <the caller's .cu file>
 //
 // A SAMPLER here:
 //   * derives from nmlmc::inner_sampler_base<real_t> (real_t = float: the FP32 path with SFU

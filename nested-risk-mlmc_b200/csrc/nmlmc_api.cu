@@ -393,7 +393,7 @@ int build_dev_portfolio(nmlmc_ctx* c, DevPortfolio<RT>& d) {
     t.phat = nullptr;
     std::vector<double> phat;
     std::vector<uint2> tab;
-    if (h.subsample == SUB_RANDOM && !h.mixed()) {
+    if (h.subsample == SUB_RANDOM) {             // the OUTER layout's draw (all methods)
         std::vector<double> pr(P);
         for (uint32_t j = 0; j < P; j++) pr[j] = (double)prob[j];
         build_alias(P, pr, tab, phat);
@@ -835,6 +835,7 @@ int tune_level(nmlmc_ctx* c, uint32_t ell, uint64_t M, bool chunks) {
 template <class RT>
 int ensure_tuned(nmlmc_ctx* c, uint32_t ell, uint64_t M) {
     if (!c->autotune || c->cfg.precision != NMLMC_PREC_FP32 || c->phase[ell].state != 0) return NMLMC_OK;
+    if (c->kind == KIND_PORTFOLIO && c->pf.mixed()) return NMLMC_OK;   // path methods: one variant
     const uint64_t Mp = M < c->ob.cap ? M : c->ob.cap;
     const CountParams cf = count_params(c->cfg, ell);
     if (Mp < 4096 || (double)Mp * (double)cf.base_count * (double)(ell + 1) < 8.0e6) return NMLMC_OK;
@@ -862,7 +863,16 @@ int sample_outer(nmlmc_ctx* c, uint32_t ell, uint64_t Mtotal, nmlmc_level_result
     NM_CUDA(cudaEventRecord(c->ev1, c->stream), "event");
     NM_CUDA(cudaMemcpyAsync(c->h_pin, c->ob.level_acc, 16 * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "d2h");
     if (tr && M) NM_CUDA(cudaMemcpyAsync(c->trace_host, tr, M * sizeof(TraceRec), cudaMemcpyDeviceToHost, c->stream), "d2h");
+    uint32_t path_limit = 0;
+    const bool paths = c->kind == KIND_PORTFOLIO && c->pf.mixed();
+    if (paths)
+        NM_CUDA(cudaMemcpyAsync(&path_limit, c->ob.counters + kCounterPathLimit, sizeof path_limit,
+                                cudaMemcpyDeviceToHost, c->stream), "d2h");
     NM_CUDA(cudaStreamSynchronize(c->stream), "sync");
+    if (path_limit) {                            // a sample exceeded kMaxPathSteps
+        NM_CUDA(cudaMemset(c->ob.counters + kCounterPathLimit, 0, sizeof path_limit), "memset");
+        return set_err(NMLMC_ERR_LIMIT);
+    }
     if (c->prof) prof_collect(c);
     float ms = 0;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
@@ -1346,12 +1356,13 @@ int nmlmc_sample(nmlmc_ctx* c, uint32_t ell, uint64_t M, nmlmc_level_result* out
     const nmlmc_config& k = c->cfg;
     // counts must fit the 32-bit per-item counters of the batched path
     if ((double)k.N0 * pow((double)k.beta, (double)ell) > 4.0e9) return set_err(NMLMC_ERR_ARG);
+    // the batched (OUTER) layout draws one option per inner sample: no Subsampling::None there
+    if (c->kind == KIND_PORTFOLIO && k.streams == NMLMC_STREAMS_OUTER && c->pf.subsample == SUB_NONE)
+        return set_err(NMLMC_ERR_ARG);
     if (M == 0) return NMLMC_OK;
     cudaSetDevice(c->device);
     int rc = ensure_portfolio(c);
     if (rc) return rc;
-    // path-simulated compute methods are defined on the reference's CORE streams only
-    if (c->kind == KIND_PORTFOLIO && c->pf.mixed() && k.streams != NMLMC_STREAMS_CORE) return set_err(NMLMC_ERR_ARG);
     if ((rc = ensure_trace(c, M))) return rc;
     const bool f64 = k.precision == NMLMC_PREC_FP64;
     if (k.streams == NMLMC_STREAMS_CORE) {
@@ -1367,6 +1378,8 @@ int nmlmc_sample_levels(nmlmc_ctx* c, uint32_t n, const uint32_t* ells, const ui
     if (!c || (n && (!ells || !Ms || !outs))) return set_err(NMLMC_ERR_ARG);
     if (!c->configured || c->kind < 0) return set_err(NMLMC_ERR_STATE);
     const nmlmc_config& k = c->cfg;
+    if (c->kind == KIND_PORTFOLIO && k.streams == NMLMC_STREAMS_OUTER && c->pf.subsample == SUB_NONE)
+        return set_err(NMLMC_ERR_ARG);          // as nmlmc_sample: no Subsampling::None on the batched layout
     bool one_submission = n > 0 && n <= kMaxSubmit && k.streams == NMLMC_STREAMS_OUTER && !c->prof &&
                           !c->trace_host && !(c->kind == KIND_PORTFOLIO && c->pf.mixed());
     for (uint32_t i = 0; i < n && one_submission; i++) {

@@ -27,9 +27,14 @@ struct CountParams {
     double tmp;          // real_t value widened
 };
 
-// Sampler kinds: the reference's model, the X = Y + Z model, the portfolio, and a caller-written
-// SAMPLER class (include/nmlmc_sampler.cuh).
-enum Kind : int { KIND_REF_MODEL = 0, KIND_SHIFT_MODEL = 1, KIND_PORTFOLIO = 2, KIND_USER = 3 };
+// Sampler kinds: the reference's model, the X = Y + Z model, the portfolio, a caller-written
+// SAMPLER class (include/nmlmc_sampler.cuh), and — on the batched layout only — the portfolio
+// with path-simulated (Exact / Unbiased) options, a kernel instantiation of its own so that the
+// Black-Scholes-only kernels carry none of the path code.
+enum Kind : int { KIND_REF_MODEL = 0, KIND_SHIFT_MODEL = 1, KIND_PORTFOLIO = 2, KIND_USER = 3, KIND_PF_PATHS = 4 };
+__host__ __device__ constexpr bool is_portfolio_kind(int kind) {
+    return kind == KIND_PORTFOLIO || kind == KIND_PF_PATHS;
+}
 enum Sub : int { SUB_NONE = 0, SUB_RANDOM = 1, SUB_UNIFORM = -1 };
 
 enum Method : int { METHOD_BS = 0, METHOD_EXACT = 1, METHOD_UNBIASED = 2 };

@@ -17,6 +17,7 @@
 
 #include "nmlmc_common.cuh"
 #include "nmlmc_internal.h"
+#include "nmlmc_paths.cuh"
 
 namespace nmlmc {
 
@@ -159,145 +160,6 @@ struct SeqNormals {
     }
 };
 
-template <class RT>
-__device__ __forceinline__ RT opt_diff_stock(const OptionTable<RT>& ot, uint32_t j, RT S0_T, RT St_T) {
-    // option_diff_from_stock (portfolio_sampler.cpp:212-219)
-    const RT mod = (RT)ot.type[j], K = ot.strike[j];
-    const RT a = xmul(mod, xsub(S0_T, K)), b = xmul(mod, xsub(St_T, K));
-    const RT start = a > (RT)0 ? a : (RT)0, finish = b > (RT)0 ? b : (RT)0;
-    return xmul(xmul(ot.w[j], xexp(xmul(-ot.r, ot.maturity[j]))), xsub(start, finish));
-}
-
-template <class RT>
-__device__ __forceinline__ RT opt_derv_stock(const OptionTable<RT>& ot, uint32_t j, RT St_T, RT S0) {
-    // option_derv_from_stock (portfolio_sampler.cpp:221-225)
-    const RT df = (RT)((ot.type[j] == 1 ? 1 : 0) - (St_T < ot.strike[j] ? 1 : 0));
-    return xmul(xmul(xmul(ot.w[j], xdiv(St_T, S0)), xexp(xmul(-ot.r, ot.maturity[j]))), df);
-}
-
-// simulate_stock_dt<with_coarse> (gbm_approx.hpp:18-57) on the three paths S[0..3) of
-// sample_inner_approx, plus (with_coarse) the coupled coarse paths S[3..6) stepping every
-// coarse_step fine steps on the summed increments.  States in double, increments in real_t.
-template <class RT>
-__device__ void stock_dt(SeqNormals<RT>& nz, double* S, uint64_t N, RT mu, RT sigma, RT t, bool milstein,
-                         bool with_coarse, uint32_t coarse_step) {
-    const RT dt = xdiv(t, (RT)N);
-    const RT sqrt_dt = xsqrt(dt);
-    const RT dt_c = xdiv(t, (RT)(N / coarse_step));
-    const double hs2 = __dmul_rn(0.5, (double)xmul(sigma, sigma));
-    const RT mudt = xmul(mu, dt), mudt_c = xmul(mu, dt_c);
-    RT dW_c = (RT)0;
-    for (uint64_t n = 0; n < N; n++) {
-        const RT dW = xmul(sqrt_dt, nz.next());
-        const RT m = milstein ? to_rt<RT>(__dmul_rn(hs2, (double)xsub(xmul(dW, dW), dt))) : (RT)0;
-        const double inc = (double)xadd(xadd(mudt, xmul(sigma, dW)), m);
-#pragma unroll
-        for (int i = 0; i < 3; i++) S[i] = __dadd_rn(S[i], __dmul_rn(S[i], inc));
-        if (with_coarse) {
-            dW_c = xadd(dW_c, dW);
-            if ((n + 1) % coarse_step == 0) {
-                const RT mc = milstein ? to_rt<RT>(__dmul_rn(hs2, (double)xsub(xmul(dW_c, dW_c), dt_c))) : (RT)0;
-                const double incc = (double)xadd(xadd(mudt_c, xmul(sigma, dW_c)), mc);
-#pragma unroll
-                for (int i = 3; i < 6; i++) S[i] = __dadd_rn(S[i], __dmul_rn(S[i], incc));
-                dW_c = (RT)0;
-            }
-        }
-    }
-}
-
-// sample_inner_exact (portfolio_sampler.cpp:470-519): exact GBM from tau to maturity for the
-// antithetic pair started at S0 and for the path started at R_tau.
-template <class RT>
-__device__ RT inner_exact(const OptionTable<RT>& ot, const RT* Rt, uint32_t j, SeqNormals<RT>& nz, double& work) {
-    const bool anti = ot.use_antithetic_risk != 0;
-    work += (double)ot.W_est[j];
-    const uint32_t s = ot.stock_ind[j];
-    const RT S0 = ot.S0[s], sg = ot.sigma[s], r = ot.r, tau = ot.tau;
-    const RT Tr = xsub(ot.maturity[j], tau);
-    const RT dW_0_tau = xmul(ot.stau, nz.next());
-    const RT dW_tau_T = xmul(xsqrt(Tr), nz.next());
-    const RT S0_t_1 = simulate_stock_ref<RT>(S0, r, sg, tau, dW_0_tau);
-    const RT S0_T_1 = simulate_stock_ref<RT>(S0_t_1, r, sg, Tr, dW_tau_T);
-    RT S0_T_2 = (RT)0;
-    if (anti) {
-        const RT S0_t_2 = simulate_stock_ref<RT>(S0, r, sg, tau, -dW_0_tau);
-        S0_T_2 = simulate_stock_ref<RT>(S0_t_2, r, sg, Tr, dW_tau_T);
-    }
-    const RT St_T = simulate_stock_ref<RT>(Rt[s], r, sg, Tr, dW_tau_T);
-    const RT v1 = opt_diff_stock(ot, j, S0_T_1, St_T);
-    const RT v2 = anti ? opt_diff_stock(ot, j, S0_T_2, St_T) : v1;
-    RT d1 = (RT)0, d2 = (RT)0;
-    if (ot.use_delta_cv) {
-        const RT diff = xsub(Rt[s], S0);
-        d1 = xmul(diff, opt_derv_stock(ot, j, S0_T_1, S0));
-        d2 = anti ? xmul(diff, opt_derv_stock(ot, j, S0_T_2, S0)) : d1;
-    }
-    return to_rt<RT>(__dmul_rn(0.5, (double)xadd(xadd(xadd(v1, v2), d1), d2)));
-}
-
-// sample_inner_approx (portfolio_sampler.cpp:539-604): fine level L with N = h0 beta^L steps
-// and, for L > 0, the coupled coarse level; payoff differences of the antithetic pair.
-template <class RT>
-__device__ RT inner_approx(const OptionTable<RT>& ot, const RT* Rt, uint32_t j, SeqNormals<RT>& nz, double& work,
-                           uint32_t L, uint64_t N_l) {
-    const uint32_t s = ot.stock_ind[j];
-    const RT S0 = ot.S0[s], sg = ot.sigma[s], r = ot.r, tau = ot.tau;
-    const RT dW = xmul(ot.stau, nz.next());
-    const RT S0_t_1 = simulate_stock_ref<RT>(S0, r, sg, tau, dW);
-    const RT S0_t_2 = simulate_stock_ref<RT>(S0, r, sg, tau, -dW);
-    const uint64_t N = (uint64_t)ot.dt_h0inv * N_l;
-    work += (double)xmul((RT)N_l, ot.W_est[j]);
-    double S[6] = {(double)S0_t_1, (double)Rt[s], (double)S0_t_2, (double)S0_t_1, (double)Rt[s], (double)S0_t_2};
-    const RT Tr = xsub(ot.maturity[j], tau);
-    if (L) {
-        stock_dt<RT>(nz, S, N, r, sg, Tr, ot.use_milstein != 0, true, ot.dt_beta);
-        work += (double)xmul((RT)(N_l / ot.dt_beta), ot.W_est[j]);
-    } else {
-        stock_dt<RT>(nz, S, N, r, sg, Tr, ot.use_milstein != 0, false, 2);
-    }
-    const bool anti = ot.use_antithetic_risk != 0;
-    const RT m = anti ? (RT)0.5 : (RT)1;
-    const RT diff = xsub(Rt[s], S0);
-    const bool do_d_f = ot.use_delta_cv && (ot.use_coarse_delta_cv || L == 0);
-    const bool do_d_c = ot.use_delta_cv && ot.use_coarse_delta_cv;
-    RT vf = 0, vc = 0, vdf = 0, vdc = 0;
-    for (int i = 0; i < (anti ? 2 : 1); i++) {
-        const int ic = 2 * i;
-        vf = xadd(vf, xmul(m, opt_diff_stock(ot, j, to_rt<RT>(S[ic]), to_rt<RT>(S[1]))));
-        if (do_d_f) vdf = xadd(vdf, xmul(m, opt_derv_stock(ot, j, to_rt<RT>(S[ic]), S0)));
-        if (L == 0) continue;
-        vc = xadd(vc, xmul(m, opt_diff_stock(ot, j, to_rt<RT>(S[ic + 3]), to_rt<RT>(S[4]))));
-        if (do_d_c) vdc = xadd(vdc, xmul(m, opt_derv_stock(ot, j, to_rt<RT>(S[ic + 3]), S0)));
-    }
-    return xadd(xsub(vf, vc), xmul(diff, xsub(vdf, vdc)));
-}
-
-// Level of sample_inner_unbiased (portfolio_sampler.cpp:521-537) from its randu_sync word:
-// L = floor(log u / (log beta * e)), P(L) proportional to beta^(e L).  Returns false (and
-// n_steps = 0) when h0 beta^L exceeds NMLMC_MAX_PATH_STEPS.
-template <class RT>
-__device__ __forceinline__ bool unbiased_level(const OptionTable<RT>& ot, uint64_t word, uint32_t& L, uint64_t& N_l) {
-    const RT e = ot.dt_prob_expo, x = (RT)ot.dt_beta;
-    const RT q = xdiv(xlog(u01_rt<RT>(word)), xmul(xlog(x), e));
-    const RT fl = sizeof(RT) == 4 ? (RT)floorf((float)q) : (RT)floor((double)q);
-    L = (uint32_t)fl;
-    N_l = 1;
-    for (uint32_t i = 0; i < L; i++) {
-        N_l *= ot.dt_beta;
-        if (N_l * ot.dt_h0inv > kMaxPathSteps) return false;
-    }
-    return N_l * ot.dt_h0inv <= kMaxPathSteps;
-}
-
-template <class RT>
-__device__ __forceinline__ RT inner_unbiased(const OptionTable<RT>& ot, const RT* Rt, uint32_t j, SeqNormals<RT>& nz,
-                                             double& work, uint32_t L, uint64_t N_l) {
-    const RT ret = inner_approx<RT>(ot, Rt, j, nz, work, L, N_l);
-    const RT e = ot.dt_prob_expo, x = (RT)ot.dt_beta;
-    const RT Lp = to_rt<RT>(__ddiv_rn((double)xpow(x, xmul(-e, (RT)L)), __dsub_rn(1.0, (double)xpow(x, e))));
-    return xmul(ret, Lp);
-}
 
 // rand_int_pdf over compute_prob (common.hpp:178-195), as sample_inner_random_option_ind
 // picks the compute method (portfolio_sampler.cpp:350-352).
@@ -402,7 +264,7 @@ __device__ void core_phase_paths(CoreCtx<RT, KIND_PORTFOLIO>& c, uint64_t count,
                     my_lword = lw;
                     uint32_t L;
                     uint64_t N_l;
-                    ok = unbiased_level<RT>(ot, lw, L, N_l);
+                    ok = unbiased_level<RT>(ot, u01_rt<RT>(lw), L, N_l);
                     n_norm = ok ? 1 + (uint64_t)ot.dt_h0inv * N_l : 0;
                 } else if (my_m == METHOD_EXACT) {
                     n_norm = 2;
@@ -419,7 +281,7 @@ __device__ void core_phase_paths(CoreCtx<RT, KIND_PORTFOLIO>& c, uint64_t count,
                 for (uint32_t k = 0; k < n_unb && ok; k++) {
                     uint32_t L;
                     uint64_t N_l;
-                    ok = unbiased_level<RT>(ot, core_word(c.key, w0 + k), L, N_l);
+                    ok = unbiased_level<RT>(ot, u01_rt<RT>(core_word(c.key, w0 + k)), L, N_l);
                     n_norm += ok ? 1 + (uint64_t)ot.dt_h0inv * N_l : 0;
                 }
             }
@@ -466,24 +328,24 @@ __device__ void core_phase_paths(CoreCtx<RT, KIND_PORTFOLIO>& c, uint64_t count,
                 if (my_m == METHOD_BS) {
                     v = portfolio_bs_value<RT>(ot, c.Rt, j, wk);
                 } else if (my_m == METHOD_EXACT) {
-                    v = inner_exact<RT>(ot, c.Rt, j, nz, wk);
+                    v = inner_exact<RT, SeqNormals<RT>>(ot, c.Rt[ot.stock_ind[j]], j, nz, wk);
                 } else {
                     uint32_t L;
                     uint64_t N_l;
-                    unbiased_level<RT>(ot, my_lword, L, N_l);
-                    v = inner_unbiased<RT>(ot, c.Rt, j, nz, wk, L, N_l);
+                    unbiased_level<RT>(ot, u01_rt<RT>(my_lword), L, N_l);
+                    v = inner_unbiased<RT, SeqNormals<RT>>(ot, c.Rt[ot.stock_ind[j]], j, nz, wk, L, N_l);
                 }
                 v = xdiv(v, prob);
             } else {
                 double acc = 0;
                 const uint32_t oe = ot.m_off[METHOD_EXACT], ou = ot.m_off[METHOD_UNBIASED];
-                for (uint32_t k = 0; k < n_exact; k++) acc += (double)inner_exact<RT>(ot, c.Rt, oe + k, nz, wk);
+                for (uint32_t k = 0; k < n_exact; k++) acc += (double)inner_exact<RT, SeqNormals<RT>>(ot, c.Rt[ot.stock_ind[oe + k]], oe + k, nz, wk);
                 const uint64_t w0 = c.sync.wpos + (uint64_t)lane * n_unb;
                 for (uint32_t k = 0; k < n_unb; k++) {
                     uint32_t L;
                     uint64_t N_l;
-                    unbiased_level<RT>(ot, core_word(c.key, w0 + k), L, N_l);
-                    acc += (double)inner_unbiased<RT>(ot, c.Rt, ou + k, nz, wk, L, N_l);
+                    unbiased_level<RT>(ot, u01_rt<RT>(core_word(c.key, w0 + k)), L, N_l);
+                    acc += (double)inner_unbiased<RT, SeqNormals<RT>>(ot, c.Rt[ot.stock_ind[ou + k]], ou + k, nz, wk, L, N_l);
                 }
                 v = to_rt<RT>(acc);
             }

@@ -78,6 +78,11 @@ struct OuterBuffers {
     void* prof_user;
 };
 
+// Device counter slot (OuterBuffers::counters) that the batched kernels set when a
+// path-simulated inner sample would exceed kMaxPathSteps (the call then fails with
+// NMLMC_ERR_LIMIT); the host clears it.
+constexpr uint32_t kCounterPathLimit = 240;
+
 // Records a failed status for nmlmc_last_error() (this thread) and returns it.
 int set_last_error(int e);
 

@@ -39,6 +39,7 @@ cudaError_t outer_level_begin(OuterBuffers& B, cudaStream_t stream) {
 NMLMC_SLT(float, KIND_REF_MODEL, PREC_FP32) NMLMC_SLT(float, KIND_SHIFT_MODEL, PREC_FP32) NMLMC_SLT(float, KIND_PORTFOLIO, PREC_FP32)
 NMLMC_SLT(float, KIND_REF_MODEL, PREC_REF32) NMLMC_SLT(float, KIND_SHIFT_MODEL, PREC_REF32) NMLMC_SLT(float, KIND_PORTFOLIO, PREC_REF32)
 NMLMC_SLT(double, KIND_REF_MODEL, PREC_FP64) NMLMC_SLT(double, KIND_SHIFT_MODEL, PREC_FP64) NMLMC_SLT(double, KIND_PORTFOLIO, PREC_FP64)
+NMLMC_SLT(float, KIND_PF_PATHS, PREC_FP32) NMLMC_SLT(float, KIND_PF_PATHS, PREC_REF32) NMLMC_SLT(double, KIND_PF_PATHS, PREC_FP64)
 #undef NMLMC_SLT
 
 template <class RT>
@@ -48,6 +49,7 @@ cudaError_t outer_sample_level(const OuterLevel<RT>& L, int kind, int prec, Oute
         if constexpr (sizeof(RT) == 8) {
             if (kind == KIND_REF_MODEL) return sample_level_t<RT, KIND_REF_MODEL, PREC_FP64>(L, B, trace, stream);
             if (kind == KIND_SHIFT_MODEL) return sample_level_t<RT, KIND_SHIFT_MODEL, PREC_FP64>(L, B, trace, stream);
+            if (L.ot.mixed) return sample_level_t<RT, KIND_PF_PATHS, PREC_FP64>(L, B, trace, stream);
             return sample_level_t<RT, KIND_PORTFOLIO, PREC_FP64>(L, B, trace, stream);
         }
         return cudaErrorInvalidValue;
@@ -56,10 +58,12 @@ cudaError_t outer_sample_level(const OuterLevel<RT>& L, int kind, int prec, Oute
         if (prec == PREC_FP32) {
             if (kind == KIND_REF_MODEL) return sample_level_t<RT, KIND_REF_MODEL, PREC_FP32>(L, B, trace, stream);
             if (kind == KIND_SHIFT_MODEL) return sample_level_t<RT, KIND_SHIFT_MODEL, PREC_FP32>(L, B, trace, stream);
+            if (L.ot.mixed) return sample_level_t<RT, KIND_PF_PATHS, PREC_FP32>(L, B, trace, stream);
             return sample_level_t<RT, KIND_PORTFOLIO, PREC_FP32>(L, B, trace, stream);
         }
         if (kind == KIND_REF_MODEL) return sample_level_t<RT, KIND_REF_MODEL, PREC_REF32>(L, B, trace, stream);
         if (kind == KIND_SHIFT_MODEL) return sample_level_t<RT, KIND_SHIFT_MODEL, PREC_REF32>(L, B, trace, stream);
+        if (L.ot.mixed) return sample_level_t<RT, KIND_PF_PATHS, PREC_REF32>(L, B, trace, stream);
         return sample_level_t<RT, KIND_PORTFOLIO, PREC_REF32>(L, B, trace, stream);
     }
     return cudaErrorInvalidValue;

@@ -32,6 +32,7 @@
 
 #include "nmlmc_common.cuh"
 #include "nmlmc_internal.h"
+#include "nmlmc_paths.cuh"
 
 namespace nmlmc {
 
@@ -45,9 +46,10 @@ enum : int {
     CNT_CLASS = 8,       // [64]: outer samples per final class
     CNT_FILL = 72,       // [64]: scatter fill per class
     CNT_TOTAL = 144,
-    CNT_QUEUE = 192      // [kMaxSegs]: tile tickets of the phase kernel's work queue, per segment
+    CNT_QUEUE = 192,     // [kMaxSegs]: tile tickets of the phase kernel's work queue, per segment
+    CNT_ERR = kCounterPathLimit   // set when a path-simulated inner sample exceeds kMaxPathSteps
 };
-static_assert(CNT_QUEUE + kMaxSegs <= 256, "counter slots");
+static_assert(CNT_QUEUE + kMaxSegs <= CNT_ERR && CNT_ERR < 256, "counter slots");
 
 // ---- accumulators -------------------------------------------------------------------------
 // FP32: compensated pair (hi + lo) — Kahan accumulation inside a thread, TwoSum merging across
@@ -77,12 +79,16 @@ template <> struct Acc<PREC_FP32> {
         return r;
     }
     __device__ __forceinline__ float value() const { return __fadd_rn(hi, lo); }
+    // plain addition: the pilots' sum of squares, which only feeds the variance estimate of the
+    // adaptive rule (sums of 4-64 squares per thread of values centred on the threshold)
+    __device__ __forceinline__ void add_sq(float v) { hi = fmaf(v, v, hi); }
 };
 
 template <> struct Acc<PREC_FP64> {
     double v;
     __device__ __forceinline__ void zero() { v = 0; }
     __device__ __forceinline__ void add(double x) { v = __dadd_rn(v, x); }
+    __device__ __forceinline__ void add_sq(double x) { v = __dadd_rn(v, __dmul_rn(x, x)); }
     __device__ __forceinline__ void merge(const Acc& o) { v = __dadd_rn(v, o.v); }
     __device__ __forceinline__ Acc shfl_xor(int m) const { Acc r; r.v = __shfl_xor_sync(0xffffffffu, v, m); return r; }
     __device__ __forceinline__ double value() const { return v; }
@@ -91,6 +97,7 @@ template <> struct Acc<PREC_REF32> {
     double v;
     __device__ __forceinline__ void zero() { v = 0; }
     __device__ __forceinline__ void add(double x) { v = __dadd_rn(v, x); }
+    __device__ __forceinline__ void add_sq(double x) { v = __dadd_rn(v, __dmul_rn(x, x)); }
     __device__ __forceinline__ void merge(const Acc& o) { v = __dadd_rn(v, o.v); }
     __device__ __forceinline__ Acc shfl_xor(int m) const { Acc r; r.v = __shfl_xor_sync(0xffffffffu, v, m); return r; }
     __device__ __forceinline__ double value() const { return v; }
@@ -153,6 +160,38 @@ __device__ __forceinline__ RT outer_normal_at(const TfKey& key, uint32_t tag, ui
     bm_pair<PREC, RT>((uint32_t)e, (uint32_t)(e >> 32), x, y);
     return (k & 1) ? y : x;
 }
+
+// ---- path-simulated inner values on the OUTER layout ----------------------------------------
+// An Exact or Unbiased option (portfolio_sampler.cpp:470-604) drawn by inner sample i of the phase
+// with tag t takes its draws from its own counter namespaces, so every inner sample stays
+// addressable whatever the number of draws it makes: normals from counter word 1 =
+// t | (i + 1) << 16 (normal k = component k & 1 of the Box-Muller pair of words 2(k >> 1),
+// 2(k >> 1) + 1), uniforms (the Unbiased level) from t | (i + 1) << 16 | 2^15, word k.
+constexpr uint64_t kPathUniform = 1ull << 15;
+__device__ __forceinline__ uint64_t path_ns(uint32_t tag, uint64_t i) { return (uint64_t)tag | ((i + 1) << 16); }
+
+template <class RT, int PREC>
+struct OuterPathNormals {
+    TfKey key;
+    uint64_t ns;
+    uint64_t p;          // next pair
+    bool have;
+    RT y;
+    __device__ __forceinline__ RT next() {
+        if (have) {
+            have = false;
+            return y;
+        }
+        uint64_t v0, v1;
+        threefry2x64(p >> 1, ns, key, v0, v1);
+        const uint64_t e = (p & 1) ? v1 : v0;
+        RT x;
+        bm_pair<PREC, RT>((uint32_t)e, (uint32_t)(e >> 32), x, y);
+        p++;
+        have = true;
+        return x;
+    }
+};
 
 // ---- portfolio inner value (BS path of portfolio::sampler) ----------------------------------
 // sample_inner_bs with option_diff_from_blackscholes and the delta CV (portfolio_sampler.cpp:
@@ -274,7 +313,7 @@ __device__ __forceinline__ void pf_chunk_fast(const TfKey& key, uint32_t tag, ui
             float x = pf_sample_loss<MODE>(v[q], ot, Rrow);
             if (S2) x += shift;
             a1.add(x);
-            if (S2) a2.add(x * x);
+            if (S2) a2.add_sq(x);
         }
     }
 }
@@ -351,7 +390,7 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
             RT d = smp.sample_inner(s0 + q, count, w);
             if (PREC == PREC_FP32 && S2) d = (RT)((float)d + shift);
             a1.add(d);
-            if (S2) a2.add(d * d);
+            if (S2) { if (PREC == PREC_FP32) a2.add_sq(d); else a2.add(d * d); }
         }
         work += w;
     } else if (KIND == KIND_SHIFT_MODEL) {       // X = Y + Z: one normal per inner sample
@@ -368,7 +407,7 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
                 RT d = (PREC == PREC_FP32) ? (RT)(Y + z[q]) : xadd(Y, z[q]);
                 if (PREC == PREC_FP32 && S2) d = (RT)((float)d + shift);
                 a1.add(d);
-                if (S2) a2.add((PREC == PREC_FP32) ? (RT)(d * d) : xmul(d, d));
+                if (S2) { if (PREC == PREC_FP32) a2.add_sq(d); else a2.add(xmul(d, d)); }
             }
         }
         work += (double)C;
@@ -389,11 +428,11 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
                 RT d = xsub(xmul(a, a), xmul(c, c));
                 if (PREC == PREC_FP32 && S2) d = (RT)((float)d + shift);
                 a1.add(d);
-                if (S2) a2.add(xmul(d, d));
+                if (S2) { if (PREC == PREC_FP32) a2.add_sq(d); else a2.add(xmul(d, d)); }
             }
         }
         work += (double)C;
-    } else if (PREC == PREC_FP32 && L.ot.fast_s) {
+    } else if (KIND == KIND_PORTFOLIO && PREC == PREC_FP32 && L.ot.fast_s) {
         // portfolio, FP32: packed records scaled by 1 / (sampling probability), the SFU
         // Black-Scholes (nmlmc_bs.cuh); X = loss_j / phat_j.  srow: the outer sample's R_tau row
         // staged in shared memory, else read from the batch buffer.
@@ -425,10 +464,34 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
             for (int q = 0; q < 2; q++) {
                 RT prob;
                 uint32_t j = pf_pick<RT>(ot, v[q], prob);
-                RT d = xdiv(pf_value<RT, RS>(ot, Rrow, j), prob);
-                work += (double)ot.W_est[j];
+                RT val;
+                if (KIND == KIND_PF_PATHS && j >= ot.m_off[1]) {
+                    // Exact / Unbiased option (sample_inner_option, portfolio_sampler.cpp:382-396)
+                    const uint64_t ns = path_ns(tag, s0 + 2 * b + q);
+                    OuterPathNormals<RT, PREC> nz{key, ns, 0, false, (RT)0};
+                    const RT Rs = Rrow[ot.stock_ind[j] * RS];
+                    if (j < ot.m_off[2]) {
+                        val = inner_exact<RT>(ot, Rs, j, nz, work);
+                    } else {
+                        uint64_t u0, u1;
+                        threefry2x64(0, ns | kPathUniform, key, u0, u1);
+                        uint32_t Lv;
+                        uint64_t N_l;
+                        if (unbiased_level<RT>(ot, u01_word<PREC, RT>((uint32_t)u0), Lv, N_l)) {
+                            val = inner_unbiased<RT>(ot, Rs, j, nz, work, Lv, N_l);
+                        } else {                 // beyond kMaxPathSteps: the call fails
+                            atomicOr(D.B.counters + CNT_ERR, 1u);
+                            val = (RT)0;
+                        }
+                    }
+                } else {
+                    val = pf_value<RT, RS>(ot, Rrow, j);
+                    work += (double)ot.W_est[j];
+                }
+                RT d = xdiv(val, prob);
+                if (PREC == PREC_FP32 && S2) d = (RT)((float)d + shift);
                 a1.add(d);
-                if (S2) a2.add(xmul(d, d));
+                if (S2) { if (PREC == PREC_FP32) a2.add_sq(d); else a2.add(xmul(d, d)); }
             }
         }
     }
@@ -870,7 +933,7 @@ __global__ void __launch_bounds__(kTile) k_outer(DevLevel<RT> D, uint32_t nb) {
             uint64_t cnt = L.cf.base_count;
             Yv[i] = smp.init_inner_sampler(cnt, w);
             *const_cast<S*>(user_state<S>(D.B, i)) = smp;
-        } else if (KIND != KIND_PORTFOLIO) {
+        } else if (!is_portfolio_kind(KIND)) {
             Yv[i] = outer_normal_at<PREC, RT>(key, PH_OUTER, 0);
         } else {
             // portfolio_sampler.cpp:293-311 on the OUTER layout: normal 0 systemic, 1 + s per stock
@@ -1001,7 +1064,7 @@ static void launch_phase_v(const DevLevel<RT>& D, const SegSet& SS, TraceRec* tr
 // resident CTAs per SM guaranteed); the parity precisions run variant 0.
 template <class RT, int KIND, int PREC, class S = NoSampler>
 static void launch_phase(const DevLevel<RT>& D, const SegSet& SS, TraceRec* trace, cudaStream_t stream) {
-    if constexpr (PREC == PREC_FP32 && KIND != KIND_USER) {
+    if constexpr (PREC == PREC_FP32 && KIND != KIND_USER && KIND != KIND_PF_PATHS) {
         if (D.L.variant == 1) return launch_phase_v<RT, KIND, PREC, 3>(D, SS, trace, stream);
         if (D.L.variant == 2) return launch_phase_v<RT, KIND, PREC, 4>(D, SS, trace, stream);
     }

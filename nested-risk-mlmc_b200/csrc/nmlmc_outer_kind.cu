@@ -1,9 +1,10 @@
 // Instantiations of the batched level sequence for one sampler kind (NMLMC_OUTER_KIND = 0
-// reference model, 1 shift model, 2 portfolio), in all three precisions; compiled once per kind.
+// reference model, 1 shift model, 2 portfolio, 4 portfolio with path-simulated options), in all
+// three precisions; compiled once per kind.
 #include "nmlmc_outer_impl.cuh"
 
 #ifndef NMLMC_OUTER_KIND
-#error "NMLMC_OUTER_KIND must be defined (0, 1 or 2)"
+#error "NMLMC_OUTER_KIND must be defined (0, 1, 2 or 4)"
 #endif
 
 namespace nmlmc {

@@ -245,12 +245,31 @@ typedef struct {
     uint64_t nword, nnorm;      /* OUTER: next word / next normal of the current phase */
     int draw_kind;              /* OUTER: 0 none yet, 1 normals, 2 uniforms (a phase is one kind) */
     uint64_t randu_count, randn_count;
+    uint64_t ninner;            /* OUTER: inner samples drawn in the current phase */
+    /* OUTER, path-simulated inner sample: its own counter namespace for normals (pns) and
+     * uniforms (pns | O_PATH_UNIFORM), next normal / uniform */
+    int path;
+    uint64_t pns, pn, pu;
 } o_cursor;
+
+/* Counter namespaces of a path-simulated inner sample on the OUTER layout: inner sample i of the
+ * phase with tag t draws its normals from counter word 1 = t | (i + 1) << 16 and its uniforms
+ * from t | (i + 1) << 16 | 2^15. */
+#define O_PATH_UNIFORM (1ull << 15)
+static uint64_t path_ns(uint64_t tag, uint64_t i) { return tag | ((i + 1) << 16); }
 
 enum { PH_OUTER = 0, PH_FINE = 1, PH_COARSE = 64, PH_FINAL = 128, PH_FINAL_C = 129 };
 
 static void cur_phase(o_cursor *k, uint64_t tag) {
-    k->tag = tag; k->nword = 0; k->nnorm = 0; k->draw_kind = 0;
+    k->tag = tag; k->nword = 0; k->nnorm = 0; k->draw_kind = 0; k->ninner = 0; k->path = 0;
+}
+
+/* word j of counter namespace ns of the current OUTER key */
+static uint32_t ns_word(const o_cursor *k, uint64_t ns, uint64_t j) {
+    uint64_t ctr[2] = {j >> 2, ns}, v[2];
+    o_threefry2x64(ctr, k->key, v);
+    uint64_t e = v[(j >> 1) & 1];
+    return (j & 1) ? (uint32_t)(e >> 32) : (uint32_t)e;
 }
 
 static uint32_t outer_word(const o_cursor *k, uint64_t j) {

@@ -169,7 +169,8 @@ class Sampler:
                               subsample=SUB_RANDOM, use_delta_cv=False, use_coarse_delta_cv=False,
                               use_antithetic_risk=True, use_milstein=True, dt_h0inv=8, dt_beta=4,
                               dt_prob_expo=-1.5):
-        """Mixed compute methods (0 BS, 1 Exact, 2 Unbiased); CORE layout only."""
+        """Mixed compute methods (0 BS, 1 Exact, 2 Unbiased); on the OUTER layout with sub-sampling
+        (each path-simulated inner sample draws from its own counter namespaces)."""
         L = _methods_bind()
         Q = len(pf["S0"])
         P = len(pf["strike"])
@@ -186,7 +187,7 @@ class Sampler:
                                        int(use_coarse_delta_cv), int(use_antithetic_risk),
                                        int(use_milstein), dt_h0inv, dt_beta, dt_prob_expo)
         if rc == -2:
-            raise ValueError("path-simulated compute methods need the CORE stream layout")
+            raise ValueError("path-simulated compute methods on the OUTER layout need sub-sampling")
         if rc != 0:
             raise ValueError("invalid portfolio (stock index, or prob not positive/non-increasing)")
 

@@ -72,8 +72,8 @@ def test_integration_python_snippets_parse():
 
 
 def test_docs_cite_files_that_exist():
-    """Every repository file named in DESIGN.md, INTEGRATION.md and README.md (tests, profiles,
-    sources, headers) exists; names of the reference's own files are not checked."""
+    """Every repository file named in the user documentation (README.md: tests,
+    profiles, sources, headers) exists; names of the reference's own files are not checked."""
     reference_files = {"common.cpp", "common.hpp", "mlmc.hpp", "model_sampler.cpp", "nested_sampler.hpp",
                        "par_nvcc.hpp", "par_omp.hpp", "portfolio_sampler.cpp", "gbm_approx.hpp",
                        "table_output.hpp", "threefry.h", "boxmuller.hpp", "uniform.hpp", "array.h",
@@ -82,7 +82,7 @@ def test_docs_cite_files_that_exist():
     roots = [ROOT, pkg, os.path.join(pkg, "csrc"), os.path.join(pkg, "nmlmc"), os.path.join(ROOT, "oracle"),
              os.path.join(ROOT, "tests"), os.path.join(ROOT, "tests", "abi"), os.path.join(ROOT, "include")]
     missing = []
-    for doc in ("DESIGN.md", "INTEGRATION.md", "README.md"):
+    for doc in ("INTEGRATION.md", "README.md"):
         text = open(os.path.join(ROOT, doc)).read()
         for m in re.finditer(r"[\w./-]+\.(?:py|md|cu|cuh|cpp|c|h|hpp|inc|json)\b", text):
             name = m.group(0).strip("./")

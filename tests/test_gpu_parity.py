@@ -248,15 +248,6 @@ def test_reference_named_portfolio_surface_methods(nm, golden):
         nm.cleanup_nestedmc_sampler()
 
 
-def test_methods_outer_layout_refused(nm):
-    """Path-simulated methods are defined on the CORE streams: the OUTER layout refuses them."""
-    s = nm.Sampler(precision=nm.PREC_FP64, streams=nm.STREAMS_OUTER, N0=32, beta=4, adaptive_r=1.5)
-    pf = O.synthetic_portfolio(2, 6, 3)
-    s.set_portfolio(pf, methods=dict(method=[0, 1, 2, 0, 1, 2]))
-    with pytest.raises(nm.NmlmcError):
-        s.sample(1, 10)
-
-
 OUTER_CASES = [
     dict(name="shift_r15", kind="model", model=1, tau=0.0, max_loss=1.0, cores=1, N0=32, beta=2,
          r=1.5, anti=True, seed=3, calls=[(0, 3000), (1, 2000), (3, 2000), (6, 1500), (9, 600)]),

@@ -141,14 +141,35 @@ def test_live_reference_random_case():
         np.testing.assert_array_equal(a["diffsums"], b["diffsums"])
 
 
-def test_methods_need_core_layout():
-    """Path-simulated compute methods are defined on the reference's CORE streams only."""
-    s = O.Sampler(O.PREC_FP64, O.STREAMS_OUTER, 1, 32, 4, 1.5, True, False, 1)
+def test_outer_path_methods_need_subsampling():
+    """On the OUTER layout every inner sample draws one option (and path-simulated options draw
+    from the inner sample's own counter namespaces): path methods need a sub-sampled mode."""
     pf = O.synthetic_portfolio(2, 4, 1)
+    s = O.Sampler(O.PREC_FP64, O.STREAMS_OUTER, 1, 32, 4, 1.5, True, False, 1)
     with pytest.raises(ValueError):
-        s.set_portfolio_methods(pf, [0, 1, 2, 0])
+        s.set_portfolio_methods(pf, [0, 1, 2, 0], subsample=O.SUB_NONE)
     s2 = O.Sampler(O.PREC_FP64, O.STREAMS_OUTER, 1, 32, 4, 1.5, True, False, 1)
-    s2.set_portfolio_methods(pf, [0, 0, 0, 0])      # all BS: the OUTER layout applies
+    s2.set_portfolio_methods(pf, [0, 1, 2, 0], subsample=O.SUB_RANDOM)
+    s2.sample(1, 20)
+
+
+def test_outer_exact_paths_average_to_black_scholes():
+    """The OUTER layout's per-inner-sample path streams give unbiased option values: with every
+    option priced by exact GBM paths (sample_inner_exact, portfolio_sampler.cpp:470-519) the inner
+    mean of each outer sample agrees with the Black-Scholes one (same outer draws, the same option
+    drawn by each inner sample) within 4 standard errors of their differences."""
+    pf = O.synthetic_portfolio(2, 8, 5, "uniform")
+    M, ell = 24, 4                                   # 32 * 4^4 = 8192 inner samples per outer sample
+    kw = dict(r=0.05, rho=0.0, max_loss=0.0, tau=1 / 52, subsample=O.SUB_UNIFORM, use_delta_cv=False)
+    bs = O.Sampler(O.PREC_FP64, O.STREAMS_OUTER, 1, 32, 4, 0.0, True, False, 3)
+    bs.set_portfolio(pf, **kw, discount=True)
+    ex = O.Sampler(O.PREC_FP64, O.STREAMS_OUTER, 1, 32, 4, 0.0, True, False, 3)
+    ex.set_portfolio_methods(pf, [1] * 8, **kw)
+    a = bs.sample(ell, M, trace=True)["trace"]["mean_big"]
+    b = ex.sample(ell, M, trace=True)["trace"]["mean_big"]
+    d = b - a
+    assert np.all(np.isfinite(d)) and np.std(d) > 0
+    assert abs(d.mean()) < 4 * d.std(ddof=1) / np.sqrt(M), (d.mean(), d.std(ddof=1))
 
 
 @pytest.mark.skipif(not O.ref_available("f64_lzcnt"), reason="oracle/_ref not built on this host")
