@@ -177,14 +177,18 @@ struct OuterPathNormals {
     uint64_t p;          // next pair
     bool have;
     RT y;
+    uint64_t v1;         // the block's second value (pairs 2b + 1)
     __device__ __forceinline__ RT next() {
         if (have) {
             have = false;
             return y;
         }
-        uint64_t v0, v1;
-        threefry2x64(p >> 1, ns, key, v0, v1);
-        const uint64_t e = (p & 1) ? v1 : v0;
+        uint64_t e;
+        if (p & 1) {
+            e = v1;                                  // the block was drawn with pair p - 1
+        } else {
+            threefry2x64(p >> 1, ns, key, e, v1);
+        }
         RT x;
         bm_pair<PREC, RT>((uint32_t)e, (uint32_t)(e >> 32), x, y);
         p++;
@@ -299,21 +303,52 @@ __device__ __forceinline__ float pf_sample_loss(uint64_t v, const OptionTable<fl
 }
 
 // C inner samples of the FP32 portfolio path from Threefry blocks b0, b0 + 1, ... (two samples per
-// block, one 64-bit value each).  Pilots (S2) accumulate the losses shifted by `shift`.
+// block, one 64-bit value each).  Pilots (S2) accumulate the losses shifted by `shift`.  With alias
+// columns the loop takes two blocks (four samples) at a time and issues their four column gathers
+// together, then the alias-column gathers of the draws that need them, so a thread has four
+// samples' L2 round trips in flight at once (4 % faster than two at a time, spills included).
 template <int PREC, uint32_t C, bool S2, int MODE>
 __device__ __forceinline__ void pf_chunk_fast(const TfKey& key, uint32_t tag, uint64_t b0,
                                               const OptionTable<float>& ot, const float2* Rrow, float shift,
                                               Acc<PREC>& a1, Acc<PREC>& a2) {
-#pragma unroll 2
-    for (uint32_t b = 0; b < C / 2; b++) {
-        uint64_t v[2];
-        threefry2x64(b0 + b, tag, key, v[0], v[1]);
+    if constexpr (MODE == PF_COLUMN) {
+#pragma unroll 1
+        for (uint32_t b = 0; b < C / 2; b += 2) {
+            uint64_t v[4];
+            threefry2x64(b0 + b, tag, key, v[0], v[1]);
+            threefry2x64(b0 + b + 1, tag, key, v[2], v[3]);
+            FastColumn c[4];
+            uint32_t coin[4];
 #pragma unroll
-        for (int q = 0; q < 2; q++) {
-            float x = pf_sample_loss<MODE>(v[q], ot, Rrow);
-            if (S2) x += shift;
-            a1.add(x);
-            if (S2) a2.add_sq(x);
+            for (int q = 0; q < 4; q++) {
+                const uint32_t j = (uint32_t)__umul64hi(v[q], (uint64_t)ot.P);
+                coin[q] = (uint32_t)((v[q] * (uint64_t)ot.P) >> 32);
+                c[q] = load_column(ot.fast_col + j);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (coin[q] >= c[q].thr) c[q] = load_column(ot.fast_col + (c[q].link >> 8));
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const float2 r = Rrow[c[q].link & 0xffu];
+                float x = column_loss_fast(c[q], r.x, r.y);
+                if (S2) x += shift;
+                a1.add(x);
+                if (S2) a2.add_sq(x);
+            }
+        }
+    } else {
+#pragma unroll 2
+        for (uint32_t b = 0; b < C / 2; b++) {
+            uint64_t v[2];
+            threefry2x64(b0 + b, tag, key, v[0], v[1]);
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                float x = pf_sample_loss<MODE>(v[q], ot, Rrow);
+                if (S2) x += shift;
+                a1.add(x);
+                if (S2) a2.add_sq(x);
+            }
         }
     }
 }
@@ -468,17 +503,35 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
                 if (KIND == KIND_PF_PATHS && j >= ot.m_off[1]) {
                     // Exact / Unbiased option (sample_inner_option, portfolio_sampler.cpp:382-396)
                     const uint64_t ns = path_ns(tag, s0 + 2 * b + q);
-                    OuterPathNormals<RT, PREC> nz{key, ns, 0, false, (RT)0};
+                    OuterPathNormals<RT, PREC> nz{key, ns, 0, false, (RT)0, 0};
                     const RT Rs = Rrow[ot.stock_ind[j] * RS];
                     if (j < ot.m_off[2]) {
-                        val = inner_exact<RT>(ot, Rs, j, nz, work);
+                        if constexpr (PREC == PREC_FP32) val = inner_exact_fast(ot, Rs, j, nz, work);
+                        else val = inner_exact<RT>(ot, Rs, j, nz, work);
                     } else {
                         uint64_t u0, u1;
                         threefry2x64(0, ns | kPathUniform, key, u0, u1);
                         uint32_t Lv;
                         uint64_t N_l;
-                        if (unbiased_level<RT>(ot, u01_word<PREC, RT>((uint32_t)u0), Lv, N_l)) {
-                            val = inner_unbiased<RT>(ot, Rs, j, nz, work, Lv, N_l);
+                        bool ok;
+                        if constexpr (PREC == PREC_FP32) {
+                            // the level in double, as the FP64 path draws it
+                            const double u = __dadd_rn(__dmul_rn((double)(uint32_t)u0, 0x1p-32), 0x1p-33);
+                            const double qL = log(u) / (log((double)ot.dt_beta) * (double)ot.dt_prob_expo);
+                            Lv = (uint32_t)floor(qL);
+                            N_l = 1;
+                            ok = true;
+                            for (uint32_t i = 0; i < Lv && ok; i++) {
+                                N_l *= ot.dt_beta;
+                                ok = N_l * ot.dt_h0inv <= kMaxPathSteps;
+                            }
+                            ok = ok && N_l * ot.dt_h0inv <= kMaxPathSteps;
+                        } else {
+                            ok = unbiased_level<RT>(ot, u01_word<PREC, RT>((uint32_t)u0), Lv, N_l);
+                        }
+                        if (ok) {
+                            if constexpr (PREC == PREC_FP32) val = inner_unbiased_fast(ot, Rs, j, nz, work, Lv, N_l);
+                            else val = inner_unbiased<RT>(ot, Rs, j, nz, work, Lv, N_l);
                         } else {                 // beyond kMaxPathSteps: the call fails
                             atomicOr(D.B.counters + CNT_ERR, 1u);
                             val = (RT)0;
@@ -1061,14 +1114,16 @@ static void launch_phase_v(const DevLevel<RT>& D, const SegSet& SS, TraceRec* tr
 }
 
 // The FP32 path has three register/occupancy variants (OuterLevel::variant 0, 1, 2 -> 1, 3, 4
-// resident CTAs per SM guaranteed); the parity precisions run variant 0.
+// resident CTAs per SM guaranteed); the parity precisions run variant 0, the FP32 kernel of
+// path-simulated portfolios three CTAs per SM (80 registers, no spills; its FP64 path states and
+// exponentials leave one CTA per SM at the compiler's own choice).
 template <class RT, int KIND, int PREC, class S = NoSampler>
 static void launch_phase(const DevLevel<RT>& D, const SegSet& SS, TraceRec* trace, cudaStream_t stream) {
     if constexpr (PREC == PREC_FP32 && KIND != KIND_USER && KIND != KIND_PF_PATHS) {
         if (D.L.variant == 1) return launch_phase_v<RT, KIND, PREC, 3>(D, SS, trace, stream);
         if (D.L.variant == 2) return launch_phase_v<RT, KIND, PREC, 4>(D, SS, trace, stream);
     }
-    launch_phase_v<RT, KIND, PREC, 1, S>(D, SS, trace, stream);
+    launch_phase_v<RT, KIND, PREC, (KIND == KIND_PF_PATHS && PREC == PREC_FP32) ? 3 : 1, S>(D, SS, trace, stream);
 }
 
 static inline uint32_t ilog2_u64(uint64_t v) {
