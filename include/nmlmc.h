@@ -324,8 +324,9 @@ int nmlmc_set_autotune(nmlmc_ctx* ctx, int32_t mode);   /* 0 off, 1 variants (de
 int nmlmc_get_phase_config(nmlmc_ctx* ctx, uint32_t ell, nmlmc_phase_config* out);
 /* Pins level ell's configuration (cfg == NULL unpins it: default, tunable again). */
 int nmlmc_set_phase_config(nmlmc_ctx* ctx, uint32_t ell, const nmlmc_phase_config* cfg);
-/* Tunes level ell now, variant and chunk length, on a probe of at most M outer samples
- * (replaces a tuned or pinned choice). */
+/* Tunes level ell now, variant and chunk length, on a probe of about 20 ms of device time (at
+ * most one batch of outer samples; the batch buffers grow to M first) — replaces a tuned or
+ * pinned choice. */
 int nmlmc_autotune_level(nmlmc_ctx* ctx, uint32_t ell, uint64_t M);
 
 /* Fault injection for tests (no counterpart in the reference): after `after` more successful

@@ -684,9 +684,13 @@ void fill_outer_result(const nmlmc_ctx* c, const double* a, uint64_t M, double s
 // Default phase configuration: up to 255 registers for the models (their inner loop is ALU-bound
 // and gains nothing from more warps), four CTAs per SM for the FP32 portfolio (its option-table
 // gathers need the warps to hide L2 latency), chunks of min(N0, 32) inner samples.
+// Defaults of the FP32 path, measured per level of the benchmark runs: the portfolio kernel at
+// 64 registers (variant 2: four CTAs per SM keep more table gathers in flight), the model kinds at
+// 80 (variant 1: fastest or within 0.3 % of it at every level of the adaptive model problem, 3-7 %
+// ahead of variant 0).
 PhaseChoice default_phase(const nmlmc_ctx* c) {
     PhaseChoice p;
-    p.variant = (c->cfg.precision == NMLMC_PREC_FP32 && c->kind == KIND_PORTFOLIO) ? 2u : 0u;
+    p.variant = c->cfg.precision != NMLMC_PREC_FP32 ? 0u : c->kind == KIND_PORTFOLIO ? 2u : 1u;
     p.chunk = c->cfg.N0 >= 32 ? 32u : c->cfg.N0;
     return p;
 }
@@ -773,15 +777,16 @@ cudaError_t time_phase_config(nmlmc_ctx* c, uint32_t ell, uint64_t Mp, const Pha
     return e;
 }
 
-// Probe size, measured: starting from min(4096, M, batch) outer samples, the default
-// configuration is timed on growing probes (at most 8x per step, launch overheads make small
-// probes look cheap) until one takes kProbeMs of device time or the probe reaches the call's M or
-// one batch.  Shorter probes mis-ranked the variants of the large-portfolio levels.  The work per
-// outer sample ranges from the base count to the maximum count of the level, too wide to predict
-// from the configuration.
+// Probe size, measured: starting from 4096 outer samples, the default configuration is timed on
+// growing probes (at most 8x per step, launch overheads make small probes look cheap) until one
+// takes kProbeMs of device time or the probe fills one batch.  The probe is not bounded by the
+// call's M (its outer samples are not the call's): probes shorter than kProbeMs mis-ranked the
+// variants of the large-portfolio levels and kept the default on the model levels whose first
+// tuned call was small.  The work per outer sample ranges from the base count to the maximum count
+// of the level, too wide to predict from the configuration.
 template <class RT>
-cudaError_t probe_size(nmlmc_ctx* c, uint32_t ell, uint64_t M, uint64_t& Mp) {
-    const uint64_t lim = M < c->ob.cap ? M : c->ob.cap;
+cudaError_t probe_size(nmlmc_ctx* c, uint32_t ell, uint64_t& Mp) {
+    const uint64_t lim = c->ob.cap;
     Mp = lim < 4096 ? lim : 4096;
     for (;;) {
         double ms = 0;
@@ -797,10 +802,10 @@ cudaError_t probe_size(nmlmc_ctx* c, uint32_t ell, uint64_t M, uint64_t& Mp) {
 }
 
 template <class RT>
-int tune_level(nmlmc_ctx* c, uint32_t ell, uint64_t M, bool chunks) {
+int tune_level(nmlmc_ctx* c, uint32_t ell, bool chunks) {
     NvtxRange nv("nmlmc autotune level");
     uint64_t Mp = 0;
-    NM_CUDA(probe_size<RT>(c, ell, M, Mp), "autotune probe size");
+    NM_CUDA(probe_size<RT>(c, ell, Mp), "autotune probe size");
     // the default stays unless another candidate is more than 3 % faster on the probe (near-ties
     // on a short probe are noise)
     PhaseChoice best = default_phase(c);
@@ -839,7 +844,7 @@ int ensure_tuned(nmlmc_ctx* c, uint32_t ell, uint64_t M) {
     const uint64_t Mp = M < c->ob.cap ? M : c->ob.cap;
     const CountParams cf = count_params(c->cfg, ell);
     if (Mp < 4096 || (double)Mp * (double)cf.base_count * (double)(ell + 1) < 8.0e6) return NMLMC_OK;
-    return tune_level<RT>(c, ell, M, c->autotune == 2);
+    return tune_level<RT>(c, ell, c->autotune == 2);
 }
 
 template <class RT>
@@ -1556,7 +1561,7 @@ int nmlmc_autotune_level(nmlmc_ctx* c, uint32_t ell, uint64_t M) {
     int rc = ensure_portfolio(c);
     if (rc || (rc = alloc_outer(c, M))) return rc;
     if (c->kind == KIND_PORTFOLIO && c->pf.mixed()) return set_err(NMLMC_ERR_ARG);
-    return tune_level<float>(c, ell, M, true);
+    return tune_level<float>(c, ell, true);
 }
 
 int nmlmc_inject_alloc_failure(int32_t after) {

@@ -16,7 +16,7 @@
 //
 // Phi(x) = erfc(-x/sqrt 2) / 2 with the rational-Chebyshev erfc of Numerical Recipes in C
 // (2nd ed., §6.2, "erfcc": fractional error below 1.2e-7 for all arguments), its exponential and
-// reciprocal on MUFU (__expf, __frcp_rn).  Measured against double erfc over |x| <= 10 the
+// reciprocal on MUFU (__expf; rcp.approx refined by one Newton-Raphson step).  Measured against double erfc over |x| <= 10 the
 // composite Phi has absolute error <= 1.8e-7 and, where Phi >= 1e-20, relative error <= 8e-6: in
 // the far tail the FP32 rounding of the exponent -z^2 (up to ~43) dominates, not the erfc fit
 // (tests/test_gpu_portfolio.py, bounds 2.5e-7 and 1e-5).  The loss of one option is then within
@@ -51,9 +51,19 @@ constexpr uint32_t kColumnMaxStocks = 256;
 constexpr uint32_t kColumnMaxOptions = 1u << 24;
 
 #ifdef __CUDACC__
+// 1 / x for normal x: the SFU estimate (PTX rcp.approx, relative error below 2^-23) refined by one
+// Newton-Raphson step in FMA form, e = 1 - x r, r' = r + r e (Markstein, IBM J. Res. Dev. 34(1),
+// 1990): the step squares the estimate's relative error, so r' is within half an ulp plus 2^-45
+// relative of 1 / x.
+__device__ __forceinline__ float rcp_nr(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return fmaf(r, fmaf(-x, r, 1.0f), r);
+}
+
 // erfc(z) for z >= 0 on the SFU (Numerical Recipes "erfcc" coefficients).
 __device__ __forceinline__ float erfc_pos_fast(float z) {
-    float t = __frcp_rn(fmaf(0.5f, z, 1.0f));
+    float t = rcp_nr(fmaf(0.5f, z, 1.0f));
     float p = fmaf(t, 0.17087277f, -0.82215223f);
     p = fmaf(t, p, 1.48851587f);
     p = fmaf(t, p, -1.13520398f);
@@ -82,11 +92,11 @@ __device__ __forceinline__ float option_loss_fast(const FastOption& o, float R, 
     return fmaf(o.cv, R, v);
 }
 
-// The same loss from an alias column: m d1 as above, m s = 1 / (m inv_s) correctly rounded
-// (within one ulp of the record's m s, the only difference from option_loss_fast).
+// The same loss from an alias column: m d1 as above, m s = 1 / (m inv_s) (rcp_nr: within one
+// ulp of the record's m s, the only difference from option_loss_fast).
 __device__ __forceinline__ float column_loss_fast(const FastColumn& c, float R, float lnR) {
     const float d1 = (lnR + c.c1) * c.inv_s;
-    const float d2 = d1 - __frcp_rn(c.inv_s);
+    const float d2 = d1 - rcp_nr(c.inv_s);
     const float n1 = norm_cdf_fast(d1), n2 = norm_cdf_fast(d2);
     const float v = fmaf(c.wR * R, n1, fmaf(c.wK, n2, c.wV0));
     return fmaf(c.cv, R, v);

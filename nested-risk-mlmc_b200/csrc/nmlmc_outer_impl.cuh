@@ -52,8 +52,9 @@ enum : int {
 static_assert(CNT_QUEUE + kMaxSegs <= CNT_ERR && CNT_ERR < 256, "counter slots");
 
 // ---- accumulators -------------------------------------------------------------------------
-// FP32: compensated pair (hi + lo) — Kahan accumulation inside a thread, TwoSum merging across
-// threads.  FP64 and REF32: double, the reference's sum_t.
+// FP32: compensated pair (hi + lo) — Kahan accumulation inside a thread (of pairs of consecutive
+// inner values where the kind draws them together), TwoSum merging across threads.  FP64 and
+// REF32: double, the reference's sum_t, one value at a time in the reference's order.
 template <int PREC> struct Acc;
 
 template <> struct Acc<PREC_FP32> {
@@ -82,12 +83,16 @@ template <> struct Acc<PREC_FP32> {
     // plain addition: the pilots' sum of squares, which only feeds the variance estimate of the
     // adaptive rule (sums of 4-64 squares per thread of values centred on the threshold)
     __device__ __forceinline__ void add_sq(float v) { hi = fmaf(v, v, hi); }
+    // two consecutive inner values: their plain sum (one rounding of a value bounded by the two
+    // summands), then the compensated step
+    __device__ __forceinline__ void add2(float v0, float v1) { add(__fadd_rn(v0, v1)); }
 };
 
 template <> struct Acc<PREC_FP64> {
     double v;
     __device__ __forceinline__ void zero() { v = 0; }
     __device__ __forceinline__ void add(double x) { v = __dadd_rn(v, x); }
+    __device__ __forceinline__ void add2(double x0, double x1) { add(x0); add(x1); }
     __device__ __forceinline__ void add_sq(double x) { v = __dadd_rn(v, __dmul_rn(x, x)); }
     __device__ __forceinline__ void merge(const Acc& o) { v = __dadd_rn(v, o.v); }
     __device__ __forceinline__ Acc shfl_xor(int m) const { Acc r; r.v = __shfl_xor_sync(0xffffffffu, v, m); return r; }
@@ -97,6 +102,7 @@ template <> struct Acc<PREC_REF32> {
     double v;
     __device__ __forceinline__ void zero() { v = 0; }
     __device__ __forceinline__ void add(double x) { v = __dadd_rn(v, x); }
+    __device__ __forceinline__ void add2(double x0, double x1) { add(x0); add(x1); }
     __device__ __forceinline__ void add_sq(double x) { v = __dadd_rn(v, __dmul_rn(x, x)); }
     __device__ __forceinline__ void merge(const Acc& o) { v = __dadd_rn(v, o.v); }
     __device__ __forceinline__ Acc shfl_xor(int m) const { Acc r; r.v = __shfl_xor_sync(0xffffffffu, v, m); return r; }
@@ -420,12 +426,16 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
         S smp(user_ws(D.B, item));
         smp.copy_outer(*user_state<S>(D.B, item));
         double w = 0;
-        for (uint32_t q = 0; q < C; q++) {
-            smp.template nm_begin_inner_of<S>(key, tag, s0 + q);
-            RT d = smp.sample_inner(s0 + q, count, w);
-            if (PREC == PREC_FP32 && S2) d = (RT)((float)d + shift);
-            a1.add(d);
-            if (S2) { if (PREC == PREC_FP32) a2.add_sq(d); else a2.add(d * d); }
+        for (uint32_t q = 0; q < C; q += 2) {
+            RT d[2];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                smp.template nm_begin_inner_of<S>(key, tag, s0 + q + h);
+                d[h] = smp.sample_inner(s0 + q + h, count, w);
+                if (PREC == PREC_FP32 && S2) d[h] = (RT)((float)d[h] + shift);
+                if (S2) { if (PREC == PREC_FP32) a2.add_sq(d[h]); else a2.add(d[h] * d[h]); }
+            }
+            a1.add2(d[0], d[1]);
         }
         work += w;
     } else if (KIND == KIND_SHIFT_MODEL) {       // X = Y + Z: one normal per inner sample
@@ -441,9 +451,11 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
             for (int q = 0; q < 4; q++) {
                 RT d = (PREC == PREC_FP32) ? (RT)(Y + z[q]) : xadd(Y, z[q]);
                 if (PREC == PREC_FP32 && S2) d = (RT)((float)d + shift);
-                a1.add(d);
+                z[q] = d;
                 if (S2) { if (PREC == PREC_FP32) a2.add_sq(d); else a2.add(xmul(d, d)); }
             }
+            a1.add2(z[0], z[1]);
+            a1.add2(z[2], z[3]);
         }
         work += (double)C;
     } else if (KIND == KIND_REF_MODEL) {         // model_sampler.cpp:62-76: two normals
@@ -462,9 +474,10 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
                 RT c = xadd(xmul(st, Y2[q]), xmul(s1t, X[q]));
                 RT d = xsub(xmul(a, a), xmul(c, c));
                 if (PREC == PREC_FP32 && S2) d = (RT)((float)d + shift);
-                a1.add(d);
+                X[q] = d;
                 if (S2) { if (PREC == PREC_FP32) a2.add_sq(d); else a2.add(xmul(d, d)); }
             }
+            a1.add2(X[0], X[1]);
         }
         work += (double)C;
     } else if (KIND == KIND_PORTFOLIO && PREC == PREC_FP32 && L.ot.fast_s) {

@@ -104,27 +104,24 @@ __device__ __forceinline__ void boxmuller32_d(uint32_t u0, uint32_t u1, double& 
     y = __dmul_rn(c, r);
 }
 
-// FP32 fast Box-Muller on the SFU: MUFU sin/cos of pi*a (absolute error <= 2^-21.4 on
-// [-pi, pi]), MUFU lg2 for the log and MUFU rsqrt for the root.  Near u = 1 the MUFU log's
-// absolute error (2^-22) would dominate the small radius, so there t = -2 ln(1 - q) is summed
-// from its series in the exact complement q = 1 - u = (~u1 + 1/2) 2^-32 (five terms; truncation
-// below 5e-12 relative for q < 1/64).  |z - z_double| <= 4e-6 over the whole range (checked
-// against boxmuller32_d in the tests).
+// FP32 fast Box-Muller on the SFU: MUFU sin/cos of the angle pi*a (absolute error <= 2^-21.4 on
+// [-pi, pi]; pi*a formed in one FMA from the word), MUFU lg2 for the log and MUFU rsqrt for the
+// root.  Near u = 1 the MUFU log's absolute error (2^-22) would dominate the small radius, so
+// there t = -2 ln(1 - q) is summed from its series in the exact complement
+// q = 1 - u = (~u1 + 1/2) 2^-32: t = q (2 + q (1 + 2q/3)), whose truncation (q^4 / 2) is below
+// 2^-20 of t for q < 1/64.  |z - z_double| <= 4e-6 over the whole range (checked against
+// boxmuller32_d in the tests).
 __device__ __forceinline__ void boxmuller32_f(uint32_t u0, uint32_t u1, float& x, float& y) {
     const float PI = 3.14159265358979f;
-    float a = fmaf((float)(int32_t)u0, 0x1p-31f, 0x1p-32f);
-    float u = fmaf((float)u1, 0x1p-32f, 0x1p-33f);
-    float q = fmaf((float)(~u1), 0x1p-32f, 0x1p-33f);
+    const float th = fmaf((float)(int32_t)u0, PI * 0x1p-31f, PI * 0x1p-32f);
+    const float u = fmaf((float)u1, 0x1p-32f, 0x1p-33f);
+    const float q = fmaf((float)(~u1), 0x1p-32f, 0x1p-33f);
     float s, c;
-    __sincosf(PI * a, &s, &c);
-    float t_log = -2.0f * 0.69314718055994531f * __log2f(u);
-    float p = fmaf(q, 0.2f, 0.25f);
-    p = fmaf(q, p, 0.33333333f);
-    p = fmaf(q, p, 0.5f);
-    p = fmaf(q, p, 1.0f);
-    float t_ser = 2.0f * q * p;
-    float t = (q < 0.015625f) ? t_ser : t_log;   // -2 ln u > 0: t_ser >= 2q >= 2^-32, t_log > 0.03
-    float r = t * rsqrtf(t);
+    __sincosf(th, &s, &c);
+    const float t_log = (-2.0f * 0.69314718055994531f) * __log2f(u);
+    const float t_ser = q * fmaf(q, fmaf(q, 0.66666667f, 1.0f), 2.0f);
+    const float t = (q < 0.015625f) ? t_ser : t_log;   // -2 ln u > 0: t_ser >= 2q >= 2^-32, t_log > 0.03
+    const float r = t * rsqrtf(t);
     x = s * r;
     y = c * r;
 }

@@ -57,7 +57,7 @@ def test_variants_are_bit_identical(nm, kind):
 
 def test_default_configuration(nm):
     m, p = _model(nm, autotune=0), _portfolio(nm, autotune=0)
-    assert m.phase_config(3) == dict(variant=0, chunk=32, state=nm.PHASE_DEFAULT, probe_ms=0.0)
+    assert m.phase_config(3) == dict(variant=1, chunk=32, state=nm.PHASE_DEFAULT, probe_ms=0.0)
     assert p.phase_config(3)["variant"] == 2 and p.phase_config(3)["chunk"] == 32
 
 

@@ -10,7 +10,7 @@ Tolerances (stated here, used below):
     1e-4 of its threshold (|ln(new_count / cur)|, the oracle's margins); at most 0.5 % of outer
     samples; level sums differ only by what the differing outer samples explain;
   * the MLMC estimate of P(L > K) within 3 eps + 4 sigma of an independent full-evaluation
-    Monte Carlo estimate over 2e5 outer samples.
+    Monte Carlo estimate over 2e6 outer samples.
 """
 import numpy as np
 import pytest
@@ -102,22 +102,23 @@ def test_fp32_level_traces_against_fp64(nm, cv):
 
 
 def test_c2_end_to_end(nm):
-    """C2: d = 20, P = 1e4, K = 99 % quantile of L over 1e5 full evaluations (seed 1); the MLMC
-    estimate of P(L > K) agrees with a direct full-evaluation estimate.  eps = 1e-3 here: with
-    uniform sub-sampling and non-adaptive levels the run to the configuration's 1e-4 takes
-    minutes (the starting level moves to ~10, 65k inner samples per outer sample)."""
+    """C2: d = 20, P = 1e4, uniform sub-sampling, 64 * 2^ell inner samples, K = 99 % quantile of L
+    over 1e5 full evaluations (seed 1); the MLMC estimate of P(L > K) agrees with a direct estimate
+    from 2e6 full evaluations (sigma ~ 7e-5).  eps = 3e-4 (about 16 s on a B200): the
+    configuration's relative 1e-2 (1e-4 absolute) takes the same sampler 225 s, with the starting
+    level at 11 and 3.4e13 inner samples."""
     pf = nm.generate_portfolio(nm.PORTFOLIO_C2, 1)
     q = sampler(nm, nm.PREC_FP32, pf, seed=1)
     K = nm.loss_quantile(q, 0.99, 100_000)
     # independent direct estimate of P(L > K) on other outer samples
-    Ld = q.full_loss(62, 0, 200_000)
+    Ld = np.concatenate([q.full_loss(62, k * 500_000, 500_000) for k in range(4)])
     p_direct = float(np.mean(Ld > K))
     sd = np.sqrt(p_direct * (1 - p_direct) / len(Ld))
     s = sampler(nm, nm.PREC_FP32, pf, seed=5, K=K)
-    eps = 1e-3
+    eps = 3e-4
     out = s.mlmc_run(targetTOL=eps, M0=1024, batched=True)
     assert abs(out["Eg"] - p_direct) < 3 * eps + 4 * sd, (out["Eg"], p_direct, sd)
-    assert 0.007 < p_direct < 0.013
+    assert 0.008 < p_direct < 0.012
 
 
 def test_c3_end_to_end_at_its_eps(nm):
