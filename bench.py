@@ -703,6 +703,75 @@ def c4_mlmc_case(args):
     print(json.dumps(line))
 
 
+C2_CONFIG = dict(workload="portfolio: d=20 GBM stocks, P=1e4 European options, uniform sub-sampling, "
+                          "64 * 2^ell inner samples, P(L>K) with K the 99% loss quantile of 1e5 full "
+                          "evaluations", stocks=20, options=10_000, generator_seed=1, tau="1/52", r=0.05,
+                 rho=0.0, sub_sampling="uniform", delta_cv=False, N0=64, beta=2, adaptive_r=0.0,
+                 antithetic=True, eps=1e-4, eps_note="the configuration's relative 1e-2 on P(L>K) ~ 0.01")
+
+
+def c2_case(args):
+    """The C2 portfolio to its eps: K from 1e5 full evaluations (seed 1), a direct estimate of
+    P(L > K) from 2e6 more, then the batched FP32 sampler to 1e-3 (a warm-up that also tunes the
+    levels, then a timed run) and to eps, and the FP64 drop-in on the reference's streams at 1e-3
+    beside the FP32 run at 1e-3."""
+    import numpy as np
+    sys.path.insert(0, PKG)
+    import nmlmc as nm
+    eps = args.eps if args.eps else C2_CONFIG["eps"]
+    pf = nm.generate_portfolio(nm.PORTFOLIO_C2, 1)
+
+    def mk(prec, streams, K, seed):
+        s = nm.Sampler(0, cores=2048, N0=64, beta=2, adaptive_r=0.0, precision=prec, streams=streams, seed=seed)
+        s.set_portfolio(pf, r=0.05, rho=0.0, max_loss=K, tau=nm.TAU_WEEK, subsample=nm.SUB_UNIFORM,
+                        use_delta_cv=False, discount=False)
+        return s
+
+    q = mk(nm.PREC_FP32, nm.STREAMS_OUTER, 0.0, 1)
+    K = nm.loss_quantile(q, 0.99, 100_000)
+    Ld = np.concatenate([q.full_loss(62, k * 500_000, 500_000) for k in range(4)])
+    q.close()
+    p_direct = float(np.mean(Ld > K))
+    sd = float(np.sqrt(p_direct * (1 - p_direct) / len(Ld)))
+    runs = {}
+    clk = None
+
+    def timed(name, s, e, batched):
+        nonlocal clk
+        cs = ClockSampler(0)
+        cs.start()
+        t = time.perf_counter()
+        out = s.mlmc_run(targetTOL=e, M0=1024, batched=batched)
+        wall = time.perf_counter() - t
+        c = cs.stop()
+        clk = clk or c
+        runs[name] = dict(eps=e, value=float(out["level_time"].sum()), e2e=wall, Eg=float(out["Eg"]),
+                          levels=int(out["nlevels"]), starting_level=int(out["starting_level"]),
+                          level_M=[int(x) for x in out["level_M"]], work=float(out["total_work"]))
+
+    s = mk(nm.PREC_FP32, nm.STREAMS_OUTER, K, 3)
+    s.mlmc_run(targetTOL=1e-3, M0=1024, batched=True)          # warm-up: tunes the levels
+    s.configure(seed=5)
+    timed("fp32_batched_1e-3", s, 1e-3, True)
+    s.configure(seed=7)
+    timed("fp32_batched", s, eps, True)
+    s.close()
+    d = mk(nm.PREC_FP64, nm.STREAMS_CORE, K, 5)
+    timed("fp64_dropin_1e-3", d, 1e-3, False)
+    d.close()
+    a = runs["fp32_batched"]
+    line = {"metric": f"time-to-eps (s) for MLMC P(L>K), d=20 portfolio with uniform sub-sampling, eps={eps:g} absolute",
+            "value": a["value"], "unit": "s", "n_gpus": 1, "higher_is_better": False, "dtype": "f32",
+            "data": "synthetic (seeded generator)", "config": dict(C2_CONFIG, eps=eps, K=K),
+            "e2e": {"value": a["e2e"], "unit": "s"}, "runs": runs,
+            "direct_estimate": {"p": p_direct, "sd": sd, "outer_samples": len(Ld)},
+            "speedup_vs_fp64_dropin_at_1e-3": {
+                "value": runs["fp64_dropin_1e-3"]["value"] / runs["fp32_batched_1e-3"]["value"],
+                "e2e": runs["fp64_dropin_1e-3"]["e2e"] / runs["fp32_batched_1e-3"]["e2e"]},
+            "clocks": clk, "vs_baseline": None}
+    print(json.dumps(line))
+
+
 def c3_sampler(nm, device, pfw, K, prec, streams, seed, cores=2048):
     s = nm.Sampler(device, cores=cores, N0=64, beta=2, adaptive_r=ADAPTIVE_R, precision=prec,
                    streams=streams, seed=seed)
@@ -937,10 +1006,10 @@ def main():
     ap.add_argument("--eps", type=float, default=None, help="target RMSE of the large-portfolio line (default 1e-4)")
     ap.add_argument("--schedule-out", default=None,
                     help="write the run's outer samples per level (bench_schedule.json format) here")
-    ap.add_argument("--case", default=None, choices=["c1", "small", "c3-level", "c3-table", "c3-sweep", "c4",
+    ap.add_argument("--case", default=None, choices=["c1", "c2", "small", "c3-level", "c3-table", "c3-sweep", "c4",
                                                       "c4-small", "c4-mlmc", "ref-model"],
                     help="default: the large portfolio to eps; c1: the adaptive model problem to eps; "
-                         "small, c3-level, c3-table, c3-sweep, c4-small: profiling cases; c4: the "
+                         "c2: the d=20 portfolio with uniform sub-sampling to eps; small, c3-level, c3-table, c3-sweep, c4-small: profiling cases; c4: the "
                          "path-simulated loss with adjoint; c4-mlmc: MLMC of the path-simulated "
                          "portfolio to eps; ref-model: the reference's model main")
     args = ap.parse_args()
@@ -960,6 +1029,8 @@ def main():
         return c3_sweep_case()
     if args.case == "c4-mlmc":
         return c4_mlmc_case(args)
+    if args.case == "c2":
+        return c2_case(args)
     if args.case in ("c4", "c4-small"):
         return c4_case(args, small=args.case == "c4-small")
     if args.case == "ref-model":

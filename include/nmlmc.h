@@ -303,7 +303,9 @@ int nmlmc_sample_levels(nmlmc_ctx* ctx, uint32_t n, const uint32_t* ells, const 
 /* ---- phase-kernel autotuner (batched FP32 path) ----------------------------------------------
  * No counterpart in the reference (its CUDA build has one fixed launch shape).  The phase kernel
  * of the OUTER layout has three register/occupancy variants (0: up to 255 registers per thread,
- * 1: three resident CTAs of 256 threads per SM guaranteed, 2: four) and a chunk length (inner
+ * 1: three resident CTAs of 256 threads per SM guaranteed, 2: four), for portfolios a fourth (3: two
+ * CTAs per SM, with the next inner samples' table gathers issued before the current ones are
+ * evaluated; other kinds run variant 0 for it) and a chunk length (inner
  * samples per thread; power of two in [4, 64] dividing N0; a level's items of n inner samples
  * take n / chunk threads, so it also sets the outer samples per warp).  With autotuning on, the
  * first nmlmc_sample / nmlmc_sample_levels call of a level with enough work times the
@@ -315,7 +317,7 @@ int nmlmc_sample_levels(nmlmc_ctx* ctx, uint32_t n, const uint32_t* ells, const 
  * across processes.  Changing the model, portfolio or configuration drops the tuned (not the
  * pinned) choices.  Tuning applies to NMLMC_PREC_FP32 only. */
 typedef struct nmlmc_phase_config {
-    uint32_t variant;          /* 0, 1, 2 (above)                                                */
+    uint32_t variant;          /* 0, 1, 2, 3 (above)                                             */
     uint32_t chunk;            /* inner samples per thread                                       */
     int32_t state;             /* get: 0 default, 1 autotuned, 2 pinned                          */
     double probe_ms;           /* get: device time of the tuned choice on its probe              */

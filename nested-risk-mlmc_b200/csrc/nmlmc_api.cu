@@ -746,7 +746,8 @@ OuterLevel<RT> outer_level_params(const nmlmc_ctx* c, uint32_t ell, uint64_t M, 
 // parameters on about 20 ms of work (probe_size), from outer samples whose
 // stream indices start at 2^55, far from any real index, so the probe changes no result — and
 // keeps the fastest for the level:
-//   1. the register/occupancy variants 0, 1, 2 at the default chunk length, another than the
+//   1. the register/occupancy variants 0, 1, 2 (and 3 for the portfolio) at the default chunk
+//      length, another than the
 //      default taken only if > 3 % faster;
 //   2. (mode 2, or an explicit nmlmc_autotune_level) half and double the chunk length at the
 //      best variant, taken only if > 3 % faster.
@@ -813,7 +814,8 @@ int tune_level(nmlmc_ctx* c, uint32_t ell, bool chunks) {
     double best_ms;
     NM_CUDA(time_phase_config<RT>(c, ell, Mp, best, best_ms), "autotune probe");
     const uint32_t v0 = best.variant;
-    for (uint32_t v = 0; v < 3; v++) {
+    const uint32_t n_var = c->kind == KIND_PORTFOLIO ? 4u : 3u;   // variant 3: portfolio only
+    for (uint32_t v = 0; v < n_var; v++) {
         if (v == v0) continue;
         PhaseChoice pc = best;
         pc.variant = v;
@@ -1543,7 +1545,7 @@ int nmlmc_set_phase_config(nmlmc_ctx* c, uint32_t ell, const nmlmc_phase_config*
         c->phase[ell] = PhaseChoice{};
         return NMLMC_OK;
     }
-    if (cfg->variant > 2 || !valid_chunk(c->cfg, cfg->chunk)) return set_err(NMLMC_ERR_ARG);
+    if (cfg->variant > 3 || !valid_chunk(c->cfg, cfg->chunk)) return set_err(NMLMC_ERR_ARG);
     PhaseChoice p;
     p.state = 2;
     p.variant = cfg->variant;

@@ -16,10 +16,11 @@
 //
 // Phi(x) = erfc(-x/sqrt 2) / 2 with the rational-Chebyshev erfc of Numerical Recipes in C
 // (2nd ed., §6.2, "erfcc": fractional error below 1.2e-7 for all arguments), its exponential and
-// reciprocal on MUFU (__expf; rcp.approx refined by one Newton-Raphson step).  Measured against double erfc over |x| <= 10 the
-// composite Phi has absolute error <= 1.8e-7 and, where Phi >= 1e-20, relative error <= 8e-6: in
-// the far tail the FP32 rounding of the exponent -z^2 (up to ~43) dominates, not the erfc fit
-// (tests/test_gpu_portfolio.py, bounds 2.5e-7 and 1e-5).  The loss of one option is then within
+// reciprocal on MUFU (ex2.approx; rcp.approx refined by one Newton-Raphson step).  Measured
+// against double erfc over |x| <= 10 the composite Phi has absolute error <= 1.8e-7 and, where
+// Phi >= 1e-20, relative error <= 8e-6: in the far tail the FP32 rounding of the exponent (up to
+// ~72 in base 2) dominates, not the erfc fit (tests/test_gpu_portfolio.py, bounds 2.5e-7 and 1e-5).
+// The loss of one option is then within
 // 1e-6 * (|wV0| + |wR R| + |wK| + |cv| (R + S0)) of the double-precision value.
 #pragma once
 #include <cstdint>
@@ -61,25 +62,30 @@ __device__ __forceinline__ float rcp_nr(float x) {
     return fmaf(r, fmaf(-x, r, 1.0f), r);
 }
 
-// erfc(z) for z >= 0 on the SFU (Numerical Recipes "erfcc" coefficients).
-__device__ __forceinline__ float erfc_pos_fast(float z) {
-    float t = rcp_nr(fmaf(0.5f, z, 1.0f));
-    float p = fmaf(t, 0.17087277f, -0.82215223f);
-    p = fmaf(t, p, 1.48851587f);
-    p = fmaf(t, p, -1.13520398f);
-    p = fmaf(t, p, 0.27886807f);
-    p = fmaf(t, p, -0.18628806f);
-    p = fmaf(t, p, 0.09678418f);
-    p = fmaf(t, p, 0.37409196f);
-    p = fmaf(t, p, 1.00002368f);
-    p = fmaf(t, p, -1.26551223f);
-    return t * __expf(fmaf(-z, z, p));
+// 2^x on the SFU (PTX ex2.approx; results below 2^-126 flush to zero).
+__device__ __forceinline__ float ex2_sfu(float x) {
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
 }
 
-// Phi(x) = erfc(-x / sqrt 2) / 2 for any x.
+// Phi(x) for any x from h = Phi(-|x|) = erfc(z) / 2, z = |x| / sqrt 2, with the Numerical Recipes
+// "erfcc" form erfc(z) = t exp(-z^2 + P(t)), t = 1 / (1 + z / 2).  The coefficients below are
+// erfcc's times log2(e), the constant term also less 1 (the half), so that
+// h = t 2^(P2(t) - |x|^2 log2(e) / 2) takes one SFU exponential and no further products.
 __device__ __forceinline__ float norm_cdf_fast(float x) {
-    const float z = fabsf(x) * 0.70710678118654752f;
-    const float h = 0.5f * erfc_pos_fast(z);          // Phi(-|x|)
+    const float a = fabsf(x);
+    const float t = rcp_nr(fmaf(a, 0.35355339f, 1.0f));    // 1 / (1 + |x| / (2 sqrt 2))
+    float p = fmaf(t, 0.24651730f, -1.18611491f);
+    p = fmaf(t, p, 2.14747453f);
+    p = fmaf(t, p, -1.63775313f);
+    p = fmaf(t, p, 0.40232158f);
+    p = fmaf(t, p, -0.26875687f);
+    p = fmaf(t, p, 0.13963005f);
+    p = fmaf(t, p, 0.53970063f);
+    p = fmaf(t, p, 1.44272923f);
+    p = fmaf(t, p, -2.82574821f);
+    const float h = t * ex2_sfu(fmaf(-a, a * 0.72134751f, p));
     return x >= 0.f ? 1.0f - h : h;
 }
 
@@ -92,11 +98,19 @@ __device__ __forceinline__ float option_loss_fast(const FastOption& o, float R, 
     return fmaf(o.cv, R, v);
 }
 
-// The same loss from an alias column: m d1 as above, m s = 1 / (m inv_s) (rcp_nr: within one
-// ulp of the record's m s, the only difference from option_loss_fast).
+// 1 / x from the SFU alone (PTX rcp.approx: relative error below 2^-23, normal x).
+__device__ __forceinline__ float rcp_sfu(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// The same loss from an alias column: m d1 as above, m s = 1 / (m inv_s) from the SFU estimate
+// (within one ulp of the record's m s, the only difference from option_loss_fast; one ulp of s
+// moves Phi(d2) by less than 2e-8).
 __device__ __forceinline__ float column_loss_fast(const FastColumn& c, float R, float lnR) {
     const float d1 = (lnR + c.c1) * c.inv_s;
-    const float d2 = d1 - rcp_nr(c.inv_s);
+    const float d2 = d1 - rcp_sfu(c.inv_s);
     const float n1 = norm_cdf_fast(d1), n2 = norm_cdf_fast(d2);
     const float v = fmaf(c.wR * R, n1, fmaf(c.wK, n2, c.wV0));
     return fmaf(c.cv, R, v);

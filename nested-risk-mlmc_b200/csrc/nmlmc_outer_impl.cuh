@@ -282,7 +282,9 @@ __device__ __forceinline__ FastColumn load_column(const FastColumn* p) {
 // How the FP32 portfolio path draws an option: uniformly (records), from the alias table
 // (alias entry, then record) or from the alias columns (column, and the alias column when the coin
 // says so).
-enum PfMode : int { PF_UNIFORM = 0, PF_ALIAS = 1, PF_COLUMN = 2 };
+// PF_COLUMN_PIPE: the alias columns with the next four samples' gathers issued before the current
+// four are evaluated (the 128-register variant).
+enum PfMode : int { PF_UNIFORM = 0, PF_ALIAS = 1, PF_COLUMN = 2, PF_COLUMN_PIPE = 3 };
 
 // Loss of the option drawn by the 64-bit value v: column j = floor(v P / 2^64), alias coin
 // (v P mod 2^64) >> 32, the option kept when coin < threshold and its alias otherwise (the same
@@ -308,11 +310,48 @@ __device__ __forceinline__ float pf_sample_loss(uint64_t v, const OptionTable<fl
     return option_loss_fast(o, r.x, r.y);
 }
 
+// Four samples of the alias-column path: the Threefry blocks blk, blk + 1 and the four column
+// gathers they select (issued together, not waited for).
+__device__ __forceinline__ void column_issue(const TfKey& key, uint32_t tag, uint64_t blk, const OptionTable<float>& ot,
+                                             FastColumn (&c)[4], uint32_t (&coin)[4]) {
+    uint64_t v[4];
+    threefry2x64(blk, tag, key, v[0], v[1]);
+    threefry2x64(blk + 1, tag, key, v[2], v[3]);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const uint32_t j = (uint32_t)__umul64hi(v[q], (uint64_t)ot.P);
+        coin[q] = (uint32_t)((v[q] * (uint64_t)ot.P) >> 32);
+        c[q] = load_column(ot.fast_col + j);
+    }
+}
+
+// The rest of those four samples: the alias-column gathers of the draws whose coin asks for them,
+// then the four losses, added to the sums in sample order (pairs into the compensated sum).
+template <int PREC, bool S2>
+__device__ __forceinline__ void column_finish(FastColumn (&c)[4], const uint32_t (&coin)[4], const OptionTable<float>& ot,
+                                              const float2* Rrow, float shift, Acc<PREC>& a1, Acc<PREC>& a2) {
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+        if (coin[q] >= c[q].thr) c[q] = load_column(ot.fast_col + (c[q].link >> 8));
+    float x[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const float2 r = Rrow[c[q].link & 0xffu];
+        x[q] = column_loss_fast(c[q], r.x, r.y);
+        if (S2) { x[q] += shift; a2.add_sq(x[q]); }
+    }
+    a1.add2(x[0], x[1]);
+    a1.add2(x[2], x[3]);
+}
+
 // C inner samples of the FP32 portfolio path from Threefry blocks b0, b0 + 1, ... (two samples per
-// block, one 64-bit value each).  Pilots (S2) accumulate the losses shifted by `shift`.  With alias
-// columns the loop takes two blocks (four samples) at a time and issues their four column gathers
-// together, then the alias-column gathers of the draws that need them, so a thread has four
-// samples' L2 round trips in flight at once (4 % faster than two at a time, spills included).
+// block, one 64-bit value each, added to the compensated sum as a pair).  Pilots (S2) accumulate
+// the losses shifted by `shift`.  With alias columns the loop takes two blocks (four samples) at a
+// time and issues their four column gathers together, then the alias-column gathers of the draws
+// that need them, so a thread has four samples' L2 round trips in flight at once (4 % faster than
+// two at a time, spills included).  PF_COLUMN_PIPE keeps two such groups, A and B: B's blocks and
+// column gathers are issued before A's alias gathers and losses, so B's round trip runs while A is
+// evaluated.  Every mode adds the samples to the sums in the same order.
 template <int PREC, uint32_t C, bool S2, int MODE>
 __device__ __forceinline__ void pf_chunk_fast(const TfKey& key, uint32_t tag, uint64_t b0,
                                               const OptionTable<float>& ot, const float2* Rrow, float shift,
@@ -320,27 +359,23 @@ __device__ __forceinline__ void pf_chunk_fast(const TfKey& key, uint32_t tag, ui
     if constexpr (MODE == PF_COLUMN) {
 #pragma unroll 1
         for (uint32_t b = 0; b < C / 2; b += 2) {
-            uint64_t v[4];
-            threefry2x64(b0 + b, tag, key, v[0], v[1]);
-            threefry2x64(b0 + b + 1, tag, key, v[2], v[3]);
             FastColumn c[4];
             uint32_t coin[4];
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const uint32_t j = (uint32_t)__umul64hi(v[q], (uint64_t)ot.P);
-                coin[q] = (uint32_t)((v[q] * (uint64_t)ot.P) >> 32);
-                c[q] = load_column(ot.fast_col + j);
-            }
-#pragma unroll
-            for (int q = 0; q < 4; q++)
-                if (coin[q] >= c[q].thr) c[q] = load_column(ot.fast_col + (c[q].link >> 8));
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const float2 r = Rrow[c[q].link & 0xffu];
-                float x = column_loss_fast(c[q], r.x, r.y);
-                if (S2) x += shift;
-                a1.add(x);
-                if (S2) a2.add_sq(x);
+            column_issue(key, tag, b0 + b, ot, c, coin);
+            column_finish<PREC, S2>(c, coin, ot, Rrow, shift, a1, a2);
+        }
+    } else if constexpr (MODE == PF_COLUMN_PIPE) {
+        constexpr uint32_t G = C / 4;           // groups of four samples
+        FastColumn ca[4], cb[4];
+        uint32_t ka[4], kb[4];
+        column_issue(key, tag, b0, ot, ca, ka);
+#pragma unroll 1
+        for (uint32_t g = 0; g < G; g += 2) {
+            if (g + 1 < G) column_issue(key, tag, b0 + 2 * (g + 1), ot, cb, kb);
+            column_finish<PREC, S2>(ca, ka, ot, Rrow, shift, a1, a2);
+            if (g + 1 < G) {
+                if (g + 2 < G) column_issue(key, tag, b0 + 2 * (g + 2), ot, ca, ka);
+                column_finish<PREC, S2>(cb, kb, ot, Rrow, shift, a1, a2);
             }
         }
     } else {
@@ -348,13 +383,13 @@ __device__ __forceinline__ void pf_chunk_fast(const TfKey& key, uint32_t tag, ui
         for (uint32_t b = 0; b < C / 2; b++) {
             uint64_t v[2];
             threefry2x64(b0 + b, tag, key, v[0], v[1]);
+            float x[2];
 #pragma unroll
             for (int q = 0; q < 2; q++) {
-                float x = pf_sample_loss<MODE>(v[q], ot, Rrow);
-                if (S2) x += shift;
-                a1.add(x);
-                if (S2) a2.add_sq(x);
+                x[q] = pf_sample_loss<MODE>(v[q], ot, Rrow);
+                if (S2) { x[q] += shift; a2.add_sq(x[q]); }
             }
+            a1.add2(x[0], x[1]);
         }
     }
 }
@@ -415,7 +450,7 @@ __device__ __forceinline__ void* user_ws(const OuterBuffers& B, uint32_t item) {
 // sample_inner, model_sampler.cpp:66-79, or the portfolio's inner value above).
 // C (inner samples per chunk) is a compile-time constant so the independent Threefry blocks of a
 // chunk can be interleaved (two at a time) for instruction-level parallelism.
-template <class RT, int KIND, int PREC, uint32_t C, bool S2, class S>
+template <class RT, int KIND, int PREC, uint32_t C, bool S2, class S, bool PIPE>
 __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t item, uint32_t tag,
                                              uint64_t s0, uint64_t count, float shift, const float2* srow,
                                              Acc<PREC>& a1, Acc<PREC>& a2, double& work) {
@@ -489,8 +524,9 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
             const float2* grow = reinterpret_cast<const float2*>(D.B.Rt) + (size_t)item * ot.Q;
             const uint64_t b0 = s0 >> 1;
             if (ot.fast_col) {
-                if (srow) pf_chunk_fast<PREC, C, S2, PF_COLUMN>(key, tag, b0, ot, srow, shift, a1, a2);
-                else pf_chunk_fast<PREC, C, S2, PF_COLUMN>(key, tag, b0, ot, grow, shift, a1, a2);
+                constexpr int CM = PIPE ? PF_COLUMN_PIPE : PF_COLUMN;
+                if (srow) pf_chunk_fast<PREC, C, S2, CM>(key, tag, b0, ot, srow, shift, a1, a2);
+                else pf_chunk_fast<PREC, C, S2, CM>(key, tag, b0, ot, grow, shift, a1, a2);
             } else if (ot.subsample == SUB_UNIFORM) {
                 if (srow) pf_chunk_fast<PREC, C, S2, PF_UNIFORM>(key, tag, b0, ot, srow, shift, a1, a2);
                 else pf_chunk_fast<PREC, C, S2, PF_UNIFORM>(key, tag, b0, ot, grow, shift, a1, a2);
@@ -563,16 +599,16 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
     }
 }
 
-template <class RT, int KIND, int PREC, bool S2, class S>
+template <class RT, int KIND, int PREC, bool S2, class S, bool PIPE>
 __device__ __forceinline__ void eval_chunk_s(const DevLevel<RT>& D, uint32_t item, uint32_t tag,
                                              uint64_t s0, uint64_t count, uint32_t C, float shift,
                                              const float2* srow, Acc<PREC>& a1, Acc<PREC>& a2, double& work) {
     switch (C) {
-    case 64: eval_chunk_c<RT, KIND, PREC, 64, S2, S>(D, item, tag, s0, count, shift, srow, a1, a2, work); break;
-    case 32: eval_chunk_c<RT, KIND, PREC, 32, S2, S>(D, item, tag, s0, count, shift, srow, a1, a2, work); break;
-    case 16: eval_chunk_c<RT, KIND, PREC, 16, S2, S>(D, item, tag, s0, count, shift, srow, a1, a2, work); break;
-    case 8: eval_chunk_c<RT, KIND, PREC, 8, S2, S>(D, item, tag, s0, count, shift, srow, a1, a2, work); break;
-    default: eval_chunk_c<RT, KIND, PREC, 4, S2, S>(D, item, tag, s0, count, shift, srow, a1, a2, work); break;
+    case 64: eval_chunk_c<RT, KIND, PREC, 64, S2, S, PIPE>(D, item, tag, s0, count, shift, srow, a1, a2, work); break;
+    case 32: eval_chunk_c<RT, KIND, PREC, 32, S2, S, PIPE>(D, item, tag, s0, count, shift, srow, a1, a2, work); break;
+    case 16: eval_chunk_c<RT, KIND, PREC, 16, S2, S, PIPE>(D, item, tag, s0, count, shift, srow, a1, a2, work); break;
+    case 8: eval_chunk_c<RT, KIND, PREC, 8, S2, S, PIPE>(D, item, tag, s0, count, shift, srow, a1, a2, work); break;
+    default: eval_chunk_c<RT, KIND, PREC, 4, S2, S, PIPE>(D, item, tag, s0, count, shift, srow, a1, a2, work); break;
     }
 }
 
@@ -583,12 +619,13 @@ __device__ __forceinline__ void eval_chunk_s(const DevLevel<RT>& D, uint32_t ite
 // threshold that the adaptive rule compares with the spread), so the one-pass variance
 // s2 - s1^2 / n does not cancel where the decision is close; the final phase accumulates d.
 // `srow`: the outer sample's R_tau row in shared memory, or nullptr (FP32 portfolio path).
-template <class RT, int KIND, int PREC, class S>
+// PIPE: the pipelined alias-column loop (the 128-register variant of the phase kernel).
+template <class RT, int KIND, int PREC, class S, bool PIPE>
 __device__ __forceinline__ void eval_chunk(const DevLevel<RT>& D, uint32_t item, uint32_t tag,
                                            uint64_t s0, uint64_t count, uint32_t C, bool want_s2, RT start,
                                            const float2* srow, Acc<PREC>& a1, Acc<PREC>& a2, double& work) {
-    if (want_s2) eval_chunk_s<RT, KIND, PREC, true, S>(D, item, tag, s0, count, C, (float)start, srow, a1, a2, work);
-    else eval_chunk_s<RT, KIND, PREC, false, S>(D, item, tag, s0, count, C, 0.f, srow, a1, a2, work);
+    if (want_s2) eval_chunk_s<RT, KIND, PREC, true, S, PIPE>(D, item, tag, s0, count, C, (float)start, srow, a1, a2, work);
+    else eval_chunk_s<RT, KIND, PREC, false, S, PIPE>(D, item, tag, s0, count, C, 0.f, srow, a1, a2, work);
 }
 
 // ---- segments of uniform chunk count ------------------------------------------------------
@@ -619,25 +656,37 @@ __device__ __forceinline__ bool pilot_decide(const DevLevel<RT>& D, const Seg& g
     const OuterLevel<RT>& L = D.L;
     const CountParams& cp = (g.mode == 0) ? L.cf : L.cc;
     const uint64_t cur = g.count;
-    RT delta2;
+    bool done;
     if (PREC == PREC_FP32) {
-        // the sums are of d + start (eval_chunk): their mean is the distance start + mean(d)
-        float s1 = (float)a1.value(), s2 = (float)a2.value(), n = (float)cur;
-        float dist = div_count(s1, cur);
-        float var = __fdiv_rn(__fsub_rn(s2, __fmul_rn(s1, dist)), n - 1.0f);
-        delta2 = (RT)__fdiv_rn(__fmul_rn(dist, dist), var);
+        // the sums are of d + start (eval_chunk): their mean is the distance start + mean(d);
+        // num = (n - 1) var, delta2 = dist^2 (n - 1) / num
+        const float s1 = (float)a1.value(), s2 = (float)a2.value(), n = (float)cur;
+        const float dist = div_count(s1, cur);
+        const float num = __fsub_rn(s2, __fmul_rn(s1, dist));
+        if (L.adaptive_r == (RT)2) {
+            const float delta2 = __fdiv_rn(__fmul_rn(dist, dist), __fdiv_rn(num, n - 1.0f));
+            done = __fdiv_rn((float)cp.tmp, delta2) <= n;
+        } else {
+            // newc = tmp delta2^(-r/2) <= cur compared in base-2 logarithms on the SFU: no pow and
+            // no division (a decision moves only within ~1e-5 relative of its threshold).  The
+            // degenerate sums decide as the power form does: delta2 = 0 (dist = 0) continues,
+            // delta2 = inf (num = 0) stops, a negative or 0/0 delta2 (NaN) continues.
+            const float l2d = fmaf(2.0f, __log2f(fabsf(dist)), __log2f(n - 1.0f) - __log2f(num));
+            done = fmaf(-0.5f * (float)L.adaptive_r, l2d, __log2f((float)cp.tmp)) <= __log2f(n);
+        }
     } else {
         double s1 = (double)a1.value(), s2 = (double)a2.value();
         RT out_var = to_rt<RT>(__dsub_rn(__ddiv_rn(s2, (double)(cur - 1)),
                                          __ddiv_rn(__dmul_rn(s1, s1), (double)(cur * (cur - 1)))));
         RT dist = xadd(start, to_rt<RT>(div_count(s1, cur)));
-        delta2 = xdiv(xmul(dist, dist), out_var);
+        RT delta2 = xdiv(xmul(dist, dist), out_var);
+        RT newc;
+        if (L.adaptive_r == (RT)2) newc = xdiv((RT)cp.tmp, delta2);
+        else newc = xmul(xpow(delta2, xdiv(-L.adaptive_r, (RT)2)), (RT)cp.tmp);
+        done = newc <= (RT)cur;
     }
-    RT newc;
-    if (L.adaptive_r == (RT)2) newc = xdiv((RT)cp.tmp, delta2);
-    else newc = xmul(xpow(delta2, xdiv(-L.adaptive_r, (RT)2)), (RT)cp.tmp);
     uint32_t* cnt = (g.mode == 0) ? D.B.cnt_f : D.B.cnt_c;
-    if (newc <= (RT)cur) { cnt[item] = (uint32_t)cur; return false; }
+    if (done) { cnt[item] = (uint32_t)cur; return false; }
     const uint64_t nxt = cur * 2;
     if (cp.max_count <= 2 * nxt) { cnt[item] = (uint32_t)cp.max_count; return false; }
     return true;
@@ -718,8 +767,9 @@ __device__ __forceinline__ void final_item(const DevLevel<RT>& D, uint32_t item,
 // The batched form of kernel_sample's per-outer-sample loop (nested_sampler.hpp:369-485): pilot
 // and final phases of many outer samples drained from device work queues.
 // MINB = CTAs per SM the register allocation must allow (1: up to 255 registers per thread,
-// 3: 80, 4: 64) — the register/occupancy variants the autotuner chooses between.  The variants
-// run the same arithmetic in the same order, so their results are identical.
+// 2: 128 with the pipelined alias-column loop, 3: 80, 4: 64) — the register/occupancy variants the
+// autotuner chooses between.  The variants run the same arithmetic in the same order, so their
+// results are identical.
 template <class RT, int KIND, int PREC, int MINB, class S = NoSampler>
 __global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet SS, TraceRec* trace) {
     __shared__ Acc<PREC> sm_a1[kWarps];
@@ -800,7 +850,7 @@ __global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet SS
                 Acc<PREC> a1, a2;
                 a1.zero();
                 a2.zero();
-                if (valid) eval_chunk<RT, KIND, PREC, S>(D, item, g.tag, (uint64_t)j * C, g.count, C, pilot, start, srow, a1, a2, wsum);
+                if (valid) eval_chunk<RT, KIND, PREC, S, MINB == 2>(D, item, g.tag, (uint64_t)j * C, g.count, C, pilot, start, srow, a1, a2, wsum);
                 const float coeff = (float)gs / (float)nch;     // 1 / groups (a power of two)
                 float ind = 0.f;
                 if (!pilot && gs == 1) ind = phi_of<KIND, S, RT>(inner_mean<RT, PREC>(start, a1, csmall), coeff);
@@ -891,7 +941,7 @@ __global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet SS
                     Acc<PREC> a1, a2;
                     a1.zero();
                     a2.zero();
-                    eval_chunk<RT, KIND, PREC, S>(D, item, g.tag, (uint64_t)j * C, g.count, C, pilot, start, srow, a1, a2, wsum);
+                    eval_chunk<RT, KIND, PREC, S, MINB == 2>(D, item, g.tag, (uint64_t)j * C, g.count, C, pilot, start, srow, a1, a2, wsum);
                     float ind = 0.f;
                     if (!pilot && gs == 1) ind = phi_of<KIND, S, RT>(inner_mean<RT, PREC>(start, a1, csmall), coeff);
                     for (uint32_t m = 1; m < 32; m <<= 1) {
@@ -1127,7 +1177,9 @@ static void launch_phase_v(const DevLevel<RT>& D, const SegSet& SS, TraceRec* tr
 }
 
 // The FP32 path has three register/occupancy variants (OuterLevel::variant 0, 1, 2 -> 1, 3, 4
-// resident CTAs per SM guaranteed); the parity precisions run variant 0, the FP32 kernel of
+// resident CTAs per SM guaranteed), and the portfolio a fourth (3 -> 2 CTAs per SM, 128 registers,
+// the pipelined alias-column loop; other kinds run variant 0 for it); the parity precisions run
+// variant 0, the FP32 kernel of
 // path-simulated portfolios three CTAs per SM (80 registers, no spills; its FP64 path states and
 // exponentials leave one CTA per SM at the compiler's own choice).
 template <class RT, int KIND, int PREC, class S = NoSampler>
@@ -1135,6 +1187,8 @@ static void launch_phase(const DevLevel<RT>& D, const SegSet& SS, TraceRec* trac
     if constexpr (PREC == PREC_FP32 && KIND != KIND_USER && KIND != KIND_PF_PATHS) {
         if (D.L.variant == 1) return launch_phase_v<RT, KIND, PREC, 3>(D, SS, trace, stream);
         if (D.L.variant == 2) return launch_phase_v<RT, KIND, PREC, 4>(D, SS, trace, stream);
+        if constexpr (KIND == KIND_PORTFOLIO)
+            if (D.L.variant == 3) return launch_phase_v<RT, KIND, PREC, 2>(D, SS, trace, stream);
     }
     launch_phase_v<RT, KIND, PREC, (KIND == KIND_PF_PATHS && PREC == PREC_FP32) ? 3 : 1, S>(D, SS, trace, stream);
 }

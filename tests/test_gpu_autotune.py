@@ -1,8 +1,8 @@
 """Phase-kernel autotuner of the batched FP32 path (nmlmc_set_autotune / nmlmc_autotune_level /
 nmlmc_get_phase_config / nmlmc_set_phase_config).
 
-* The three register/occupancy variants run the same arithmetic: bit-identical level sums and
-  per-outer-sample traces on the same streams.
+* The register/occupancy variants (the portfolio's pipelined one included) run the same
+  arithmetic: bit-identical level sums and per-outer-sample traces on the same streams.
 * Tuning probes use stream indices far from the real ones: a tuned call returns exactly what the
   same configuration returns when pinned in a context that never tuned.
 * Another chunk length regroups the FP32 compensated inner sums: results stay within the FP32
@@ -43,7 +43,7 @@ def _same(a, b):
 def test_variants_are_bit_identical(nm, kind):
     ell, M = (6, 6000) if kind == "model" else (4, 3000)
     ref = None
-    for v in (0, 1, 2):
+    for v in (0, 1, 2, 3):                      # 3: the portfolio's pipelined variant (variant 0 elsewhere)
         s = _model(nm, autotune=0) if kind == "model" else _portfolio(nm, autotune=0)
         s.set_phase_config(ell, variant=v)
         assert s.phase_config(ell)["state"] == nm.PHASE_PINNED and s.phase_config(ell)["variant"] == v
@@ -115,7 +115,7 @@ def test_explicit_tuning_and_chunk_bound(nm):
 def test_invalid_and_unpinned_configurations(nm):
     s = _model(nm, autotune=0)
     with pytest.raises(nm.NmlmcError):
-        s.set_phase_config(2, variant=3)
+        s.set_phase_config(2, variant=4)
     with pytest.raises(nm.NmlmcError):
         s.set_phase_config(2, chunk=24)          # not a power of two
     with pytest.raises(nm.NmlmcError):
