@@ -16,10 +16,10 @@
 //
 // Phi(x) = erfc(-x/sqrt 2) / 2 with the rational-Chebyshev erfc of Numerical Recipes in C
 // (2nd ed., §6.2, "erfcc": fractional error below 1.2e-7 for all arguments), its exponential and
-// reciprocal on MUFU (ex2.approx; rcp.approx refined by one Newton-Raphson step).  Measured
-// against double erfc over |x| <= 10 the composite Phi has absolute error <= 1.8e-7 and, where
-// Phi >= 1e-20, relative error <= 8e-6: in the far tail the FP32 rounding of the exponent (up to
-// ~72 in base 2) dominates, not the erfc fit (tests/test_gpu_portfolio.py, bounds 2.5e-7 and 1e-5).
+// reciprocal on MUFU (ex2.approx, rcp.approx).  Measured against double erfc over |x| <= 10 the
+// composite Phi has absolute error <= 2.1e-7 and, where Phi >= 1e-20, relative error <= 5e-6: in
+// the far tail the FP32 rounding of the exponent (up to ~72 in base 2) dominates, not the erfc fit
+// (tests/test_gpu_portfolio.py, bounds 2.5e-7 and 1e-5).
 // The loss of one option is then within
 // 1e-6 * (|wV0| + |wR R| + |wK| + |cv| (R + S0)) of the double-precision value.
 #pragma once
@@ -52,14 +52,11 @@ constexpr uint32_t kColumnMaxStocks = 256;
 constexpr uint32_t kColumnMaxOptions = 1u << 24;
 
 #ifdef __CUDACC__
-// 1 / x for normal x: the SFU estimate (PTX rcp.approx, relative error below 2^-23) refined by one
-// Newton-Raphson step in FMA form, e = 1 - x r, r' = r + r e (Markstein, IBM J. Res. Dev. 34(1),
-// 1990): the step squares the estimate's relative error, so r' is within half an ulp plus 2^-45
-// relative of 1 / x.
-__device__ __forceinline__ float rcp_nr(float x) {
+// 1 / x from the SFU alone (PTX rcp.approx: relative error below 2^-23, normal x).
+__device__ __forceinline__ float rcp_sfu(float x) {
     float r;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return fmaf(r, fmaf(-x, r, 1.0f), r);
+    return r;
 }
 
 // 2^x on the SFU (PTX ex2.approx; results below 2^-126 flush to zero).
@@ -75,7 +72,7 @@ __device__ __forceinline__ float ex2_sfu(float x) {
 // h = t 2^(P2(t) - |x|^2 log2(e) / 2) takes one SFU exponential and no further products.
 __device__ __forceinline__ float norm_cdf_fast(float x) {
     const float a = fabsf(x);
-    const float t = rcp_nr(fmaf(a, 0.35355339f, 1.0f));    // 1 / (1 + |x| / (2 sqrt 2))
+    const float t = rcp_sfu(fmaf(a, 0.35355339f, 1.0f));    // 1 / (1 + |x| / (2 sqrt 2))
     float p = fmaf(t, 0.24651730f, -1.18611491f);
     p = fmaf(t, p, 2.14747453f);
     p = fmaf(t, p, -1.63775313f);
@@ -96,13 +93,6 @@ __device__ __forceinline__ float option_loss_fast(const FastOption& o, float R, 
     const float n1 = norm_cdf_fast(d1), n2 = norm_cdf_fast(d2);
     const float v = fmaf(o.wR * R, n1, fmaf(o.wK, n2, o.wV0));
     return fmaf(o.cv, R, v);
-}
-
-// 1 / x from the SFU alone (PTX rcp.approx: relative error below 2^-23, normal x).
-__device__ __forceinline__ float rcp_sfu(float x) {
-    float r;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
 }
 
 // The same loss from an alias column: m d1 as above, m s = 1 / (m inv_s) from the SFU estimate

@@ -232,10 +232,19 @@ __device__ __forceinline__ RT pf_value(const OptionTable<RT>& ot, const RT* Rrow
 // exact in every precision.  Uniform sub-sampling takes j (prob 1 / P); importance sub-sampling
 // (Subsampling::Random) flips the column's alias coin (v P mod 2^64) >> 32 — O(1) instead of the
 // reference's CDF binary search, the distribution of the table's exact masses phat.
+// j and the coin from two 32 x 32 -> 64-bit products (P < 2^32): v P = 2^32 (v_hi P + (v_lo P >> 32))
+// + (v_lo P mod 2^32), and the bracket stays below 2^64.
+__device__ __forceinline__ void draw_column(uint64_t v, uint32_t P, uint32_t& j, uint32_t& coin) {
+    const uint64_t lo = (uint64_t)(uint32_t)v * P;
+    const uint64_t hi = (uint64_t)(uint32_t)(v >> 32) * P + (lo >> 32);
+    j = (uint32_t)(hi >> 32);
+    coin = (uint32_t)hi;
+}
+
 __device__ __forceinline__ uint32_t pf_index(const uint2* alias, uint32_t P, uint64_t v) {
-    const uint32_t j = (uint32_t)__umul64hi(v, (uint64_t)P);
+    uint32_t j, coin;
+    draw_column(v, P, j, coin);
     if (!alias) return j;
-    const uint32_t coin = (uint32_t)((v * (uint64_t)P) >> 32);
     const uint2 e = alias[j];
     return coin < e.x ? j : e.y;
 }
@@ -291,9 +300,9 @@ enum PfMode : int { PF_UNIFORM = 0, PF_ALIAS = 1, PF_COLUMN = 2, PF_COLUMN_PIPE 
 // option in every mode); Rrow holds (R, ln R) per stock of this outer sample.
 template <int MODE>
 __device__ __forceinline__ float pf_sample_loss(uint64_t v, const OptionTable<float>& ot, const float2* Rrow) {
-    const uint32_t j = (uint32_t)__umul64hi(v, (uint64_t)ot.P);
+    uint32_t j, coin;
+    draw_column(v, ot.P, j, coin);
     if (MODE == PF_COLUMN) {
-        const uint32_t coin = (uint32_t)((v * (uint64_t)ot.P) >> 32);
         FastColumn c = load_column(ot.fast_col + j);
         if (coin >= c.thr) c = load_column(ot.fast_col + (c.link >> 8));
         const float2 r = Rrow[c.link & 0xffu];
@@ -301,7 +310,6 @@ __device__ __forceinline__ float pf_sample_loss(uint64_t v, const OptionTable<fl
     }
     uint32_t i = j;
     if (MODE == PF_ALIAS) {
-        const uint32_t coin = (uint32_t)((v * (uint64_t)ot.P) >> 32);
         const uint2 e = load_alias(ot.alias + j);
         i = coin < e.x ? j : e.y;
     }
@@ -319,8 +327,8 @@ __device__ __forceinline__ void column_issue(const TfKey& key, uint32_t tag, uin
     threefry2x64(blk + 1, tag, key, v[2], v[3]);
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-        const uint32_t j = (uint32_t)__umul64hi(v[q], (uint64_t)ot.P);
-        coin[q] = (uint32_t)((v[q] * (uint64_t)ot.P) >> 32);
+        uint32_t j;
+        draw_column(v[q], ot.P, j, coin[q]);
         c[q] = load_column(ot.fast_col + j);
     }
 }

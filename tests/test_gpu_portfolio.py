@@ -37,7 +37,7 @@ def sampler(nm, prec, pf, seed=0, **kw):
 def test_fast_norm_cdf_bound(nm):
     """Phi of the FP32 Black-Scholes (rational erfc, SFU exponential and reciprocal) against the
     double-precision Phi over |x| <= 10: absolute error <= 2.5e-7; relative error <= 1e-5 where
-    Phi >= 1e-20 (measured 1.8e-7 and 8e-6; the FP32 exponent -z^2 limits the far tail)."""
+    Phi >= 1e-20 (measured 2.0e-7 and 4.5e-6; the FP32 exponent limits the far tail)."""
     from math import erfc, sqrt
     x = np.concatenate([np.linspace(-10, 10, 200001), np.random.default_rng(1).uniform(-10, 10, 100000)])
     x = x.astype(np.float32)
@@ -104,9 +104,9 @@ def test_fp32_level_traces_against_fp64(nm, cv):
 def test_c2_end_to_end(nm):
     """C2: d = 20, P = 1e4, uniform sub-sampling, 64 * 2^ell inner samples, K = 99 % quantile of L
     over 1e5 full evaluations (seed 1); the MLMC estimate of P(L > K) agrees with a direct estimate
-    from 2e6 full evaluations (sigma ~ 7e-5).  eps = 3e-4 (about 16 s on a B200): the
-    configuration's relative 1e-2 (1e-4 absolute) takes the same sampler 225 s, with the starting
-    level at 11 and 3.4e13 inner samples."""
+    from 2e6 full evaluations (sigma ~ 7e-5).  eps = 3e-4 (about 15 s on a B200): the
+    configuration's relative 1e-2 (1e-4 absolute) takes the same sampler about 170 s, with the
+    starting level at 11 and 3e13 inner samples (bench.py --case c2)."""
     pf = nm.generate_portfolio(nm.PORTFOLIO_C2, 1)
     q = sampler(nm, nm.PREC_FP32, pf, seed=1)
     K = nm.loss_quantile(q, 0.99, 100_000)
