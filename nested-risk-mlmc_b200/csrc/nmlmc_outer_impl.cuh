@@ -458,6 +458,128 @@ __device__ __forceinline__ void* user_ws(const OuterBuffers& B, uint32_t item) {
 // sample_inner, model_sampler.cpp:66-79, or the portfolio's inner value above).
 // C (inner samples per chunk) is a compile-time constant so the independent Threefry blocks of a
 // chunk can be interleaved (two at a time) for instruction-level parallelism.
+// ---- path-simulated portfolio, FP32 -------------------------------------------------------
+// Steps N_l = beta^L of an Unbiased level (false when h0 N_l exceeds kMaxPathSteps).
+__device__ __forceinline__ bool level_steps(const OptionTable<float>& ot, uint32_t Lv, uint64_t& N_l) {
+    N_l = 1;
+    bool ok = true;
+    for (uint32_t i = 0; i < Lv && ok; i++) {
+        N_l *= ot.dt_beta;
+        ok = N_l * ot.dt_h0inv <= kMaxPathSteps;
+    }
+    return ok && N_l * ot.dt_h0inv <= kMaxPathSteps;
+}
+
+// The Unbiased level of the inner sample with path namespace ns, drawn in double as the FP64 path
+// draws it (sample_inner_unbiased, portfolio_sampler.cpp:521-537), and its steps.
+__device__ __forceinline__ bool level_fp32(const OptionTable<float>& ot, const TfKey& key, uint64_t ns,
+                                           uint32_t& Lv, uint64_t& N_l) {
+    uint64_t u0, u1;
+    threefry2x64(0, ns | kPathUniform, key, u0, u1);
+    const double u = __dadd_rn(__dmul_rn((double)(uint32_t)u0, 0x1p-32), 0x1p-33);
+    const double qL = log(u) / (log((double)ot.dt_beta) * (double)ot.dt_prob_expo);
+    Lv = (uint32_t)floor(qL);
+    return level_steps(ot, Lv, N_l);
+}
+
+// Inner samples of a chunk of at most kPathSortChunk per thread are evaluated in the order of
+// their cost class (0 Black-Scholes, 1 Exact, 2 + L for an Unbiased option at level L <= 12, 15
+// beyond), each thread its own order: the Unbiased level makes a sample's cost vary by powers of
+// beta, and in sample order every step of a warp waits for the longest path among its 32 lanes
+// (about 8x the mean at beta = 2, P(L) ~ 2^(-1.5 L)).  A first pass draws every sample's option
+// and level and keeps the option index and class in shared memory (5 bytes per sample and
+// thread); the second evaluates them cheapest class first.  The sums receive the same values in
+// another order.
+constexpr uint32_t kPathSortChunk = 32;
+constexpr size_t kPathSortSmemBytes = (size_t)kPathSortChunk * kTile * (sizeof(uint32_t) + 1);
+
+template <uint32_t C, bool S2, int PREC>
+__device__ __forceinline__ void pf_paths_sorted(const DevLevel<float>& D, const TfKey& key, uint32_t tag, uint64_t s0,
+                                                const float* Rrow, float shift, Acc<PREC>& a1, Acc<PREC>& a2,
+                                                double& work) {
+    static_assert(C <= kPathSortChunk, "sorted path chunk");
+    extern __shared__ float2 k_phase_rows[];     // the phase kernel's dynamic shared memory
+    const OptionTable<float>& ot = D.L.ot;
+    uint32_t* jbuf = reinterpret_cast<uint32_t*>(k_phase_rows) + threadIdx.x;                 // [q * kTile]
+    uint8_t* cbuf = reinterpret_cast<uint8_t*>(reinterpret_cast<uint32_t*>(k_phase_rows) + kPathSortChunk * kTile) +
+                    threadIdx.x;
+    // pass 1: option, class; the samples of classes {0, 1, 2}, 3, 4, 5, 6 and >= 7 as bit sets
+    uint32_t m0 = 0, m1 = 0, m2 = 0, m3 = 0, m4 = 0, m5 = 0;
+#pragma unroll 1
+    for (uint32_t b = 0; b < C / 2; b++) {
+        uint64_t v[2];
+        threefry2x64((s0 >> 1) + b, tag, key, v[0], v[1]);
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const uint32_t q = 2 * b + h;
+            float prob;
+            const uint32_t j = pf_pick<float>(ot, v[h], prob);
+            uint32_t c = 0;
+            if (j >= ot.m_off[1]) {
+                if (j < ot.m_off[2]) {
+                    c = 1;
+                } else {
+                    uint32_t Lv;
+                    uint64_t N_l;
+                    const bool ok = level_fp32(ot, key, path_ns(tag, s0 + q), Lv, N_l);
+                    c = (ok && Lv <= 12) ? 2 + Lv : 15u;
+                }
+            }
+            jbuf[q * kTile] = j;
+            cbuf[q * kTile] = (uint8_t)c;
+            const uint32_t bit = 1u << q;
+            if (c <= 2) m0 |= bit;
+            else if (c == 3) m1 |= bit;
+            else if (c == 4) m2 |= bit;
+            else if (c == 5) m3 |= bit;
+            else if (c == 6) m4 |= bit;
+            else m5 |= bit;
+        }
+    }
+    // pass 2: cheapest class first, sample order within a set
+#pragma unroll 1
+    for (uint32_t k = 0; k < C; k++) {
+        uint32_t q;
+        if (m0) { q = __ffs(m0) - 1; m0 &= m0 - 1; }
+        else if (m1) { q = __ffs(m1) - 1; m1 &= m1 - 1; }
+        else if (m2) { q = __ffs(m2) - 1; m2 &= m2 - 1; }
+        else if (m3) { q = __ffs(m3) - 1; m3 &= m3 - 1; }
+        else if (m4) { q = __ffs(m4) - 1; m4 &= m4 - 1; }
+        else { q = __ffs(m5) - 1; m5 &= m5 - 1; }
+        const uint32_t j = jbuf[q * kTile];
+        const uint32_t c = cbuf[q * kTile];
+        const float prob = ot.subsample == SUB_UNIFORM ? ot.inv_count_prob : ot.phat[j];
+        float val;
+        if (c == 0) {
+            val = pf_value<float, 2>(ot, Rrow, j);
+            work += (double)ot.W_est[j];
+        } else {
+            const uint64_t ns = path_ns(tag, s0 + q);
+            OuterPathNormals<float, PREC_FP32> nz{key, ns, 0, false, 0.f, 0};
+            const float Rs = Rrow[ot.stock_ind[j] * 2];
+            if (c == 1) {
+                val = inner_exact_fast(ot, Rs, j, nz, work);
+            } else {
+                uint32_t Lv;
+                uint64_t N_l;
+                bool ok;
+                if (c < 15) { Lv = c - 2; ok = level_steps(ot, Lv, N_l); }
+                else ok = level_fp32(ot, key, ns, Lv, N_l);
+                if (ok) {
+                    val = inner_unbiased_fast(ot, Rs, j, nz, work, Lv, N_l);
+                } else {                         // beyond kMaxPathSteps: the call fails
+                    atomicOr(D.B.counters + CNT_ERR, 1u);
+                    val = 0.f;
+                }
+            }
+        }
+        float d = __fdiv_rn(val, prob);
+        if (S2) d = __fadd_rn(d, shift);
+        a1.add(d);
+        if (S2) a2.add_sq(d);
+    }
+}
+
 template <class RT, int KIND, int PREC, uint32_t C, bool S2, class S, bool PIPE>
 __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t item, uint32_t tag,
                                              uint64_t s0, uint64_t count, float shift, const float2* srow,
@@ -544,6 +666,11 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
             }
         }
         work += (double)C;
+    } else if constexpr (KIND == KIND_PF_PATHS && PREC == PREC_FP32 && C <= kPathSortChunk) {
+        if constexpr (sizeof(RT) == 4) {
+            const float* Rrow = reinterpret_cast<const float*>(D.B.Rt) + (size_t)item * L.ot.Q * 2;
+            pf_paths_sorted<C, S2, PREC>(D, key, tag, s0, Rrow, shift, a1, a2, work);
+        }
     } else {                                     // portfolio: one 64-bit value per inner sample
         const OptionTable<RT>& ot = L.ot;
         constexpr uint32_t RS = RStride<PREC>::v;
@@ -572,17 +699,7 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
                         uint64_t N_l;
                         bool ok;
                         if constexpr (PREC == PREC_FP32) {
-                            // the level in double, as the FP64 path draws it
-                            const double u = __dadd_rn(__dmul_rn((double)(uint32_t)u0, 0x1p-32), 0x1p-33);
-                            const double qL = log(u) / (log((double)ot.dt_beta) * (double)ot.dt_prob_expo);
-                            Lv = (uint32_t)floor(qL);
-                            N_l = 1;
-                            ok = true;
-                            for (uint32_t i = 0; i < Lv && ok; i++) {
-                                N_l *= ot.dt_beta;
-                                ok = N_l * ot.dt_h0inv <= kMaxPathSteps;
-                            }
-                            ok = ok && N_l * ot.dt_h0inv <= kMaxPathSteps;
+                            ok = level_fp32(ot, key, ns, Lv, N_l);
                         } else {
                             ok = unbiased_level<RT>(ot, u01_word<PREC, RT>((uint32_t)u0), Lv, N_l);
                         }
@@ -1155,7 +1272,9 @@ static __global__ void __launch_bounds__(256) k_reduce_blocks(const double* bloc
 // portfolio path (set as the kernel's maximum once, before the occupancy query and the first
 // launch).
 template <int KIND, int PREC>
-constexpr size_t phase_dyn_smem() { return (KIND == KIND_PORTFOLIO && PREC == PREC_FP32) ? kRowSmemBytes : 0; }
+constexpr size_t phase_dyn_smem() {
+    return PREC != PREC_FP32 ? 0 : KIND == KIND_PORTFOLIO ? kRowSmemBytes : KIND == KIND_PF_PATHS ? kPathSortSmemBytes : 0;
+}
 
 template <class RT, int KIND, int PREC, int MINB, class S = NoSampler>
 static int phase_grid(int cap) {
