@@ -106,3 +106,21 @@ def test_outer_layout_refuses_no_subsampling(nm):
         s.set_portfolio(pf, subsample=nmlmc.SUB_NONE, methods=methods)
         with pytest.raises(nm.NmlmcError):
             s.sample(1, 10)
+
+
+@pytest.mark.parametrize("prec_name", ["fp32", "fp64"])
+def test_outer_paths_beyond_the_step_limit_fail(nm, prec_name):
+    """An Unbiased inner sample whose h0 beta^L steps exceed NMLMC_MAX_PATH_STEPS fails the call
+    with ERR_LIMIT before any path is stepped: with 1 / h0 = 2^24 + 1 every level does."""
+    import nmlmc
+    case = CASES[0]
+    pf = O.synthetic_portfolio(**case["pf"])
+    s = nmlmc.Sampler(N0=case["N0"], beta=case["beta"], adaptive_r=case["r"],
+                      precision=nm.PREC_FP32 if prec_name == "fp32" else nm.PREC_FP64,
+                      streams=nmlmc.STREAMS_OUTER, seed=4)
+    s.set_portfolio(pf, r=0.05, rho=case["rho"], max_loss=case["max_loss"], tau=1 / 52, subsample=case["sub"],
+                    use_delta_cv=case["cv"],
+                    methods=dict(method=[2] * len(pf["w"]), dt_h0inv=(1 << 24) + 1, use_milstein=True))
+    with pytest.raises(nm.NmlmcError) as err:
+        s.sample(1, 64)
+    assert err.value.status == nm.ERR_LIMIT
