@@ -649,14 +649,10 @@ C4_MLMC = dict(workload="path-simulated portfolio: d=50 GBM stocks, P=1e5 option
                milstein=True, antithetic_risk=True, eps=1e-3)
 
 
-def c4_mlmc_case(args):
-    """Time-to-eps of the path-simulated portfolio: the batched FP32 sampler (OUTER streams, each
-    path-simulated inner sample on its own counter namespaces) against the FP64 drop-in on the
-    reference's stream layout (2048 virtual cores), both measured to the same eps."""
+def c4_mlmc_portfolio(nm):
+    """The path-simulated portfolio of the MLMC line: the large portfolio's generator with d = 50,
+    P = 1e5 (seed 1), options sorted by |w|, every option on the Unbiased method."""
     import numpy as np
-    sys.path.insert(0, PKG)
-    import nmlmc as nm
-    eps = args.eps if args.eps else C4_MLMC["eps"]
     pf = nm.generate_portfolio(dict(nm.PORTFOLIO_C3, Q=C4_MLMC["stocks"], P=C4_MLMC["options"]), 1)
     order = np.argsort(-np.abs(pf["w"]), kind="stable")
     for k in ("strike", "maturity", "w", "stock_ind", "type"):
@@ -664,6 +660,31 @@ def c4_mlmc_case(args):
     pf = dict(pf, prob=np.abs(pf["w"]))
     methods = dict(method=np.full(len(pf["w"]), nm.METHOD_UNBIASED, np.int32), dt_h0inv=1, dt_beta=2,
                    dt_prob_expo=-1.5, use_milstein=True, use_antithetic_risk=True)
+    return pf, methods
+
+
+def c4_level_case():
+    """Profiling case of the path-simulated phase kernel (FP32): two level-8 calls of 4000 outer
+    samples and two level-12 calls of 1000, K = 1676.5 (the 99 % Black-Scholes loss quantile)."""
+    sys.path.insert(0, PKG)
+    import nmlmc as nm
+    pf, methods = c4_mlmc_portfolio(nm)
+    s = nm.Sampler(0, N0=64, beta=2, adaptive_r=ADAPTIVE_R, precision=nm.PREC_FP32, streams=nm.STREAMS_OUTER, seed=3)
+    s.set_portfolio(pf, r=0.05, rho=0.0, max_loss=1676.5013260915875, tau=nm.TAU_WEEK, subsample=nm.SUB_RANDOM,
+                    use_delta_cv=True, discount=True, methods=methods)
+    for ell, M in ((8, 4000), (8, 4000), (12, 1000), (12, 1000)):
+        r = s.sample(ell, M)
+        print(f"level {ell} M {M}: {r['seconds'] * 1e3:.3f} ms, {r['stats'][0] / r['seconds']:.3e} inner/s")
+
+
+def c4_mlmc_case(args):
+    """Time-to-eps of the path-simulated portfolio: the batched FP32 sampler (OUTER streams, each
+    path-simulated inner sample on its own counter namespaces) against the FP64 drop-in on the
+    reference's stream layout (2048 virtual cores), both measured to the same eps."""
+    sys.path.insert(0, PKG)
+    import nmlmc as nm
+    eps = args.eps if args.eps else C4_MLMC["eps"]
+    pf, methods = c4_mlmc_portfolio(nm)
 
     def mk(prec, streams, K, seed, methods_on=True):
         s = nm.Sampler(0, cores=2048, N0=64, beta=2, adaptive_r=ADAPTIVE_R, precision=prec, streams=streams,
@@ -1007,11 +1028,12 @@ def main():
     ap.add_argument("--schedule-out", default=None,
                     help="write the run's outer samples per level (bench_schedule.json format) here")
     ap.add_argument("--case", default=None, choices=["c1", "c2", "small", "c3-level", "c3-table", "c3-sweep", "c4",
-                                                      "c4-small", "c4-mlmc", "ref-model"],
+                                                      "c4-small", "c4-mlmc", "c4-level", "ref-model"],
                     help="default: the large portfolio to eps; c1: the adaptive model problem to eps; "
-                         "c2: the d=20 portfolio with uniform sub-sampling to eps; small, c3-level, c3-table, c3-sweep, c4-small: profiling cases; c4: the "
+                         "c2: the d=20 portfolio with uniform sub-sampling to eps; c4: the "
                          "path-simulated loss with adjoint; c4-mlmc: MLMC of the path-simulated "
-                         "portfolio to eps; ref-model: the reference's model main")
+                         "portfolio to eps; ref-model: the reference's model main; small, c3-level, "
+                         "c3-table, c3-sweep, c4-small, c4-level: profiling cases")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -1031,6 +1053,8 @@ def main():
         return c4_mlmc_case(args)
     if args.case == "c2":
         return c2_case(args)
+    if args.case == "c4-level":
+        return c4_level_case()
     if args.case in ("c4", "c4-small"):
         return c4_case(args, small=args.case == "c4-small")
     if args.case == "ref-model":
