@@ -184,6 +184,16 @@ struct OuterPathNormals {
     bool have;
     RT y;
     uint64_t v1;         // the block's second value (pairs 2b + 1)
+    // positions the stream at normal k (the next next() returns normal k)
+    __device__ __forceinline__ void seek(uint64_t k) {
+        p = k >> 1;
+        have = false;
+        if (p & 1) {                                 // next() takes pair p from the cached v1
+            uint64_t e0;
+            threefry2x64(p >> 1, ns, key, e0, v1);
+        }
+        if (k & 1) (void)next();                     // normal k is the second of pair p
+    }
     __device__ __forceinline__ RT next() {
         if (have) {
             have = false;
@@ -493,20 +503,97 @@ __device__ __forceinline__ bool level_fp32(const OptionTable<float>& ot, const T
 constexpr uint32_t kPathSortChunk = 32;
 constexpr size_t kPathSortSmemBytes = (size_t)kPathSortChunk * kTile * (sizeof(uint32_t) + 1);
 
+// Unbiased samples at levels >= kCoopLevel (and those whose level is recomputed) are evaluated by
+// the whole warp, one at a time: the fine and coarse paths of the Milstein / Euler scheme are
+// products of per-step growth factors S_N = S_0 prod (1 + inc_n), so each lane multiplies the
+// factors of a contiguous range of coarse steps (drawing its normals at their stream positions)
+// and a butterfly product combines the lanes.  The same values as the sequential stepper up to
+// the order of the double products.  Rare (0.55 % of the samples at beta = 2, P(L) ~ 2^(-1.5 L)),
+// these samples carried about a fifth of the steps and, evaluated by one lane, kept the other 31
+// lanes of the warp and the other warps of the CTA waiting at the tile's barrier.
+constexpr uint32_t kCoopLevel = 5;
+
+// loss * weight of an Unbiased sample (inner_unbiased_fast) evaluated by all 32 lanes of the warp;
+// every lane returns the value, `work` is the owner's to add.
+__device__ __forceinline__ float inner_unbiased_coop(const OptionTable<float>& ot, float Rs, uint32_t j,
+                                                     const TfKey& key, uint64_t ns, uint32_t L, uint64_t N_l,
+                                                     uint32_t lane) {
+    const uint32_t s = ot.stock_ind[j];
+    const float S0 = ot.S0[s], sg = ot.sigma[s], r = ot.r, tau = ot.tau, T = ot.maturity[j], K = ot.strike[j];
+    const float m = (float)ot.type[j], wdisc = ot.w[j] * __expf(-r * T);
+    const float mu_t = (r - 0.5f * sg * sg) * tau;
+    OuterPathNormals<float, PREC_FP32> nz{key, ns, 0, false, 0.f, 0};
+    const float dW0 = ot.stau * nz.next();
+    const float S0_t_1 = S0 * __expf(fmaf(sg, dW0, mu_t));
+    const float S0_t_2 = S0 * __expf(fmaf(-sg, dW0, mu_t));
+    const uint64_t N = (uint64_t)ot.dt_h0inv * N_l;
+    const uint32_t cs = ot.dt_beta;                          // fine steps per coarse step (L > 0)
+    const uint64_t Nc = N / cs;
+    const float Tr = T - tau;
+    const float dt = Tr / (float)N, sqrt_dt = sqrtf(dt), dt_c = dt * (float)cs;
+    const float hs2 = ot.use_milstein ? 0.5f * sg * sg : 0.f;
+    // this lane's coarse steps [c0, c1): fine steps c0 cs .. c1 cs - 1, normals 1 + n
+    const uint64_t c0 = Nc * lane / 32, c1 = Nc * (lane + 1) / 32;
+    double Ff = 1.0, Fc = 1.0;
+    if (c1 > c0) {
+        nz.seek(1 + c0 * cs);
+        for (uint64_t c = c0; c < c1; c++) {
+            float dW_c = 0.f;
+            for (uint32_t i = 0; i < cs; i++) {
+                const float dW = sqrt_dt * nz.next();
+                const double inc = (double)fmaf(hs2, fmaf(dW, dW, -dt), fmaf(sg, dW, r * dt));
+                Ff = fma(Ff, inc, Ff);
+                dW_c += dW;
+            }
+            const double incc = (double)fmaf(hs2, fmaf(dW_c, dW_c, -dt_c), fmaf(sg, dW_c, r * dt_c));
+            Fc = fma(Fc, incc, Fc);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        Ff *= __shfl_xor_sync(0xffffffffu, Ff, o);
+        Fc *= __shfl_xor_sync(0xffffffffu, Fc, o);
+    }
+    const double S[6] = {(double)S0_t_1 * Ff, (double)Rs * Ff, (double)S0_t_2 * Ff,
+                         (double)S0_t_1 * Fc, (double)Rs * Fc, (double)S0_t_2 * Fc};
+    const bool anti = ot.use_antithetic_risk != 0;
+    const float half = anti ? 0.5f : 1.f;
+    const float diff = Rs - S0;
+    const bool do_d_f = ot.use_delta_cv && ot.use_coarse_delta_cv;   // L > 0
+    const bool do_d_c = ot.use_delta_cv && ot.use_coarse_delta_cv;
+    float vf = 0.f, vc = 0.f, vdf = 0.f, vdc = 0.f;
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        if (i == 1 && !anti) break;
+        const int ic = 2 * i;
+        vf += half * opt_diff_stock_fast(wdisc, m, K, (float)S[ic], (float)S[1]);
+        if (do_d_f) vdf += half * opt_derv_stock_fast(wdisc, m > 0.f, K, (float)S[ic], S0);
+        vc += half * opt_diff_stock_fast(wdisc, m, K, (float)S[ic + 3], (float)S[4]);
+        if (do_d_c) vdc += half * opt_derv_stock_fast(wdisc, m > 0.f, K, (float)S[ic + 3], S0);
+    }
+    const float ret = (vf - vc) + diff * (vdf - vdc);
+    const float e = ot.dt_prob_expo, lb = __log2f((float)ot.dt_beta);
+    return ret * (exp2f(-e * lb * (float)L) / (1.0f - exp2f(e * lb)));
+}
+
+// `own`: this lane evaluates a chunk (lanes past the end of a segment's last tile take part in
+// the warp's cooperative samples only).  All 32 lanes of the warp call it together.
 template <uint32_t C, bool S2, int PREC>
 __device__ __forceinline__ void pf_paths_sorted(const DevLevel<float>& D, const TfKey& key, uint32_t tag, uint64_t s0,
                                                 const float* Rrow, float shift, Acc<PREC>& a1, Acc<PREC>& a2,
-                                                double& work) {
+                                                double& work, bool own) {
     static_assert(C <= kPathSortChunk, "sorted path chunk");
     extern __shared__ float2 k_phase_rows[];     // the phase kernel's dynamic shared memory
     const OptionTable<float>& ot = D.L.ot;
     uint32_t* jbuf = reinterpret_cast<uint32_t*>(k_phase_rows) + threadIdx.x;                 // [q * kTile]
     uint8_t* cbuf = reinterpret_cast<uint8_t*>(reinterpret_cast<uint32_t*>(k_phase_rows) + kPathSortChunk * kTile) +
                     threadIdx.x;
-    // pass 1: option, class; the samples of classes {0, 1, 2}, 3, 4, 5, 6 and >= 7 as bit sets
+    // pass 1: option, class; the samples of classes {0, 1, 2}, 3, 4, 5, 6 (levels 1-4) as bit
+    // sets, and those the warp evaluates together (levels >= kCoopLevel, class 15)
+    static_assert(kCoopLevel == 5, "class sets");
     uint32_t m0 = 0, m1 = 0, m2 = 0, m3 = 0, m4 = 0, m5 = 0;
 #pragma unroll 1
-    for (uint32_t b = 0; b < C / 2; b++) {
+    for (uint32_t b = 0; b < (own ? C / 2 : 0u); b++) {
         uint64_t v[2];
         threefry2x64((s0 >> 1) + b, tag, key, v[0], v[1]);
 #pragma unroll
@@ -536,16 +623,18 @@ __device__ __forceinline__ void pf_paths_sorted(const DevLevel<float>& D, const 
             else m5 |= bit;
         }
     }
-    // pass 2: cheapest class first, sample order within a set
+    // pass 2: cheapest class first, sample order within a set; each lane its own samples
 #pragma unroll 1
-    for (uint32_t k = 0; k < C; k++) {
+    for (;;) {
+        const bool has = (m0 | m1 | m2 | m3 | m4) != 0;
+        if (!__any_sync(0xffffffffu, has)) break;
+        if (!has) continue;
         uint32_t q;
         if (m0) { q = __ffs(m0) - 1; m0 &= m0 - 1; }
         else if (m1) { q = __ffs(m1) - 1; m1 &= m1 - 1; }
         else if (m2) { q = __ffs(m2) - 1; m2 &= m2 - 1; }
         else if (m3) { q = __ffs(m3) - 1; m3 &= m3 - 1; }
-        else if (m4) { q = __ffs(m4) - 1; m4 &= m4 - 1; }
-        else { q = __ffs(m5) - 1; m5 &= m5 - 1; }
+        else { q = __ffs(m4) - 1; m4 &= m4 - 1; }
         const uint32_t j = jbuf[q * kTile];
         const uint32_t c = cbuf[q * kTile];
         const float prob = ot.subsample == SUB_UNIFORM ? ot.inv_count_prob : ot.phat[j];
@@ -578,12 +667,55 @@ __device__ __forceinline__ void pf_paths_sorted(const DevLevel<float>& D, const 
         a1.add(d);
         if (S2) a2.add_sq(d);
     }
+    // pass 3: the deep samples of all lanes, one at a time by the whole warp (its owner first by
+    // lane, then in sample order)
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t* jcol = reinterpret_cast<const uint32_t*>(k_phase_rows) + (threadIdx.x & ~31u);
+    const uint8_t* ccol = reinterpret_cast<const uint8_t*>(reinterpret_cast<const uint32_t*>(k_phase_rows) +
+                                                           kPathSortChunk * kTile) + (threadIdx.x & ~31u);
+#pragma unroll 1
+    for (;;) {
+        const unsigned pend = __ballot_sync(0xffffffffu, m5 != 0);
+        if (!pend) break;
+        const uint32_t src = __ffs(pend) - 1;
+        uint32_t myq = 0;
+        if (lane == src) { myq = __ffs(m5) - 1; m5 &= m5 - 1; }
+        const uint32_t q = __shfl_sync(0xffffffffu, myq, src);
+        const uint32_t j = jcol[q * kTile + src];
+        const uint32_t c = ccol[q * kTile + src];
+        const TfKey skey{__shfl_sync(0xffffffffu, key.k0, src), __shfl_sync(0xffffffffu, key.k1, src),
+                         __shfl_sync(0xffffffffu, key.k2, src)};
+        const uint64_t ns = path_ns(tag, __shfl_sync(0xffffffffu, s0, src) + q);
+        const float Rs = __shfl_sync(0xffffffffu, lane == src ? Rrow[ot.stock_ind[j] * 2] : 0.f, src);
+        uint32_t Lv;
+        uint64_t N_l;
+        bool ok;
+        if (c < 15) { Lv = c - 2; ok = level_steps(ot, Lv, N_l); }
+        else ok = level_fp32(ot, skey, ns, Lv, N_l);
+        float val = 0.f;
+        if (ok) val = inner_unbiased_coop(ot, Rs, j, skey, ns, Lv, N_l, lane);
+        if (lane == src) {
+            if (ok) {
+                const float West = ot.W_est[j];
+                work += (double)((float)N_l * West);
+                work += (double)((float)(N_l / ot.dt_beta) * West);
+            } else {                                     // beyond kMaxPathSteps: the call fails
+                atomicOr(D.B.counters + CNT_ERR, 1u);
+            }
+            const float prob = ot.subsample == SUB_UNIFORM ? ot.inv_count_prob : ot.phat[j];
+            float d = __fdiv_rn(val, prob);
+            if (S2) d = __fadd_rn(d, shift);
+            a1.add(d);
+            if (S2) a2.add_sq(d);
+        }
+    }
 }
 
 template <class RT, int KIND, int PREC, uint32_t C, bool S2, class S, bool PIPE>
 __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t item, uint32_t tag,
                                              uint64_t s0, uint64_t count, float shift, const float2* srow,
-                                             Acc<PREC>& a1, Acc<PREC>& a2, double& work) {
+                                             Acc<PREC>& a1, Acc<PREC>& a2, double& work, bool own) {
+    if (!own && !(KIND == KIND_PF_PATHS && PREC == PREC_FP32 && C <= kPathSortChunk)) return;
     const OuterLevel<RT>& L = D.L;
     const TfKey key = tf_key(L.seed, outer_stream_id(L.ell, L.first_index + item));
     const RT* Yv = reinterpret_cast<const RT*>(D.B.Yv);
@@ -669,7 +801,7 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
     } else if constexpr (KIND == KIND_PF_PATHS && PREC == PREC_FP32 && C <= kPathSortChunk) {
         if constexpr (sizeof(RT) == 4) {
             const float* Rrow = reinterpret_cast<const float*>(D.B.Rt) + (size_t)item * L.ot.Q * 2;
-            pf_paths_sorted<C, S2, PREC>(D, key, tag, s0, Rrow, shift, a1, a2, work);
+            pf_paths_sorted<C, S2, PREC>(D, key, tag, s0, Rrow, shift, a1, a2, work, own);
         }
     } else {                                     // portfolio: one 64-bit value per inner sample
         const OptionTable<RT>& ot = L.ot;
@@ -727,13 +859,14 @@ __device__ __forceinline__ void eval_chunk_c(const DevLevel<RT>& D, uint32_t ite
 template <class RT, int KIND, int PREC, bool S2, class S, bool PIPE>
 __device__ __forceinline__ void eval_chunk_s(const DevLevel<RT>& D, uint32_t item, uint32_t tag,
                                              uint64_t s0, uint64_t count, uint32_t C, float shift,
-                                             const float2* srow, Acc<PREC>& a1, Acc<PREC>& a2, double& work) {
+                                             const float2* srow, Acc<PREC>& a1, Acc<PREC>& a2, double& work,
+                                             bool own) {
     switch (C) {
-    case 64: eval_chunk_c<RT, KIND, PREC, 64, S2, S, PIPE>(D, item, tag, s0, count, shift, srow, a1, a2, work); break;
-    case 32: eval_chunk_c<RT, KIND, PREC, 32, S2, S, PIPE>(D, item, tag, s0, count, shift, srow, a1, a2, work); break;
-    case 16: eval_chunk_c<RT, KIND, PREC, 16, S2, S, PIPE>(D, item, tag, s0, count, shift, srow, a1, a2, work); break;
-    case 8: eval_chunk_c<RT, KIND, PREC, 8, S2, S, PIPE>(D, item, tag, s0, count, shift, srow, a1, a2, work); break;
-    default: eval_chunk_c<RT, KIND, PREC, 4, S2, S, PIPE>(D, item, tag, s0, count, shift, srow, a1, a2, work); break;
+    case 64: eval_chunk_c<RT, KIND, PREC, 64, S2, S, PIPE>(D, item, tag, s0, count, shift, srow, a1, a2, work, own); break;
+    case 32: eval_chunk_c<RT, KIND, PREC, 32, S2, S, PIPE>(D, item, tag, s0, count, shift, srow, a1, a2, work, own); break;
+    case 16: eval_chunk_c<RT, KIND, PREC, 16, S2, S, PIPE>(D, item, tag, s0, count, shift, srow, a1, a2, work, own); break;
+    case 8: eval_chunk_c<RT, KIND, PREC, 8, S2, S, PIPE>(D, item, tag, s0, count, shift, srow, a1, a2, work, own); break;
+    default: eval_chunk_c<RT, KIND, PREC, 4, S2, S, PIPE>(D, item, tag, s0, count, shift, srow, a1, a2, work, own); break;
     }
 }
 
@@ -745,12 +878,15 @@ __device__ __forceinline__ void eval_chunk_s(const DevLevel<RT>& D, uint32_t ite
 // s2 - s1^2 / n does not cancel where the decision is close; the final phase accumulates d.
 // `srow`: the outer sample's R_tau row in shared memory, or nullptr (FP32 portfolio path).
 // PIPE: the pipelined alias-column loop (the 128-register variant of the phase kernel).
+// own: this thread's chunk is real (false for threads past the end of a segment's last tile,
+// which take part only in the warp-cooperative samples of the FP32 path-simulated kernel).
 template <class RT, int KIND, int PREC, class S, bool PIPE>
 __device__ __forceinline__ void eval_chunk(const DevLevel<RT>& D, uint32_t item, uint32_t tag,
                                            uint64_t s0, uint64_t count, uint32_t C, bool want_s2, RT start,
-                                           const float2* srow, Acc<PREC>& a1, Acc<PREC>& a2, double& work) {
-    if (want_s2) eval_chunk_s<RT, KIND, PREC, true, S, PIPE>(D, item, tag, s0, count, C, (float)start, srow, a1, a2, work);
-    else eval_chunk_s<RT, KIND, PREC, false, S, PIPE>(D, item, tag, s0, count, C, 0.f, srow, a1, a2, work);
+                                           const float2* srow, Acc<PREC>& a1, Acc<PREC>& a2, double& work,
+                                           bool own = true) {
+    if (want_s2) eval_chunk_s<RT, KIND, PREC, true, S, PIPE>(D, item, tag, s0, count, C, (float)start, srow, a1, a2, work, own);
+    else eval_chunk_s<RT, KIND, PREC, false, S, PIPE>(D, item, tag, s0, count, C, 0.f, srow, a1, a2, work, own);
 }
 
 // ---- segments of uniform chunk count ------------------------------------------------------
@@ -975,7 +1111,11 @@ __global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet SS
                 Acc<PREC> a1, a2;
                 a1.zero();
                 a2.zero();
-                if (valid) eval_chunk<RT, KIND, PREC, S, MINB == 2>(D, item, g.tag, (uint64_t)j * C, g.count, C, pilot, start, srow, a1, a2, wsum);
+                // the FP32 path-simulated kernel evaluates deep samples warp-wide: all lanes call
+                constexpr bool kCoopKind = KIND == KIND_PF_PATHS && PREC == PREC_FP32;
+                if (valid || (kCoopKind && C <= kPathSortChunk))
+                    eval_chunk<RT, KIND, PREC, S, MINB == 2>(D, item, g.tag, (uint64_t)j * C, g.count, C, pilot, start,
+                                                             srow, a1, a2, wsum, valid);
                 const float coeff = (float)gs / (float)nch;     // 1 / groups (a power of two)
                 float ind = 0.f;
                 if (!pilot && gs == 1) ind = phi_of<KIND, S, RT>(inner_mean<RT, PREC>(start, a1, csmall), coeff);

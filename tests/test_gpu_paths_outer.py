@@ -34,6 +34,12 @@ CASES = [
     dict(name="K_uniform_euler", pf=dict(Q=2, P=12, seed=22, prob="uniform"), sub=O.SUB_UNIFORM, cv=True,
          rho=0.0, max_loss=0.2, N0=32, beta=2, r=1.5, seed=8, anti_risk=False, milstein=False, coarse_cv=True,
          methods=[2, 0, 1, 1, 2, 0, 0, 1, 0, 2, 1, 2], calls=[(0, 300), (2, 200), (4, 80)]),
+    # deep Unbiased levels (P(L) ~ 2^(-1.1 L), h0 = 1: about 2 % of the samples at L >= 5, which
+    # the FP32 kernel evaluates warp-wide)
+    dict(name="L_deep_levels", pf=dict(Q=3, P=24, seed=23, prob="w"), sub=O.SUB_RANDOM, cv=True, rho=0.1,
+         max_loss=0.3, N0=32, beta=2, r=1.5, seed=9, anti_risk=True, milstein=True, coarse_cv=True,
+         methods=[2, 2, 2, 0, 2, 2, 1, 2, 2, 2, 2, 2, 2, 0, 2, 2, 2, 2, 1, 2, 2, 2, 2, 2],
+         dt=dict(dt_h0inv=1, dt_beta=2, dt_prob_expo=-1.1), calls=[(0, 300), (2, 200), (3, 120)]),
 ]
 
 
@@ -45,10 +51,11 @@ def pair(nm, case, o_prec, g_prec):
     flags = dict(use_coarse_delta_cv=case["coarse_cv"], use_antithetic_risk=case["anti_risk"],
                  use_milstein=case["milstein"])
     o = O.Sampler(o_prec, O.STREAMS_OUTER, 1, case["N0"], case["beta"], case["r"], True, False, case["seed"])
-    o.set_portfolio_methods(pf, case["methods"], **kw, **flags)
+    dt = case.get("dt", {})
+    o.set_portfolio_methods(pf, case["methods"], **kw, **flags, **dt)
     g = nmlmc.Sampler(N0=case["N0"], beta=case["beta"], adaptive_r=case["r"], precision=g_prec,
                       streams=nmlmc.STREAMS_OUTER, seed=case["seed"])
-    g.set_portfolio(pf, **kw, methods=dict(method=case["methods"], **flags))
+    g.set_portfolio(pf, **kw, methods=dict(method=case["methods"], **flags, **dt))
     return o, g
 
 
