@@ -83,6 +83,8 @@ template <> struct Acc<PREC_FP32> {
     // plain addition: the pilots' sum of squares, which only feeds the variance estimate of the
     // adaptive rule (sums of 4-64 squares per thread of values centred on the threshold)
     __device__ __forceinline__ void add_sq(float v) { hi = fmaf(v, v, hi); }
+    // the pilots' sum of squares across lanes: a plain sum, like add_sq (its lo stays zero)
+    __device__ __forceinline__ void sq_merge_xor(int m) { hi = __fadd_rn(hi, __shfl_xor_sync(0xffffffffu, hi, m)); }
     // two consecutive inner values: their plain sum (one rounding of a value bounded by the two
     // summands), then the compensated step
     __device__ __forceinline__ void add2(float v0, float v1) { add(__fadd_rn(v0, v1)); }
@@ -91,6 +93,7 @@ template <> struct Acc<PREC_FP32> {
 template <> struct Acc<PREC_FP64> {
     double v;
     __device__ __forceinline__ void zero() { v = 0; }
+    __device__ __forceinline__ void sq_merge_xor(int m) { v = __dadd_rn(v, __shfl_xor_sync(0xffffffffu, v, m)); }
     __device__ __forceinline__ void add(double x) { v = __dadd_rn(v, x); }
     __device__ __forceinline__ void add2(double x0, double x1) { add(x0); add(x1); }
     __device__ __forceinline__ void add_sq(double x) { v = __dadd_rn(v, __dmul_rn(x, x)); }
@@ -101,6 +104,7 @@ template <> struct Acc<PREC_FP64> {
 template <> struct Acc<PREC_REF32> {
     double v;
     __device__ __forceinline__ void zero() { v = 0; }
+    __device__ __forceinline__ void sq_merge_xor(int m) { v = __dadd_rn(v, __shfl_xor_sync(0xffffffffu, v, m)); }
     __device__ __forceinline__ void add(double x) { v = __dadd_rn(v, x); }
     __device__ __forceinline__ void add2(double x0, double x1) { add(x0); add(x1); }
     __device__ __forceinline__ void add_sq(double x) { v = __dadd_rn(v, __dmul_rn(x, x)); }
@@ -1122,7 +1126,7 @@ __global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet SS
                 const uint32_t wl = nch < 32 ? nch : 32;
                 for (uint32_t m = 1; m < wl; m <<= 1) {
                     a1.merge(a1.shfl_xor(m));
-                    if (pilot) a2.merge(a2.shfl_xor(m));
+                    if (pilot) a2.sq_merge_xor(m);
                     else {
                         ind += __shfl_xor_sync(0xffffffffu, ind, m);
                         if (2 * m == gs) ind = phi_of<KIND, S, RT>(inner_mean<RT, PREC>(start, a1, csmall), coeff);
@@ -1211,7 +1215,7 @@ __global__ void __launch_bounds__(kTile, MINB) k_phase(DevLevel<RT> D, SegSet SS
                     if (!pilot && gs == 1) ind = phi_of<KIND, S, RT>(inner_mean<RT, PREC>(start, a1, csmall), coeff);
                     for (uint32_t m = 1; m < 32; m <<= 1) {
                         a1.merge(a1.shfl_xor(m));
-                        if (pilot) a2.merge(a2.shfl_xor(m));
+                        if (pilot) a2.sq_merge_xor(m);
                         else {
                             ind += __shfl_xor_sync(0xffffffffu, ind, m);
                             if (2 * m == gs) ind = phi_of<KIND, S, RT>(inner_mean<RT, PREC>(start, a1, csmall), coeff);
