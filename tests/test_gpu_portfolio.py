@@ -105,7 +105,7 @@ def test_c2_end_to_end(nm):
     """C2: d = 20, P = 1e4, uniform sub-sampling, 64 * 2^ell inner samples, K = 99 % quantile of L
     over 1e5 full evaluations (seed 1); the MLMC estimate of P(L > K) agrees with a direct estimate
     from 2e6 full evaluations (sigma ~ 7e-5).  eps = 3e-4 (about 15 s on a B200): the
-    configuration's relative 1e-2 (1e-4 absolute) takes the same sampler about 170 s, with the
+    configuration's relative 1e-2 (1e-4 absolute) takes the same sampler about 150 s, with the
     starting level at 11 and 3e13 inner samples (bench.py --case c2)."""
     pf = nm.generate_portfolio(nm.PORTFOLIO_C2, 1)
     q = sampler(nm, nm.PREC_FP32, pf, seed=1)
