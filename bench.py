@@ -388,10 +388,13 @@ def reference_arm(args):
 def small_case():
     """Fixed level calls of the FP32 sampler (the profiling case): level 0 with 2^24 outer samples
     (fine only, 32 inner samples each) and level 8 with 2^16 (adaptive pilots and the antithetic
-    final phase).  Device memory: the batch buffers, grown to 2^24 outer samples (~600 MB)."""
+    final phase), on the default register variant without tuning probes, so the first phase-kernel
+    launch is level 0's first pilot round.  Device memory: the batch buffers, grown to 2^24 outer
+    samples (~600 MB)."""
     sys.path.insert(0, PKG)
     import nmlmc as nm
     s = make_sampler(nm, 0, nm.PREC_FP32, nm.STREAMS_OUTER, seed=0)
+    s.set_autotune(0)
     for ell, M in ((0, 1 << 24), (8, 1 << 16), (0, 1 << 24), (8, 1 << 16)):
         r = s.sample(ell, M)
         print(f"level {ell} M {M}: {r['seconds'] * 1e3:.3f} ms, {r['stats'][0] / r['seconds']:.3e} inner/s")
