@@ -684,7 +684,9 @@ __device__ __forceinline__ void pf_paths_sorted(const DevLevel<float>& D, const 
         if (S2) a2.add_sq(d);
     }
     // pass 3: the deep samples of all lanes, one at a time by the whole warp (its owner first by
-    // lane, then in sample order)
+    // lane, then in sample order); the lanes read each other's pass-1 entries after the warp
+    // barrier orders them
+    __syncwarp();
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t* jcol = reinterpret_cast<const uint32_t*>(k_phase_rows) + (threadIdx.x & ~31u);
     const uint8_t* ccol = reinterpret_cast<const uint8_t*>(reinterpret_cast<const uint32_t*>(k_phase_rows) +
