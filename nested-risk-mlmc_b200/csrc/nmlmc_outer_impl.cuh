@@ -606,7 +606,7 @@ __device__ __forceinline__ void pf_paths_sorted(const DevLevel<float>& D, const 
                     threadIdx.x;
     // pass 1: option, class; the samples of classes {0, 1, 2}, 3, 4, 5, 6 (levels 1-4) as bit
     // sets, and those the warp evaluates together (levels >= kCoopLevel, class 15)
-    static_assert(kCoopLevel == 5, "class sets");
+    static_assert(kCoopLevel >= 1 && kCoopLevel <= 5, "class sets");
     uint32_t m0 = 0, m1 = 0, m2 = 0, m3 = 0, m4 = 0, m5 = 0;
 #pragma unroll 1
     for (uint32_t b = 0; b < (own ? C / 2 : 0u); b++) {
@@ -631,7 +631,8 @@ __device__ __forceinline__ void pf_paths_sorted(const DevLevel<float>& D, const 
             jbuf[q * kTile] = j;
             cbuf[q * kTile] = (uint8_t)c;
             const uint32_t bit = 1u << q;
-            if (c <= 2) m0 |= bit;
+            if (c >= 2 + kCoopLevel) m5 |= bit;
+            else if (c <= 2) m0 |= bit;
             else if (c == 3) m1 |= bit;
             else if (c == 4) m2 |= bit;
             else if (c == 5) m3 |= bit;
